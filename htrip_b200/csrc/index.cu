@@ -1,0 +1,920 @@
+// Host side of the B200 HTRIP index: geometry tables, the device arena,
+// build / update / query orchestration and the C ABI of include/htrip_b200.h.
+//
+// Reference call stacks mirrored here (ozaslan/htrip):
+//   build               src/minplus_oracle.cpp:48-137
+//   onBatchCellsOpened  src/minplus_oracle.cpp:530-729
+//   onCellOpened        src/minplus_oracle.cpp:139-177 (same state as a batch of one)
+//   queryAllPairs       src/minplus_oracle.cpp:934-1419
+#include "../../include/htrip_b200.h"
+#include "kernels.cuh"
+#include "minplus.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <string>
+#include <vector>
+
+using hb::MatSet;
+
+namespace {
+
+thread_local std::string g_err;
+
+htrip_status fail(htrip_status s, const std::string& msg) {
+    g_err = msg;
+    return s;
+}
+
+struct CudaError {
+    cudaError_t e;
+    const char* what;
+};
+
+inline void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError{e, what};
+}
+
+// Canonical perimeter order of a side-s tile (reference getTilePorts,
+// src/leaf_tile.cpp:11-30): top row, bottom row, left column without
+// corners, right column without corners.
+void port_local(int s, int p, int& r, int& c) {
+    if (p < s) { r = 0; c = p; }
+    else if (p < 2 * s) { r = s - 1; c = p - s; }
+    else if (p < 3 * s - 2) { r = p - 2 * s + 1; c = 0; }
+    else { r = p - (3 * s - 2) + 1; c = s - 1; }
+}
+
+// Inverse of port_local (reference getPortIndexInTile, internal_node.cpp:290-304).
+int port_index(int r, int c, int s) {
+    if (r == 0 && c >= 0 && c < s) return c;
+    if (r == s - 1 && c >= 0 && c < s) return s + c;
+    if (c == 0 && r > 0 && r < s - 1) return 2 * s + r - 1;
+    if (c == s - 1 && r > 0 && r < s - 1) return 3 * s - 2 + r - 1;
+    return -1;
+}
+
+int pad_order(int n) {
+    if (n <= 64) return 64;
+    if (n <= 128) return 128;
+    return (n + 255) / 256 * 256;
+}
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void reserve(size_t m) {
+        if (m <= n) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        ck(cudaMalloc(&p, m * sizeof(T)), "cudaMalloc");
+        n = m;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+struct Level {
+    int lvl = 0;
+    int side = 0;      // tile side (b for leaves, s for nodes)
+    int cs = 0;        // child side (nodes)
+    int n = 0;         // logical order (b^2 or nV)
+    int NP = 0;        // padded order
+    int nExt = 0;      // 4*side - 4
+    int nP = 0;        // ports per child (nodes)
+    int nodes_x = 0;
+    int nnodes = 0;
+    std::vector<int> ext;    // exterior port -> matrix index
+    std::vector<int> seams;  // 6 ints per seam candidate
+    int nseams = 0;
+    DevBuf<int> d_ext, d_seams;
+    DevBuf<uint16_t> mat;
+    DevBuf<uint8_t> kflag;
+    DevBuf<int> klist, kcnt;
+    DevBuf<uint8_t> dec;
+    MatSet ms() const { return MatSet{mat.p, n, NP}; }
+};
+
+}  // namespace
+
+struct htrip_index {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int b = 16, g = 2;
+    bool built = false;
+    int S = 0, H = 0, rows = 0, cols = 0, leaves_x = 0;
+    std::vector<Level> L;
+    DevBuf<uint8_t> pass;
+    // closure scratch
+    DevBuf<uint16_t> panel;
+    DevBuf<uint8_t> pflags;
+    DevBuf<int> active;
+    DevBuf<int> upd;        // uploaded per-update lists
+    DevBuf<uint16_t> snap;
+    DevBuf<int> pivots;
+    // query scratch
+    DevBuf<int> qplan;
+    DevBuf<uint16_t> qX[2], qY, qM, qout;
+    DevBuf<int> qkidx;
+    DevBuf<int32_t> qvps;
+    htrip_batch_stats stats{0, 0, 0};
+    std::vector<int> h_pinned_dummy;
+
+    ~htrip_index() { release(); }
+    void release() {
+        for (auto& l : L) {
+            l.d_ext.release(); l.d_seams.release(); l.mat.release(); l.kflag.release();
+            l.klist.release(); l.kcnt.release(); l.dec.release();
+        }
+        L.clear();
+        pass.release(); panel.release(); pflags.release(); active.release(); upd.release();
+        snap.release(); pivots.release(); qplan.release(); qX[0].release(); qX[1].release();
+        qY.release(); qM.release(); qout.release(); qkidx.release(); qvps.release();
+    }
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Geometry
+// ---------------------------------------------------------------------------
+void make_levels(htrip_index* h) {
+    const int b = h->b, g = h->g;
+    h->L.clear();
+    h->L.resize(h->H + 1);
+    Level& L0 = h->L[0];
+    L0.lvl = 0;
+    L0.side = b;
+    L0.n = b * b;
+    L0.NP = pad_order(L0.n);
+    L0.nExt = 4 * b - 4;
+    L0.nodes_x = h->S / b;
+    L0.nnodes = L0.nodes_x * L0.nodes_x;
+    L0.ext.resize(L0.nExt);
+    for (int e = 0; e < L0.nExt; ++e) {
+        int r, c;
+        port_local(b, e, r, c);
+        L0.ext[e] = r * b + c;
+    }
+    int cs = b;
+    for (int l = 1; l <= h->H; ++l) {
+        Level& Lv = h->L[l];
+        Lv.lvl = l;
+        Lv.cs = cs;
+        Lv.side = cs * g;
+        Lv.nP = 4 * cs - 4;
+        Lv.n = g * g * Lv.nP;
+        Lv.NP = pad_order(Lv.n);
+        Lv.nExt = 4 * Lv.side - 4;
+        Lv.nodes_x = h->S / Lv.side;
+        Lv.nnodes = Lv.nodes_x * Lv.nodes_x;
+        // V_U coordinate lookup (node-local) -> index
+        const int s = Lv.side;
+        auto vidx = [&](int r, int c) -> int {
+            if (r < 0 || c < 0 || r >= s || c >= s) return -1;
+            const int q = (r / cs) * g + (c / cs);
+            const int p = port_index(r % cs, c % cs, cs);
+            return p < 0 ? -1 : q * Lv.nP + p;
+        };
+        Lv.ext.resize(Lv.nExt);
+        for (int e = 0; e < Lv.nExt; ++e) {
+            int r, c;
+            port_local(s, e, r, c);
+            Lv.ext[e] = vidx(r, c);
+        }
+        // Seam candidates: 4-adjacent V_U pairs in different children
+        // (reference InternalNode ctor, internal_node.cpp:72-89).
+        Lv.seams.clear();
+        for (int q = 0; q < g * g; ++q) {
+            const int cy = q / g, cx = q % g;
+            for (int p = 0; p < Lv.nP; ++p) {
+                int pr, pc;
+                port_local(cs, p, pr, pc);
+                const int r = cy * cs + pr, c = cx * cs + pc;
+                const int u = q * Lv.nP + p;
+                const int nb[2][2] = {{r, c + 1}, {r + 1, c}};
+                for (auto& rc : nb) {
+                    const int v = vidx(rc[0], rc[1]);
+                    if (v < 0 || v / Lv.nP == q) continue;
+                    Lv.seams.insert(Lv.seams.end(), {u, v, r, c, rc[0], rc[1]});
+                }
+            }
+        }
+        Lv.nseams = (int)Lv.seams.size() / 6;
+        cs *= g;
+    }
+}
+
+void alloc_levels(htrip_index* h) {
+    for (auto& Lv : h->L) {
+        Lv.mat.reserve((size_t)Lv.nnodes * Lv.NP * Lv.NP);
+        Lv.d_ext.reserve(std::max(1, Lv.nExt));
+        ck(cudaMemcpyAsync(Lv.d_ext.p, Lv.ext.data(), Lv.nExt * sizeof(int), cudaMemcpyHostToDevice, h->stream), "ext");
+        if (Lv.nseams) {
+            Lv.d_seams.reserve(Lv.seams.size());
+            ck(cudaMemcpyAsync(Lv.d_seams.p, Lv.seams.data(), Lv.seams.size() * sizeof(int), cudaMemcpyHostToDevice,
+                               h->stream), "seams");
+        }
+        Lv.kflag.reserve((size_t)Lv.nnodes * Lv.NP);
+        ck(cudaMemsetAsync(Lv.kflag.p, 0, (size_t)Lv.nnodes * Lv.NP, h->stream), "kflag");
+        Lv.klist.reserve((size_t)Lv.nnodes * Lv.NP);
+        Lv.kcnt.reserve(Lv.nnodes);
+        Lv.dec.reserve(Lv.nnodes);
+    }
+    h->pivots.reserve(1);
+}
+
+// Closure of the listed matrices of level `Lv` over their pivot flags.
+void close_matrices(htrip_index* h, Level& Lv, const std::vector<int>& act) {
+    if (act.empty()) return;
+    cudaStream_t st = h->stream;
+    const size_t per = (size_t)hb::kPivotChunk * Lv.NP;
+    const size_t cap = std::max<size_t>(1, (size_t)(128u << 20) / (per * sizeof(uint16_t)));
+    std::vector<int> kc(Lv.nnodes);
+    for (size_t c0 = 0; c0 < act.size(); c0 += cap) {
+        const int na = (int)std::min(cap, act.size() - c0);
+        h->active.reserve(na);
+        ck(cudaMemcpyAsync(h->active.p, act.data() + c0, na * sizeof(int), cudaMemcpyHostToDevice, st), "active");
+        hb::launch_compact_pivots(Lv.kflag.p, Lv.NP, h->active.p, na, Lv.klist.p, Lv.kcnt.p, st);
+        ck(cudaGetLastError(), "compact");
+        ck(cudaMemcpyAsync(kc.data(), Lv.kcnt.p, Lv.nnodes * sizeof(int), cudaMemcpyDeviceToHost, st), "kcnt");
+        ck(cudaStreamSynchronize(st), "sync kcnt");
+        int maxk = 0;
+        for (int i = 0; i < na; ++i) maxk = std::max(maxk, kc[act[c0 + i]]);
+        if (maxk == 0) continue;
+        h->panel.reserve(per * na);
+        h->pflags.reserve((size_t)na * (Lv.NP / hb::kFlagTile));
+        const int rounds = (maxk + hb::kPivotChunk - 1) / hb::kPivotChunk;
+        for (int r = 0; r < rounds; ++r) {
+            hb::launch_closure_round(Lv.ms(), h->active.p, na, Lv.klist.p, Lv.kcnt.p, r, h->panel.p, h->pflags.p, st);
+            ck(cudaGetLastError(), "closure round");
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Build (reference MinPlusOracle::build, minplus_oracle.cpp:48-137)
+// ---------------------------------------------------------------------------
+void do_build(htrip_index* h, const uint8_t* observed, int rows, int cols) {
+    const int b = h->b, g = h->g;
+    int S = b;
+    while (S < std::max(rows, cols)) S *= g;
+    int H = 0;
+    for (int t = S / b; t > 1; t /= g) ++H;
+    h->release();
+    h->built = false;
+    h->S = S;
+    h->H = H;
+    h->rows = rows;
+    h->cols = cols;
+    h->leaves_x = S / b;
+    make_levels(h);
+    alloc_levels(h);
+    cudaStream_t st = h->stream;
+    // Passability mirror, padded to S x S (outside the grid = not passable).
+    std::vector<uint8_t> pass((size_t)S * S, 0);
+    for (int r = 0; r < rows; ++r)
+        for (int c = 0; c < cols; ++c) pass[(size_t)r * S + c] = observed[(size_t)r * cols + c] == 1;
+    h->pass.reserve(pass.size());
+    ck(cudaMemcpyAsync(h->pass.p, pass.data(), pass.size(), cudaMemcpyHostToDevice, st), "pass");
+    Level& L0 = h->L[0];
+    hb::launch_leaf_bfs(h->pass.p, S, b, h->leaves_x, L0.nnodes, L0.ms(), st);
+    ck(cudaGetLastError(), "leaf bfs");
+    for (int l = 1; l <= H; ++l) {
+        Level& Lv = h->L[l];
+        Level& Lc = h->L[l - 1];
+        hb::launch_node_init(Lv.ms(), Lc.ms(), Lc.d_ext.p, Lv.nP, g, Lv.nodes_x, Lc.nodes_x, Lv.nnodes, st);
+        ck(cudaGetLastError(), "node init");
+        hb::launch_seams_build(Lv.ms(), Lv.d_seams.p, Lv.nseams, h->pass.p, S, Lv.side, Lv.nodes_x, Lv.nnodes,
+                               Lv.kflag.p, st);
+        ck(cudaGetLastError(), "seams build");
+        std::vector<int> act(Lv.nnodes);
+        std::iota(act.begin(), act.end(), 0);
+        close_matrices(h, Lv, act);
+    }
+    ck(cudaStreamSynchronize(st), "build sync");
+    h->built = true;
+}
+
+// ---------------------------------------------------------------------------
+// Batched opening (reference onBatchCellsOpened, minplus_oracle.cpp:530-729)
+// ---------------------------------------------------------------------------
+int find_lca_level(const htrip_index* h, int r1, int c1, int r2, int c2) {
+    int t1x = c1 / h->b, t1y = r1 / h->b, t2x = c2 / h->b, t2y = r2 / h->b;
+    if (t1x == t2x && t1y == t2y) return 0;
+    for (int l = 1; l <= h->H; ++l) {
+        t1x /= h->g; t1y /= h->g; t2x /= h->g; t2y /= h->g;
+        if (t1x == t2x && t1y == t2y) return l;
+    }
+    return h->H + 1;
+}
+
+// V_U index of global cell (r, c) in its level-l node (findVertexIndex,
+// internal_node.cpp:306-319).
+int vertex_index(const Level& Lv, int g, int r, int c) {
+    const int lr = r % Lv.side, lc = c % Lv.side;
+    const int q = (lr / Lv.cs) * g + (lc / Lv.cs);
+    const int p = port_index(lr % Lv.cs, lc % Lv.cs, Lv.cs);
+    return p < 0 ? -1 : q * Lv.nP + p;
+}
+
+void do_open(htrip_index* h, const int32_t* rc, int n, const uint8_t* obs, int rows, int cols, bool record_stats) {
+    cudaStream_t st = h->stream;
+    const int b = h->b, g = h->g, H = h->H, S = h->S;
+    auto passable = [&](int r, int c) { return r >= 0 && c >= 0 && r < rows && c < cols && obs[(size_t)r * cols + c] == 1; };
+    auto weight_ok = [&](int r, int c) {  // GridMap::getCellWeight(p) < INF (grid_map.hpp:273-278)
+        return r >= 0 && c >= 0 && r < rows && c < cols && obs[(size_t)r * cols + c] != 2;
+    };
+    static const int dr[4] = {-1, 1, 0, 0};
+    static const int dc[4] = {0, 0, -1, 1};
+    Level& L0 = h->L[0];
+    // 1. bucket cells by leaf, in first-touch order
+    std::vector<int> leaf_slot(L0.nnodes, -1);
+    std::vector<int> leaves;
+    std::vector<std::vector<int>> edges;  // per touched leaf: (u, v) pairs
+    std::vector<std::vector<std::vector<int>>> seams(H + 1);  // [lvl][slot] (u, v) pairs
+    std::vector<std::vector<int>> seam_nodes(H + 1);
+    std::vector<std::vector<int>> seam_slot(H + 1);
+    for (int l = 1; l <= H; ++l) seam_slot[l].assign(h->L[l].nnodes, -1);
+    for (int i = 0; i < n; ++i) {
+        const int r = rc[2 * i], c = rc[2 * i + 1];
+        if (r < 0 || c < 0 || r >= S || c >= S) continue;
+        const int tx = c / b, ty = r / b, leaf = ty * h->leaves_x + tx;
+        if (leaf_slot[leaf] < 0) {
+            leaf_slot[leaf] = (int)leaves.size();
+            leaves.push_back(leaf);
+            edges.emplace_back();
+        }
+        if (!weight_ok(r, c)) continue;
+        for (int d = 0; d < 4; ++d) {
+            const int nr = r + dr[d], nc = c + dc[d];
+            if (!passable(nr, nc)) continue;
+            if (nc / b == tx && nr / b == ty) {
+                auto& e = edges[leaf_slot[leaf]];
+                e.push_back((r - ty * b) * b + (c - tx * b));
+                e.push_back((nr - ty * b) * b + (nc - tx * b));
+            } else {
+                const int lca = find_lca_level(h, r, c, nr, nc);
+                if (lca < 1 || lca > H) continue;
+                const Level& Lv = h->L[lca];
+                const int node = (r / Lv.side) * Lv.nodes_x + (c / Lv.side);
+                int& slot = seam_slot[lca][node];
+                if (slot < 0) {
+                    slot = (int)seam_nodes[lca].size();
+                    seam_nodes[lca].push_back(node);
+                    seams[lca].emplace_back();
+                }
+                const int u = vertex_index(Lv, g, r, c), v = vertex_index(Lv, g, nr, nc);
+                if (u >= 0 && v >= 0) {
+                    seams[lca][slot].push_back(u);
+                    seams[lca][slot].push_back(v);
+                }
+            }
+        }
+    }
+    if (record_stats) h->stats = {0, 0, 0};
+    if (leaves.empty()) return;
+    int n_dirty = 0;
+    // 2. leaves: edge insert + closure over pivots
+    {
+        std::vector<int> buf;
+        std::vector<int> eoff(leaves.size() + 1, 0);
+        for (size_t i = 0; i < leaves.size(); ++i) eoff[i + 1] = eoff[i] + (int)edges[i].size() / 2;
+        buf.insert(buf.end(), eoff.begin(), eoff.end());
+        for (auto& e : edges) buf.insert(buf.end(), e.begin(), e.end());
+        h->upd.reserve(buf.size() + leaves.size());
+        h->active.reserve(leaves.size());
+        ck(cudaMemcpyAsync(h->active.p, leaves.data(), leaves.size() * sizeof(int), cudaMemcpyHostToDevice, st), "act");
+        ck(cudaMemcpyAsync(h->upd.p, buf.data(), buf.size() * sizeof(int), cudaMemcpyHostToDevice, st), "upd");
+        ck(cudaMemsetAsync(h->pivots.p, 0, sizeof(int), st), "piv");
+        ck(cudaMemsetAsync(L0.dec.p, 0, L0.nnodes, st), "dec0");
+        const int na = (int)leaves.size();
+        if (H > 0) {
+            h->snap.reserve((size_t)na * L0.nExt * L0.nExt);
+            hb::launch_ext_snapshot(L0.ms(), L0.d_ext.p, L0.nExt, h->active.p, na, h->snap.p, st);
+        }
+        hb::launch_leaf_edges(L0.ms(), h->active.p, na, h->upd.p, h->upd.p + eoff.size(), L0.kflag.p, h->pivots.p, st);
+        ck(cudaGetLastError(), "leaf edges");
+        int npiv = 0;
+        ck(cudaMemcpyAsync(&npiv, h->pivots.p, sizeof(int), cudaMemcpyDeviceToHost, st), "piv d2h");
+        close_matrices(h, L0, leaves);
+        if (H > 0) {
+            ck(cudaMemcpyAsync(h->active.p, leaves.data(), leaves.size() * sizeof(int), cudaMemcpyHostToDevice, st), "act");
+            hb::launch_ext_compare(L0.ms(), L0.d_ext.p, L0.nExt, h->active.p, na, h->snap.p, L0.dec.p, st);
+            ck(cudaGetLastError(), "compare");
+        }
+        ck(cudaStreamSynchronize(st), "sync");
+        if (record_stats) {
+            h->stats.n_touched_leaves = na;
+            h->stats.n_pivots = npiv;
+        }
+    }
+    // 3. levels 1..H
+    std::vector<int> cand = leaves;  // candidates of the level below
+    std::vector<uint8_t> child_dec;
+    for (int l = 1; l <= H; ++l) {
+        Level& Lv = h->L[l];
+        Level& Lc = h->L[l - 1];
+        child_dec.resize(Lc.nnodes);
+        ck(cudaMemcpyAsync(child_dec.data(), Lc.dec.p, Lc.nnodes, cudaMemcpyDeviceToHost, st), "dec d2h");
+        ck(cudaStreamSynchronize(st), "sync dec");
+        // candidates: parents of flagged children, plus seam nodes
+        std::vector<int> slot_of(Lv.nnodes, -1);
+        std::vector<int> act;
+        for (int c : cand) {
+            if (!child_dec[c]) continue;
+            const int cx = c % Lc.nodes_x, cy = c / Lc.nodes_x;
+            const int p = (cy / g) * Lv.nodes_x + (cx / g);
+            if (slot_of[p] < 0) { slot_of[p] = (int)act.size(); act.push_back(p); }
+        }
+        for (int node : seam_nodes[l])
+            if (slot_of[node] < 0) { slot_of[node] = (int)act.size(); act.push_back(node); }
+        n_dirty += (int)act.size();
+        if (act.empty()) {
+            // nothing changes at this level; higher levels only see seams
+            cand.clear();
+            ck(cudaMemsetAsync(Lv.dec.p, 0, Lv.nnodes, st), "dec");
+            continue;
+        }
+        const int na = (int)act.size();
+        std::vector<int> buf(na + 1, 0);
+        for (int i = 0; i < na; ++i) {
+            const int sl = seam_slot[l][act[i]];
+            buf[i + 1] = buf[i] + (sl >= 0 ? (int)seams[l][sl].size() / 2 : 0);
+        }
+        for (int i = 0; i < na; ++i) {
+            const int sl = seam_slot[l][act[i]];
+            if (sl >= 0) buf.insert(buf.end(), seams[l][sl].begin(), seams[l][sl].end());
+        }
+        h->active.reserve(na);
+        h->upd.reserve(buf.size());
+        ck(cudaMemcpyAsync(h->active.p, act.data(), na * sizeof(int), cudaMemcpyHostToDevice, st), "act");
+        ck(cudaMemcpyAsync(h->upd.p, buf.data(), buf.size() * sizeof(int), cudaMemcpyHostToDevice, st), "upd");
+        ck(cudaMemsetAsync(Lv.dec.p, 0, Lv.nnodes, st), "dec");
+        const bool root = (l == H);
+        if (!root) {
+            h->snap.reserve((size_t)na * Lv.nExt * Lv.nExt);
+            hb::launch_ext_snapshot(Lv.ms(), Lv.d_ext.p, Lv.nExt, h->active.p, na, h->snap.p, st);
+        }
+        hb::launch_node_child_insert(Lv.ms(), Lc.ms(), Lc.d_ext.p, Lv.nP, g, Lv.nodes_x, Lc.nodes_x, h->active.p, na,
+                                     Lc.dec.p, Lv.kflag.p, st);
+        hb::launch_node_seams(Lv.ms(), h->active.p, na, h->upd.p, h->upd.p + na + 1, Lv.kflag.p, st);
+        ck(cudaGetLastError(), "node insert");
+        close_matrices(h, Lv, act);
+        if (!root) {
+            ck(cudaMemcpyAsync(h->active.p, act.data(), na * sizeof(int), cudaMemcpyHostToDevice, st), "act");
+            hb::launch_ext_compare(Lv.ms(), Lv.d_ext.p, Lv.nExt, h->active.p, na, h->snap.p, Lv.dec.p, st);
+            ck(cudaGetLastError(), "compare");
+        }
+        cand = act;
+    }
+    ck(cudaStreamSynchronize(st), "open sync");
+    if (record_stats) h->stats.n_dirty_ancestors = n_dirty;
+}
+
+// ---------------------------------------------------------------------------
+// Query (reference queryAllPairs, minplus_oracle.cpp:934-1419)
+// ---------------------------------------------------------------------------
+struct QueryPlan {
+    std::vector<int> buf;
+    int n_sorted = 0;
+    int o_vp0 = 0, o_inv = 0;
+    std::vector<int> o_cg, n_cg, o_ng, n_ng, o_qoff, max_cg, max_ng;
+};
+
+void make_plan(const htrip_index* h, const int32_t* vps, const uint8_t* pass_flags, int k, QueryPlan& P) {
+    const int b = h->b, g = h->g, H = h->H;
+    struct V { uint64_t key; int orig; int tx, ty; };
+    std::vector<V> v;
+    v.reserve(k);
+    for (int i = 0; i < k; ++i) {
+        if (!pass_flags[i]) continue;
+        const int r = vps[2 * i], c = vps[2 * i + 1];
+        const int tx = c / b, ty = r / b;
+        uint64_t key = 0, mul = 1;
+        int x = tx, y = ty;
+        for (int l = 0; l < std::max(H, 1); ++l) {
+            key += (uint64_t)((y % g) * g + (x % g)) * mul;
+            mul *= (uint64_t)(g * g);
+            x /= g;
+            y /= g;
+        }
+        v.push_back({key, i, tx, ty});
+    }
+    std::stable_sort(v.begin(), v.end(), [](const V& a, const V& c) { return a.key < c.key; });
+    const int ns = (int)v.size();
+    P.n_sorted = ns;
+    P.buf.clear();
+    P.o_vp0 = 0;
+    P.buf.resize(4 * ns + k);
+    P.o_inv = 4 * ns;
+    for (int i = 0; i < k; ++i) P.buf[P.o_inv + i] = -1;
+    for (int i = 0; i < ns; ++i) {
+        const int r = vps[2 * v[i].orig], c = vps[2 * v[i].orig + 1];
+        P.buf[4 * i] = v[i].ty * h->leaves_x + v[i].tx;
+        P.buf[4 * i + 1] = (r % b) * b + (c % b);
+        P.buf[P.o_inv + v[i].orig] = i;
+    }
+    for (int i = 0; i < ns;) {
+        int j = i;
+        while (j < ns && P.buf[4 * j] == P.buf[4 * i]) ++j;
+        for (int t = i; t < j; ++t) { P.buf[4 * t + 2] = i; P.buf[4 * t + 3] = j; }
+        i = j;
+    }
+    P.o_cg.assign(H + 1, 0); P.n_cg.assign(H + 1, 0); P.o_ng.assign(H + 1, 0); P.n_ng.assign(H + 1, 0);
+    P.o_qoff.assign(H + 1, 0); P.max_cg.assign(H + 1, 0); P.max_ng.assign(H + 1, 0);
+    for (int l = 1; l <= H; ++l) {
+        const Level& Lv = h->L[l];
+        const Level& Lc = h->L[l - 1];
+        std::vector<int> child(ns), node(ns), quad(ns);
+        for (int i = 0; i < ns; ++i) {
+            const int cxp = v[i].tx * b / Lc.side, cyp = v[i].ty * b / Lc.side;
+            child[i] = cyp * Lc.nodes_x + cxp;
+            node[i] = (cyp / g) * Lv.nodes_x + (cxp / g);
+            quad[i] = (cyp % g) * g + (cxp % g);
+        }
+        P.o_cg[l] = (int)P.buf.size();
+        int ncg = 0;
+        std::vector<int> cg_start;
+        for (int i = 0; i < ns;) {
+            int j = i;
+            while (j < ns && child[j] == child[i]) ++j;
+            P.buf.insert(P.buf.end(), {node[i], quad[i], i, j - i});
+            P.max_cg[l] = std::max(P.max_cg[l], j - i);
+            cg_start.push_back(i);
+            ++ncg;
+            i = j;
+        }
+        P.n_cg[l] = ncg;
+        P.o_ng[l] = (int)P.buf.size();
+        int nng = 0;
+        for (int i = 0, cgi = 0; i < ns;) {
+            int j = i;
+            while (j < ns && node[j] == node[i]) ++j;
+            while (cgi < ncg && cg_start[cgi] < i) ++cgi;
+            P.buf.insert(P.buf.end(), {i, j, cgi});
+            P.max_ng[l] = std::max(P.max_ng[l], j - i);
+            ++nng;
+            i = j;
+        }
+        P.n_ng[l] = nng;
+        P.o_qoff[l] = (int)P.buf.size();
+        for (int i = 0; i < ns; ++i) P.buf.push_back(quad[i] * Lv.nP);
+    }
+}
+
+void run_query(htrip_index* h, const QueryPlan& P, int k, uint16_t* out_dev) {
+    cudaStream_t st = h->stream;
+    const int H = h->H, ns = P.n_sorted;
+    h->qplan.reserve(std::max<size_t>(1, P.buf.size()));
+    ck(cudaMemcpyAsync(h->qplan.p, P.buf.data(), P.buf.size() * sizeof(int), cudaMemcpyHostToDevice, st), "plan");
+    const int* plan = h->qplan.p;
+    const int ldm = std::max(8, (ns + 7) / 8 * 8);
+    int maxExt = 0, maxNP = 0, maxnP = 0, maxcg = 1;
+    for (int l = 0; l <= H; ++l) maxExt = std::max(maxExt, h->L[l].nExt);
+    for (int l = 1; l <= H; ++l) {
+        maxNP = std::max(maxNP, h->L[l].NP);
+        maxnP = std::max(maxnP, h->L[l].nP);
+        maxcg = std::max(maxcg, P.n_cg[l]);
+    }
+    const int ldx = ldm;
+    h->qM.reserve((size_t)ldm * ldm);
+    h->qX[0].reserve((size_t)maxExt * ldx);
+    h->qX[1].reserve((size_t)maxExt * ldx);
+    h->qY.reserve(std::max<size_t>(1, (size_t)ns * maxNP));
+    h->qkidx.reserve((size_t)maxcg * (maxnP + 1) + 1);
+    // M := INF (upper triangle is what finalize reads)
+    hb::launch_fill_u16(h->qM.p, (size_t)ldm * ldm, hb::INF, st);
+    hb::launch_query_level0(h->L[0].ms(), h->L[0].d_ext.p, h->L[0].nExt, plan + P.o_vp0, ns, h->qX[0].p, ldx,
+                            h->qM.p, ldm, st);
+    ck(cudaGetLastError(), "level0");
+    int cur = 0;
+    for (int l = 1; l <= H; ++l) {
+        const Level& Lv = h->L[l];
+        hb::launch_query_project(Lv.ms(), Lv.nP, plan + P.o_cg[l], P.n_cg[l], P.max_cg[l], h->qX[cur].p, ldx,
+                                 h->qY.p, maxNP, h->qkidx.p, st);
+        ck(cudaGetLastError(), "project");
+        if (l < H) {
+            hb::launch_query_lift(h->qY.p, maxNP, Lv.d_ext.p, Lv.nExt, ns, h->qX[cur ^ 1].p, ldx, st);
+            ck(cudaGetLastError(), "lift");
+        }
+        hb::launch_query_meet(plan + P.o_ng[l], P.n_ng[l], plan + P.o_qoff[l], h->qY.p, maxNP, h->qX[cur].p, ldx,
+                              Lv.nP, h->qM.p, ldm, P.max_ng[l], st);
+        ck(cudaGetLastError(), "meet");
+        cur ^= 1;
+    }
+    hb::launch_query_finalize(h->qM.p, ldm, plan + P.o_inv, k, out_dev, st);
+    ck(cudaGetLastError(), "finalize");
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+#define HTRIP_GUARD_BEGIN try {
+#define HTRIP_GUARD_END                                                                     \
+    }                                                                                       \
+    catch (const CudaError& ce) {                                                           \
+        if (ce.e == cudaErrorMemoryAllocation) {                                            \
+            cudaGetLastError();                                                             \
+            return fail(HTRIP_ERR_OOM, std::string("out of device memory in ") + ce.what);   \
+        }                                                                                   \
+        return fail(HTRIP_ERR_CUDA, std::string(ce.what) + ": " + cudaGetErrorString(ce.e)); \
+    }                                                                                       \
+    catch (const std::bad_alloc&) {                                                         \
+        return fail(HTRIP_ERR_OOM, "host allocation failed");                               \
+    }
+
+extern "C" {
+
+const char* htrip_last_error(void) { return g_err.c_str(); }
+
+htrip_status htrip_create(htrip_config cfg, int device, htrip_index** out) {
+    if (!out) return fail(HTRIP_ERR_INVALID, "null out");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(HTRIP_ERR_NO_DEVICE, "no CUDA device");
+    }
+    if (device < 0 || device >= ndev) return fail(HTRIP_ERR_INVALID, "bad device ordinal");
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    auto* h = new htrip_index();
+    h->device = device;
+    h->b = cfg.tile_size_b;
+    h->g = cfg.group;
+    ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
+    *out = h;
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_destroy(htrip_index* h) {
+    if (!h) return HTRIP_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    h->release();
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return HTRIP_OK;
+}
+
+htrip_status htrip_build(htrip_index* h, const uint8_t* observed, int32_t rows, int32_t cols) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    // HierarchyConfig::isValid (types.hpp:221-224) and build()'s own checks (minplus_oracle.cpp:49-52)
+    const int b = h->b, g = h->g;
+    if (!(b > 0 && g >= 2 && g * g <= 256)) return fail(HTRIP_ERR_INVALID, "invalid HierarchyConfig");
+    if (std::max(rows, cols) <= 0) return fail(HTRIP_ERR_INVALID, "empty grid");
+    if (b < 2 || b > 32) return fail(HTRIP_ERR_UNSUPPORTED, "tile_size_b must be in [2, 32]");
+    if (!observed || rows < 0 || cols < 0) return fail(HTRIP_ERR_INVALID, "bad grid");
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    do_build(h, observed, rows, cols);
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_open_cells(htrip_index* h, const int32_t* rc, int32_t n, const uint8_t* observed, int32_t rows,
+                              int32_t cols) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    if (!h->built) return fail(HTRIP_ERR_NOT_BUILT, "index not built");
+    if (n < 0 || (n > 0 && !rc) || !observed) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    do_open(h, rc, n, observed, rows, cols, true);
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_open_cell(htrip_index* h, int32_t r, int32_t c, const uint8_t* observed, int32_t rows, int32_t cols) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    if (!h->built) return fail(HTRIP_ERR_NOT_BUILT, "index not built");
+    if (!observed) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    const int32_t rc[2] = {r, c};
+    do_open(h, rc, 1, observed, rows, cols, false);
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_query_all_pairs(htrip_index* h, const int32_t* vps, int32_t k, const uint8_t* observed, int32_t rows,
+                                   int32_t cols, uint16_t* out) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    if (!h->built) return fail(HTRIP_ERR_NOT_BUILT, "index not built");
+    if (k < 0 || (k > 0 && (!vps || !out)) || !observed) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    if (k == 0) return HTRIP_OK;
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    std::vector<uint8_t> pf(k);
+    for (int i = 0; i < k; ++i) {
+        const int r = vps[2 * i], c = vps[2 * i + 1];
+        pf[i] = (r >= 0 && c >= 0 && r < rows && c < cols && observed[(size_t)r * cols + c] == 1 && r < h->S && c < h->S);
+    }
+    QueryPlan P;
+    make_plan(h, vps, pf.data(), k, P);
+    h->qout.reserve((size_t)k * k);
+    run_query(h, P, k, h->qout.p);
+    ck(cudaMemcpyAsync(out, h->qout.p, (size_t)k * k * sizeof(uint16_t), cudaMemcpyDeviceToHost, h->stream), "out");
+    ck(cudaStreamSynchronize(h->stream), "query sync");
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_query_all_pairs_dev(htrip_index* h, const int32_t* vps_dev, const uint8_t* passable_dev, int32_t k,
+                                       uint16_t* out_dev) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    if (!h->built) return fail(HTRIP_ERR_NOT_BUILT, "index not built");
+    if (k < 0 || (k > 0 && (!vps_dev || !passable_dev || !out_dev))) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    if (k == 0) return HTRIP_OK;
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    // The viewpoint plan (Morton grouping per level) is built on the host.
+    std::vector<int32_t> vps(2 * (size_t)k);
+    std::vector<uint8_t> pf(k);
+    ck(cudaMemcpyAsync(vps.data(), vps_dev, vps.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream), "vps");
+    ck(cudaMemcpyAsync(pf.data(), passable_dev, k, cudaMemcpyDeviceToHost, h->stream), "pf");
+    ck(cudaStreamSynchronize(h->stream), "sync");
+    for (int i = 0; i < k; ++i) {
+        const int r = vps[2 * i], c = vps[2 * i + 1];
+        if (r < 0 || c < 0 || r >= h->S || c >= h->S) pf[i] = 0;
+    }
+    QueryPlan P;
+    make_plan(h, vps.data(), pf.data(), k, P);
+    run_query(h, P, k, out_dev);
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_clone(const htrip_index* src, htrip_index** out) {
+    if (!src || !out) return fail(HTRIP_ERR_INVALID, "null argument");
+    *out = nullptr;
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(src->device), "cudaSetDevice");
+    ck(cudaStreamSynchronize(src->stream), "sync");
+    auto* h = new htrip_index();
+    h->device = src->device;
+    h->b = src->b;
+    h->g = src->g;
+    try {
+        ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
+        if (src->built) {
+            h->S = src->S; h->H = src->H; h->rows = src->rows; h->cols = src->cols; h->leaves_x = src->leaves_x;
+            make_levels(h);
+            alloc_levels(h);
+            for (int l = 0; l <= h->H; ++l)
+                ck(cudaMemcpyAsync(h->L[l].mat.p, src->L[l].mat.p, h->L[l].mat.n * sizeof(uint16_t),
+                                   cudaMemcpyDeviceToDevice, h->stream), "clone copy");
+            h->pass.reserve(src->pass.n);
+            ck(cudaMemcpyAsync(h->pass.p, src->pass.p, src->pass.n, cudaMemcpyDeviceToDevice, h->stream), "clone pass");
+            ck(cudaStreamSynchronize(h->stream), "clone sync");
+            h->built = true;
+            h->stats = src->stats;
+        }
+    } catch (...) {
+        htrip_destroy(h);
+        throw;
+    }
+    *out = h;
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_sync(htrip_index* h) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    HTRIP_GUARD_BEGIN
+    ck(cudaStreamSynchronize(h->stream), "sync");
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+void* htrip_stream(htrip_index* h) { return h ? (void*)h->stream : nullptr; }
+
+htrip_status htrip_shape(const htrip_index* h, int32_t* S, int32_t* H, int32_t* leaves_x) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    if (S) *S = h->S;
+    if (H) *H = h->H;
+    if (leaves_x) *leaves_x = h->leaves_x;
+    return HTRIP_OK;
+}
+
+htrip_status htrip_last_batch_stats(const htrip_index* h, htrip_batch_stats* out) {
+    if (!h || !out) return fail(HTRIP_ERR_INVALID, "null argument");
+    *out = h->stats;
+    return HTRIP_OK;
+}
+
+htrip_status htrip_memory_bytes(const htrip_index* h, uint64_t* reference_bytes, uint64_t* device_bytes) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    uint64_t ref = 0, dev = 0;
+    if (h->built) {
+        const Level& L0 = h->L[0];
+        ref += (uint64_t)L0.nnodes * ((uint64_t)L0.n * L0.n + (uint64_t)L0.nExt * L0.nExt) * 2;
+        for (int l = 1; l <= h->H; ++l) {
+            const Level& Lv = h->L[l];
+            ref += (uint64_t)Lv.nnodes *
+                   ((uint64_t)Lv.n * Lv.n + (uint64_t)Lv.nExt * Lv.nExt + (uint64_t)Lv.n * Lv.nExt) * 2;
+        }
+        for (const auto& Lv : h->L)
+            dev += (Lv.mat.n + Lv.klist.n * 2 + Lv.kcnt.n * 2) * sizeof(uint16_t) + Lv.kflag.n + Lv.dec.n +
+                   (Lv.d_ext.n + Lv.d_seams.n) * sizeof(int);
+        dev += h->pass.n + h->panel.n * 2 + h->pflags.n + h->snap.n * 2 + h->qY.n * 2 + h->qM.n * 2 +
+               (h->qX[0].n + h->qX[1].n) * 2 + h->qkidx.n * 4 + h->qout.n * 2;
+    }
+    if (reference_bytes) *reference_bytes = ref;
+    if (device_bytes) *device_bytes = dev;
+    return HTRIP_OK;
+}
+
+static htrip_status read_block(const htrip_index* h, int lvl, int node, const int* rows, int nr, const int* cols,
+                               int nc, uint16_t* out) {
+    const Level& Lv = h->L[lvl];
+    DevBuf<int> idx;
+    DevBuf<uint16_t> tmp;
+    idx.reserve(nr + nc);
+    tmp.reserve(std::max(1, nr * nc));
+    cudaStream_t st = h->stream;
+    ck(cudaMemcpyAsync(idx.p, rows, nr * sizeof(int), cudaMemcpyHostToDevice, st), "idx");
+    ck(cudaMemcpyAsync(idx.p + nr, cols, nc * sizeof(int), cudaMemcpyHostToDevice, st), "idx");
+    hb::launch_gather_block(Lv.mat.p + (size_t)node * Lv.NP * Lv.NP, Lv.NP, idx.p, nr, idx.p + nr, nc, tmp.p, st);
+    ck(cudaGetLastError(), "gather");
+    ck(cudaMemcpyAsync(out, tmp.p, (size_t)nr * nc * sizeof(uint16_t), cudaMemcpyDeviceToHost, st), "d2h");
+    ck(cudaStreamSynchronize(st), "sync");
+    idx.release();
+    tmp.release();
+    return HTRIP_OK;
+}
+
+static bool valid_node(const htrip_index* h, int lvl, int node) {
+    return h && h->built && lvl >= 0 && lvl <= h->H && node >= 0 && node < h->L[lvl].nnodes;
+}
+
+htrip_status htrip_read_leaf_D(const htrip_index* h, int32_t leaf, uint16_t* out) {
+    if (!valid_node(h, 0, leaf) || !out) return fail(HTRIP_ERR_INVALID, "bad leaf");
+    HTRIP_GUARD_BEGIN
+    std::vector<int> id(h->L[0].n);
+    std::iota(id.begin(), id.end(), 0);
+    return read_block(h, 0, leaf, id.data(), (int)id.size(), id.data(), (int)id.size(), out);
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_read_leaf_S(const htrip_index* h, int32_t leaf, uint16_t* out) {
+    if (!valid_node(h, 0, leaf) || !out) return fail(HTRIP_ERR_INVALID, "bad leaf");
+    HTRIP_GUARD_BEGIN
+    const auto& e = h->L[0].ext;
+    return read_block(h, 0, leaf, e.data(), (int)e.size(), e.data(), (int)e.size(), out);
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_read_node_DU(const htrip_index* h, int32_t lvl, int32_t node, uint16_t* out) {
+    if (lvl < 1 || !valid_node(h, lvl, node) || !out) return fail(HTRIP_ERR_INVALID, "bad node");
+    HTRIP_GUARD_BEGIN
+    std::vector<int> id(h->L[lvl].n);
+    std::iota(id.begin(), id.end(), 0);
+    return read_block(h, lvl, node, id.data(), (int)id.size(), id.data(), (int)id.size(), out);
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_read_node_SU(const htrip_index* h, int32_t lvl, int32_t node, uint16_t* out) {
+    if (lvl < 1 || !valid_node(h, lvl, node) || !out) return fail(HTRIP_ERR_INVALID, "bad node");
+    HTRIP_GUARD_BEGIN
+    const auto& e = h->L[lvl].ext;
+    return read_block(h, lvl, node, e.data(), (int)e.size(), e.data(), (int)e.size(), out);
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_read_node_C2E(const htrip_index* h, int32_t lvl, int32_t node, int32_t quad, uint16_t* out) {
+    if (lvl < 1 || !valid_node(h, lvl, node) || !out || quad < 0 || quad >= h->g * h->g)
+        return fail(HTRIP_ERR_INVALID, "bad node");
+    HTRIP_GUARD_BEGIN
+    const Level& Lv = h->L[lvl];
+    std::vector<int> rows(Lv.nP);
+    std::iota(rows.begin(), rows.end(), quad * Lv.nP);
+    return read_block(h, lvl, node, rows.data(), (int)rows.size(), Lv.ext.data(), (int)Lv.ext.size(), out);
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_level_dims(const htrip_index* h, int32_t lvl, int32_t* n, int32_t* n_ext, int32_t* n_child_ports,
+                              int32_t* n_nodes) {
+    if (!h || !h->built || lvl < 0 || lvl > h->H) return fail(HTRIP_ERR_INVALID, "bad level");
+    const Level& Lv = h->L[lvl];
+    if (n) *n = Lv.n;
+    if (n_ext) *n_ext = Lv.nExt;
+    if (n_child_ports) *n_child_ports = Lv.nP;
+    if (n_nodes) *n_nodes = Lv.nnodes;
+    return HTRIP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,773 @@
+// sm_100a kernels of the HTRIP min-plus hierarchy.
+//
+// Layout: every tropical matrix (leaf D, node D_U) is a dense row-major u16
+// square of logical order n padded to NP (multiple of 64) with INF in the
+// padding; matrix m of a level lives at base + m*NP*NP.  All arithmetic is
+// the exact clamped min-plus of minplus.cuh, so every result is identical to
+// the reference's scalar / AVX2 arithmetic.
+#include "kernels.cuh"
+#include "minplus.cuh"
+
+#include <algorithm>
+
+namespace hb {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ uint16_t* mat_ptr(const MatSet& M, int m) {
+    return M.base + (size_t)m * M.NP * M.NP;
+}
+
+// ---------------------------------------------------------------------------
+// Leaf APSP: one warp per source cell, bit-parallel BFS.  Lane r owns row r
+// of the b x b leaf as a bitmask; a BFS level is one shift/shuffle step, so
+// the BFS level number is the reference's BFS distance (leaf_tile.cpp:111-152).
+// Non-passable sources keep the tropical identity row (leaf_tile.cpp:66-68).
+// ---------------------------------------------------------------------------
+constexpr int kBfsWarps = 8;
+
+__global__ void __launch_bounds__(kBfsWarps * 32)
+leaf_bfs_kernel(const uint8_t* __restrict__ pass, int S, int b, int leaves_x, MatSet L) {
+    extern __shared__ __align__(16) uint16_t sm_rows[];
+    const int leaf = blockIdx.y;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int src = blockIdx.x * kBfsWarps + warp;
+    const int NP = L.NP, n = b * b;
+    if (src >= NP) return;
+    uint16_t* row = sm_rows + (size_t)warp * NP;
+    const int ty = leaf / leaves_x, tx = leaf % leaves_x;
+    const int R0 = ty * b, C0 = tx * b;
+    uint32_t m = 0;
+    if (lane < b) {
+        const uint8_t* p = pass + (size_t)(R0 + lane) * S + C0;
+        for (int c = 0; c < b; ++c) m |= (uint32_t)(p[c] != 0) << c;
+    }
+    for (int j = lane; j < NP; j += 32) row[j] = INF;
+    __syncwarp();
+    if (src < n) {
+        const int sr = src / b, sc = src % b;
+        const uint32_t srow = __shfl_sync(FULL, m, sr);
+        if (lane == 0) row[src] = 0;
+        if ((srow >> sc) & 1u) {
+            const uint32_t rowmask = (b == 32) ? FULL : ((1u << b) - 1u);
+            uint32_t vis = (lane == sr) ? (1u << sc) : 0u;
+            uint32_t front = vis;
+            for (int d = 1;; ++d) {
+                uint32_t up = __shfl_up_sync(FULL, front, 1);
+                uint32_t dn = __shfl_down_sync(FULL, front, 1);
+                if (lane == 0) up = 0;
+                if (lane == 31) dn = 0;
+                const uint32_t nb = ((front << 1) | (front >> 1) | up | dn) & rowmask;
+                uint32_t nw = nb & m & ~vis;
+                vis |= nw;
+                front = nw;
+                if (!__any_sync(FULL, nw)) break;
+                while (nw) {
+                    const int c = __ffs(nw) - 1;
+                    nw &= nw - 1;
+                    row[lane * b + c] = (uint16_t)d;
+                }
+            }
+        }
+    }
+    __syncwarp();
+    uint4* dst = reinterpret_cast<uint4*>(mat_ptr(L, leaf) + (size_t)src * NP);
+    const uint4* s4 = reinterpret_cast<const uint4*>(row);
+    for (int j = lane; j < NP / 8; j += 32) dst[j] = s4[j];
+}
+
+// ---------------------------------------------------------------------------
+// Node initial D_U (internal_node.cpp:98-145): entry (i, j) of node n is the
+// child summary S_q[p][p'] when i = q*nP + p and j = q*nP + p' lie in the
+// same child block q, INF otherwise (and in the padding).  S_q is the child
+// matrix restricted to its exterior ports: child[ext[p]][ext[p']].
+// ---------------------------------------------------------------------------
+__global__ void node_init_kernel(MatSet N, MatSet Cm, const int* __restrict__ cext, int nP, int g,
+                                 int nodes_x, int child_nodes_x) {
+    const int node = blockIdx.y;
+    const int NP = N.NP, nV = N.n;
+    const size_t chunk = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // 8 entries
+    const size_t per_row = NP / 8;
+    if (chunk >= (size_t)NP * per_row) return;
+    const int i = (int)(chunk / per_row);
+    const int j0 = (int)(chunk % per_row) * 8;
+    uint16_t v[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) v[t] = INF;
+    if (i < nV) {
+        const int q = i / nP, p = i - q * nP;
+        const int tx = node % nodes_x, ty = node / nodes_x;
+        const int cx = q % g, cy = q / g;
+        const int child = (ty * g + cy) * child_nodes_x + (tx * g + cx);
+        const uint16_t* crow = mat_ptr(Cm, child) + (size_t)cext[p] * Cm.NP;
+        const int lo = q * nP, hi = lo + nP;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const int j = j0 + t;
+            if (j >= lo && j < hi) v[t] = crow[cext[j - lo]];
+        }
+    }
+    uint4 o;
+    o.x = v[0] | ((uint32_t)v[1] << 16);
+    o.y = v[2] | ((uint32_t)v[3] << 16);
+    o.z = v[4] | ((uint32_t)v[5] << 16);
+    o.w = v[6] | ((uint32_t)v[7] << 16);
+    reinterpret_cast<uint4*>(mat_ptr(N, node) + (size_t)i * NP)[j0 / 8] = o;
+}
+
+// Build-time seams: both cells Free -> unit edge, both endpoints are pivots.
+__global__ void seams_build_kernel(MatSet N, const int* __restrict__ seams, int n_seams,
+                                   const uint8_t* __restrict__ pass, int S, int side, int nodes_x,
+                                   uint8_t* kflag) {
+    const int node = blockIdx.y;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_seams) return;
+    const int* e = seams + 6 * s;
+    const int R0 = (node / nodes_x) * side, C0 = (node % nodes_x) * side;
+    if (!pass[(size_t)(R0 + e[2]) * S + C0 + e[3]] || !pass[(size_t)(R0 + e[4]) * S + C0 + e[5]]) return;
+    uint16_t* D = mat_ptr(N, node);
+    const int NP = N.NP;
+    D[(size_t)e[0] * NP + e[1]] = 1;
+    D[(size_t)e[1] * NP + e[0]] = 1;
+    kflag[(size_t)node * NP + e[0]] = 1;
+    kflag[(size_t)node * NP + e[1]] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// Pivot compaction: flags -> ascending index list, one CTA per matrix.
+// ---------------------------------------------------------------------------
+__global__ void compact_pivots_kernel(uint8_t* kflag, int NP, const int* __restrict__ active,
+                                      int* klist, int* kcnt) {
+    __shared__ int warp_tot[32];
+    __shared__ int base;
+    const int m = active[blockIdx.x];
+    uint8_t* f = kflag + (size_t)m * NP;
+    int* out = klist + (size_t)m * NP;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    for (int j0 = 0; j0 < NP; j0 += blockDim.x) {
+        const int j = j0 + threadIdx.x;
+        const bool on = j < NP && f[j];
+        const unsigned bal = __ballot_sync(FULL, on);
+        if (lane == 0) warp_tot[warp] = __popc(bal);
+        __syncthreads();
+        int off = base;
+        for (int w = 0; w < warp; ++w) off += warp_tot[w];
+        if (on) {
+            out[off + __popc(bal & ((1u << lane) - 1u))] = j;
+            f[j] = 0;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int w = 0; w < nw; ++w) t += warp_tot[w];
+            base += t;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) kcnt[m] = base;
+}
+
+// ---------------------------------------------------------------------------
+// Blocked pivot-set Kleene closure, one round over pivots Kc (|Kc| = mk <= B):
+//   T  = D[Kc, Kc], closed in shared memory (Floyd-Warshall over Kc),
+//   R' = T* (x) D[Kc, :]                (panel kernel, B x NP per matrix)
+//   D  = min(D, R'^T (x) R')            (syrk kernel; D is symmetric, so
+//                                        R'[k][i] = (D[:,Kc] (x) T*)[i][k])
+// This is exactly the reference's sequential relaxation over the same pivots
+// (leaf_tile.cpp:348-371, internal_node.cpp:201-231, :372-399): both give
+// the unique shortest-path closure through the pivot set.
+// ---------------------------------------------------------------------------
+constexpr int kPanelSlab = 256;
+
+__global__ void __launch_bounds__(256)
+closure_panel_kernel(MatSet M, const int* __restrict__ active, const int* __restrict__ klist,
+                     const int* __restrict__ kcnt, int round, uint16_t* panel, uint8_t* flags) {
+    constexpr int B = kPivotChunk;
+    __shared__ uint16_t T[B][B + 2];
+    __shared__ __align__(16) uint16_t Dk[B][kPanelSlab];
+    __shared__ int kc[B];
+    const int slot = blockIdx.y;
+    const int m = active[slot];
+    const int NP = M.NP;
+    const int mk = min(B, kcnt[m] - round * B);
+    if (mk <= 0) return;
+    const int* K = klist + (size_t)m * NP + round * B;
+    const uint16_t* D = mat_ptr(M, m);
+    const int tid = threadIdx.x;
+    if (tid < mk) kc[tid] = K[tid];
+    __syncthreads();
+    for (int idx = tid; idx < B * B; idx += blockDim.x) {
+        const int a = idx / B, c = idx % B;
+        T[a][c] = (a < mk && c < mk) ? D[(size_t)kc[a] * NP + kc[c]] : (a == c ? 0 : INF);
+    }
+    __syncthreads();
+    for (int kk = 0; kk < mk; ++kk) {
+        for (int idx = tid; idx < mk * mk; idx += blockDim.x) {
+            const int a = idx / mk, c = idx % mk;
+            const uint32_t alt = sat_add(T[a][kk], T[kk][c]);
+            if (alt < T[a][c]) T[a][c] = (uint16_t)alt;
+        }
+        __syncthreads();
+    }
+    const int slab0 = blockIdx.x * kPanelSlab;
+    const int w = min(kPanelSlab, NP - slab0);
+    for (int idx = tid; idx < mk * (w / 8); idx += blockDim.x) {
+        const int a = idx / (w / 8), c8 = idx % (w / 8);
+        reinterpret_cast<uint4*>(&Dk[a][0])[c8] =
+            reinterpret_cast<const uint4*>(D + (size_t)kc[a] * NP + slab0)[c8];
+    }
+    __syncthreads();
+    uint16_t* P = panel + (size_t)slot * B * NP;
+    // Each thread: one pivot row a and a run of column pairs.
+    __shared__ int tile_any[kPanelSlab / kFlagTile];
+    if (tid < kPanelSlab / kFlagTile) tile_any[tid] = 0;
+    __syncthreads();
+    const int pairs = w / 2;
+    for (int idx = tid; idx < B * pairs; idx += blockDim.x) {
+        const int a = idx / pairs, cp = idx % pairs;
+        uint32_t acc = INF2;
+        if (a < mk) {
+            const uint32_t* dk = reinterpret_cast<const uint32_t*>(&Dk[0][0]) + cp;
+            for (int c = 0; c < mk; ++c) {
+                const uint32_t t = T[a][c];
+                if (t >= INF) continue;
+                acc = acc_clamp(acc, dk[c * (kPanelSlab / 2)], splat(t), splat(INF - t));
+            }
+            if (acc != INF2) tile_any[(2 * cp) / kFlagTile] = 1;
+        }
+        reinterpret_cast<uint32_t*>(P + (size_t)a * NP + slab0)[cp] = acc;
+    }
+    __syncthreads();
+    if (tid < w / kFlagTile) flags[(size_t)slot * (NP / kFlagTile) + slab0 / kFlagTile + tid] = tile_any[tid] ? 1 : 0;
+}
+
+// Register-tiled symmetric rank-|Kc| min-plus update.  Warp w owns RW rows
+// of the CTA tile; all 32 lanes of a warp share those rows, so the pivot
+// value a = R'[k][row] is warp-uniform and the fast / clamped / skip choice
+// never diverges.  Each lane owns CP packed column pairs.
+template <int RW, int CP>
+__global__ void __launch_bounds__(256)
+closure_syrk_kernel(MatSet M, const int* __restrict__ active, const int* __restrict__ kcnt, int round,
+                    const uint16_t* __restrict__ panel, const uint8_t* __restrict__ flags) {
+    constexpr int B = kPivotChunk;
+    constexpr int MT = 8 * RW;
+    constexpr int NT = 64 * CP;
+    extern __shared__ __align__(16) uint16_t sm[];
+    uint16_t* As = sm;            // [B][MT]
+    uint16_t* Bs = sm + B * MT;   // [B][NT]
+    const int slot = blockIdx.z;
+    const int m = active[slot];
+    const int NP = M.NP;
+    const int mk = min(B, kcnt[m] - round * B);
+    if (mk <= 0) return;
+    const int i0 = blockIdx.y * MT, j0 = blockIdx.x * NT;
+    const uint8_t* fl = flags + (size_t)slot * (NP / kFlagTile);
+    bool any_i = false, any_j = false;
+    for (int t = 0; t < MT / kFlagTile + (MT % kFlagTile ? 1 : 0); ++t) any_i |= fl[(i0 + t * kFlagTile) / kFlagTile] != 0;
+    for (int t = 0; t < NT / kFlagTile + (NT % kFlagTile ? 1 : 0); ++t) any_j |= fl[(j0 + t * kFlagTile) / kFlagTile] != 0;
+    if (!any_i || !any_j) return;
+    const uint16_t* P = panel + (size_t)slot * B * NP;
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < mk * (MT / 8); idx += blockDim.x) {
+        const int a = idx / (MT / 8), c8 = idx % (MT / 8);
+        reinterpret_cast<uint4*>(As + a * MT)[c8] = reinterpret_cast<const uint4*>(P + (size_t)a * NP + i0)[c8];
+    }
+    for (int idx = tid; idx < mk * (NT / 8); idx += blockDim.x) {
+        const int a = idx / (NT / 8), c8 = idx % (NT / 8);
+        reinterpret_cast<uint4*>(Bs + a * NT)[c8] = reinterpret_cast<const uint4*>(P + (size_t)a * NP + j0)[c8];
+    }
+    const int warp = tid >> 5, lane = tid & 31;
+    uint16_t* D = mat_ptr(M, m);
+    uint32_t acc[RW][CP];
+    const int col = j0 + lane * 2 * CP;
+#pragma unroll
+    for (int r = 0; r < RW; ++r) {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(D + (size_t)(i0 + warp * RW + r) * NP + col);
+#pragma unroll
+        for (int c = 0; c < CP; ++c) acc[r][c] = src[c];
+    }
+    __syncthreads();
+    for (int k = 0; k < mk; ++k) {
+        uint32_t bv[CP];
+#pragma unroll
+        for (int c = 0; c < CP; ++c) bv[c] = reinterpret_cast<const uint32_t*>(Bs + k * NT + lane * 2 * CP)[c];
+        const uint16_t* arow = As + k * MT + warp * RW;
+#pragma unroll
+        for (int r = 0; r < RW; ++r) {
+            const uint32_t a = arow[r];
+            if (a <= INF_HEADROOM) {
+                const uint32_t aa = splat(a);
+#pragma unroll
+                for (int c = 0; c < CP; ++c) acc[r][c] = acc_fast(acc[r][c], bv[c], aa);
+            } else if (a < INF) {
+                const uint32_t aa = splat(a), tt = splat(INF - a);
+#pragma unroll
+                for (int c = 0; c < CP; ++c) acc[r][c] = acc_clamp(acc[r][c], bv[c], aa, tt);
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RW; ++r) {
+        uint32_t* dst = reinterpret_cast<uint32_t*>(D + (size_t)(i0 + warp * RW + r) * NP + col);
+#pragma unroll
+        for (int c = 0; c < CP; ++c) dst[c] = acc[r][c];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Incremental inserts.
+// ---------------------------------------------------------------------------
+// In-leaf edges, processed sequentially per leaf like the reference loop
+// (leaf_tile.cpp:311-330): an edge counts (and its endpoints become pivots)
+// only if it shortens D[u][v].
+__global__ void leaf_edges_kernel(MatSet L, const int* __restrict__ active, const int* __restrict__ eoff,
+                                  const int* __restrict__ edges, uint8_t* kflag, int* pivots) {
+    if (threadIdx.x != 0) return;
+    const int m = active[blockIdx.x];
+    uint16_t* D = mat_ptr(L, m);
+    const int NP = L.NP;
+    uint8_t* f = kflag + (size_t)m * NP;
+    int np = 0;
+    for (int e = eoff[blockIdx.x]; e < eoff[blockIdx.x + 1]; ++e) {
+        const int u = edges[2 * e], v = edges[2 * e + 1];
+        if (1 < D[(size_t)u * NP + v]) {
+            D[(size_t)u * NP + v] = 1;
+            D[(size_t)v * NP + u] = 1;
+            if (!f[u]) { f[u] = 1; ++np; }
+            if (!f[v]) { f[v] = 1; ++np; }
+        }
+    }
+    atomicAdd(pivots, np);
+}
+
+// Child-summary decreases (internal_node.cpp:343-353).  Inserting every child
+// summary entry that is smaller than the parent's is the same as inserting
+// the reference's decrease list: entries that did not decrease can never be
+// smaller than the parent's (the parent block is <= the old summary).
+__global__ void node_child_insert_kernel(MatSet N, MatSet Cm, const int* __restrict__ cext, int nP, int g,
+                                         int nodes_x, int child_nodes_x, const int* __restrict__ active,
+                                         const uint8_t* __restrict__ child_dec, uint8_t* kflag) {
+    const int node = active[blockIdx.z];
+    const int q = blockIdx.y;
+    const int tx = node % nodes_x, ty = node / nodes_x;
+    const int child = (ty * g + q / g) * child_nodes_x + (tx * g + q % g);
+    if (!child_dec[child]) return;
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (size_t)nP * nP) return;
+    const int p = (int)(idx / nP), pp = (int)(idx % nP);
+    const uint16_t w = mat_ptr(Cm, child)[(size_t)cext[p] * Cm.NP + cext[pp]];
+    uint16_t* D = mat_ptr(N, node);
+    const int u = q * nP + p, v = q * nP + pp;
+    if (w < D[(size_t)u * N.NP + v]) {
+        D[(size_t)u * N.NP + v] = w;  // (v, u) is written by its own thread
+        kflag[(size_t)node * N.NP + u] = 1;
+        kflag[(size_t)node * N.NP + v] = 1;
+    }
+}
+
+// Update-time seams (internal_node.cpp:356-365), sequential per node.
+__global__ void node_seams_kernel(MatSet N, const int* __restrict__ active, const int* __restrict__ soff,
+                                  const int* __restrict__ seams, uint8_t* kflag) {
+    if (threadIdx.x != 0) return;
+    const int node = active[blockIdx.x];
+    uint16_t* D = mat_ptr(N, node);
+    const int NP = N.NP;
+    for (int s = soff[blockIdx.x]; s < soff[blockIdx.x + 1]; ++s) {
+        const int u = seams[2 * s], v = seams[2 * s + 1];
+        if (1 < D[(size_t)u * NP + v]) {
+            D[(size_t)u * NP + v] = 1;
+            D[(size_t)v * NP + u] = 1;
+            kflag[(size_t)node * NP + u] = 1;
+            kflag[(size_t)node * NP + v] = 1;
+        }
+    }
+}
+
+__global__ void ext_snapshot_kernel(MatSet M, const int* __restrict__ ext, int nExt, const int* __restrict__ active,
+                                    uint16_t* snap) {
+    const int slot = blockIdx.y;
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (size_t)nExt * nExt) return;
+    const int a = (int)(idx / nExt), c = (int)(idx % nExt);
+    snap[(size_t)slot * nExt * nExt + idx] = mat_ptr(M, active[slot])[(size_t)ext[a] * M.NP + ext[c]];
+}
+
+__global__ void ext_compare_kernel(MatSet M, const int* __restrict__ ext, int nExt, const int* __restrict__ active,
+                                   const uint16_t* __restrict__ snap, uint8_t* dec) {
+    const int slot = blockIdx.y;
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = active[slot];
+    bool d = false;
+    if (idx < (size_t)nExt * nExt) {
+        const int a = (int)(idx / nExt), c = (int)(idx % nExt);
+        d = mat_ptr(M, m)[(size_t)ext[a] * M.NP + ext[c]] < snap[(size_t)slot * nExt * nExt + idx];
+    }
+    if (__any_sync(FULL, d) && (threadIdx.x & 31) == 0) dec[m] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// Query.
+// ---------------------------------------------------------------------------
+__global__ void query_level0_kernel(MatSet L, const int* __restrict__ ext, int nExt, const int* __restrict__ vp,
+                                    uint16_t* X0t, int ldx, uint16_t* Mq, int ldm) {
+    const int j = blockIdx.x;
+    const int leaf = vp[4 * j], u = vp[4 * j + 1], g1 = vp[4 * j + 3];
+    const uint16_t* row = mat_ptr(L, leaf) + (size_t)u * L.NP;
+    for (int p = threadIdx.x; p < nExt; p += blockDim.x) X0t[(size_t)p * ldx + j] = row[ext[p]];
+    for (int jj = j + 1 + threadIdx.x; jj < g1; jj += blockDim.x) {
+        const uint16_t d = row[vp[4 * jj + 1]];
+        Mq[(size_t)j * ldm + jj] = d;
+    }
+}
+
+__global__ void query_active_kernel(const int* __restrict__ groups, int nP, const uint16_t* __restrict__ Xt,
+                                    int ldx, int* kidx, int* kcount, int kstride) {
+    __shared__ int warp_tot[32];
+    __shared__ int base;
+    const int gi = blockIdx.x;
+    const int start = groups[4 * gi + 2], cnt = groups[4 * gi + 3];
+    int* out = kidx + (size_t)gi * kstride;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    for (int p0 = 0; p0 < nP; p0 += blockDim.x) {
+        const int p = p0 + threadIdx.x;
+        bool on = false;
+        if (p < nP) {
+            const uint16_t* x = Xt + (size_t)p * ldx + start;
+            for (int i = 0; i < cnt && !on; ++i) on = x[i] < INF;
+        }
+        const unsigned bal = __ballot_sync(FULL, on);
+        if (lane == 0) warp_tot[warp] = __popc(bal);
+        __syncthreads();
+        int off = base;
+        for (int w = 0; w < warp; ++w) off += warp_tot[w];
+        if (on) out[off + __popc(bal & ((1u << lane) - 1u))] = p;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int w = 0; w < nw; ++w) t += warp_tot[w];
+            base += t;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) kcount[gi] = base;
+}
+
+// Y[start+i][n0 .. n0+NT) = min_t Xt[kidx[t]][start+i] + D_U[q*nP + kidx[t]][...]
+// CTA: WM x WN warps (runtime), warp tile RW rows x 64*CP columns.
+constexpr int kProjKC = 32;
+
+template <int RW, int CP>
+__global__ void __launch_bounds__(256)
+query_project_kernel(MatSet N, int nP, const int* __restrict__ groups, const uint16_t* __restrict__ Xt, int ldx,
+                     uint16_t* Y, int ldy, const int* __restrict__ kidx, const int* __restrict__ kcount,
+                     int kstride, int WM, int WN) {
+    constexpr int KC = kProjKC;
+    extern __shared__ __align__(16) uint16_t sm[];
+    const int MT = WM * RW, NT = WN * 64 * CP;
+    uint16_t* As = sm;             // [KC][MT]
+    uint16_t* Bs = sm + KC * MT;   // [KC][NT]
+    const int gi = blockIdx.z;
+    const int node = groups[4 * gi], q = groups[4 * gi + 1], start = groups[4 * gi + 2], cnt = groups[4 * gi + 3];
+    const int m0 = blockIdx.y * MT;
+    if (m0 >= cnt) return;
+    const int n0 = blockIdx.x * NT;
+    const int NP = N.NP;
+    if (n0 >= NP) return;
+    const int nA = kcount[gi];
+    const int* kl = kidx + (size_t)gi * kstride;
+    const uint16_t* D = mat_ptr(N, node) + (size_t)q * nP * NP;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int wm = warp / WN, wn = warp % WN;
+    uint32_t acc[RW][CP];
+#pragma unroll
+    for (int r = 0; r < RW; ++r)
+#pragma unroll
+        for (int c = 0; c < CP; ++c) acc[r][c] = INF2;
+    const int ncol = min(NT, NP - n0);
+    for (int t0 = 0; t0 < nA; t0 += KC) {
+        const int kc = min(KC, nA - t0);
+        for (int idx = tid; idx < KC * MT; idx += blockDim.x) {
+            const int t = idx / MT, i = idx % MT;
+            uint16_t v = INF;
+            if (t < kc && m0 + i < cnt) v = Xt[(size_t)kl[t0 + t] * ldx + start + m0 + i];
+            As[t * MT + i] = v;
+        }
+        for (int idx = tid; idx < KC * (NT / 8); idx += blockDim.x) {
+            const int t = idx / (NT / 8), c8 = idx % (NT / 8);
+            uint4 v = make_uint4(INF2, INF2, INF2, INF2);
+            if (t < kc && c8 * 8 < ncol) v = reinterpret_cast<const uint4*>(D + (size_t)kl[t0 + t] * NP + n0)[c8];
+            reinterpret_cast<uint4*>(Bs + t * NT)[c8] = v;
+        }
+        __syncthreads();
+        for (int t = 0; t < kc; ++t) {
+            uint32_t bv[CP];
+#pragma unroll
+            for (int c = 0; c < CP; ++c)
+                bv[c] = reinterpret_cast<const uint32_t*>(Bs + t * NT + wn * 64 * CP + lane * 2 * CP)[c];
+            const uint16_t* arow = As + t * MT + wm * RW;
+#pragma unroll
+            for (int r = 0; r < RW; ++r) {
+                const uint32_t a = arow[r];
+                if (a <= INF_HEADROOM) {
+                    const uint32_t aa = splat(a);
+#pragma unroll
+                    for (int c = 0; c < CP; ++c) acc[r][c] = acc_fast(acc[r][c], bv[c], aa);
+                } else if (a < INF) {
+                    const uint32_t aa = splat(a), tt = splat(INF - a);
+#pragma unroll
+                    for (int c = 0; c < CP; ++c) acc[r][c] = acc_clamp(acc[r][c], bv[c], aa, tt);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    const int col = n0 + wn * 64 * CP + lane * 2 * CP;
+    if (col < NP) {
+#pragma unroll
+        for (int r = 0; r < RW; ++r) {
+            const int i = m0 + wm * RW + r;
+            if (i < cnt) {
+                uint32_t* dst = reinterpret_cast<uint32_t*>(Y + (size_t)(start + i) * ldy + col);
+#pragma unroll
+                for (int c = 0; c < CP; ++c) dst[c] = acc[r][c];
+            }
+        }
+    }
+}
+
+__global__ void query_lift_kernel(const uint16_t* __restrict__ Y, int ldy, const int* __restrict__ ext, int nExt,
+                                  int k, uint16_t* Xn, int ldx) {
+    const int e = blockIdx.y;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nExt || j >= k) return;
+    Xn[(size_t)e * ldx + j] = Y[(size_t)j * ldy + ext[e]];
+}
+
+// One warp per (row i, block of 32 columns j > i) of a node group.
+__global__ void query_meet_kernel(const int* __restrict__ ngroups, const int* __restrict__ qoff,
+                                  const uint16_t* __restrict__ Y, int ldy, const uint16_t* __restrict__ Xt, int ldx,
+                                  int nP, uint16_t* Mq, int ldm) {
+    const int ng = blockIdx.x;
+    const int start = ngroups[3 * ng], end = ngroups[3 * ng + 1];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = start + blockIdx.y * (blockDim.x >> 5) + warp;
+    if (i >= end) return;
+    const uint16_t* yrow = Y + (size_t)i * ldy;
+    for (int jb = i + 1; jb < end; jb += 32) {
+        const int j = jb + lane;
+        if (j < end) {
+            const uint16_t* y = yrow + qoff[j];
+            const uint16_t* x = Xt + j;
+            uint32_t best = INF;
+            for (int p = 0; p < nP; ++p) {
+                const uint32_t s = (uint32_t)y[p] + x[(size_t)p * ldx];
+                best = s < best ? s : best;
+            }
+            uint16_t* dst = Mq + (size_t)i * ldm + j;
+            if (best < *dst) *dst = (uint16_t)best;
+        }
+    }
+}
+
+__global__ void query_finalize_kernel(const uint16_t* __restrict__ Mq, int ldm, const int* __restrict__ inv, int k,
+                                      uint16_t* out) {
+    const int a = blockIdx.y;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= k) return;
+    const int ia = inv[a], ic = inv[c];
+    uint16_t v = INF;
+    if (ia >= 0 && ic >= 0) {
+        if (ia == ic) v = 0;
+        else v = ia < ic ? Mq[(size_t)ia * ldm + ic] : Mq[(size_t)ic * ldm + ia];
+    }
+    out[(size_t)a * k + c] = v;
+}
+
+__global__ void gather_block_kernel(const uint16_t* __restrict__ mat, int NP, const int* __restrict__ rows, int nr,
+                                    const int* __restrict__ cols, int nc, uint16_t* out) {
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (size_t)nr * nc) return;
+    const int a = (int)(idx / nc), c = (int)(idx % nc);
+    out[idx] = mat[(size_t)rows[a] * NP + cols[c]];
+}
+
+__global__ void fill_u16_kernel(uint16_t* p, size_t n, uint16_t v) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
+inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Launch wrappers
+// ---------------------------------------------------------------------------
+void launch_leaf_bfs(const uint8_t* pass, int S, int b, int leaves_x, int n_leaves, MatSet leaves,
+                     cudaStream_t st) {
+    dim3 grid(blocks_for(leaves.NP, kBfsWarps), n_leaves);
+    const size_t smem = (size_t)kBfsWarps * leaves.NP * sizeof(uint16_t);
+    leaf_bfs_kernel<<<grid, kBfsWarps * 32, smem, st>>>(pass, S, b, leaves_x, leaves);
+}
+
+void launch_node_init(MatSet node, MatSet child, const int* child_ext, int nP, int g, int nodes_x,
+                      int child_nodes_x, int n_nodes, cudaStream_t st) {
+    const size_t chunks = (size_t)node.NP * (node.NP / 8);
+    dim3 grid(blocks_for(chunks, 256), n_nodes);
+    node_init_kernel<<<grid, 256, 0, st>>>(node, child, child_ext, nP, g, nodes_x, child_nodes_x);
+}
+
+void launch_seams_build(MatSet node, const int* seams, int n_seams, const uint8_t* pass, int S, int side,
+                        int nodes_x, int n_nodes, uint8_t* kflag, cudaStream_t st) {
+    if (n_seams == 0) return;
+    dim3 grid(blocks_for(n_seams, 128), n_nodes);
+    seams_build_kernel<<<grid, 128, 0, st>>>(node, seams, n_seams, pass, S, side, nodes_x, kflag);
+}
+
+void launch_compact_pivots(uint8_t* kflag, int NP, const int* active, int n_active, int* klist, int* kcnt,
+                           cudaStream_t st) {
+    if (n_active == 0) return;
+    compact_pivots_kernel<<<n_active, 256, 0, st>>>(kflag, NP, active, klist, kcnt);
+}
+
+template <int RW, int CP>
+static void launch_syrk_t(MatSet M, const int* active, int n_active, const int* kcnt, int round,
+                          const uint16_t* panel, const uint8_t* flags, cudaStream_t st) {
+    constexpr int MT = 8 * RW, NT = 64 * CP;
+    const size_t smem = (size_t)kPivotChunk * (MT + NT) * sizeof(uint16_t);
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(closure_syrk_kernel<RW, CP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        configured = true;
+    }
+    dim3 grid(M.NP / NT, M.NP / MT, n_active);
+    closure_syrk_kernel<RW, CP><<<grid, 256, smem, st>>>(M, active, kcnt, round, panel, flags);
+}
+
+void launch_closure_round(MatSet M, const int* active, int n_active, const int* klist, const int* kcnt,
+                          int round, uint16_t* panel, uint8_t* flags, cudaStream_t st) {
+    if (n_active == 0) return;
+    dim3 pgrid(blocks_for(M.NP, kPanelSlab), n_active);
+    closure_panel_kernel<<<pgrid, 256, 0, st>>>(M, active, klist, kcnt, round, panel, flags);
+    if (M.NP >= 256) launch_syrk_t<16, 4>(M, active, n_active, kcnt, round, panel, flags, st);
+    else if (M.NP >= 128) launch_syrk_t<16, 2>(M, active, n_active, kcnt, round, panel, flags, st);
+    else launch_syrk_t<8, 1>(M, active, n_active, kcnt, round, panel, flags, st);
+}
+
+void launch_leaf_edges(MatSet leaves, const int* active, int n_active, const int* eoff, const int* edges,
+                       uint8_t* kflag, int* pivots, cudaStream_t st) {
+    if (n_active == 0) return;
+    leaf_edges_kernel<<<n_active, 32, 0, st>>>(leaves, active, eoff, edges, kflag, pivots);
+}
+
+void launch_node_child_insert(MatSet node, MatSet child, const int* child_ext, int nP, int g, int nodes_x,
+                              int child_nodes_x, const int* active, int n_active, const uint8_t* child_dec,
+                              uint8_t* kflag, cudaStream_t st) {
+    if (n_active == 0) return;
+    dim3 grid(blocks_for((size_t)nP * nP, 256), g * g, n_active);
+    node_child_insert_kernel<<<grid, 256, 0, st>>>(node, child, child_ext, nP, g, nodes_x, child_nodes_x, active,
+                                                   child_dec, kflag);
+}
+
+void launch_node_seams(MatSet node, const int* active, int n_active, const int* soff, const int* seams,
+                       uint8_t* kflag, cudaStream_t st) {
+    if (n_active == 0) return;
+    node_seams_kernel<<<n_active, 32, 0, st>>>(node, active, soff, seams, kflag);
+}
+
+void launch_ext_snapshot(MatSet M, const int* ext, int nExt, const int* active, int n_active, uint16_t* snap,
+                         cudaStream_t st) {
+    if (n_active == 0) return;
+    dim3 grid(blocks_for((size_t)nExt * nExt, 256), n_active);
+    ext_snapshot_kernel<<<grid, 256, 0, st>>>(M, ext, nExt, active, snap);
+}
+
+void launch_ext_compare(MatSet M, const int* ext, int nExt, const int* active, int n_active, const uint16_t* snap,
+                        uint8_t* dec, cudaStream_t st) {
+    if (n_active == 0) return;
+    dim3 grid(blocks_for((size_t)nExt * nExt, 256), n_active);
+    ext_compare_kernel<<<grid, 256, 0, st>>>(M, ext, nExt, active, snap, dec);
+}
+
+void launch_query_level0(MatSet leaves, const int* ext, int nExt, const int* vp, int k, uint16_t* X0t, int ldx,
+                         uint16_t* M, int ldm, cudaStream_t st) {
+    if (k == 0) return;
+    query_level0_kernel<<<k, 128, 0, st>>>(leaves, ext, nExt, vp, X0t, ldx, M, ldm);
+}
+
+template <int RW, int CP>
+static void launch_project_t(MatSet node, int nP, const int* groups, int n_groups, int max_group,
+                             const uint16_t* Xt, int ldx, uint16_t* Y, int ldy, const int* kidx, const int* kcount,
+                             int kstride, int WM, int WN, cudaStream_t st) {
+    const int MT = WM * RW, NT = WN * 64 * CP;
+    const size_t smem = (size_t)kProjKC * (MT + NT) * sizeof(uint16_t);
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(query_project_kernel<RW, CP>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        configured = true;
+    }
+    dim3 grid(blocks_for(node.NP, NT), blocks_for(max_group, MT), n_groups);
+    query_project_kernel<RW, CP><<<grid, WM * WN * 32, smem, st>>>(node, nP, groups, Xt, ldx, Y, ldy, kidx, kcount,
+                                                                    kstride, WM, WN);
+}
+
+void launch_query_project(MatSet node, int nP, const int* groups, int n_groups, int max_group, const uint16_t* Xt,
+                          int ldx, uint16_t* Y, int ldy, int* kidx, cudaStream_t st) {
+    if (n_groups == 0) return;
+    int* kcount = kidx + (size_t)n_groups * nP;  // caller reserves n_groups extra ints
+    query_active_kernel<<<n_groups, 256, 0, st>>>(groups, nP, Xt, ldx, kidx, kcount, nP);
+    // Column tile: 8 warps x 128 columns = 1024, narrowed for small matrices.
+    int WN = node.NP >= 1024 ? 8 : node.NP / 128;
+    if (WN < 1) WN = 1;
+    if (node.NP < 128) {
+        // 64-wide matrices: CP = 1 (64 columns per warp).
+        int WM = max_group >= 8 ? 8 : (max_group >= 4 ? 4 : 1);
+        launch_project_t<4, 1>(node, nP, groups, n_groups, max_group, Xt, ldx, Y, ldy, kidx, kcount, nP, WM, 1, st);
+        return;
+    }
+    if (max_group <= 4) {
+        launch_project_t<4, 2>(node, nP, groups, n_groups, max_group, Xt, ldx, Y, ldy, kidx, kcount, nP, 1, WN, st);
+    } else {
+        const int WM = 8 / WN >= 1 ? 8 / WN : 1;
+        launch_project_t<16, 2>(node, nP, groups, n_groups, max_group, Xt, ldx, Y, ldy, kidx, kcount, nP, WM, WN, st);
+    }
+}
+
+void launch_query_lift(const uint16_t* Y, int ldy, const int* ext, int nExt, int k, uint16_t* Xt_next, int ldx,
+                       cudaStream_t st) {
+    if (k == 0) return;
+    dim3 grid(blocks_for(k, 128), nExt);
+    query_lift_kernel<<<grid, 128, 0, st>>>(Y, ldy, ext, nExt, k, Xt_next, ldx);
+}
+
+void launch_query_meet(const int* ngroups, int n_ngroups, const int* qoff, const uint16_t* Y, int ldy,
+                       const uint16_t* Xt, int ldx, int nP, uint16_t* M, int ldm, int max_w, cudaStream_t st) {
+    if (n_ngroups == 0) return;
+    dim3 grid(n_ngroups, blocks_for(max_w, 8));
+    query_meet_kernel<<<grid, 256, 0, st>>>(ngroups, qoff, Y, ldy, Xt, ldx, nP, M, ldm);
+}
+
+void launch_query_finalize(const uint16_t* M, int ldm, const int* inv, int k, uint16_t* out, cudaStream_t st) {
+    if (k == 0) return;
+    dim3 grid(blocks_for(k, 128), k);
+    query_finalize_kernel<<<grid, 128, 0, st>>>(M, ldm, inv, k, out);
+}
+
+void launch_fill_u16(uint16_t* ptr, size_t n, uint16_t value, cudaStream_t st) {
+    if (n == 0) return;
+    fill_u16_kernel<<<(unsigned)std::min<size_t>(blocks_for(n, 256), 148 * 8), 256, 0, st>>>(ptr, n, value);
+}
+
+void launch_gather_block(const uint16_t* mat, int NP, const int* rows, int nr, const int* cols, int nc,
+                         uint16_t* out, cudaStream_t st) {
+    const size_t n = (size_t)nr * nc;
+    if (n == 0) return;
+    gather_block_kernel<<<blocks_for(n, 256), 256, 0, st>>>(mat, NP, rows, nr, cols, nc, out);
+}
+
+}  // namespace hb

@@ -1,0 +1,299 @@
+"""Python mirror of ``htrip::MinPlusOracle`` over the C ABI (include/htrip_b200.h).
+
+Same names, argument meaning and error behaviour as the reference class
+(include/htrip/minplus_oracle.hpp):
+
+* ``MinPlusOracle(HierarchyConfig)``                       minplus_oracle.hpp:59
+* ``build(grid) -> bool``       False on an invalid config / empty grid  :78
+* ``onCellOpened(p, grid)``                                              :109
+* ``onBatchCellsOpened(cells, grid)``                                    :171
+* ``queryAllPairs(vps, grid, out=None, scratch=None) -> (k, k) uint16``  :337-348
+* ``depth()``, ``totalMemoryBytes()``, ``last_batch_stats``, ``S``, ``H``
+
+The index lives in HBM on one CUDA device.  There is no CPU fallback: if the
+CUDA library cannot be loaded or no device is present, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import build as _build
+
+INF = 60000
+
+_U8P = C.POINTER(C.c_uint8)
+_U16P = C.POINTER(C.c_uint16)
+_I32P = C.POINTER(C.c_int32)
+_U64P = C.POINTER(C.c_uint64)
+
+
+class HtripError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"htrip status {status}: {msg}")
+        self.status = status
+
+
+class _Config(C.Structure):
+    _fields_ = [("tile_size_b", C.c_int32), ("group", C.c_int32)]
+
+
+class _Stats(C.Structure):
+    _fields_ = [("n_touched_leaves", C.c_int32), ("n_dirty_ancestors", C.c_int32), ("n_pivots", C.c_int32)]
+
+
+_lib = None
+
+EXPORTS = (
+    "htrip_last_error", "htrip_create", "htrip_destroy", "htrip_clone", "htrip_build", "htrip_open_cells",
+    "htrip_open_cell", "htrip_query_all_pairs", "htrip_query_all_pairs_dev", "htrip_sync", "htrip_stream",
+    "htrip_shape", "htrip_last_batch_stats", "htrip_memory_bytes", "htrip_read_leaf_D", "htrip_read_leaf_S",
+    "htrip_read_node_DU", "htrip_read_node_SU", "htrip_read_node_C2E", "htrip_level_dims",
+)
+
+
+def load_library(path: str | None = None):
+    """Load (and if needed build) libhtrip_b200.so and declare its C ABI."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or _build.LIB
+    if not os.path.exists(path):
+        _build.build()
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    I = C.c_int32
+    lib.htrip_last_error.restype = C.c_char_p
+    lib.htrip_create.argtypes = [_Config, C.c_int, C.POINTER(P)]
+    lib.htrip_destroy.argtypes = [P]
+    lib.htrip_clone.argtypes = [P, C.POINTER(P)]
+    lib.htrip_build.argtypes = [P, _U8P, I, I]
+    lib.htrip_open_cells.argtypes = [P, _I32P, I, _U8P, I, I]
+    lib.htrip_open_cell.argtypes = [P, I, I, _U8P, I, I]
+    lib.htrip_query_all_pairs.argtypes = [P, _I32P, I, _U8P, I, I, _U16P]
+    lib.htrip_query_all_pairs_dev.argtypes = [P, C.c_void_p, C.c_void_p, I, C.c_void_p]
+    lib.htrip_sync.argtypes = [P]
+    lib.htrip_stream.restype = C.c_void_p
+    lib.htrip_stream.argtypes = [P]
+    lib.htrip_shape.argtypes = [P, _I32P, _I32P, _I32P]
+    lib.htrip_last_batch_stats.argtypes = [P, C.POINTER(_Stats)]
+    lib.htrip_memory_bytes.argtypes = [P, _U64P, _U64P]
+    for f in ("htrip_read_leaf_D", "htrip_read_leaf_S"):
+        getattr(lib, f).argtypes = [P, I, _U16P]
+    for f in ("htrip_read_node_DU", "htrip_read_node_SU"):
+        getattr(lib, f).argtypes = [P, I, I, _U16P]
+    lib.htrip_read_node_C2E.argtypes = [P, I, I, I, _U16P]
+    lib.htrip_level_dims.argtypes = [P, I, _I32P, _I32P, _I32P, _I32P]
+    for f in EXPORTS:
+        if f not in ("htrip_last_error", "htrip_stream"):
+            getattr(lib, f).restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def _check(status: int):
+    if status != 0:
+        raise HtripError(status, _lib.htrip_last_error().decode())
+
+
+@dataclass
+class HierarchyConfig:
+    """Reference HierarchyConfig (include/htrip/types.hpp:199-225)."""
+    tile_size_b: int = 16
+    group_w: int = 2
+    group_h: int = 2
+    hybrid_k_threshold: int = 0
+
+    def isValid(self) -> bool:
+        return (self.tile_size_b > 0 and self.group_w >= 2 and self.group_h >= 2
+                and self.group_w == self.group_h and self.group_w * self.group_h <= 256)
+
+
+class GridMap:
+    """Occupancy grid: ``observed`` is a (rows, cols) uint8 CellState array."""
+
+    def __init__(self, observed: np.ndarray):
+        self.observed = np.ascontiguousarray(observed, dtype=np.uint8)
+
+    @property
+    def rows(self):
+        return self.observed.shape[0]
+
+    @property
+    def cols(self):
+        return self.observed.shape[1]
+
+    def isPassable(self, r: int, c: int) -> bool:
+        return 0 <= r < self.rows and 0 <= c < self.cols and self.observed[r, c] == 1
+
+    def setObserved(self, r: int, c: int, state: int):
+        if 0 <= r < self.rows and 0 <= c < self.cols:
+            self.observed[r, c] = state
+
+
+@dataclass
+class LastBatchStats:
+    n_touched_leaves: int = 0
+    n_dirty_ancestors: int = 0
+    n_pivots: int = 0
+
+
+def _grid_args(grid):
+    obs = grid.observed if isinstance(grid, GridMap) else np.ascontiguousarray(grid, dtype=np.uint8)
+    return obs, obs.ctypes.data_as(_U8P), obs.shape[0], obs.shape[1]
+
+
+def _rc(pts) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(pts, dtype=np.int32).reshape(-1, 2))
+
+
+class MinPlusOracle:
+    """B200-resident HTRIP index with the reference's MinPlusOracle interface."""
+
+    def __init__(self, config: HierarchyConfig | None = None, device: int = 0, _handle=None):
+        self.lib = load_library()
+        self.config = config or HierarchyConfig()
+        self.device = device
+        if _handle is not None:
+            self.h = _handle
+        else:
+            h = C.c_void_p()
+            cfg = _Config(self.config.tile_size_b, self.config.group_w)
+            _check(self.lib.htrip_create(cfg, device, C.byref(h)))
+            self.h = h
+        self.last_batch_stats = LastBatchStats()
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.lib.htrip_destroy(h)
+            self.h = None
+
+    def clone(self) -> "MinPlusOracle":
+        h = C.c_void_p()
+        _check(self.lib.htrip_clone(self.h, C.byref(h)))
+        o = MinPlusOracle(self.config, self.device, _handle=h)
+        o.last_batch_stats = LastBatchStats(**vars(self.last_batch_stats))
+        return o
+
+    # -- build ------------------------------------------------------------
+    def build(self, grid) -> bool:
+        if not self.config.isValid():
+            return False
+        obs, ptr, rows, cols = _grid_args(grid)
+        st = self.lib.htrip_build(self.h, ptr, rows, cols)
+        if st == 1:  # HTRIP_ERR_INVALID: the reference returns false
+            return False
+        _check(st)
+        return True
+
+    def depth(self) -> int:
+        return self.H
+
+    @property
+    def S(self) -> int:
+        return self._shape()[0]
+
+    @property
+    def H(self) -> int:
+        return self._shape()[1]
+
+    @property
+    def num_leaf_tiles_x(self) -> int:
+        return self._shape()[2]
+
+    num_leaf_tiles_y = num_leaf_tiles_x
+
+    def _shape(self):
+        s, h, lx = C.c_int32(), C.c_int32(), C.c_int32()
+        _check(self.lib.htrip_shape(self.h, C.byref(s), C.byref(h), C.byref(lx)))
+        return s.value, h.value, lx.value
+
+    # -- updates ----------------------------------------------------------
+    def onBatchCellsOpened(self, cells, grid):
+        rc = _rc(cells)
+        obs, ptr, rows, cols = _grid_args(grid)
+        _check(self.lib.htrip_open_cells(self.h, rc.ctypes.data_as(_I32P), len(rc), ptr, rows, cols))
+        st = _Stats()
+        _check(self.lib.htrip_last_batch_stats(self.h, C.byref(st)))
+        self.last_batch_stats = LastBatchStats(st.n_touched_leaves, st.n_dirty_ancestors, st.n_pivots)
+
+    def onCellOpened(self, p, grid):
+        obs, ptr, rows, cols = _grid_args(grid)
+        _check(self.lib.htrip_open_cell(self.h, int(p[0]), int(p[1]), ptr, rows, cols))
+
+    # -- queries ----------------------------------------------------------
+    def queryAllPairs(self, viewpoints, grid, out: np.ndarray | None = None, scratch=None) -> np.ndarray:
+        rc = _rc(viewpoints)
+        k = len(rc)
+        if out is None or out.shape != (k, k) or out.dtype != np.uint16 or not out.flags.c_contiguous:
+            out = np.empty((k, k), dtype=np.uint16)
+        if k == 0:
+            return out
+        obs, ptr, rows, cols = _grid_args(grid)
+        _check(self.lib.htrip_query_all_pairs(self.h, rc.ctypes.data_as(_I32P), k, ptr, rows, cols,
+                                              out.ctypes.data_as(_U16P)))
+        return out
+
+    def queryAllPairsDevice(self, vps_dev_ptr: int, passable_dev_ptr: int, k: int, out_dev_ptr: int):
+        """Stream-ordered query on device-resident inputs (see htrip_query_all_pairs_dev)."""
+        _check(self.lib.htrip_query_all_pairs_dev(self.h, C.c_void_p(vps_dev_ptr), C.c_void_p(passable_dev_ptr),
+                                                  k, C.c_void_p(out_dev_ptr)))
+
+    def stream(self) -> int:
+        return int(self.lib.htrip_stream(self.h) or 0)
+
+    def synchronize(self):
+        _check(self.lib.htrip_sync(self.h))
+
+    # -- accounting / state read-back ---------------------------------------
+    def totalMemoryBytes(self) -> int:
+        ref, dev = C.c_uint64(), C.c_uint64()
+        _check(self.lib.htrip_memory_bytes(self.h, C.byref(ref), C.byref(dev)))
+        return ref.value
+
+    def deviceMemoryBytes(self) -> int:
+        ref, dev = C.c_uint64(), C.c_uint64()
+        _check(self.lib.htrip_memory_bytes(self.h, C.byref(ref), C.byref(dev)))
+        return dev.value
+
+    def level_dims(self, lvl: int):
+        a = [C.c_int32() for _ in range(4)]
+        _check(self.lib.htrip_level_dims(self.h, lvl, *[C.byref(x) for x in a]))
+        return tuple(x.value for x in a)
+
+    def leaf_D(self, i: int) -> np.ndarray:
+        n = self.config.tile_size_b ** 2
+        out = np.empty((n, n), dtype=np.uint16)
+        _check(self.lib.htrip_read_leaf_D(self.h, i, out.ctypes.data_as(_U16P)))
+        return out
+
+    def leaf_S(self, i: int) -> np.ndarray:
+        p = 4 * self.config.tile_size_b - 4
+        out = np.empty((p, p), dtype=np.uint16)
+        _check(self.lib.htrip_read_leaf_S(self.h, i, out.ctypes.data_as(_U16P)))
+        return out
+
+    def node_DU(self, lvl: int, node: int) -> np.ndarray:
+        n = self.level_dims(lvl)[0]
+        out = np.empty((n, n), dtype=np.uint16)
+        _check(self.lib.htrip_read_node_DU(self.h, lvl, node, out.ctypes.data_as(_U16P)))
+        return out
+
+    def node_SU(self, lvl: int, node: int) -> np.ndarray:
+        ne = self.level_dims(lvl)[1]
+        out = np.empty((ne, ne), dtype=np.uint16)
+        _check(self.lib.htrip_read_node_SU(self.h, lvl, node, out.ctypes.data_as(_U16P)))
+        return out
+
+    def node_C2E(self, lvl: int, node: int, quad: int) -> np.ndarray:
+        n, ne, np_, _ = self.level_dims(lvl)
+        out = np.empty(np_ * ne, dtype=np.uint16)
+        _check(self.lib.htrip_read_node_C2E(self.h, lvl, node, quad, out.ctypes.data_as(_U16P)))
+        return out
+
+
+HTripOracle = MinPlusOracle

@@ -1,0 +1,147 @@
+/*
+ * htrip_b200 C ABI: B200-resident HTRIP min-plus hierarchy.
+ *
+ * The reference (ozaslan/htrip) has no C ABI: its boundary is the C++ class
+ * htrip::MinPlusOracle (include/htrip/minplus_oracle.hpp).  Each entry point
+ * below replaces one member of that class; the C++ drop-in in
+ * include/htrip/minplus_oracle.hpp of this repository calls exactly these.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only.  Unless a name ends in _dev, every array
+ *    argument is HOST memory; the call copies it to / from the device itself.
+ *  - Cells and viewpoints are int32 pairs (r, c), row-major "rc" arrays.
+ *  - Grids are uint8 CellState arrays, rows*cols, row-major:
+ *      0 Unknown, 1 Free, 2 Obstacle   (reference include/htrip/types.hpp:100)
+ *    Only Free is passable (reference grid_map.hpp:142).
+ *  - Distances are uint16 with HTRIP_INF = 60000 for "unreachable".
+ *  - Every call returns an htrip_status (0 = ok).  A failed call leaves the
+ *    index as it was before the call, except HTRIP_ERR_CUDA, after which the
+ *    handle must be destroyed.
+ *  - A handle is not thread-safe; distinct handles may be used concurrently
+ *    (each owns a CUDA stream).  Calls are synchronous on return.
+ */
+#ifndef HTRIP_B200_H
+#define HTRIP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HTRIP_INF 60000
+
+typedef enum {
+    HTRIP_OK = 0,
+    HTRIP_ERR_INVALID = 1,     /* bad argument / invalid HierarchyConfig        */
+    HTRIP_ERR_NOT_BUILT = 2,   /* update or query before a successful build    */
+    HTRIP_ERR_OOM = 3,         /* device allocation failed (index unchanged)   */
+    HTRIP_ERR_UNSUPPORTED = 4, /* e.g. tile side outside [2, 32]               */
+    HTRIP_ERR_CUDA = 5,        /* CUDA runtime error; destroy the handle       */
+    HTRIP_ERR_NO_DEVICE = 6    /* no CUDA device / extension unusable          */
+} htrip_status;
+
+typedef struct htrip_index htrip_index; /* opaque */
+
+typedef struct {
+    int32_t tile_size_b; /* leaf side b                  (types.hpp:200) */
+    int32_t group;       /* g = group_w = group_h        (types.hpp:201-202) */
+} htrip_config;
+
+typedef struct {
+    int32_t n_touched_leaves;  /* MinPlusOracle::LastBatchStats (minplus_oracle.hpp:251-256) */
+    int32_t n_dirty_ancestors;
+    int32_t n_pivots;
+} htrip_batch_stats;
+
+/* Last error message of the calling thread (static storage). */
+const char* htrip_last_error(void);
+
+/* explicit MinPlusOracle(HierarchyConfig)      minplus_oracle.hpp:59
+ * `device` selects the CUDA device.  Config validity is checked at build,
+ * as in the reference (HierarchyConfig::isValid, types.hpp:221). */
+htrip_status htrip_create(htrip_config cfg, int device, htrip_index** out);
+
+/* ~MinPlusOracle                                                         */
+htrip_status htrip_destroy(htrip_index* h);
+
+/* MinPlusOracle copy constructor (bench_update_latency.cpp:178,186):
+ * deep device-side clone of the whole index.                             */
+htrip_status htrip_clone(const htrip_index* h, htrip_index** out);
+
+/* bool build(const GridMap&)                   minplus_oracle.hpp:78
+ * observed: rows*cols CellState bytes.  Returns HTRIP_ERR_INVALID where the
+ * reference returns false (invalid config, rows or cols <= 0).           */
+htrip_status htrip_build(htrip_index* h, const uint8_t* observed, int32_t rows, int32_t cols);
+
+/* void onBatchCellsOpened(cells, grid)         minplus_oracle.hpp:171
+ * The caller has already written the cells as Free into `observed`
+ * (the grid it passes is read for the cells' neighbours only).           */
+htrip_status htrip_open_cells(htrip_index* h, const int32_t* rc, int32_t n,
+                              const uint8_t* observed, int32_t rows, int32_t cols);
+
+/* void onCellOpened(Point, grid)               minplus_oracle.hpp:109
+ * Same index state as htrip_open_cells with one cell; like the reference it
+ * leaves last_batch_stats untouched.                                      */
+htrip_status htrip_open_cell(htrip_index* h, int32_t r, int32_t c,
+                             const uint8_t* observed, int32_t rows, int32_t cols);
+
+/* void queryAllPairs(vps, grid, out, HTripQueryScratch&) const
+ *                                              minplus_oracle.hpp:337-341
+ * out: k*k uint16 row-major.  Diagonal 0 for Free viewpoints, INF rows and
+ * columns for viewpoints that are not Free in `observed`.                 */
+htrip_status htrip_query_all_pairs(htrip_index* h, const int32_t* vps, int32_t k,
+                                   const uint8_t* observed, int32_t rows, int32_t cols,
+                                   uint16_t* out);
+
+/* Same query with the per-viewpoint passability already decided by the
+ * caller (passable[i] != 0 iff viewpoint i is Free).  vps/passable/out are
+ * DEVICE pointers; the call is stream-ordered on the index's stream and
+ * returns without synchronising (htrip_sync waits).                       */
+htrip_status htrip_query_all_pairs_dev(htrip_index* h, const int32_t* vps_dev,
+                                       const uint8_t* passable_dev, int32_t k,
+                                       uint16_t* out_dev);
+
+/* Wait for all work queued on the index's stream.                         */
+htrip_status htrip_sync(htrip_index* h);
+
+/* The index's CUDA stream (a cudaStream_t) for callers that order their own
+ * work after stream-ordered calls.                                        */
+void* htrip_stream(htrip_index* h);
+
+/* public members S, H, num_leaf_tiles_x (minplus_oracle.hpp:42-45)        */
+htrip_status htrip_shape(const htrip_index* h, int32_t* S, int32_t* H, int32_t* leaves_x);
+
+/* last_batch_stats                             minplus_oracle.hpp:256     */
+htrip_status htrip_last_batch_stats(const htrip_index* h, htrip_batch_stats* out);
+
+/* size_t totalMemoryBytes() const              minplus_oracle.hpp:385
+ * reference_bytes: the reference's accounting of the same index (D, S,
+ * D_U, S_U and child_to_ext sizes, minplus_oracle.cpp:2116-2134);
+ * device_bytes: HBM actually held by this index.                         */
+htrip_status htrip_memory_bytes(const htrip_index* h, uint64_t* reference_bytes,
+                                uint64_t* device_bytes);
+
+/* State read-back for bitwise comparison with the reference's public
+ * members (host output arrays):
+ *   leaves[i].D   (b^2 x b^2)          leaf_tile.hpp:70
+ *   leaves[i].S   ((4b-4)^2)           leaf_tile.hpp:71
+ *   levels[l-1][n].D_U (nV x nV)       internal_node.hpp:53
+ *   levels[l-1][n].S_U (nExt x nExt)   internal_node.hpp:54
+ *   levels[l-1][n].child_to_ext[q] (nP x nExt)  internal_node.hpp:55
+ * `n` is the row-major node index at level l (tileIndexAtLevel).          */
+htrip_status htrip_read_leaf_D(const htrip_index* h, int32_t leaf, uint16_t* out);
+htrip_status htrip_read_leaf_S(const htrip_index* h, int32_t leaf, uint16_t* out);
+htrip_status htrip_read_node_DU(const htrip_index* h, int32_t lvl, int32_t node, uint16_t* out);
+htrip_status htrip_read_node_SU(const htrip_index* h, int32_t lvl, int32_t node, uint16_t* out);
+htrip_status htrip_read_node_C2E(const htrip_index* h, int32_t lvl, int32_t node, int32_t quad,
+                                 uint16_t* out);
+/* nV, nExt and per-child port count nP of level `lvl` (0 = leaves: n=b^2). */
+htrip_status htrip_level_dims(const htrip_index* h, int32_t lvl, int32_t* n, int32_t* n_ext,
+                              int32_t* n_child_ports, int32_t* n_nodes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HTRIP_B200_H */

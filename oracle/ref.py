@@ -1,0 +1,191 @@
+"""ctypes bindings to the CPU checkers (TEST INFRASTRUCTURE ONLY).
+
+* ``RefOracle``  - the unmodified reference ``htrip::MinPlusOracle`` and
+  ``htrip::BfsOracle`` (oracle/_ref/libhtrip_ref.so, built by oracle/Makefile
+  from the reference sources).
+* ``PortOracle`` - the plain-C restatement of the same algorithm
+  (oracle/_build/liboracle_port.so, built from oracle/htrip_oracle.c).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
+arm import this module.  The product (htrip_b200) never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SO = os.path.join(HERE, "_ref", "libhtrip_ref.so")
+PORT_SO = os.path.join(HERE, "_build", "liboracle_port.so")
+
+_P = C.c_void_p
+_I = C.c_int
+_U8P = C.POINTER(C.c_uint8)
+_U16P = C.POINTER(C.c_uint16)
+_I32P = C.POINTER(C.c_int32)
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def _rc(pts) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(pts, dtype=np.int32).reshape(-1, 2))
+
+
+_ref_lib = None
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def _load_ref():
+    global _ref_lib
+    if _ref_lib is None:
+        lib = C.CDLL(REF_SO)
+        lib.ref_create.restype = _P
+        lib.ref_create.argtypes = [_I, _I]
+        lib.ref_destroy.argtypes = [_P]
+        lib.ref_clone.restype = _P
+        lib.ref_clone.argtypes = [_P]
+        lib.ref_set_grid.argtypes = [_P, _U8P, _I, _I]
+        lib.ref_set_cells.argtypes = [_P, _I32P, _I, _I]
+        lib.ref_build.restype = _I
+        lib.ref_build.argtypes = [_P]
+        lib.ref_open_batch.argtypes = [_P, _I32P, _I]
+        lib.ref_open_cell.argtypes = [_P, _I, _I]
+        lib.ref_query.argtypes = [_P, _I32P, _I, _U16P]
+        lib.ref_time_query.restype = C.c_double
+        lib.ref_time_query.argtypes = [_P, _I32P, _I, _I, _I, _U16P]
+        lib.ref_bfs_all_pairs.argtypes = [_P, _I32P, _I, _U16P]
+        for f in ("ref_S", "ref_H", "ref_num_leaves"):
+            getattr(lib, f).restype = _I
+            getattr(lib, f).argtypes = [_P]
+        lib.ref_num_nodes.restype = _I
+        lib.ref_num_nodes.argtypes = [_P, _I]
+        lib.ref_total_memory.restype = C.c_ulonglong
+        lib.ref_total_memory.argtypes = [_P]
+        lib.ref_stats.argtypes = [_P, _I32P]
+        lib.ref_leaf_D.restype = _I
+        lib.ref_leaf_D.argtypes = [_P, _I, _U16P]
+        lib.ref_leaf_S.restype = _I
+        lib.ref_leaf_S.argtypes = [_P, _I, _U16P]
+        lib.ref_node_DU.restype = _I
+        lib.ref_node_DU.argtypes = [_P, _I, _I, _U16P]
+        lib.ref_node_SU.restype = _I
+        lib.ref_node_SU.argtypes = [_P, _I, _I, _U16P]
+        lib.ref_node_C2E.restype = _I
+        lib.ref_node_C2E.argtypes = [_P, _I, _I, _I, _U16P]
+        lib.ref_node_geometry.restype = _I
+        lib.ref_node_geometry.argtypes = [_P, _I, _I, _I32P, _I32P, _I32P]
+        _ref_lib = lib
+    return _ref_lib
+
+
+class RefOracle:
+    """The reference MinPlusOracle with its own GridMap copy."""
+
+    def __init__(self, b: int, g: int = 2, _handle=None):
+        self.lib = _load_ref()
+        self.b, self.g = b, g
+        self.h = _handle if _handle is not None else self.lib.ref_create(b, g)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.ref_destroy(self.h)
+            self.h = None
+
+    def clone(self) -> "RefOracle":
+        return RefOracle(self.b, self.g, _handle=self.lib.ref_clone(self.h))
+
+    def set_grid(self, observed: np.ndarray):
+        obs = np.ascontiguousarray(observed, dtype=np.uint8)
+        self.rows, self.cols = obs.shape
+        self.lib.ref_set_grid(self.h, _p(obs, _U8P), self.rows, self.cols)
+
+    def set_cells(self, cells, state: int):
+        rc = _rc(cells)
+        self.lib.ref_set_cells(self.h, _p(rc, _I32P), len(rc), state)
+
+    def build(self) -> bool:
+        return bool(self.lib.ref_build(self.h))
+
+    def open_batch(self, cells):
+        rc = _rc(cells)
+        self.lib.ref_open_batch(self.h, _p(rc, _I32P), len(rc))
+
+    def open_cell(self, r: int, c: int):
+        self.lib.ref_open_cell(self.h, r, c)
+
+    def query(self, vps) -> np.ndarray:
+        rc = _rc(vps)
+        out = np.empty((len(rc), len(rc)), dtype=np.uint16)
+        self.lib.ref_query(self.h, _p(rc, _I32P), len(rc), _p(out, _U16P))
+        return out
+
+    def time_query(self, vps, nthreads: int, reps: int):
+        rc = _rc(vps)
+        out = np.empty((len(rc), len(rc)), dtype=np.uint16)
+        sec = self.lib.ref_time_query(self.h, _p(rc, _I32P), len(rc), nthreads, reps, _p(out, _U16P))
+        return sec, out
+
+    def bfs(self, vps) -> np.ndarray:
+        rc = _rc(vps)
+        out = np.empty((len(rc), len(rc)), dtype=np.uint16)
+        self.lib.ref_bfs_all_pairs(self.h, _p(rc, _I32P), len(rc), _p(out, _U16P))
+        return out
+
+    @property
+    def S(self):
+        return self.lib.ref_S(self.h)
+
+    @property
+    def H(self):
+        return self.lib.ref_H(self.h)
+
+    def num_leaves(self):
+        return self.lib.ref_num_leaves(self.h)
+
+    def num_nodes(self, lvl):
+        return self.lib.ref_num_nodes(self.h, lvl)
+
+    def total_memory(self):
+        return int(self.lib.ref_total_memory(self.h))
+
+    def stats(self):
+        out = np.zeros(3, dtype=np.int32)
+        self.lib.ref_stats(self.h, _p(out, _I32P))
+        return tuple(int(x) for x in out)
+
+    def leaf_D(self, i):
+        n = self.b * self.b
+        out = np.empty((n, n), dtype=np.uint16)
+        self.lib.ref_leaf_D(self.h, i, _p(out, _U16P))
+        return out
+
+    def leaf_S(self, i):
+        p = 4 * self.b - 4
+        out = np.empty((p, p), dtype=np.uint16)
+        self.lib.ref_leaf_S(self.h, i, _p(out, _U16P))
+        return out
+
+    def node_DU(self, lvl, n):
+        nv = self.lib.ref_node_DU(self.h, lvl, n, None)
+        out = np.empty((nv, nv), dtype=np.uint16)
+        self.lib.ref_node_DU(self.h, lvl, n, _p(out, _U16P))
+        return out
+
+    def node_SU(self, lvl, n):
+        ne = self.lib.ref_node_SU(self.h, lvl, n, None)
+        out = np.empty((ne, ne), dtype=np.uint16)
+        self.lib.ref_node_SU(self.h, lvl, n, _p(out, _U16P))
+        return out
+
+    def node_C2E(self, lvl, n, q):
+        cnt = self.lib.ref_node_C2E(self.h, lvl, n, q, None)
+        out = np.empty(cnt, dtype=np.uint16)
+        self.lib.ref_node_C2E(self.h, lvl, n, q, _p(out, _U16P))
+        return out
