@@ -189,3 +189,104 @@ class RefOracle:
         out = np.empty(cnt, dtype=np.uint16)
         self.lib.ref_node_C2E(self.h, lvl, n, q, _p(out, _U16P))
         return out
+
+
+_port_lib = None
+
+
+def port_available() -> bool:
+    return os.path.exists(PORT_SO)
+
+
+def _load_port():
+    global _port_lib
+    if _port_lib is None:
+        lib = C.CDLL(PORT_SO)
+        lib.orc_create.restype = _P
+        lib.orc_create.argtypes = [_I, _I]
+        lib.orc_destroy.argtypes = [_P]
+        lib.orc_build.restype = _I
+        lib.orc_build.argtypes = [_P, _U8P, _I, _I]
+        lib.orc_open_batch.argtypes = [_P, _I32P, _I, _U8P, _I, _I]
+        lib.orc_query.argtypes = [_P, _I32P, _I, _U8P, _I, _I, _U16P]
+        lib.orc_stats.argtypes = [_P, _I32P]
+        lib.orc_S.restype = _I
+        lib.orc_S.argtypes = [_P]
+        lib.orc_H.restype = _I
+        lib.orc_H.argtypes = [_P]
+        lib.orc_leaf_D.restype = _I
+        lib.orc_leaf_D.argtypes = [_P, _I, _U16P]
+        lib.orc_node_DU.restype = _I
+        lib.orc_node_DU.argtypes = [_P, _I, _I, _U16P]
+        lib.orc_bfs_all_pairs.argtypes = [_U8P, _I, _I, _I32P, _I, _U16P]
+        _port_lib = lib
+    return _port_lib
+
+
+class PortOracle:
+    """The plain-C restatement (oracle/htrip_oracle.c); the grid is passed per call."""
+
+    def __init__(self, b: int, g: int = 2):
+        self.lib = _load_port()
+        self.b, self.g = b, g
+        self.h = self.lib.orc_create(b, g)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.orc_destroy(self.h)
+            self.h = None
+
+    @staticmethod
+    def _g(grid):
+        obs = np.ascontiguousarray(grid, dtype=np.uint8)
+        return obs, _p(obs, _U8P), obs.shape[0], obs.shape[1]
+
+    def build(self, grid) -> bool:
+        obs, ptr, r, c = self._g(grid)
+        return bool(self.lib.orc_build(self.h, ptr, r, c))
+
+    def open_batch(self, cells, grid):
+        rc = _rc(cells)
+        obs, ptr, r, c = self._g(grid)
+        self.lib.orc_open_batch(self.h, _p(rc, _I32P), len(rc), ptr, r, c)
+
+    def query(self, vps, grid) -> np.ndarray:
+        rc = _rc(vps)
+        obs, ptr, r, c = self._g(grid)
+        out = np.empty((len(rc), len(rc)), dtype=np.uint16)
+        self.lib.orc_query(self.h, _p(rc, _I32P), len(rc), ptr, r, c, _p(out, _U16P))
+        return out
+
+    def stats(self):
+        out = np.zeros(3, dtype=np.int32)
+        self.lib.orc_stats(self.h, _p(out, _I32P))
+        return tuple(int(x) for x in out)
+
+    @property
+    def S(self):
+        return self.lib.orc_S(self.h)
+
+    @property
+    def H(self):
+        return self.lib.orc_H(self.h)
+
+    def leaf_D(self, i):
+        n = self.lib.orc_leaf_D(self.h, i, None)
+        out = np.empty((n, n), dtype=np.uint16)
+        self.lib.orc_leaf_D(self.h, i, _p(out, _U16P))
+        return out
+
+    def node_DU(self, lvl, node):
+        n = self.lib.orc_node_DU(self.h, lvl, node, None)
+        out = np.empty((n, n), dtype=np.uint16)
+        self.lib.orc_node_DU(self.h, lvl, node, _p(out, _U16P))
+        return out
+
+
+def port_bfs(grid, vps) -> np.ndarray:
+    lib = _load_port()
+    obs = np.ascontiguousarray(grid, dtype=np.uint8)
+    rc = _rc(vps)
+    out = np.empty((len(rc), len(rc)), dtype=np.uint16)
+    lib.orc_bfs_all_pairs(_p(obs, _U8P), obs.shape[0], obs.shape[1], _p(rc, _I32P), len(rc), _p(out, _U16P))
+    return out
