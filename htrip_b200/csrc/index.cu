@@ -97,7 +97,7 @@ struct Level {
     std::vector<int> ext;    // exterior port -> matrix index
     std::vector<int> seams;  // 6 ints per seam candidate
     int nseams = 0;
-    DevBuf<int> d_ext, d_seams;
+    DevBuf<int> d_ext, d_seams, d_ext_inv;
     DevBuf<uint16_t> mat;
     DevBuf<uint8_t> kflag;
     DevBuf<int> klist, kcnt;
@@ -124,7 +124,14 @@ struct htrip_index {
     DevBuf<int> pivots;
     // query scratch
     DevBuf<int> qplan;
-    DevBuf<uint16_t> qX[2], qY, qM, qout;
+    DevBuf<uint16_t> qX[3], qY[2], qout;
+    DevBuf<uint8_t> qflags;
+    DevBuf<int> qstatus;
+    DevBuf<unsigned> qbar;
+    int qgrid = 0;
+    DevBuf<uint8_t> qparams;
+    alignas(16) unsigned char h_qparams[sizeof(hb::QueryParams)];
+    DevBuf<uint32_t> qM;
     DevBuf<int> qkidx;
     DevBuf<int32_t> qvps;
     htrip_batch_stats stats{0, 0, 0};
@@ -133,13 +140,13 @@ struct htrip_index {
     ~htrip_index() { release(); }
     void release() {
         for (auto& l : L) {
-            l.d_ext.release(); l.d_seams.release(); l.mat.release(); l.kflag.release();
+            l.d_ext.release(); l.d_seams.release(); l.d_ext_inv.release(); l.mat.release(); l.kflag.release();
             l.klist.release(); l.kcnt.release(); l.dec.release();
         }
         L.clear();
         pass.release(); panel.release(); pflags.release(); active.release(); upd.release();
-        snap.release(); pivots.release(); qplan.release(); qX[0].release(); qX[1].release();
-        qY.release(); qM.release(); qout.release(); qkidx.release(); qvps.release();
+        snap.release(); pivots.release(); qplan.release(); for (auto& x : qX) x.release(); for (auto& y : qY) y.release();
+        qM.release(); qout.release(); qkidx.release(); qvps.release(); qflags.release(); qstatus.release(); qbar.release(); qparams.release();
     }
 };
 
@@ -225,6 +232,13 @@ void alloc_levels(htrip_index* h) {
             ck(cudaMemcpyAsync(Lv.d_seams.p, Lv.seams.data(), Lv.seams.size() * sizeof(int), cudaMemcpyHostToDevice,
                                h->stream), "seams");
         }
+        if (Lv.lvl >= 1) {
+            std::vector<int> inv(Lv.NP, -1);
+            for (int e = 0; e < Lv.nExt; ++e) inv[Lv.ext[e]] = e;
+            Lv.d_ext_inv.reserve(Lv.NP);
+            ck(cudaMemcpyAsync(Lv.d_ext_inv.p, inv.data(), Lv.NP * sizeof(int), cudaMemcpyHostToDevice, h->stream),
+               "ext_inv");
+        }
         Lv.kflag.reserve((size_t)Lv.nnodes * Lv.NP);
         ck(cudaMemsetAsync(Lv.kflag.p, 0, (size_t)Lv.nnodes * Lv.NP, h->stream), "kflag");
         Lv.klist.reserve((size_t)Lv.nnodes * Lv.NP);
@@ -232,6 +246,10 @@ void alloc_levels(htrip_index* h) {
         Lv.dec.reserve(Lv.nnodes);
     }
     h->pivots.reserve(1);
+    h->qstatus.reserve(1);
+    h->qbar.reserve(2);
+    ck(cudaMemsetAsync(h->qstatus.p, 0, sizeof(int), h->stream), "status");
+    ck(cudaMemsetAsync(h->qbar.p, 0, 2 * sizeof(unsigned), h->stream), "barrier");
 }
 
 // Closure of the listed matrices of level `Lv` over their pivot flags.
@@ -487,10 +505,25 @@ void do_open(htrip_index* h, const int32_t* rc, int n, const uint8_t* obs, int r
 // ---------------------------------------------------------------------------
 struct QueryPlan {
     std::vector<int> buf;
-    int n_sorted = 0;
-    int o_vp0 = 0, o_inv = 0;
-    std::vector<int> o_cg, n_cg, o_ng, n_ng, o_qoff, max_cg, max_ng;
+    int n_sorted = 0, k = 0;
+    int ldv = 8;   // slot stride of X / Yt
+    int ldm = 8;   // stride of the sorted-order M
+    int cfg = 0;
+    int o_vp0 = 0, o_inv = 0, o_l0 = 0, n_l0 = 0;
+    struct Lvl {
+        int o_groups = 0, n_groups = 0, max_group = 0, slots = 0;
+        int o_items = 0, n_items = 0;
+        int o_meet = 0, n_meet = 0;
+        int o_s2v = 0, o_lift = 0;
+        size_t flags_off = 0;
+    };
+    std::vector<Lvl> lv;
+    size_t flags_total = 0;
 };
+
+// Tile configuration of a query (hb::query_config_tile); the autotuner may
+// override the default choice per (index shape, viewpoint count) bucket.
+int choose_query_cfg(const htrip_index* h, int ns, int root_group);
 
 void make_plan(const htrip_index* h, const int32_t* vps, const uint8_t* pass_flags, int k, QueryPlan& P) {
     const int b = h->b, g = h->g, H = h->H;
@@ -514,9 +547,11 @@ void make_plan(const htrip_index* h, const int32_t* vps, const uint8_t* pass_fla
     std::stable_sort(v.begin(), v.end(), [](const V& a, const V& c) { return a.key < c.key; });
     const int ns = (int)v.size();
     P.n_sorted = ns;
+    P.k = k;
+    P.ldm = std::max(8, (ns + 7) / 8 * 8);
     P.buf.clear();
     P.o_vp0 = 0;
-    P.buf.resize(4 * ns + k);
+    P.buf.resize(4 * (size_t)ns + k);
     P.o_inv = 4 * ns;
     for (int i = 0; i < k; ++i) P.buf[P.o_inv + i] = -1;
     for (int i = 0; i < ns; ++i) {
@@ -531,90 +566,192 @@ void make_plan(const htrip_index* h, const int32_t* vps, const uint8_t* pass_fla
         for (int t = i; t < j; ++t) { P.buf[4 * t + 2] = i; P.buf[4 * t + 3] = j; }
         i = j;
     }
-    P.o_cg.assign(H + 1, 0); P.n_cg.assign(H + 1, 0); P.o_ng.assign(H + 1, 0); P.n_ng.assign(H + 1, 0);
-    P.o_qoff.assign(H + 1, 0); P.max_cg.assign(H + 1, 0); P.max_ng.assign(H + 1, 0);
+    // Child groups of every level.
+    struct CG { int node, quad, start, cnt, slot0; };
+    std::vector<std::vector<CG>> cgs(H + 1);
+    P.lv.assign(H + 1, QueryPlan::Lvl());
     for (int l = 1; l <= H; ++l) {
         const Level& Lv = h->L[l];
         const Level& Lc = h->L[l - 1];
-        std::vector<int> child(ns), node(ns), quad(ns);
+        QueryPlan::Lvl& Q = P.lv[l];
+        int prev_child = -1;
         for (int i = 0; i < ns; ++i) {
             const int cxp = v[i].tx * b / Lc.side, cyp = v[i].ty * b / Lc.side;
-            child[i] = cyp * Lc.nodes_x + cxp;
-            node[i] = (cyp / g) * Lv.nodes_x + (cxp / g);
-            quad[i] = (cyp % g) * g + (cxp % g);
+            const int child = cyp * Lc.nodes_x + cxp;
+            if (child != prev_child) {
+                cgs[l].push_back({(cyp / g) * Lv.nodes_x + (cxp / g), (cyp % g) * g + (cxp % g), i, 0, 0});
+                prev_child = child;
+            }
+            cgs[l].back().cnt++;
         }
-        P.o_cg[l] = (int)P.buf.size();
-        int ncg = 0;
-        std::vector<int> cg_start;
-        for (int i = 0; i < ns;) {
-            int j = i;
-            while (j < ns && child[j] == child[i]) ++j;
-            P.buf.insert(P.buf.end(), {node[i], quad[i], i, j - i});
-            P.max_cg[l] = std::max(P.max_cg[l], j - i);
-            cg_start.push_back(i);
-            ++ncg;
-            i = j;
+        for (const CG& c : cgs[l]) Q.max_group = std::max(Q.max_group, c.cnt);
+        Q.n_groups = (int)cgs[l].size();
+    }
+    P.cfg = choose_query_cfg(h, ns, H >= 1 ? P.lv[H].max_group : ns);
+    const hb::QueryTile tile = hb::query_config_tile(P.cfg);
+    const int RW = tile.RW, NC = tile.NCOL;
+    // Slot layout: every child group's run starts on an RW boundary.
+    std::vector<std::vector<int>> slot_of(H + 1);
+    int max_slots = ns;
+    for (int l = 1; l <= H; ++l) {
+        QueryPlan::Lvl& Q = P.lv[l];
+        int slot = 0;
+        slot_of[l].assign(ns, 0);
+        for (CG& c : cgs[l]) {
+            c.slot0 = slot;
+            for (int t = 0; t < c.cnt; ++t) slot_of[l][c.start + t] = slot + t;
+            slot += (c.cnt + RW - 1) / RW * RW;
         }
-        P.n_cg[l] = ncg;
-        P.o_ng[l] = (int)P.buf.size();
-        int nng = 0;
-        for (int i = 0, cgi = 0; i < ns;) {
-            int j = i;
-            while (j < ns && node[j] == node[i]) ++j;
-            while (cgi < ncg && cg_start[cgi] < i) ++cgi;
-            P.buf.insert(P.buf.end(), {i, j, cgi});
-            P.max_ng[l] = std::max(P.max_ng[l], j - i);
-            ++nng;
-            i = j;
+        Q.slots = slot;
+        max_slots = std::max(max_slots, slot);
+        Q.flags_off = P.flags_total;
+        P.flags_total += (size_t)Q.n_groups * h->L[l].nP;
+    }
+    P.ldv = (max_slots + 256 + 7) / 8 * 8;
+    // Level-0 table: per level-1 slot {sorted index or -1, level-1 group}.
+    P.o_l0 = (int)P.buf.size();
+    if (H >= 1) {
+        P.n_l0 = P.lv[1].slots;
+        P.buf.resize(P.buf.size() + 2 * (size_t)P.n_l0, -1);
+        for (int gi = 0; gi < (int)cgs[1].size(); ++gi)
+            for (int t = 0; t < cgs[1][gi].cnt; ++t) {
+                P.buf[P.o_l0 + 2 * (cgs[1][gi].slot0 + t)] = cgs[1][gi].start + t;
+                P.buf[P.o_l0 + 2 * (cgs[1][gi].slot0 + t) + 1] = gi;
+            }
+    } else {
+        P.n_l0 = 0;
+    }
+    const int target_items = 296;
+    for (int l = 1; l <= H; ++l) {
+        const Level& Lv = h->L[l];
+        QueryPlan::Lvl& Q = P.lv[l];
+        const auto& G = cgs[l];
+        Q.o_groups = (int)P.buf.size();
+        for (const CG& c : G) P.buf.insert(P.buf.end(), {c.node, c.quad, c.slot0, c.cnt, c.start});
+        // project items; at the root a viewpoint of child q meets only
+        // viewpoints of children >= q (i < j), so earlier blocks are skipped.
+        Q.o_items = (int)P.buf.size();
+        for (int gi = 0; gi < (int)G.size(); ++gi) {
+            const int n_begin = (l == H) ? (G[gi].quad * Lv.nP) / NC * NC : 0;
+            for (int m0 = 0; m0 < G[gi].cnt; m0 += RW)
+                for (int n0 = n_begin; n0 < Lv.NP; n0 += NC) P.buf.insert(P.buf.end(), {gi, m0, n0});
         }
-        P.n_ng[l] = nng;
-        P.o_qoff[l] = (int)P.buf.size();
-        for (int i = 0; i < ns; ++i) P.buf.push_back(quad[i] * Lv.nP);
+        Q.n_items = ((int)P.buf.size() - Q.o_items) / 3;
+        Q.o_s2v = (int)P.buf.size();
+        P.buf.resize(P.buf.size() + Q.slots + NC, -1);
+        for (const CG& c : G)
+            for (int t = 0; t < c.cnt; ++t) P.buf[Q.o_s2v + c.slot0 + t] = c.start + t;
+        // meet items: rows = RW viewpoints j of child group c2, lanes = NC
+        // viewpoint slots i of the node before or in c2.
+        std::vector<int> base;
+        for (int gi = 0; gi < (int)G.size();) {
+            int ge = gi;
+            while (ge < (int)G.size() && G[ge].node == G[gi].node) ++ge;
+            const int sW = G[gi].slot0;
+            for (int c2 = gi; c2 < ge; ++c2) {
+                const int s2 = G[c2].slot0, e2 = s2 + G[c2].cnt;
+                for (int i0 = sW; i0 < e2 - 1; i0 += NC)
+                    for (int jb = 0; jb < G[c2].cnt; jb += RW) {
+                        const int j0 = s2 + jb, nj = std::min(RW, G[c2].cnt - jb);
+                        if (i0 >= j0 + nj - 1) continue;
+                        base.insert(base.end(), {i0, j0, nj, c2, G[c2].quad * Lv.nP});
+                    }
+            }
+            gi = ge;
+        }
+        const int nbase = (int)base.size() / 5;
+        int ks = nbase ? (target_items + nbase - 1) / nbase : 1;
+        ks = std::max(1, std::min(ks, (Lv.nP + 63) / 64));
+        const int kstep = ((Lv.nP + ks - 1) / ks + 31) / 32 * 32;
+        Q.o_meet = (int)P.buf.size();
+        for (int t = 0; t < nbase; ++t)
+            for (int kb = 0; kb < Lv.nP; kb += kstep)
+                P.buf.insert(P.buf.end(), {base[5 * t], base[5 * t + 1], base[5 * t + 2], base[5 * t + 3],
+                                           base[5 * t + 4], kb, std::min(Lv.nP, kb + kstep)});
+        Q.n_meet = ((int)P.buf.size() - Q.o_meet) / 7;
+        // lift table: level-l slot -> {level-(l+1) slot, level-(l+1) group}
+        if (l < H) {
+            Q.o_lift = (int)P.buf.size();
+            P.buf.resize(P.buf.size() + 2 * (size_t)Q.slots, 0);
+            const auto& Gn = cgs[l + 1];
+            for (int gn = 0; gn < (int)Gn.size(); ++gn)
+                for (int t = 0; t < Gn[gn].cnt; ++t) {
+                    const int i = Gn[gn].start + t;
+                    P.buf[Q.o_lift + 2 * slot_of[l][i]] = Gn[gn].slot0 + t;
+                    P.buf[Q.o_lift + 2 * slot_of[l][i] + 1] = gn;
+                }
+        }
     }
 }
 
-void run_query(htrip_index* h, const QueryPlan& P, int k, uint16_t* out_dev) {
+void run_query(htrip_index* h, const QueryPlan& P, uint16_t* out_dev) {
     cudaStream_t st = h->stream;
-    const int H = h->H, ns = P.n_sorted;
+    const int H = h->H, ldv = P.ldv, ldm = P.ldm;
+    if (H > hb::kMaxQueryLevels) throw CudaError{cudaErrorInvalidValue, "hierarchy deeper than the query supports"};
+    for (int l = 1; l <= H; ++l)
+        if (h->L[l].nP > hb::query_max_ports())
+            throw CudaError{cudaErrorInvalidValue, "child port count above the query kernel's list capacity"};
     h->qplan.reserve(std::max<size_t>(1, P.buf.size()));
     ck(cudaMemcpyAsync(h->qplan.p, P.buf.data(), P.buf.size() * sizeof(int), cudaMemcpyHostToDevice, st), "plan");
     const int* plan = h->qplan.p;
-    const int ldm = std::max(8, (ns + 7) / 8 * 8);
-    int maxExt = 0, maxNP = 0, maxnP = 0, maxcg = 1;
+    int maxExt = 0, maxNP = 64;
     for (int l = 0; l <= H; ++l) maxExt = std::max(maxExt, h->L[l].nExt);
-    for (int l = 1; l <= H; ++l) {
-        maxNP = std::max(maxNP, h->L[l].NP);
-        maxnP = std::max(maxnP, h->L[l].nP);
-        maxcg = std::max(maxcg, P.n_cg[l]);
-    }
-    const int ldx = ldm;
+    for (int l = 1; l <= H; ++l) maxNP = std::max(maxNP, h->L[l].NP);
     h->qM.reserve((size_t)ldm * ldm);
-    h->qX[0].reserve((size_t)maxExt * ldx);
-    h->qX[1].reserve((size_t)maxExt * ldx);
-    h->qY.reserve(std::max<size_t>(1, (size_t)ns * maxNP));
-    h->qkidx.reserve((size_t)maxcg * (maxnP + 1) + 1);
-    // M := INF (upper triangle is what finalize reads)
-    hb::launch_fill_u16(h->qM.p, (size_t)ldm * ldm, hb::INF, st);
-    hb::launch_query_level0(h->L[0].ms(), h->L[0].d_ext.p, h->L[0].nExt, plan + P.o_vp0, ns, h->qX[0].p, ldx,
-                            h->qM.p, ldm, st);
-    ck(cudaGetLastError(), "level0");
-    int cur = 0;
+    for (int i = 0; i < 3; ++i) h->qX[i].reserve((size_t)maxExt * ldv);
+    for (int i = 0; i < 2; ++i) h->qY[i].reserve((size_t)maxNP * ldv);
+    h->qflags.reserve(std::max<size_t>(1, P.flags_total));
+    ck(cudaMemsetAsync(h->qM.p, 0xFF, (size_t)ldm * ldm * sizeof(uint32_t), st), "M");
+    if (P.flags_total) ck(cudaMemsetAsync(h->qflags.p, 0, P.flags_total, st), "flags");
+    hb::QueryParams Q{};
+    Q.H = H;
+    Q.k = P.k;
+    Q.ns = P.n_sorted;
+    Q.ldv = ldv;
+    Q.ldm = ldm;
+    Q.n_l0_slots = P.n_l0;
+    Q.nExt0 = h->L[0].nExt;
+    Q.cfg = P.cfg;
+    Q.vp0 = plan + P.o_vp0;
+    Q.inv = plan + P.o_inv;
+    Q.l0 = plan + P.o_l0;
+    Q.ext0 = h->L[0].d_ext.p;
+    Q.leaves = h->L[0].ms();
+    for (int i = 0; i < 3; ++i) Q.X[i] = h->qX[i].p;
+    for (int i = 0; i < 2; ++i) Q.Y[i] = h->qY[i].p;
+    Q.M = h->qM.p;
+    Q.out = out_dev;
+    Q.status = h->qstatus.p;
+    Q.bar = h->qbar.p;
     for (int l = 1; l <= H; ++l) {
         const Level& Lv = h->L[l];
-        hb::launch_query_project(Lv.ms(), Lv.nP, plan + P.o_cg[l], P.n_cg[l], P.max_cg[l], h->qX[cur].p, ldx,
-                                 h->qY.p, maxNP, h->qkidx.p, st);
-        ck(cudaGetLastError(), "project");
-        if (l < H) {
-            hb::launch_query_lift(h->qY.p, maxNP, Lv.d_ext.p, Lv.nExt, ns, h->qX[cur ^ 1].p, ldx, st);
-            ck(cudaGetLastError(), "lift");
-        }
-        hb::launch_query_meet(plan + P.o_ng[l], P.n_ng[l], plan + P.o_qoff[l], h->qY.p, maxNP, h->qX[cur].p, ldx,
-                              Lv.nP, h->qM.p, ldm, P.max_ng[l], st);
-        ck(cudaGetLastError(), "meet");
-        cur ^= 1;
+        const QueryPlan::Lvl& L = P.lv[l];
+        hb::QueryLevel& q = Q.lv[l];
+        q.D = Lv.mat.p;
+        q.NP = Lv.NP;
+        q.nP = Lv.nP;
+        q.ext_inv = Lv.d_ext_inv.p;
+        q.groups = plan + L.o_groups;
+        q.flags = h->qflags.p + L.flags_off;
+        q.items = plan + L.o_items;
+        q.n_items = L.n_items;
+        q.meet = plan + L.o_meet;
+        q.n_meet = L.n_meet;
+        q.s2v = plan + L.o_s2v;
+        q.lift = l < H ? plan + L.o_lift : nullptr;
+        q.store_y = 1;
     }
-    hb::launch_query_finalize(h->qM.p, ldm, plan + P.o_inv, k, out_dev, st);
-    ck(cudaGetLastError(), "finalize");
+    if (h->qgrid == 0) h->qgrid = hb::query_grid_blocks(h->device);
+    h->qparams.reserve(sizeof(hb::QueryParams));
+    std::memcpy(h->h_qparams, &Q, sizeof(Q));
+    ck(cudaMemcpyAsync(h->qparams.p, h->h_qparams, sizeof(Q), cudaMemcpyHostToDevice, st), "params");
+    ck(hb::launch_query(reinterpret_cast<const hb::QueryParams*>(h->qparams.p), P.cfg, h->qgrid, st), "query kernel");
+}
+
+int choose_query_cfg(const htrip_index* h, int ns, int root_group) {
+    (void)h;
+    (void)ns;
+    return root_group >= 24 ? 2 : 1;
 }
 
 }  // namespace
@@ -726,9 +863,15 @@ htrip_status htrip_query_all_pairs(htrip_index* h, const int32_t* vps, int32_t k
     QueryPlan P;
     make_plan(h, vps, pf.data(), k, P);
     h->qout.reserve((size_t)k * k);
-    run_query(h, P, k, h->qout.p);
+    run_query(h, P, h->qout.p);
+    int status = 0;
     ck(cudaMemcpyAsync(out, h->qout.p, (size_t)k * k * sizeof(uint16_t), cudaMemcpyDeviceToHost, h->stream), "out");
+    ck(cudaMemcpyAsync(&status, h->qstatus.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "status");
     ck(cudaStreamSynchronize(h->stream), "query sync");
+    if (status != 0) {
+        cudaMemsetAsync(h->qstatus.p, 0, sizeof(int), h->stream);
+        return fail(HTRIP_ERR_CUDA, "query kernel: grid barrier timed out");
+    }
     return HTRIP_OK;
     HTRIP_GUARD_END
 }
@@ -753,7 +896,7 @@ htrip_status htrip_query_all_pairs_dev(htrip_index* h, const int32_t* vps_dev, c
     }
     QueryPlan P;
     make_plan(h, vps.data(), pf.data(), k, P);
-    run_query(h, P, k, out_dev);
+    run_query(h, P, out_dev);
     return HTRIP_OK;
     HTRIP_GUARD_END
 }
@@ -830,8 +973,10 @@ htrip_status htrip_memory_bytes(const htrip_index* h, uint64_t* reference_bytes,
         for (const auto& Lv : h->L)
             dev += (Lv.mat.n + Lv.klist.n * 2 + Lv.kcnt.n * 2) * sizeof(uint16_t) + Lv.kflag.n + Lv.dec.n +
                    (Lv.d_ext.n + Lv.d_seams.n) * sizeof(int);
-        dev += h->pass.n + h->panel.n * 2 + h->pflags.n + h->snap.n * 2 + h->qY.n * 2 + h->qM.n * 2 +
-               (h->qX[0].n + h->qX[1].n) * 2 + h->qkidx.n * 4 + h->qout.n * 2;
+        dev += h->pass.n + h->panel.n * 2 + h->pflags.n + h->snap.n * 2 + h->qM.n * 4 + h->qflags.n +
+               h->qkidx.n * 4 + h->qout.n * 2 + h->qplan.n * 4;
+        for (const auto& x : h->qX) dev += x.n * 2;
+        for (const auto& y : h->qY) dev += y.n * 2;
     }
     if (reference_bytes) *reference_bytes = ref;
     if (device_bytes) *device_bytes = dev;

@@ -409,186 +409,6 @@ __global__ void ext_compare_kernel(MatSet M, const int* __restrict__ ext, int nE
     if (__any_sync(FULL, d) && (threadIdx.x & 31) == 0) dec[m] = 1;
 }
 
-// ---------------------------------------------------------------------------
-// Query.
-// ---------------------------------------------------------------------------
-__global__ void query_level0_kernel(MatSet L, const int* __restrict__ ext, int nExt, const int* __restrict__ vp,
-                                    uint16_t* X0t, int ldx, uint16_t* Mq, int ldm) {
-    const int j = blockIdx.x;
-    const int leaf = vp[4 * j], u = vp[4 * j + 1], g1 = vp[4 * j + 3];
-    const uint16_t* row = mat_ptr(L, leaf) + (size_t)u * L.NP;
-    for (int p = threadIdx.x; p < nExt; p += blockDim.x) X0t[(size_t)p * ldx + j] = row[ext[p]];
-    for (int jj = j + 1 + threadIdx.x; jj < g1; jj += blockDim.x) {
-        const uint16_t d = row[vp[4 * jj + 1]];
-        Mq[(size_t)j * ldm + jj] = d;
-    }
-}
-
-__global__ void query_active_kernel(const int* __restrict__ groups, int nP, const uint16_t* __restrict__ Xt,
-                                    int ldx, int* kidx, int* kcount, int kstride) {
-    __shared__ int warp_tot[32];
-    __shared__ int base;
-    const int gi = blockIdx.x;
-    const int start = groups[4 * gi + 2], cnt = groups[4 * gi + 3];
-    int* out = kidx + (size_t)gi * kstride;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    if (threadIdx.x == 0) base = 0;
-    __syncthreads();
-    for (int p0 = 0; p0 < nP; p0 += blockDim.x) {
-        const int p = p0 + threadIdx.x;
-        bool on = false;
-        if (p < nP) {
-            const uint16_t* x = Xt + (size_t)p * ldx + start;
-            for (int i = 0; i < cnt && !on; ++i) on = x[i] < INF;
-        }
-        const unsigned bal = __ballot_sync(FULL, on);
-        if (lane == 0) warp_tot[warp] = __popc(bal);
-        __syncthreads();
-        int off = base;
-        for (int w = 0; w < warp; ++w) off += warp_tot[w];
-        if (on) out[off + __popc(bal & ((1u << lane) - 1u))] = p;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int t = 0;
-            for (int w = 0; w < nw; ++w) t += warp_tot[w];
-            base += t;
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) kcount[gi] = base;
-}
-
-// Y[start+i][n0 .. n0+NT) = min_t Xt[kidx[t]][start+i] + D_U[q*nP + kidx[t]][...]
-// CTA: WM x WN warps (runtime), warp tile RW rows x 64*CP columns.
-constexpr int kProjKC = 32;
-
-template <int RW, int CP>
-__global__ void __launch_bounds__(256)
-query_project_kernel(MatSet N, int nP, const int* __restrict__ groups, const uint16_t* __restrict__ Xt, int ldx,
-                     uint16_t* Y, int ldy, const int* __restrict__ kidx, const int* __restrict__ kcount,
-                     int kstride, int WM, int WN) {
-    constexpr int KC = kProjKC;
-    extern __shared__ __align__(16) uint16_t sm[];
-    const int MT = WM * RW, NT = WN * 64 * CP;
-    uint16_t* As = sm;             // [KC][MT]
-    uint16_t* Bs = sm + KC * MT;   // [KC][NT]
-    const int gi = blockIdx.z;
-    const int node = groups[4 * gi], q = groups[4 * gi + 1], start = groups[4 * gi + 2], cnt = groups[4 * gi + 3];
-    const int m0 = blockIdx.y * MT;
-    if (m0 >= cnt) return;
-    const int n0 = blockIdx.x * NT;
-    const int NP = N.NP;
-    if (n0 >= NP) return;
-    const int nA = kcount[gi];
-    const int* kl = kidx + (size_t)gi * kstride;
-    const uint16_t* D = mat_ptr(N, node) + (size_t)q * nP * NP;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int wm = warp / WN, wn = warp % WN;
-    uint32_t acc[RW][CP];
-#pragma unroll
-    for (int r = 0; r < RW; ++r)
-#pragma unroll
-        for (int c = 0; c < CP; ++c) acc[r][c] = INF2;
-    const int ncol = min(NT, NP - n0);
-    for (int t0 = 0; t0 < nA; t0 += KC) {
-        const int kc = min(KC, nA - t0);
-        for (int idx = tid; idx < KC * MT; idx += blockDim.x) {
-            const int t = idx / MT, i = idx % MT;
-            uint16_t v = INF;
-            if (t < kc && m0 + i < cnt) v = Xt[(size_t)kl[t0 + t] * ldx + start + m0 + i];
-            As[t * MT + i] = v;
-        }
-        for (int idx = tid; idx < KC * (NT / 8); idx += blockDim.x) {
-            const int t = idx / (NT / 8), c8 = idx % (NT / 8);
-            uint4 v = make_uint4(INF2, INF2, INF2, INF2);
-            if (t < kc && c8 * 8 < ncol) v = reinterpret_cast<const uint4*>(D + (size_t)kl[t0 + t] * NP + n0)[c8];
-            reinterpret_cast<uint4*>(Bs + t * NT)[c8] = v;
-        }
-        __syncthreads();
-        for (int t = 0; t < kc; ++t) {
-            uint32_t bv[CP];
-#pragma unroll
-            for (int c = 0; c < CP; ++c)
-                bv[c] = reinterpret_cast<const uint32_t*>(Bs + t * NT + wn * 64 * CP + lane * 2 * CP)[c];
-            const uint16_t* arow = As + t * MT + wm * RW;
-#pragma unroll
-            for (int r = 0; r < RW; ++r) {
-                const uint32_t a = arow[r];
-                if (a <= INF_HEADROOM) {
-                    const uint32_t aa = splat(a);
-#pragma unroll
-                    for (int c = 0; c < CP; ++c) acc[r][c] = acc_fast(acc[r][c], bv[c], aa);
-                } else if (a < INF) {
-                    const uint32_t aa = splat(a), tt = splat(INF - a);
-#pragma unroll
-                    for (int c = 0; c < CP; ++c) acc[r][c] = acc_clamp(acc[r][c], bv[c], aa, tt);
-                }
-            }
-        }
-        __syncthreads();
-    }
-    const int col = n0 + wn * 64 * CP + lane * 2 * CP;
-    if (col < NP) {
-#pragma unroll
-        for (int r = 0; r < RW; ++r) {
-            const int i = m0 + wm * RW + r;
-            if (i < cnt) {
-                uint32_t* dst = reinterpret_cast<uint32_t*>(Y + (size_t)(start + i) * ldy + col);
-#pragma unroll
-                for (int c = 0; c < CP; ++c) dst[c] = acc[r][c];
-            }
-        }
-    }
-}
-
-__global__ void query_lift_kernel(const uint16_t* __restrict__ Y, int ldy, const int* __restrict__ ext, int nExt,
-                                  int k, uint16_t* Xn, int ldx) {
-    const int e = blockIdx.y;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nExt || j >= k) return;
-    Xn[(size_t)e * ldx + j] = Y[(size_t)j * ldy + ext[e]];
-}
-
-// One warp per (row i, block of 32 columns j > i) of a node group.
-__global__ void query_meet_kernel(const int* __restrict__ ngroups, const int* __restrict__ qoff,
-                                  const uint16_t* __restrict__ Y, int ldy, const uint16_t* __restrict__ Xt, int ldx,
-                                  int nP, uint16_t* Mq, int ldm) {
-    const int ng = blockIdx.x;
-    const int start = ngroups[3 * ng], end = ngroups[3 * ng + 1];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = start + blockIdx.y * (blockDim.x >> 5) + warp;
-    if (i >= end) return;
-    const uint16_t* yrow = Y + (size_t)i * ldy;
-    for (int jb = i + 1; jb < end; jb += 32) {
-        const int j = jb + lane;
-        if (j < end) {
-            const uint16_t* y = yrow + qoff[j];
-            const uint16_t* x = Xt + j;
-            uint32_t best = INF;
-            for (int p = 0; p < nP; ++p) {
-                const uint32_t s = (uint32_t)y[p] + x[(size_t)p * ldx];
-                best = s < best ? s : best;
-            }
-            uint16_t* dst = Mq + (size_t)i * ldm + j;
-            if (best < *dst) *dst = (uint16_t)best;
-        }
-    }
-}
-
-__global__ void query_finalize_kernel(const uint16_t* __restrict__ Mq, int ldm, const int* __restrict__ inv, int k,
-                                      uint16_t* out) {
-    const int a = blockIdx.y;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= k) return;
-    const int ia = inv[a], ic = inv[c];
-    uint16_t v = INF;
-    if (ia >= 0 && ic >= 0) {
-        if (ia == ic) v = 0;
-        else v = ia < ic ? Mq[(size_t)ia * ldm + ic] : Mq[(size_t)ic * ldm + ia];
-    }
-    out[(size_t)a * k + c] = v;
-}
-
 __global__ void gather_block_kernel(const uint16_t* __restrict__ mat, int NP, const int* __restrict__ rows, int nr,
                                     const int* __restrict__ cols, int nc, uint16_t* out) {
     const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -692,70 +512,6 @@ void launch_ext_compare(MatSet M, const int* ext, int nExt, const int* active, i
     if (n_active == 0) return;
     dim3 grid(blocks_for((size_t)nExt * nExt, 256), n_active);
     ext_compare_kernel<<<grid, 256, 0, st>>>(M, ext, nExt, active, snap, dec);
-}
-
-void launch_query_level0(MatSet leaves, const int* ext, int nExt, const int* vp, int k, uint16_t* X0t, int ldx,
-                         uint16_t* M, int ldm, cudaStream_t st) {
-    if (k == 0) return;
-    query_level0_kernel<<<k, 128, 0, st>>>(leaves, ext, nExt, vp, X0t, ldx, M, ldm);
-}
-
-template <int RW, int CP>
-static void launch_project_t(MatSet node, int nP, const int* groups, int n_groups, int max_group,
-                             const uint16_t* Xt, int ldx, uint16_t* Y, int ldy, const int* kidx, const int* kcount,
-                             int kstride, int WM, int WN, cudaStream_t st) {
-    const int MT = WM * RW, NT = WN * 64 * CP;
-    const size_t smem = (size_t)kProjKC * (MT + NT) * sizeof(uint16_t);
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(query_project_kernel<RW, CP>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-        configured = true;
-    }
-    dim3 grid(blocks_for(node.NP, NT), blocks_for(max_group, MT), n_groups);
-    query_project_kernel<RW, CP><<<grid, WM * WN * 32, smem, st>>>(node, nP, groups, Xt, ldx, Y, ldy, kidx, kcount,
-                                                                    kstride, WM, WN);
-}
-
-void launch_query_project(MatSet node, int nP, const int* groups, int n_groups, int max_group, const uint16_t* Xt,
-                          int ldx, uint16_t* Y, int ldy, int* kidx, cudaStream_t st) {
-    if (n_groups == 0) return;
-    int* kcount = kidx + (size_t)n_groups * nP;  // caller reserves n_groups extra ints
-    query_active_kernel<<<n_groups, 256, 0, st>>>(groups, nP, Xt, ldx, kidx, kcount, nP);
-    // Column tile: 8 warps x 128 columns = 1024, narrowed for small matrices.
-    int WN = node.NP >= 1024 ? 8 : node.NP / 128;
-    if (WN < 1) WN = 1;
-    if (node.NP < 128) {
-        // 64-wide matrices: CP = 1 (64 columns per warp).
-        int WM = max_group >= 8 ? 8 : (max_group >= 4 ? 4 : 1);
-        launch_project_t<4, 1>(node, nP, groups, n_groups, max_group, Xt, ldx, Y, ldy, kidx, kcount, nP, WM, 1, st);
-        return;
-    }
-    if (max_group <= 4) {
-        launch_project_t<4, 2>(node, nP, groups, n_groups, max_group, Xt, ldx, Y, ldy, kidx, kcount, nP, 1, WN, st);
-    } else {
-        const int WM = 8 / WN >= 1 ? 8 / WN : 1;
-        launch_project_t<16, 2>(node, nP, groups, n_groups, max_group, Xt, ldx, Y, ldy, kidx, kcount, nP, WM, WN, st);
-    }
-}
-
-void launch_query_lift(const uint16_t* Y, int ldy, const int* ext, int nExt, int k, uint16_t* Xt_next, int ldx,
-                       cudaStream_t st) {
-    if (k == 0) return;
-    dim3 grid(blocks_for(k, 128), nExt);
-    query_lift_kernel<<<grid, 128, 0, st>>>(Y, ldy, ext, nExt, k, Xt_next, ldx);
-}
-
-void launch_query_meet(const int* ngroups, int n_ngroups, const int* qoff, const uint16_t* Y, int ldy,
-                       const uint16_t* Xt, int ldx, int nP, uint16_t* M, int ldm, int max_w, cudaStream_t st) {
-    if (n_ngroups == 0) return;
-    dim3 grid(n_ngroups, blocks_for(max_w, 8));
-    query_meet_kernel<<<grid, 256, 0, st>>>(ngroups, qoff, Y, ldy, Xt, ldx, nP, M, ldm);
-}
-
-void launch_query_finalize(const uint16_t* M, int ldm, const int* inv, int k, uint16_t* out, cudaStream_t st) {
-    if (k == 0) return;
-    dim3 grid(blocks_for(k, 128), k);
-    query_finalize_kernel<<<grid, 128, 0, st>>>(M, ldm, inv, k, out);
 }
 
 void launch_fill_u16(uint16_t* ptr, size_t n, uint16_t value, cudaStream_t st) {

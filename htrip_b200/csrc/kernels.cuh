@@ -74,37 +74,54 @@ void launch_ext_snapshot(MatSet M, const int* ext, int nExt, const int* active, 
 void launch_ext_compare(MatSet M, const int* ext, int nExt, const int* active, int n_active,
                         const uint16_t* snap, uint8_t* dec, cudaStream_t st);
 
-// --- query -------------------------------------------------------------------
-// Level-0 extraction (minplus_oracle.cpp:990-1048): X0t[p*ldx + j] =
-// leaf D[u_j][ext[p]] for viewpoint j (sorted order), and same-leaf pairs
-// into M (k x k, sorted order).  vp: per sorted viewpoint {leaf, u, leaf
-// group start, leaf group end} (4 ints).
-void launch_query_level0(MatSet leaves, const int* ext, int nExt, const int* vp, int k, uint16_t* X0t,
-                         int ldx, uint16_t* M, int ldm, cudaStream_t st);
+// --- query (query.cu) -------------------------------------------------------
+constexpr int kMaxQueryLevels = 16;
+constexpr int kNumQueryConfigs = 4;
 
-// Grouped gather-GEMM Y[i][:] = min_p X[i][p] + D_U[off + p][:] for the
-// viewpoints i of each child group.  groups: 4 ints {node, quad, start,
-// count} per group.  Active port lists are built inside.
-void launch_query_project(MatSet node, int nP, const int* groups, int n_groups, int max_group,
-                          const uint16_t* Xt, int ldx, uint16_t* Y, int ldy, int* kidx,
-                          cudaStream_t st);
+// Warp tile of a query work item: RW viewpoint rows x NCOL columns.
+struct QueryTile {
+    int RW;
+    int NCOL;
+};
+QueryTile query_config_tile(int cfg);
+int query_default_config(int NP, int max_group);
 
-// Lift X_next t[e][j] = Y[j][ext[e]] for all viewpoints j in [0, k).
-void launch_query_lift(const uint16_t* Y, int ldy, const int* ext, int nExt, int k, uint16_t* Xt_next,
-                       int ldx, cudaStream_t st);
+struct QueryLevel {
+    const uint16_t* D;      // level matrices (NP x NP each)
+    int NP, nP;
+    const int* ext_inv;     // column -> exterior port index or -1 (NP)
+    const int* groups;      // 5 ints per child group {node, quad, slot0, cnt, sorted0}
+    uint8_t* flags;         // [group][nP] finite-port flags of X_{l-1}
+    const int* items;       // project items {group, m0, n0}
+    int n_items;
+    const int* meet;        // meet items {i0, j0, nj, group, coloff, kb, ke}
+    int n_meet;
+    const int* s2v;         // level-l slot -> sorted viewpoint or -1
+    const int* lift;        // level-l slot -> {level-(l+1) slot, level-(l+1) group}
+    int store_y;
+};
 
-// Meet: for every node group (range [start, end) of sorted viewpoints) and
-// i < j in it: M[i][j] = min(M[i][j], min_p Y[i][qoff[j]+p] + Xt[p][j]).
-// ngroups: 3 ints {start, end, first child group} per node; qoff[j] = the
-// V_U offset of viewpoint j's child block.
-void launch_query_meet(const int* ngroups, int n_ngroups, const int* qoff, const uint16_t* Y, int ldy,
-                       const uint16_t* Xt, int ldx, int nP, uint16_t* M, int ldm, int max_w,
-                       cudaStream_t st);
+struct QueryParams {
+    int H, k, ns, ldv, ldm, n_l0_slots, nExt0, cfg;
+    const int* vp0;         // per sorted viewpoint {leaf, u, leaf-run start, leaf-run end}
+    const int* inv;         // original index -> sorted index or -1
+    const int* l0;          // per level-1 slot {sorted index or -1, level-1 group}
+    const int* ext0;        // leaf port -> cell
+    MatSet leaves;
+    uint16_t* X[3];         // port vectors X_l in P.X[l % 3] ([port][ldv])
+    uint16_t* Y[2];         // projections Yt_l in P.Y[l & 1] ([column][ldv])
+    uint32_t* M;            // sorted-order pair matrix (ldm), preset to 0xFFFFFFFF
+    uint16_t* out;          // k x k result
+    int* status;            // 0 ok, 1 grid barrier timeout
+    unsigned* bar;          // grid barrier {count, generation}
+    QueryLevel lv[kMaxQueryLevels + 1];
+};
 
-// Final un-permute: out[a*k + c] = M[inv[a]][inv[c]]; rows/cols of
-// non-passable viewpoints INF, diagonal 0 for passable ones.
-void launch_query_finalize(const uint16_t* M, int ldm, const int* inv, int k, uint16_t* out,
-                           cudaStream_t st);
+// Cooperative launch of the persistent query kernel on `grid` blocks; the
+// parameter block lives in device memory (P_dev).
+int query_grid_blocks(int device);
+int query_max_ports();  // largest per-child port count the query kernel handles
+cudaError_t launch_query(const QueryParams* P_dev, int cfg, int grid, cudaStream_t st);
 
 // ptr[0 .. n) = value.
 void launch_fill_u16(uint16_t* ptr, size_t n, uint16_t value, cudaStream_t st);

@@ -1,0 +1,418 @@
+// queryAllPairs on the device (reference MinPlusOracle::queryAllPairs,
+// src/minplus_oracle.cpp:934-1419) as ONE persistent cooperative kernel.
+//
+// Viewpoints are sorted by the base-g^2 Morton code of their leaf, so at
+// every level the viewpoints of one node, and of one child of a node, form a
+// contiguous run ("child group").  At level l each child group owns a run of
+// "slots" that starts on an 8-slot (16-byte) boundary; the port vectors
+// X_{l-1} (ports x slots) and the projections Yt_l (node columns x slots) are
+// stored in level-l slot order.
+//
+// Work is cut into warp-sized items (no shared memory, no CTA barriers): a
+// warp keeps RW rows x 64*CP columns of packed u16 accumulators and streams
+// its operand rows from L2/HBM.  The rows of a warp are warp-uniform, the
+// columns are spread over the lanes.
+//
+//   level 0  X0[p][s] = leaf D[u][port p] for every viewpoint (+ finite-port
+//            flags of its level-1 child group) and same-leaf pairs
+//            (minplus_oracle.cpp:990-1048).
+//   project Yt_l[c][s] = min_p X_{l-1}[p][s] (+) D_U[q*nP + p][c] over the ports
+//            p finite for some viewpoint of the group (row compaction,
+//            minplus_oracle.cpp:1185-1215).  The exterior columns are the lift
+//            X_l = X_{l-1} (x) child_to_ext (:1113-1154); the epilogue writes
+//            them straight into X_l (level-(l+1) slot order) with the next
+//            level's flags.
+//   meet     M[i][j] = min(M[i][j], min_p Yt_l[q_j*nP + p][i] (+) X_{l-1}[p][j])
+//            for i < j in one node: the inter-child meets (:1157-1326) and the
+//            intra-child shortcut (:1328-1411) are one formula.  Split-K items
+//            combine with atomicMin on a 32-bit k x k matrix.
+//
+// Phases: [level 0] | [project 1] | [project 2 + meet 1] | ... |
+// [project H + meet H-1] | [meet H] | [finalize], separated by grid
+// barriers (H + 2 in total); meets of level l-1 overlap projects of level l
+// because Yt and X are double / triple buffered.
+//
+// Every sum is the exact clamped tropical product of minplus.cuh, so the
+// matrix equals the reference's bit for bit.
+#include "kernels.cuh"
+#include "minplus.cuh"
+
+#include <algorithm>
+
+namespace hb {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// Branch-free exact update: c' = min(c, min(b, INF - a) + a) per 16-bit lane
+// for any a in [0, INF] (a == INF gives min(b, 0) + INF = INF: no change).
+// aa = a in both halves.  min(b, INF - a) + a <= INF, so the packed add never
+// carries across the halves.
+template <int CP>
+__device__ __forceinline__ void row_update(uint32_t (&acc)[CP], const uint32_t (&bv)[CP], uint32_t aa) {
+    const uint32_t tt = INF2 - aa;
+#pragma unroll
+    for (int c = 0; c < CP; ++c) acc[c] = min2(add2(min2(bv[c], tt), aa), acc[c]);
+}
+
+template <int CP>
+__device__ __forceinline__ void ldg_pairs(uint32_t (&bv)[CP], const uint16_t* p) {
+    if constexpr (CP == 4) {
+        const uint4 v = __ldcg(reinterpret_cast<const uint4*>(p));
+        bv[0] = v.x; bv[1] = v.y; bv[2] = v.z; bv[3] = v.w;
+    } else if constexpr (CP == 2) {
+        const uint2 v = __ldcg(reinterpret_cast<const uint2*>(p));
+        bv[0] = v.x; bv[1] = v.y;
+    } else {
+        bv[0] = __ldcg(reinterpret_cast<const unsigned int*>(p));
+    }
+}
+
+// RW consecutive u16 row values (16-byte aligned) -> RW/2 packed pairs.
+template <int RW>
+__device__ __forceinline__ void ldg_rows(uint32_t (&a)[RW / 2], const uint16_t* p) {
+#pragma unroll
+    for (int h = 0; h < RW / 8; ++h) {
+        const uint4 v = __ldcg(reinterpret_cast<const uint4*>(p) + h);
+        a[4 * h] = v.x; a[4 * h + 1] = v.y; a[4 * h + 2] = v.z; a[4 * h + 3] = v.w;
+    }
+}
+
+constexpr int kThreads = 512;
+constexpr int kWarps = kThreads / 32;
+
+// Warp w of the CTA streams list entries t = w*U + 16*U*i + u of the
+// compacted row list kl[0..n):
+//   acc[r][c] = min over its rows p of A[p*lda + r] (+) B[p*ldb + lane pair c].
+// U rows per warp are in flight (their loads precede the arithmetic), so a CTA
+// keeps 16*U operand rows in flight.
+template <int RW, int CP, int U = (RW * CP >= 32 ? 4 : 8)>
+__device__ __forceinline__ void warp_minplus_list(uint32_t (&acc)[RW][CP], const int* kl, int n, int warp,
+                                                  const uint16_t* __restrict__ A, int lda,
+                                                  const uint16_t* __restrict__ B, int ldb) {
+    for (int t0 = warp * U; t0 < n; t0 += kWarps * U) {
+        int rows[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) rows[u] = t0 + u < n ? kl[t0 + u] : -1;
+        uint32_t bv[U][CP];
+        uint32_t av[U][RW / 2];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (rows[u] >= 0) {
+                ldg_pairs<CP>(bv[u], B + (size_t)rows[u] * ldb);
+                ldg_rows<RW>(av[u], A + (size_t)rows[u] * lda);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (rows[u] >= 0) {
+#pragma unroll
+                for (int r2 = 0; r2 < RW / 2; ++r2) {
+                    row_update<CP>(acc[2 * r2], bv[u], __byte_perm(av[u][r2], 0, 0x1010));
+                    row_update<CP>(acc[2 * r2 + 1], bv[u], __byte_perm(av[u][r2], 0, 0x3232));
+                }
+            }
+        }
+    }
+}
+
+// Compacts the set flags of rows [kb, ke) into kl (ascending); returns the
+// count (block-wide scan; every thread gets the total).
+__device__ __forceinline__ int compact_flags(const uint8_t* __restrict__ flags, int kb, int ke, int* kl, int* wsum) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n = ke - kb;
+    const int per = (n + kThreads - 1) / kThreads;
+    const int p0 = kb + tid * per, p1 = min(ke, p0 + per);
+    int cntl = 0;
+    for (int p = p0; p < p1; ++p) cntl += flags[p] != 0;
+    int incl = cntl;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    int base = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+        if (w < warp) base += wsum[w];
+        total += wsum[w];
+    }
+    int pos = base + incl - cntl;
+    for (int p = p0; p < p1; ++p)
+        if (flags[p]) kl[pos++] = p;
+    __syncthreads();
+    return total;
+}
+
+// Min-reduction of the 16 warps' accumulators through shared memory; the
+// reduced tile ends up in every warp's acc (warp 0 uses it).
+template <int RW, int CP>
+__device__ __forceinline__ void cta_reduce(uint32_t (&acc)[RW][CP], uint32_t* red) {
+    constexpr int E = RW * CP * 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+    for (int r = 0; r < RW; ++r)
+#pragma unroll
+        for (int c = 0; c < CP; ++c) red[warp * E + (r * CP + c) * 32 + lane] = acc[r][c];
+    __syncthreads();
+    for (int e = tid; e < E; e += kThreads) {
+        uint32_t m = red[e];
+#pragma unroll
+        for (int w = 1; w < kWarps; ++w) m = min2(m, red[w * E + e]);
+        red[e] = m;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < RW; ++r)
+#pragma unroll
+        for (int c = 0; c < CP; ++c) acc[r][c] = red[(r * CP + c) * 32 + lane];
+}
+
+// Grid barrier with a bounded spin; a timeout sets *status and the kernel
+// finishes without waiting further (the host reports the error).
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* status) {
+    __syncthreads();
+    bool ok = true;
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = bar + 1;
+        const unsigned gen = *vgen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(bar, 1u);
+        if (arrived == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            unsigned it = 0;
+            while (*vgen == gen) {
+                if (++it > (1u << 24)) {
+                    atomicExch(status, 1);
+                    ok = false;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok && *(volatile int*)status == 0;
+}
+
+// ---------------------------------------------------------------------------
+// Work item bodies.
+// ---------------------------------------------------------------------------
+// Shared memory of the persistent kernel: compacted row list (nP <= 4096
+// ports), scan partials and the split-K reduction buffer.
+constexpr int kMaxList = 4096 + 64;
+template <int RW, int CP>
+constexpr size_t query_smem_bytes() {
+    return (size_t)kMaxList * sizeof(int) + (size_t)kWarps * RW * CP * 32 * sizeof(uint32_t);
+}
+
+// project item {group, m0, n0}: tile of RW slots x 64*CP node columns; the
+// 16 warps split the group's finite ports.
+template <int RW, int CP>
+__device__ void do_project(const QueryParams& P, const QueryLevel& L, const QueryLevel* Ln, int item, int l,
+                           int* kl, int* wsum, uint32_t* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int* it = L.items + 3 * item;
+    const int gi = it[0], m0 = it[1], n0 = it[2];
+    const int* G = L.groups + 5 * gi;
+    const int node = G[0], q = G[1], slot0 = G[2], cnt = G[3];
+    const int nA = compact_flags(L.flags + (size_t)gi * L.nP, 0, L.nP, kl, wsum);
+    const uint16_t* D = L.D + (size_t)node * L.NP * L.NP + (size_t)q * L.nP * L.NP;
+    const int col = n0 + lane * 2 * CP;
+    const bool live_col = col < L.NP;
+    const uint16_t* Xp = P.X[(l - 1) % 3] + slot0 + m0;
+    uint32_t acc[RW][CP];
+#pragma unroll
+    for (int r = 0; r < RW; ++r)
+#pragma unroll
+        for (int c = 0; c < CP; ++c) acc[r][c] = INF2;
+    warp_minplus_list<RW, CP>(acc, kl, nA, warp, Xp, P.ldv, D + (live_col ? col : n0), L.NP);
+    cta_reduce<RW, CP>(acc, red);
+    if (warp == 0 && live_col) {
+        uint16_t* Y = P.Y[l & 1];
+#pragma unroll
+        for (int cc = 0; cc < 2 * CP; ++cc) {
+            uint16_t v[RW];
+#pragma unroll
+            for (int r = 0; r < RW; ++r)
+                v[r] = (uint16_t)((cc & 1) ? (acc[r][cc >> 1] >> 16) : (acc[r][cc >> 1] & 0xffffu));
+            if (L.store_y) {
+                uint16_t* y = Y + (size_t)(col + cc) * P.ldv + slot0 + m0;
+#pragma unroll
+                for (int r8 = 0; r8 < RW / 8; ++r8) {
+                    uint4 o;
+                    o.x = v[8 * r8] | ((uint32_t)v[8 * r8 + 1] << 16);
+                    o.y = v[8 * r8 + 2] | ((uint32_t)v[8 * r8 + 3] << 16);
+                    o.z = v[8 * r8 + 4] | ((uint32_t)v[8 * r8 + 5] << 16);
+                    o.w = v[8 * r8 + 6] | ((uint32_t)v[8 * r8 + 7] << 16);
+                    reinterpret_cast<uint4*>(y)[r8] = o;
+                }
+            }
+            if (Ln) {  // lift: exterior column e of this node -> X_l[e][level-(l+1) slot]
+                const int e = L.ext_inv[col + cc];
+                if (e >= 0) {
+                    uint16_t* Xn = P.X[l % 3] + (size_t)e * P.ldv;
+#pragma unroll
+                    for (int r = 0; r < RW; ++r) {
+                        if (m0 + r < cnt) {
+                            const int* ls = L.lift + 2 * (slot0 + m0 + r);
+                            Xn[ls[0]] = v[r];
+                            if (v[r] < INF) Ln->flags[(size_t)ls[1] * Ln->nP + e] = 1;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();  // kl / red are reused by the next item
+}
+
+// meet item {i0, j0, nj, g2, coloff, kb, ke}: rows = RW viewpoints j of
+// child group g2 (slots j0..), lanes = 64*CP viewpoint slots i (from i0).
+template <int RW, int CP>
+__device__ void do_meet(const QueryParams& P, const QueryLevel& L, int item, int l, int* kl, int* wsum,
+                        uint32_t* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int* it = L.meet + 7 * item;
+    const int i0 = it[0], j0 = it[1], nj = it[2], g2 = it[3], coloff = it[4], kb = it[5], ke = it[6];
+    const int nA = compact_flags(L.flags + (size_t)g2 * L.nP, kb, ke, kl, wsum);
+    const uint16_t* Xp = P.X[(l - 1) % 3] + j0;
+    const uint16_t* Y = P.Y[l & 1] + (size_t)coloff * P.ldv + i0 + lane * 2 * CP;
+    uint32_t acc[RW][CP];
+#pragma unroll
+    for (int r = 0; r < RW; ++r)
+#pragma unroll
+        for (int c = 0; c < CP; ++c) acc[r][c] = INF2;
+    warp_minplus_list<RW, CP>(acc, kl, nA, warp, Xp, P.ldv, Y, P.ldv);
+    cta_reduce<RW, CP>(acc, red);
+    if (warp == 0) {
+#pragma unroll
+        for (int r = 0; r < RW; ++r) {
+            if (r >= nj) break;
+            const int vj = L.s2v[j0 + r];
+#pragma unroll
+            for (int cc = 0; cc < 2 * CP; ++cc) {
+                const int vi = L.s2v[i0 + lane * 2 * CP + cc];
+                const uint32_t v = (cc & 1) ? (acc[r][cc >> 1] >> 16) : (acc[r][cc >> 1] & 0xffffu);
+                if (vi >= 0 && vi < vj && v < INF) atomicMin(&P.M[(size_t)vi * P.ldm + vj], v);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <int RW, int CP>
+__global__ void __launch_bounds__(kThreads, 1) q_persistent_kernel(const QueryParams* __restrict__ Pp) {
+    extern __shared__ __align__(16) int qsm[];
+    int* kl = qsm;
+    uint32_t* red = reinterpret_cast<uint32_t*>(qsm + kMaxList);
+    __shared__ int wsum[kWarps];
+    const QueryParams& P = *Pp;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nt = gridDim.x * blockDim.x;
+    // level 0: X0 in level-1 slot order (+ level-1 flags), same-leaf pairs
+    {
+        const int S1 = P.n_l0_slots;
+        const int total = S1 * P.nExt0;
+        for (int t = gt; t < total; t += nt) {
+            const int p = t / S1, s = t - p * S1;
+            const int j = P.l0[2 * s];
+            if (j < 0) continue;
+            const int* v = P.vp0 + 4 * j;
+            const uint16_t d = P.leaves.base[((size_t)v[0] * P.leaves.NP + v[1]) * P.leaves.NP + P.ext0[p]];
+            P.X[0][(size_t)p * P.ldv + s] = d;
+            if (d < INF && P.H >= 1) P.lv[1].flags[(size_t)P.l0[2 * s + 1] * P.nExt0 + p] = 1;
+        }
+        for (int j = gt; j < P.ns; j += nt) {
+            const int* v = P.vp0 + 4 * j;
+            const uint16_t* row = P.leaves.base + ((size_t)v[0] * P.leaves.NP + v[1]) * P.leaves.NP;
+            for (int jj = j + 1; jj < v[3]; ++jj) P.M[(size_t)j * P.ldm + jj] = row[P.vp0[4 * jj + 1]];
+        }
+    }
+    if (!grid_barrier(P.bar, P.status)) return;
+    for (int l = 1; l <= P.H + 1; ++l) {
+        const int lp = l <= P.H ? l : 0;  // project level of this phase
+        const int lm = l - 1;              // meet level of this phase
+        const QueryLevel* Lp = lp >= 1 ? &P.lv[lp] : nullptr;
+        const QueryLevel* Lm = lm >= 1 ? &P.lv[lm] : nullptr;
+        const QueryLevel* Ln = (lp >= 1 && lp < P.H) ? &P.lv[lp + 1] : nullptr;
+        const int np = Lp ? Lp->n_items : 0;
+        const int nm = Lm ? Lm->n_meet : 0;
+        for (int w = blockIdx.x; w < np + nm; w += gridDim.x) {
+            if (w < np) do_project<RW, CP>(P, *Lp, Ln, w, lp, kl, wsum, red);
+            else do_meet<RW, CP>(P, *Lm, w - np, lm, kl, wsum, red);
+        }
+        if (!grid_barrier(P.bar, P.status)) return;
+    }
+    // finalize: out[a][c]
+    for (int t = gt; t < P.k * P.k; t += nt) {
+        const int a = t / P.k, c = t - a * P.k;
+        const int ia = P.inv[a], ic = P.inv[c];
+        uint32_t v = INF;
+        if (ia >= 0 && ic >= 0) {
+            if (ia == ic) v = 0;
+            else v = min(ia < ic ? P.M[(size_t)ia * P.ldm + ic] : P.M[(size_t)ic * P.ldm + ia], (uint32_t)INF);
+        }
+        P.out[t] = (uint16_t)v;
+    }
+}
+
+}  // namespace
+
+// Tile shapes (rows RW x columns 64*CP per warp item) of the configurations
+// the persistent kernel implements; the autotuner picks one per level.
+QueryTile query_config_tile(int cfg) {
+    static const QueryTile t[kNumQueryConfigs] = {{8, 64}, {8, 128}, {16, 128}, {8, 256}};
+    return t[cfg];
+}
+
+int query_default_config(int NP, int max_group) {
+    if (max_group >= 12) return 2;
+    return NP >= 256 ? 1 : 0;
+}
+
+namespace {
+typedef void (*QueryKernel)(const QueryParams*);
+const QueryKernel kQueryKernels[kNumQueryConfigs] = {q_persistent_kernel<8, 1>, q_persistent_kernel<8, 2>,
+                                                     q_persistent_kernel<16, 2>, q_persistent_kernel<8, 4>};
+const size_t kQuerySmem[kNumQueryConfigs] = {query_smem_bytes<8, 1>(), query_smem_bytes<8, 2>(),
+                                             query_smem_bytes<16, 2>(), query_smem_bytes<8, 4>()};
+
+void configure_query_kernels() {
+    static bool done = false;
+    if (done) return;
+    for (int c = 0; c < kNumQueryConfigs; ++c)
+        cudaFuncSetAttribute(kQueryKernels[c], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kQuerySmem[c]);
+    done = true;
+}
+}  // namespace
+
+int query_max_ports() { return kMaxList - 64; }
+
+int query_grid_blocks(int device) {
+    configure_query_kernels();
+    int sms = 0, per = 1 << 30;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    for (int c = 0; c < kNumQueryConfigs; ++c) {
+        int p = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, kQueryKernels[c], kThreads, kQuerySmem[c]);
+        per = std::min(per, p);
+    }
+    return sms * std::max(1, per);
+}
+
+cudaError_t launch_query(const QueryParams* P_dev, int cfg, int grid, cudaStream_t st) {
+    configure_query_kernels();
+    void* args[] = {const_cast<QueryParams**>(&P_dev)};
+    return cudaLaunchCooperativeKernel((const void*)kQueryKernels[cfg], dim3(grid), dim3(kThreads), args,
+                                       kQuerySmem[cfg], st);
+}
+
+}  // namespace hb
