@@ -129,6 +129,9 @@ struct htrip_index {
     DevBuf<int> qstatus;
     DevBuf<unsigned> qbar;
     int qgrid = 0;
+    cudaEvent_t qev[2] = {nullptr, nullptr};
+    bool qev_valid = false;
+    uint64_t last_h2d = 0, last_d2h = 0;
     DevBuf<uint8_t> qparams;
     alignas(16) unsigned char h_qparams[sizeof(hb::QueryParams)];
     DevBuf<uint32_t> qM;
@@ -745,7 +748,16 @@ void run_query(htrip_index* h, const QueryPlan& P, uint16_t* out_dev) {
     h->qparams.reserve(sizeof(hb::QueryParams));
     std::memcpy(h->h_qparams, &Q, sizeof(Q));
     ck(cudaMemcpyAsync(h->qparams.p, h->h_qparams, sizeof(Q), cudaMemcpyHostToDevice, st), "params");
+    h->last_h2d = P.buf.size() * sizeof(int) + sizeof(Q);
+    h->last_d2h = 0;
+    if (!h->qev[0]) {
+        ck(cudaEventCreate(&h->qev[0]), "event");
+        ck(cudaEventCreate(&h->qev[1]), "event");
+    }
+    ck(cudaEventRecord(h->qev[0], st), "event");
     ck(hb::launch_query(reinterpret_cast<const hb::QueryParams*>(h->qparams.p), P.cfg, h->qgrid, st), "query kernel");
+    ck(cudaEventRecord(h->qev[1], st), "event");
+    h->qev_valid = true;
 }
 
 int choose_query_cfg(const htrip_index* h, int ns, int root_group) {
@@ -803,6 +815,8 @@ htrip_status htrip_destroy(htrip_index* h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->release();
+    for (auto& e : h->qev)
+        if (e) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return HTRIP_OK;
@@ -867,6 +881,7 @@ htrip_status htrip_query_all_pairs(htrip_index* h, const int32_t* vps, int32_t k
     int status = 0;
     ck(cudaMemcpyAsync(out, h->qout.p, (size_t)k * k * sizeof(uint16_t), cudaMemcpyDeviceToHost, h->stream), "out");
     ck(cudaMemcpyAsync(&status, h->qstatus.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "status");
+    h->last_d2h = (uint64_t)k * k * sizeof(uint16_t) + sizeof(int);
     ck(cudaStreamSynchronize(h->stream), "query sync");
     if (status != 0) {
         cudaMemsetAsync(h->qstatus.p, 0, sizeof(int), h->stream);
@@ -897,6 +912,7 @@ htrip_status htrip_query_all_pairs_dev(htrip_index* h, const int32_t* vps_dev, c
     QueryPlan P;
     make_plan(h, vps.data(), pf.data(), k, P);
     run_query(h, P, out_dev);
+    h->last_d2h = vps.size() * sizeof(int32_t) + pf.size();
     return HTRIP_OK;
     HTRIP_GUARD_END
 }
@@ -933,6 +949,74 @@ htrip_status htrip_clone(const htrip_index* src, htrip_index** out) {
     *out = h;
     return HTRIP_OK;
     HTRIP_GUARD_END
+}
+
+htrip_status htrip_query_work(const htrip_index* h, const int32_t* vps, int32_t k, const uint8_t* observed,
+                              int32_t rows, int32_t cols, uint64_t* alg_bytes, uint64_t* alg_ops) {
+    if (!h || !h->built || k < 0 || (k > 0 && !vps) || !observed) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    const int b = h->b, g = h->g, H = h->H;
+    uint64_t bytes = 0, ops = 0;
+    std::vector<int> tx, ty;
+    for (int i = 0; i < k; ++i) {
+        const int r = vps[2 * i], c = vps[2 * i + 1];
+        if (r < 0 || c < 0 || r >= rows || c >= cols || observed[(size_t)r * cols + c] != 1) continue;
+        tx.push_back(c / b);
+        ty.push_back(r / b);
+    }
+    const uint64_t n = tx.size();
+    bytes += n * (uint64_t)h->L[0].nExt * 2;  // level-0 port gathers
+    for (int l = 1; l <= H; ++l) {
+        const Level& Lv = h->L[l];
+        const Level& Lc = h->L[l - 1];
+        const uint64_t nP = Lv.nP, nExt = Lv.nExt;
+        // viewpoint count per (node, quad)
+        std::vector<std::pair<int, int>> key;
+        for (size_t i = 0; i < n; ++i) {
+            const int cx = tx[i] * b / Lc.side, cy = ty[i] * b / Lc.side;
+            key.push_back({(cy / g) * Lv.nodes_x + cx / g, (cy % g) * g + cx % g});
+        }
+        std::sort(key.begin(), key.end());
+        for (size_t i = 0; i < key.size();) {
+            size_t j = i;
+            while (j < key.size() && key[j].first == key[i].first) ++j;
+            std::vector<uint64_t> cnt;  // per active child of this node
+            for (size_t a = i; a < j;) {
+                size_t c = a;
+                while (c < j && key[c].second == key[a].second) ++c;
+                cnt.push_back(c - a);
+                a = c;
+            }
+            for (size_t a = 0; a < cnt.size(); ++a) {
+                if (l < H) { bytes += nP * nExt * 2; ops += cnt[a] * nP * nExt; }
+                for (size_t c = a + 1; c < cnt.size(); ++c) {
+                    bytes += nP * nP * 2;
+                    ops += cnt[a] * nP * nP + cnt[a] * cnt[c] * nP;
+                }
+                if (cnt[a] >= 2) { bytes += nP * nP * 2; ops += cnt[a] * nP * nP + cnt[a] * cnt[a] * nP; }
+            }
+            i = j;
+        }
+    }
+    if (alg_bytes) *alg_bytes = bytes;
+    if (alg_ops) *alg_ops = ops;
+    return HTRIP_OK;
+}
+
+htrip_status htrip_last_query_kernel_ms(const htrip_index* h, float* ms) {
+    if (!h || !ms) return fail(HTRIP_ERR_INVALID, "null argument");
+    if (!h->qev_valid) return fail(HTRIP_ERR_INVALID, "no query has run");
+    HTRIP_GUARD_BEGIN
+    ck(cudaEventSynchronize(h->qev[1]), "event sync");
+    ck(cudaEventElapsedTime(ms, h->qev[0], h->qev[1]), "event time");
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_last_query_io(const htrip_index* h, uint64_t* h2d_bytes, uint64_t* d2h_bytes) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    if (h2d_bytes) *h2d_bytes = h->last_h2d;
+    if (d2h_bytes) *d2h_bytes = h->last_d2h;
+    return HTRIP_OK;
 }
 
 htrip_status htrip_sync(htrip_index* h) {

@@ -51,7 +51,8 @@ EXPORTS = (
     "htrip_last_error", "htrip_create", "htrip_destroy", "htrip_clone", "htrip_build", "htrip_open_cells",
     "htrip_open_cell", "htrip_query_all_pairs", "htrip_query_all_pairs_dev", "htrip_sync", "htrip_stream",
     "htrip_shape", "htrip_last_batch_stats", "htrip_memory_bytes", "htrip_read_leaf_D", "htrip_read_leaf_S",
-    "htrip_read_node_DU", "htrip_read_node_SU", "htrip_read_node_C2E", "htrip_level_dims",
+    "htrip_read_node_DU", "htrip_read_node_SU", "htrip_read_node_C2E", "htrip_level_dims", "htrip_query_work",
+    "htrip_last_query_kernel_ms", "htrip_last_query_io",
 )
 
 
@@ -87,6 +88,9 @@ def load_library(path: str | None = None):
         getattr(lib, f).argtypes = [P, I, I, _U16P]
     lib.htrip_read_node_C2E.argtypes = [P, I, I, I, _U16P]
     lib.htrip_level_dims.argtypes = [P, I, _I32P, _I32P, _I32P, _I32P]
+    lib.htrip_query_work.argtypes = [P, _I32P, I, _U8P, I, I, _U64P, _U64P]
+    lib.htrip_last_query_kernel_ms.argtypes = [P, C.POINTER(C.c_float)]
+    lib.htrip_last_query_io.argtypes = [P, _U64P, _U64P]
     for f in EXPORTS:
         if f not in ("htrip_last_error", "htrip_stream"):
             getattr(lib, f).restype = C.c_int
@@ -242,6 +246,26 @@ class MinPlusOracle:
         """Stream-ordered query on device-resident inputs (see htrip_query_all_pairs_dev)."""
         _check(self.lib.htrip_query_all_pairs_dev(self.h, C.c_void_p(vps_dev_ptr), C.c_void_p(passable_dev_ptr),
                                                   k, C.c_void_p(out_dev_ptr)))
+
+    def queryWork(self, viewpoints, grid):
+        """(algorithmic bytes, min-plus ops) of queryAllPairs on these viewpoints."""
+        rc = _rc(viewpoints)
+        obs, ptr, rows, cols = _grid_args(grid)
+        b, o = C.c_uint64(), C.c_uint64()
+        _check(self.lib.htrip_query_work(self.h, rc.ctypes.data_as(_I32P), len(rc), ptr, rows, cols,
+                                         C.byref(b), C.byref(o)))
+        return b.value, o.value
+
+    def lastQueryKernelMs(self) -> float:
+        ms = C.c_float()
+        _check(self.lib.htrip_last_query_kernel_ms(self.h, C.byref(ms)))
+        return ms.value
+
+    def lastQueryIO(self):
+        """(host->device, device->host) bytes copied by the last query call."""
+        a, b = C.c_uint64(), C.c_uint64()
+        _check(self.lib.htrip_last_query_io(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def stream(self) -> int:
         return int(self.lib.htrip_stream(self.h) or 0)

@@ -103,6 +103,21 @@ htrip_status htrip_query_all_pairs_dev(htrip_index* h, const int32_t* vps_dev,
                                        const uint8_t* passable_dev, int32_t k,
                                        uint16_t* out_dev);
 
+/* Measurement helpers (no reference counterpart).
+ * htrip_query_work: the algorithmic HBM bytes and min-plus operations of a
+ * queryAllPairs on these viewpoints: k*(4b-4) level-0 gathers; per level and
+ * node, per child holding viewpoints a lift of nP*nExt entries (below the
+ * root), per child pair a meet block of nP*nP, per child with >= 2
+ * viewpoints an intra-child block of nP*nP (2 bytes each); operations
+ * |V|*nP*nExt per lift, |V1|*nP*nP + |V1|*|V2|*nP per meet, |V|*nP*nP +
+ * |V|^2*nP per intra-child block.
+ * htrip_last_query_kernel_ms: device time of the last query kernel.
+ * htrip_last_query_io: host<->device bytes the last query call copied.     */
+htrip_status htrip_query_work(const htrip_index* h, const int32_t* vps, int32_t k, const uint8_t* observed,
+                              int32_t rows, int32_t cols, uint64_t* alg_bytes, uint64_t* alg_ops);
+htrip_status htrip_last_query_kernel_ms(const htrip_index* h, float* ms);
+htrip_status htrip_last_query_io(const htrip_index* h, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
+
 /* Wait for all work queued on the index's stream.                         */
 htrip_status htrip_sync(htrip_index* h);
 
