@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <numeric>
 #include <string>
@@ -766,6 +767,43 @@ int choose_query_cfg(const htrip_index* h, int ns, int root_group) {
     return root_group >= 24 ? 2 : 1;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free query scratch (htrip_query_all_pairs_noalloc).
+//
+// Some callers cannot allocate device memory once they are running: a
+// serving process whose pool allocator reserved all of HBM at start-up, or a
+// real-time planning loop where cudaMalloc / cudaFree (cudaFree waits for the
+// whole device) are not allowed after initialisation.  For them the query's
+// device scratch (plan, port vectors, projections, pair matrix, flags,
+// barrier words, parameter block and output staging) is carved from this
+// fixed array instead of the index's own growable buffers.  Every GPU that
+// loads this module holds the array until the process exits.
+//
+// In host code `g_noalloc_scratch` is only a host-side stand-in for the
+// symbol; the device address is looked up once per device with
+// cudaGetSymbolAddress (with that device current) and cached.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocScratchBytes = size_t(64) << 20;  // 64 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;                                  // guards set-up and serialises calls
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};    // device address per ordinal
+
+// Device address of the scratch array on the current device `dev`
+// (the first call on a device performs the look-up).
+unsigned char* noalloc_scratch(int dev) {
+    if (dev < 0 || dev >= kNoAllocMaxDevices) throw CudaError{cudaErrorInvalidDevice, "device ordinal above 63"};
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        ck(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(static scratch)");
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    return g_noalloc_ptr[dev];
+}
+
+inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
 }  // namespace
 
 // ===========================================================================
@@ -913,6 +951,116 @@ htrip_status htrip_query_all_pairs_dev(htrip_index* h, const int32_t* vps_dev, c
     make_plan(h, vps.data(), pf.data(), k, P);
     run_query(h, P, out_dev);
     h->last_d2h = vps.size() * sizeof(int32_t) + pf.size();
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+// Same query as htrip_query_all_pairs, with every piece of device scratch
+// carved from the fixed module-scope array above: no cudaMalloc / cudaFree
+// and no growth of the index's own buffers.  A process-wide lock is held
+// from the first write to the array until the result is back on the host,
+// so calls through this entry point never overlap on the GPU (calls that
+// did overlap would race on the shared array).
+htrip_status htrip_query_all_pairs_noalloc(htrip_index* h, const int32_t* vps, int32_t k, const uint8_t* observed,
+                                           int32_t rows, int32_t cols, uint16_t* out) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    if (!h->built) return fail(HTRIP_ERR_NOT_BUILT, "index not built");
+    if (k < 0 || (k > 0 && (!vps || !out)) || !observed) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    if (k == 0) return HTRIP_OK;
+    const int H = h->H;
+    if (H > hb::kMaxQueryLevels) return fail(HTRIP_ERR_UNSUPPORTED, "hierarchy deeper than the query supports");
+    for (int l = 1; l <= H; ++l)
+        if (h->L[l].nP > hb::query_max_ports())
+            return fail(HTRIP_ERR_UNSUPPORTED, "child port count above the query kernel's list capacity");
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    std::vector<uint8_t> pf(k);
+    for (int i = 0; i < k; ++i) {
+        const int r = vps[2 * i], c = vps[2 * i + 1];
+        pf[i] = (r >= 0 && c >= 0 && r < rows && c < cols && observed[(size_t)r * cols + c] == 1 && r < h->S && c < h->S);
+    }
+    QueryPlan P;
+    make_plan(h, vps, pf.data(), k, P);
+    // Scratch layout (every piece 256-byte aligned).
+    int maxExt = 0, maxNP = 64;
+    for (int l = 0; l <= H; ++l) maxExt = std::max(maxExt, h->L[l].nExt);
+    for (int l = 1; l <= H; ++l) maxNP = std::max(maxNP, h->L[l].NP);
+    size_t off = 0;
+    auto take = [&](size_t bytes) { const size_t o = off; off += align256(std::max<size_t>(bytes, 1)); return o; };
+    const size_t o_params = take(sizeof(hb::QueryParams));
+    const size_t o_words = take(4 * sizeof(unsigned));  // {status, barrier count, barrier generation}
+    const size_t o_plan = take(P.buf.size() * sizeof(int));
+    const size_t o_M = take((size_t)P.ldm * P.ldm * sizeof(uint32_t));
+    const size_t o_flags = take(P.flags_total);
+    size_t o_X[3], o_Y[2];
+    for (auto& o : o_X) o = take((size_t)maxExt * P.ldv * sizeof(uint16_t));
+    for (auto& o : o_Y) o = take((size_t)maxNP * P.ldv * sizeof(uint16_t));
+    const size_t o_out = take((size_t)k * k * sizeof(uint16_t));
+    if (off > kNoAllocScratchBytes)
+        return fail(HTRIP_ERR_UNSUPPORTED, "query needs " + std::to_string(off) +
+                                               " bytes of device scratch; the allocation-free entry point has " +
+                                               std::to_string(kNoAllocScratchBytes) + " (fewer viewpoints or a smaller map)");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    unsigned char* base = noalloc_scratch(h->device);
+    cudaStream_t st = h->stream;
+    int* words = reinterpret_cast<int*>(base + o_words);
+    int* plan = reinterpret_cast<int*>(base + o_plan);
+    uint32_t* M = reinterpret_cast<uint32_t*>(base + o_M);
+    uint8_t* flags = base + o_flags;
+    uint16_t* dout = reinterpret_cast<uint16_t*>(base + o_out);
+    // The array keeps the previous call's contents: reset what must start cleared.
+    ck(cudaMemcpyAsync(plan, P.buf.data(), P.buf.size() * sizeof(int), cudaMemcpyHostToDevice, st), "plan");
+    ck(cudaMemsetAsync(words, 0, 4 * sizeof(unsigned), st), "barrier words");
+    ck(cudaMemsetAsync(M, 0xFF, (size_t)P.ldm * P.ldm * sizeof(uint32_t), st), "M");
+    if (P.flags_total) ck(cudaMemsetAsync(flags, 0, P.flags_total, st), "flags");
+    hb::QueryParams Q{};
+    Q.H = H;
+    Q.k = P.k;
+    Q.ns = P.n_sorted;
+    Q.ldv = P.ldv;
+    Q.ldm = P.ldm;
+    Q.n_l0_slots = P.n_l0;
+    Q.nExt0 = h->L[0].nExt;
+    Q.cfg = P.cfg;
+    Q.vp0 = plan + P.o_vp0;
+    Q.inv = plan + P.o_inv;
+    Q.l0 = plan + P.o_l0;
+    Q.ext0 = h->L[0].d_ext.p;
+    Q.leaves = h->L[0].ms();
+    for (int i = 0; i < 3; ++i) Q.X[i] = reinterpret_cast<uint16_t*>(base + o_X[i]);
+    for (int i = 0; i < 2; ++i) Q.Y[i] = reinterpret_cast<uint16_t*>(base + o_Y[i]);
+    Q.M = M;
+    Q.out = dout;
+    Q.status = words;
+    Q.bar = reinterpret_cast<unsigned*>(words + 1);
+    for (int l = 1; l <= H; ++l) {
+        const Level& Lv = h->L[l];
+        const QueryPlan::Lvl& L = P.lv[l];
+        hb::QueryLevel& q = Q.lv[l];
+        q.D = Lv.mat.p;
+        q.NP = Lv.NP;
+        q.nP = Lv.nP;
+        q.ext_inv = Lv.d_ext_inv.p;
+        q.groups = plan + L.o_groups;
+        q.flags = flags + L.flags_off;
+        q.items = plan + L.o_items;
+        q.n_items = L.n_items;
+        q.meet = plan + L.o_meet;
+        q.n_meet = L.n_meet;
+        q.s2v = plan + L.o_s2v;
+        q.lift = l < H ? plan + L.o_lift : nullptr;
+        q.store_y = 1;
+    }
+    if (h->qgrid == 0) h->qgrid = hb::query_grid_blocks(h->device);
+    // Pageable host -> device: the call returns once the source is staged.
+    ck(cudaMemcpyAsync(base + o_params, &Q, sizeof(Q), cudaMemcpyHostToDevice, st), "params");
+    ck(hb::launch_query(reinterpret_cast<const hb::QueryParams*>(base + o_params), P.cfg, h->qgrid, st),
+       "query kernel");
+    int status = 0;
+    ck(cudaMemcpyAsync(out, dout, (size_t)k * k * sizeof(uint16_t), cudaMemcpyDeviceToHost, st), "out");
+    ck(cudaMemcpyAsync(&status, words, sizeof(int), cudaMemcpyDeviceToHost, st), "status");
+    ck(cudaStreamSynchronize(st), "query sync");
+    if (status != 0) return fail(HTRIP_ERR_CUDA, "query kernel: grid barrier timed out");
     return HTRIP_OK;
     HTRIP_GUARD_END
 }

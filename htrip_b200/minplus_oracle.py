@@ -52,7 +52,7 @@ EXPORTS = (
     "htrip_open_cell", "htrip_query_all_pairs", "htrip_query_all_pairs_dev", "htrip_sync", "htrip_stream",
     "htrip_shape", "htrip_last_batch_stats", "htrip_memory_bytes", "htrip_read_leaf_D", "htrip_read_leaf_S",
     "htrip_read_node_DU", "htrip_read_node_SU", "htrip_read_node_C2E", "htrip_level_dims", "htrip_query_work",
-    "htrip_last_query_kernel_ms", "htrip_last_query_io",
+    "htrip_last_query_kernel_ms", "htrip_last_query_io", "htrip_query_all_pairs_noalloc",
 )
 
 
@@ -76,6 +76,7 @@ def load_library(path: str | None = None):
     lib.htrip_open_cell.argtypes = [P, I, I, _U8P, I, I]
     lib.htrip_query_all_pairs.argtypes = [P, _I32P, I, _U8P, I, I, _U16P]
     lib.htrip_query_all_pairs_dev.argtypes = [P, C.c_void_p, C.c_void_p, I, C.c_void_p]
+    lib.htrip_query_all_pairs_noalloc.argtypes = [P, _I32P, I, _U8P, I, I, _U16P]
     lib.htrip_sync.argtypes = [P]
     lib.htrip_stream.restype = C.c_void_p
     lib.htrip_stream.argtypes = [P]
@@ -240,6 +241,21 @@ class MinPlusOracle:
         obs, ptr, rows, cols = _grid_args(grid)
         _check(self.lib.htrip_query_all_pairs(self.h, rc.ctypes.data_as(_I32P), k, ptr, rows, cols,
                                               out.ctypes.data_as(_U16P)))
+        return out
+
+    def queryAllPairsNoAlloc(self, viewpoints, grid, out: np.ndarray | None = None) -> np.ndarray:
+        """queryAllPairs through htrip_query_all_pairs_noalloc: the device
+        scratch comes from the library's fixed 64 MiB array, nothing is
+        allocated on the device (for callers that may not allocate)."""
+        rc = _rc(viewpoints)
+        k = len(rc)
+        if out is None or out.shape != (k, k) or out.dtype != np.uint16 or not out.flags.c_contiguous:
+            out = np.empty((k, k), dtype=np.uint16)
+        if k == 0:
+            return out
+        obs, ptr, rows, cols = _grid_args(grid)
+        _check(self.lib.htrip_query_all_pairs_noalloc(self.h, rc.ctypes.data_as(_I32P), k, ptr, rows, cols,
+                                                      out.ctypes.data_as(_U16P)))
         return out
 
     def queryAllPairsDevice(self, vps_dev_ptr: int, passable_dev_ptr: int, k: int, out_dev_ptr: int):

@@ -103,6 +103,28 @@ htrip_status htrip_query_all_pairs_dev(htrip_index* h, const int32_t* vps_dev,
                                        const uint8_t* passable_dev, int32_t k,
                                        uint16_t* out_dev);
 
+/* Allocation-free queryAllPairs (no counterpart in the reference).
+ * For callers that may not allocate device memory after start-up, e.g. a
+ * serving process whose pool allocator already holds all of HBM, or a
+ * real-time planning loop where cudaMalloc / cudaFree (which waits for the
+ * whole device) are forbidden.  Same arguments, result and errors as
+ * htrip_query_all_pairs (host viewpoints and grid in, host k*k matrix out);
+ * all device scratch comes from one fixed 64 MiB array compiled into the
+ * library, which every GPU that loads it holds until the process exits.
+ *  - No cudaMalloc / cudaFree / allocating library routine is called.
+ *  - A query whose scratch would exceed 64 MiB is rejected with
+ *    HTRIP_ERR_UNSUPPORTED and a message giving the bytes it needs (it
+ *    grows with k^2 and with k times the map side).
+ *  - The first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - All calls on a device share the array and it keeps the last call's
+ *    contents (every call clears what must start cleared).  Calls that
+ *    overlapped on the GPU would race on it, so this entry point holds a
+ *    process-wide lock until its result is on the host.                   */
+htrip_status htrip_query_all_pairs_noalloc(htrip_index* h, const int32_t* vps, int32_t k,
+                                           const uint8_t* observed, int32_t rows, int32_t cols,
+                                           uint16_t* out);
+
 /* Measurement helpers (no reference counterpart).
  * htrip_query_work: the algorithmic HBM bytes and min-plus operations of a
  * queryAllPairs on these viewpoints: k*(4b-4) level-0 gathers; per level and
