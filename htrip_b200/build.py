@@ -16,6 +16,9 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libhtrip_b200.so")
+CPP_LIB = os.path.join(PKG, "libhtrip.so")   # C++20 htrip::MinPlusOracle drop-in
+HOST = os.path.join(PKG, "host")
+CXX = os.environ.get("CXX", "g++")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -41,6 +44,28 @@ def up_to_date(target, inputs):
 
 
 def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
+    """Build libhtrip_b200.so (CUDA, sm_100a) and the C++ drop-in libhtrip.so."""
+    lib = build_cuda(force, verbose, ptxas_info)
+    build_cpp(force, verbose)
+    return lib
+
+
+def build_cpp(force: bool = False, verbose: bool = False) -> str:
+    """libhtrip.so: the C++20 htrip::MinPlusOracle of include/htrip/, linked
+    against libhtrip_b200.so (found next to it through an $ORIGIN rpath)."""
+    srcs = sorted(glob.glob(os.path.join(HOST, "*.cpp")))
+    inputs = srcs + [LIB] + sorted(glob.glob(os.path.join(ROOT, "include", "htrip", "*.hpp")))
+    if not force and up_to_date(CPP_LIB, inputs):
+        return CPP_LIB
+    cmd = [CXX, "-std=c++20", "-O2", "-fPIC", "-shared", "-Wall", "-Wextra", "-I" + os.path.join(ROOT, "include"),
+           "-o", CPP_LIB, *srcs, "-L" + PKG, "-lhtrip_b200", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return CPP_LIB
+
+
+def build_cuda(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
     if not force and not ptxas_info and up_to_date(LIB, deps()):
         return LIB
     objdir = os.path.join(PKG, "_build")

@@ -1,0 +1,143 @@
+// htrip_b200 C++20 drop-in for htrip::MinPlusOracle.
+//
+// Same class name, members and call signatures as the reference's
+// include/htrip/minplus_oracle.hpp (ozaslan/htrip), so callers compile
+// unchanged; the index itself lives in the HBM of one CUDA device and every
+// method calls the C ABI of include/htrip_b200.h (libhtrip_b200.so):
+//
+//   explicit MinPlusOracle(HierarchyConfig)              minplus_oracle.hpp:59
+//   bool build(const GridMap&)                           :78
+//   int depth() const                                    :83
+//   leafIndex / tileIndexAtLevel / findLcaLevel          :88, :95, :370
+//   void onCellOpened(Point, const GridMap&)             :109
+//   void onBatchCellsOpened(const std::vector<Point>&,
+//                           const GridMap&)              :171
+//   struct HTripQueryScratch (caller-owned, reused)      :189-238
+//   struct LastBatchStats / last_batch_stats             :251-256
+//   void queryAllPairs(vps, grid, out, scratch) const    :337-341
+//   std::vector<dist_t> queryAllPairs(vps, grid) const   :348-349
+//   size_t totalMemoryBytes() const                      :385
+//   copy construction / assignment (deep copy, as the reference's
+//   value-type oracle: bench_update_latency.cpp:178,186)
+//
+// Behaviour shared with the reference: build returns false on an invalid
+// config or an empty grid; cells and viewpoints outside the grid are
+// ignored / answered with INF rows; a viewpoint that is not Free has an INF
+// row, column and diagonal.  Differences: the index is not a host object
+// (no `leaves` / `levels` members; use numLeaves()), hybrid_k_threshold is
+// ignored (there is no CPU fallback), and a CUDA failure throws DeviceError.
+// A MinPlusOracle is not thread-safe; distinct oracles may be used from
+// different threads (each owns a CUDA stream).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "grid_map.hpp"
+#include "types.hpp"
+
+struct htrip_index;  // opaque device index (include/htrip_b200.h)
+
+namespace htrip {
+
+// A CUDA or device-side failure inside the library (the reference has no
+// failure mode there).  `status` is the htrip_status of the C ABI.
+class DeviceError : public std::runtime_error {
+public:
+    DeviceError(int status, const std::string& msg) : std::runtime_error(msg), status(status) {}
+    int status;
+};
+
+class MinPlusOracle {
+public:
+    HierarchyConfig config;
+    int S = 0;
+    int H = 0;
+    int num_leaf_tiles_x = 0;
+    int num_leaf_tiles_y = 0;
+
+    struct LastBatchStats {
+        int n_touched_leaves = 0;
+        int n_dirty_ancestors = 0;
+        int n_pivots = 0;
+    };
+    LastBatchStats last_batch_stats{};
+
+    uint32_t update_counter = 0;  // incremented by every update call
+    uint64_t epoch = 0;           // incremented by every build
+
+    // Caller-owned query workspace, reused across calls so that a warm query
+    // does not allocate host memory.  The device workspace belongs to the
+    // oracle and is kept between calls.
+    struct HTripQueryScratch {
+        std::vector<int32_t> rc;  // viewpoints as (row, col) int32 pairs
+
+        void ensureCapacity(size_t k, int /*H*/ = 0, size_t /*num_leaves*/ = 0) {
+            if (rc.capacity() < 2 * k) rc.reserve(2 * k);
+        }
+    };
+    mutable HTripQueryScratch query_scratch;  // used by the 2-argument queryAllPairs
+
+    // Index on CUDA device 0 with the default config (b = 16, 2 x 2 groups).
+    MinPlusOracle();
+    // Index on CUDA device `device`.  Throws DeviceError when no CUDA device
+    // is usable (there is no CPU fallback).
+    explicit MinPlusOracle(HierarchyConfig cfg, int device = 0);
+    ~MinPlusOracle();
+    MinPlusOracle(const MinPlusOracle& other);             // deep device-to-device copy
+    MinPlusOracle& operator=(const MinPlusOracle& other);  // deep device-to-device copy
+    MinPlusOracle(MinPlusOracle&& other) noexcept;
+    MinPlusOracle& operator=(MinPlusOracle&& other) noexcept;
+
+    bool build(const GridMap& grid);
+
+    [[nodiscard]] int depth() const noexcept { return H; }
+    [[nodiscard]] int leafIndex(int tx, int ty) const noexcept { return ty * num_leaf_tiles_x + tx; }
+    // Row-major index of tile (tx, ty) among the level-`lvl` tiles (side b*g^lvl).
+    [[nodiscard]] int tileIndexAtLevel(int lvl, int tx, int ty) const noexcept;
+    // Lowest level whose node holds both cells (0: same leaf, H + 1: none).
+    [[nodiscard]] int findLcaLevel(Point p1, Point p2) const noexcept;
+
+    // The caller has already set p (or every cell of the batch) Free in
+    // grid.observed.  onCellOpened leaves last_batch_stats untouched, as the
+    // reference's single-cell path does.
+    void onCellOpened(Point p, const GridMap& grid);
+    void onBatchCellsOpened(const std::vector<Point>& newly_opened, const GridMap& grid);
+
+    // k x k row-major matrix of exact 4-connected distances (INF when
+    // unreachable), resized and filled by the call.
+    void queryAllPairs(const std::vector<Point>& viewpoints, const GridMap& grid, std::vector<dist_t>& out_matrix,
+                       HTripQueryScratch& scratch) const;
+    [[nodiscard]] std::vector<dist_t> queryAllPairs(const std::vector<Point>& viewpoints,
+                                                    const GridMap& grid) const;
+
+    // The reference's accounting of the same index: bytes of every D, S,
+    // D_U, S_U and child_to_ext table.
+    [[nodiscard]] size_t totalMemoryBytes() const noexcept;
+    // Bytes of HBM this index actually holds (arena and workspaces).
+    [[nodiscard]] size_t deviceMemoryBytes() const noexcept;
+    // Number of leaf tiles (the reference's leaves.size()).
+    [[nodiscard]] size_t numLeaves() const noexcept {
+        return size_t(num_leaf_tiles_x) * size_t(num_leaf_tiles_y);
+    }
+    [[nodiscard]] int device() const noexcept { return device_; }
+    // The C ABI handle (for stream-ordered calls of include/htrip_b200.h).
+    [[nodiscard]] htrip_index* handle() const noexcept { return h_; }
+
+private:
+    void create();
+    void destroy() noexcept;
+    void refreshShape();
+
+    htrip_index* h_ = nullptr;
+    int device_ = 0;
+    bool built_ = false;
+    mutable std::vector<int32_t> cells_;  // reused (row, col) staging of update calls
+};
+
+using HTripOracle = MinPlusOracle;
+
+}  // namespace htrip
