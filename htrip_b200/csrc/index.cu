@@ -106,6 +106,46 @@ struct Level {
     MatSet ms() const { return MatSet{mat.p, n, NP}; }
 };
 
+// Pinned host buffer (grows, never shrinks).
+struct HostBuf {
+    unsigned char* p = nullptr;
+    size_t n = 0;
+    void reserve(size_t m) {
+        if (m <= n) return;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+        ck(cudaHostAlloc(reinterpret_cast<void**>(&p), m, cudaHostAllocDefault), "cudaHostAlloc");
+        n = m;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+// Device scratch of query launches: an arena laid out per launch
+// (LaunchLayout), pinned staging of its head and of the results, the grid
+// size of the cooperative kernel and the events around the last launch.
+struct QueryArena {
+    DevBuf<unsigned char> dev;
+    HostBuf stage, outstage;
+    int grid = 0;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    bool ev_valid = false;
+    uint64_t last_h2d = 0, last_d2h = 0;
+    void release() {
+        dev.release();
+        stage.release();
+        outstage.release();
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        ev[0] = ev[1] = nullptr;
+        ev_valid = false;
+    }
+};
+
 }  // namespace
 
 struct htrip_index {
@@ -123,23 +163,15 @@ struct htrip_index {
     DevBuf<int> upd;        // uploaded per-update lists
     DevBuf<uint16_t> snap;
     DevBuf<int> pivots;
-    // query scratch
-    DevBuf<int> qplan;
-    DevBuf<uint16_t> qX[3], qY[2], qout;
-    DevBuf<uint8_t> qflags;
-    DevBuf<int> qstatus;
-    DevBuf<unsigned> qbar;
-    int qgrid = 0;
-    cudaEvent_t qev[2] = {nullptr, nullptr};
-    bool qev_valid = false;
-    uint64_t last_h2d = 0, last_d2h = 0;
-    DevBuf<uint8_t> qparams;
-    alignas(16) unsigned char h_qparams[sizeof(hb::QueryParams)];
-    DevBuf<uint32_t> qM;
-    DevBuf<int> qkidx;
-    DevBuf<int32_t> qvps;
+    // opening read-back: pinned host words (pivots, pivot counts, decrease
+    // flags) and the device array the counts are gathered into
+    int max_nodes = 0;
+    HostBuf rb;
+    DevBuf<int> rb_dev;
+    // query scratch: one device arena per launch (QueryArena) plus pinned
+    // host staging for its parameter block / plans and for the result
+    QueryArena q;
     htrip_batch_stats stats{0, 0, 0};
-    std::vector<int> h_pinned_dummy;
 
     ~htrip_index() { release(); }
     void release() {
@@ -149,9 +181,18 @@ struct htrip_index {
         }
         L.clear();
         pass.release(); panel.release(); pflags.release(); active.release(); upd.release();
-        snap.release(); pivots.release(); qplan.release(); for (auto& x : qX) x.release(); for (auto& y : qY) y.release();
-        qM.release(); qout.release(); qkidx.release(); qvps.release(); qflags.release(); qstatus.release(); qbar.release(); qparams.release();
+        snap.release(); pivots.release(); rb.release(); rb_dev.release();
+        q.release();
     }
+};
+
+// A launch context for batched calls over many indexes of one device
+// (htrip_query_batch / htrip_open_batch): its own stream and query arena.
+struct htrip_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    QueryArena q;
+    ~htrip_batch() { q.release(); }
 };
 
 namespace {
@@ -250,10 +291,10 @@ void alloc_levels(htrip_index* h) {
         Lv.dec.reserve(Lv.nnodes);
     }
     h->pivots.reserve(1);
-    h->qstatus.reserve(1);
-    h->qbar.reserve(2);
-    ck(cudaMemsetAsync(h->qstatus.p, 0, sizeof(int), h->stream), "status");
-    ck(cudaMemsetAsync(h->qbar.p, 0, 2 * sizeof(unsigned), h->stream), "barrier");
+    h->max_nodes = 1;
+    for (auto& Lv : h->L) h->max_nodes = std::max(h->max_nodes, Lv.nnodes);
+    h->rb.reserve(sizeof(int) * (1 + (size_t)h->max_nodes) + h->max_nodes);
+    h->rb_dev.reserve(h->max_nodes);
 }
 
 // Closure of the listed matrices of level `Lv` over their pivot flags.
@@ -350,8 +391,42 @@ int vertex_index(const Level& Lv, int g, int r, int c) {
     return p < 0 ? -1 : q * Lv.nP + p;
 }
 
-void do_open(htrip_index* h, const int32_t* rc, int n, const uint8_t* obs, int rows, int cols, bool record_stats) {
-    cudaStream_t st = h->stream;
+// One onBatchCellsOpened call as a staged task.  Every level l = 0..H takes
+// two stages, each ending in a small device->host read into pinned memory:
+//   insert(l): leaves: in-leaf edges (pivots marked); nodes: the parents of
+//              children whose summary decreased plus the nodes holding new
+//              seams get the decreased child entries and the seams inserted;
+//              then the pivot flags are compacted  -> pivot counts to host
+//   close(l):  blocked closure over the pivots, then the exterior block is
+//              compared with its snapshot       -> decrease flags to host
+// A host wait separates the stages.  htrip_open_cells runs one task alone;
+// htrip_open_batch advances the tasks of many indexes stage by stage, each
+// on its index's own stream, with one wait per stage for all of them.
+struct OpenTask {
+    htrip_index* h = nullptr;
+    bool record_stats = true;
+    // host bucketing (minplus_oracle.cpp:539-598)
+    std::vector<int> leaves;                             // touched leaves, first-touch order
+    std::vector<std::vector<int>> edges;                 // per touched leaf: (u, v) pairs
+    std::vector<std::vector<std::vector<int>>> seams;    // [lvl][slot]: (u, v) V_U pairs
+    std::vector<std::vector<int>> seam_nodes, seam_slot;
+    // progress
+    std::vector<int> act, cand;  // active matrices of this level / the level below
+    int n_dirty = 0;
+    bool skip = false;           // nothing changes at the current level
+    size_t cap = 0;              // closure chunk (matrices) of the current level
+};
+
+// Pinned read-back words of a task: [pivots][kcnt of every node][dec bytes].
+inline int* rb_kcnt(htrip_index* h) { return reinterpret_cast<int*>(h->rb.p) + 1; }
+inline int* rb_pivots(htrip_index* h) { return reinterpret_cast<int*>(h->rb.p); }
+inline uint8_t* rb_dec(htrip_index* h) { return h->rb.p + sizeof(int) * (1 + (size_t)h->max_nodes); }
+
+void open_prepare(OpenTask& T, htrip_index* h, const int32_t* rc, int n, const uint8_t* obs, int rows, int cols,
+                  bool record_stats) {
+    T = OpenTask();
+    T.h = h;
+    T.record_stats = record_stats;
     const int b = h->b, g = h->g, H = h->H, S = h->S;
     auto passable = [&](int r, int c) { return r >= 0 && c >= 0 && r < rows && c < cols && obs[(size_t)r * cols + c] == 1; };
     auto weight_ok = [&](int r, int c) {  // GridMap::getCellWeight(p) < INF (grid_map.hpp:273-278)
@@ -360,29 +435,26 @@ void do_open(htrip_index* h, const int32_t* rc, int n, const uint8_t* obs, int r
     static const int dr[4] = {-1, 1, 0, 0};
     static const int dc[4] = {0, 0, -1, 1};
     Level& L0 = h->L[0];
-    // 1. bucket cells by leaf, in first-touch order
     std::vector<int> leaf_slot(L0.nnodes, -1);
-    std::vector<int> leaves;
-    std::vector<std::vector<int>> edges;  // per touched leaf: (u, v) pairs
-    std::vector<std::vector<std::vector<int>>> seams(H + 1);  // [lvl][slot] (u, v) pairs
-    std::vector<std::vector<int>> seam_nodes(H + 1);
-    std::vector<std::vector<int>> seam_slot(H + 1);
-    for (int l = 1; l <= H; ++l) seam_slot[l].assign(h->L[l].nnodes, -1);
+    T.seams.resize(H + 1);
+    T.seam_nodes.resize(H + 1);
+    T.seam_slot.resize(H + 1);
+    for (int l = 1; l <= H; ++l) T.seam_slot[l].assign(h->L[l].nnodes, -1);
     for (int i = 0; i < n; ++i) {
         const int r = rc[2 * i], c = rc[2 * i + 1];
         if (r < 0 || c < 0 || r >= S || c >= S) continue;
         const int tx = c / b, ty = r / b, leaf = ty * h->leaves_x + tx;
         if (leaf_slot[leaf] < 0) {
-            leaf_slot[leaf] = (int)leaves.size();
-            leaves.push_back(leaf);
-            edges.emplace_back();
+            leaf_slot[leaf] = (int)T.leaves.size();
+            T.leaves.push_back(leaf);
+            T.edges.emplace_back();
         }
         if (!weight_ok(r, c)) continue;
         for (int d = 0; d < 4; ++d) {
             const int nr = r + dr[d], nc = c + dc[d];
             if (!passable(nr, nc)) continue;
             if (nc / b == tx && nr / b == ty) {
-                auto& e = edges[leaf_slot[leaf]];
+                auto& e = T.edges[leaf_slot[leaf]];
                 e.push_back((r - ty * b) * b + (c - tx * b));
                 e.push_back((nr - ty * b) * b + (nc - tx * b));
             } else {
@@ -390,118 +462,179 @@ void do_open(htrip_index* h, const int32_t* rc, int n, const uint8_t* obs, int r
                 if (lca < 1 || lca > H) continue;
                 const Level& Lv = h->L[lca];
                 const int node = (r / Lv.side) * Lv.nodes_x + (c / Lv.side);
-                int& slot = seam_slot[lca][node];
+                int& slot = T.seam_slot[lca][node];
                 if (slot < 0) {
-                    slot = (int)seam_nodes[lca].size();
-                    seam_nodes[lca].push_back(node);
-                    seams[lca].emplace_back();
+                    slot = (int)T.seam_nodes[lca].size();
+                    T.seam_nodes[lca].push_back(node);
+                    T.seams[lca].emplace_back();
                 }
                 const int u = vertex_index(Lv, g, r, c), v = vertex_index(Lv, g, nr, nc);
                 if (u >= 0 && v >= 0) {
-                    seams[lca][slot].push_back(u);
-                    seams[lca][slot].push_back(v);
+                    T.seams[lca][slot].push_back(u);
+                    T.seams[lca][slot].push_back(v);
                 }
             }
         }
     }
     if (record_stats) h->stats = {0, 0, 0};
-    if (leaves.empty()) return;
-    int n_dirty = 0;
-    // 2. leaves: edge insert + closure over pivots
-    {
+}
+
+bool open_has_work(const OpenTask& T) { return !T.leaves.empty(); }
+
+// Stage insert(l) of T (issued on the index's stream, not waited for).
+void open_insert(OpenTask& T, int l) {
+    htrip_index* h = T.h;
+    cudaStream_t st = h->stream;
+    const int g = h->g, H = h->H;
+    Level& Lv = h->L[l];
+    T.skip = false;
+    if (l == 0) {
+        T.act = T.leaves;
         std::vector<int> buf;
-        std::vector<int> eoff(leaves.size() + 1, 0);
-        for (size_t i = 0; i < leaves.size(); ++i) eoff[i + 1] = eoff[i] + (int)edges[i].size() / 2;
+        std::vector<int> eoff(T.leaves.size() + 1, 0);
+        for (size_t i = 0; i < T.leaves.size(); ++i) eoff[i + 1] = eoff[i] + (int)T.edges[i].size() / 2;
         buf.insert(buf.end(), eoff.begin(), eoff.end());
-        for (auto& e : edges) buf.insert(buf.end(), e.begin(), e.end());
-        h->upd.reserve(buf.size() + leaves.size());
-        h->active.reserve(leaves.size());
-        ck(cudaMemcpyAsync(h->active.p, leaves.data(), leaves.size() * sizeof(int), cudaMemcpyHostToDevice, st), "act");
+        for (auto& e : T.edges) buf.insert(buf.end(), e.begin(), e.end());
+        const int na = (int)T.act.size();
+        h->upd.reserve(buf.size());
+        h->active.reserve(na);
+        ck(cudaMemcpyAsync(h->active.p, T.act.data(), na * sizeof(int), cudaMemcpyHostToDevice, st), "act");
         ck(cudaMemcpyAsync(h->upd.p, buf.data(), buf.size() * sizeof(int), cudaMemcpyHostToDevice, st), "upd");
         ck(cudaMemsetAsync(h->pivots.p, 0, sizeof(int), st), "piv");
-        ck(cudaMemsetAsync(L0.dec.p, 0, L0.nnodes, st), "dec0");
-        const int na = (int)leaves.size();
+        ck(cudaMemsetAsync(Lv.dec.p, 0, Lv.nnodes, st), "dec0");
         if (H > 0) {
-            h->snap.reserve((size_t)na * L0.nExt * L0.nExt);
-            hb::launch_ext_snapshot(L0.ms(), L0.d_ext.p, L0.nExt, h->active.p, na, h->snap.p, st);
-        }
-        hb::launch_leaf_edges(L0.ms(), h->active.p, na, h->upd.p, h->upd.p + eoff.size(), L0.kflag.p, h->pivots.p, st);
-        ck(cudaGetLastError(), "leaf edges");
-        int npiv = 0;
-        ck(cudaMemcpyAsync(&npiv, h->pivots.p, sizeof(int), cudaMemcpyDeviceToHost, st), "piv d2h");
-        close_matrices(h, L0, leaves);
-        if (H > 0) {
-            ck(cudaMemcpyAsync(h->active.p, leaves.data(), leaves.size() * sizeof(int), cudaMemcpyHostToDevice, st), "act");
-            hb::launch_ext_compare(L0.ms(), L0.d_ext.p, L0.nExt, h->active.p, na, h->snap.p, L0.dec.p, st);
-            ck(cudaGetLastError(), "compare");
-        }
-        ck(cudaStreamSynchronize(st), "sync");
-        if (record_stats) {
-            h->stats.n_touched_leaves = na;
-            h->stats.n_pivots = npiv;
-        }
-    }
-    // 3. levels 1..H
-    std::vector<int> cand = leaves;  // candidates of the level below
-    std::vector<uint8_t> child_dec;
-    for (int l = 1; l <= H; ++l) {
-        Level& Lv = h->L[l];
-        Level& Lc = h->L[l - 1];
-        child_dec.resize(Lc.nnodes);
-        ck(cudaMemcpyAsync(child_dec.data(), Lc.dec.p, Lc.nnodes, cudaMemcpyDeviceToHost, st), "dec d2h");
-        ck(cudaStreamSynchronize(st), "sync dec");
-        // candidates: parents of flagged children, plus seam nodes
-        std::vector<int> slot_of(Lv.nnodes, -1);
-        std::vector<int> act;
-        for (int c : cand) {
-            if (!child_dec[c]) continue;
-            const int cx = c % Lc.nodes_x, cy = c / Lc.nodes_x;
-            const int p = (cy / g) * Lv.nodes_x + (cx / g);
-            if (slot_of[p] < 0) { slot_of[p] = (int)act.size(); act.push_back(p); }
-        }
-        for (int node : seam_nodes[l])
-            if (slot_of[node] < 0) { slot_of[node] = (int)act.size(); act.push_back(node); }
-        n_dirty += (int)act.size();
-        if (act.empty()) {
-            // nothing changes at this level; higher levels only see seams
-            cand.clear();
-            ck(cudaMemsetAsync(Lv.dec.p, 0, Lv.nnodes, st), "dec");
-            continue;
-        }
-        const int na = (int)act.size();
-        std::vector<int> buf(na + 1, 0);
-        for (int i = 0; i < na; ++i) {
-            const int sl = seam_slot[l][act[i]];
-            buf[i + 1] = buf[i] + (sl >= 0 ? (int)seams[l][sl].size() / 2 : 0);
-        }
-        for (int i = 0; i < na; ++i) {
-            const int sl = seam_slot[l][act[i]];
-            if (sl >= 0) buf.insert(buf.end(), seams[l][sl].begin(), seams[l][sl].end());
-        }
-        h->active.reserve(na);
-        h->upd.reserve(buf.size());
-        ck(cudaMemcpyAsync(h->active.p, act.data(), na * sizeof(int), cudaMemcpyHostToDevice, st), "act");
-        ck(cudaMemcpyAsync(h->upd.p, buf.data(), buf.size() * sizeof(int), cudaMemcpyHostToDevice, st), "upd");
-        ck(cudaMemsetAsync(Lv.dec.p, 0, Lv.nnodes, st), "dec");
-        const bool root = (l == H);
-        if (!root) {
             h->snap.reserve((size_t)na * Lv.nExt * Lv.nExt);
             hb::launch_ext_snapshot(Lv.ms(), Lv.d_ext.p, Lv.nExt, h->active.p, na, h->snap.p, st);
         }
-        hb::launch_node_child_insert(Lv.ms(), Lc.ms(), Lc.d_ext.p, Lv.nP, g, Lv.nodes_x, Lc.nodes_x, h->active.p, na,
-                                     Lc.dec.p, Lv.kflag.p, st);
+        hb::launch_leaf_edges(Lv.ms(), h->active.p, na, h->upd.p, h->upd.p + eoff.size(), Lv.kflag.p, h->pivots.p,
+                              st);
+        ck(cudaGetLastError(), "leaf edges");
+        ck(cudaMemcpyAsync(rb_pivots(h), h->pivots.p, sizeof(int), cudaMemcpyDeviceToHost, st), "piv d2h");
+    } else {
+        // candidates: parents of children whose summary decreased, plus seam nodes
+        Level& Lc = h->L[l - 1];
+        const uint8_t* child_dec = rb_dec(h);
+        std::vector<int> slot_of(Lv.nnodes, -1);
+        T.act.clear();
+        for (int c : T.cand) {
+            if (!child_dec[c]) continue;
+            const int cx = c % Lc.nodes_x, cy = c / Lc.nodes_x;
+            const int p = (cy / g) * Lv.nodes_x + (cx / g);
+            if (slot_of[p] < 0) { slot_of[p] = (int)T.act.size(); T.act.push_back(p); }
+        }
+        for (int node : T.seam_nodes[l])
+            if (slot_of[node] < 0) { slot_of[node] = (int)T.act.size(); T.act.push_back(node); }
+        T.n_dirty += (int)T.act.size();
+        if (T.act.empty()) {
+            // nothing changes at this level; higher levels only see seams
+            T.skip = true;
+            T.cand.clear();
+            std::memset(rb_dec(h), 0, Lv.nnodes);
+            ck(cudaMemsetAsync(Lv.dec.p, 0, Lv.nnodes, st), "dec");
+            return;
+        }
+        const int na = (int)T.act.size();
+        std::vector<int> buf(na + 1, 0);
+        for (int i = 0; i < na; ++i) {
+            const int sl = T.seam_slot[l][T.act[i]];
+            buf[i + 1] = buf[i] + (sl >= 0 ? (int)T.seams[l][sl].size() / 2 : 0);
+        }
+        for (int i = 0; i < na; ++i) {
+            const int sl = T.seam_slot[l][T.act[i]];
+            if (sl >= 0) buf.insert(buf.end(), T.seams[l][sl].begin(), T.seams[l][sl].end());
+        }
+        // The decrease flags of the level below are consumed on the device
+        // (child insert) before Lv.dec is cleared for this level.
+        h->active.reserve(na);
+        h->upd.reserve(buf.size());
+        ck(cudaMemcpyAsync(h->active.p, T.act.data(), na * sizeof(int), cudaMemcpyHostToDevice, st), "act");
+        ck(cudaMemcpyAsync(h->upd.p, buf.data(), buf.size() * sizeof(int), cudaMemcpyHostToDevice, st), "upd");
+        ck(cudaMemsetAsync(Lv.dec.p, 0, Lv.nnodes, st), "dec");
+        if (l < H) {
+            h->snap.reserve((size_t)na * Lv.nExt * Lv.nExt);
+            hb::launch_ext_snapshot(Lv.ms(), Lv.d_ext.p, Lv.nExt, h->active.p, na, h->snap.p, st);
+        }
+        hb::launch_node_child_insert(Lv.ms(), Lc.ms(), Lc.d_ext.p, Lv.nP, g, Lv.nodes_x, Lc.nodes_x, h->active.p,
+                                     na, Lc.dec.p, Lv.kflag.p, st);
         hb::launch_node_seams(Lv.ms(), h->active.p, na, h->upd.p, h->upd.p + na + 1, Lv.kflag.p, st);
         ck(cudaGetLastError(), "node insert");
-        close_matrices(h, Lv, act);
-        if (!root) {
-            ck(cudaMemcpyAsync(h->active.p, act.data(), na * sizeof(int), cudaMemcpyHostToDevice, st), "act");
-            hb::launch_ext_compare(Lv.ms(), Lv.d_ext.p, Lv.nExt, h->active.p, na, h->snap.p, Lv.dec.p, st);
-            ck(cudaGetLastError(), "compare");
-        }
-        cand = act;
     }
-    ck(cudaStreamSynchronize(st), "open sync");
-    if (record_stats) h->stats.n_dirty_ancestors = n_dirty;
+    const int na = (int)T.act.size();
+    hb::launch_compact_pivots(Lv.kflag.p, Lv.NP, h->active.p, na, Lv.klist.p, Lv.kcnt.p, st);
+    ck(cudaGetLastError(), "compact");
+    // pivot counts of the active matrices, in act order
+    hb::launch_gather_counts(Lv.kcnt.p, h->active.p, na, h->rb_dev.p, st);
+    ck(cudaGetLastError(), "gather counts");
+    ck(cudaMemcpyAsync(rb_kcnt(h), h->rb_dev.p, na * sizeof(int), cudaMemcpyDeviceToHost, st), "kcnt d2h");
+}
+
+// Stage close(l) of T: closure rounds over the pivot counts read back by
+// insert(l), then the summary comparison whose flags insert(l+1) reads.
+void open_close(OpenTask& T, int l) {
+    htrip_index* h = T.h;
+    if (T.skip) return;
+    cudaStream_t st = h->stream;
+    const int H = h->H;
+    Level& Lv = h->L[l];
+    const int na = (int)T.act.size();
+    const int* kc = rb_kcnt(h);
+    const size_t per = (size_t)hb::kPivotChunk * Lv.NP;
+    const size_t cap = std::max<size_t>(1, (size_t)(128u << 20) / (per * sizeof(uint16_t)));
+    for (size_t c0 = 0; c0 < (size_t)na; c0 += cap) {
+        const int nc = (int)std::min(cap, (size_t)na - c0);
+        int maxk = 0;
+        for (int i = 0; i < nc; ++i) maxk = std::max(maxk, kc[c0 + i]);
+        if (maxk == 0) continue;
+        h->panel.reserve(per * nc);
+        h->pflags.reserve((size_t)nc * (Lv.NP / hb::kFlagTile));
+        const int rounds = (maxk + hb::kPivotChunk - 1) / hb::kPivotChunk;
+        for (int r = 0; r < rounds; ++r) {
+            hb::launch_closure_round(Lv.ms(), h->active.p + c0, nc, Lv.klist.p, Lv.kcnt.p, r, h->panel.p,
+                                     h->pflags.p, st);
+            ck(cudaGetLastError(), "closure round");
+        }
+    }
+    if (l == 0 && T.record_stats) {
+        h->stats.n_touched_leaves = na;
+        h->stats.n_pivots = *rb_pivots(h);
+    }
+    if (l < H) {
+        hb::launch_ext_compare(Lv.ms(), Lv.d_ext.p, Lv.nExt, h->active.p, na, h->snap.p, Lv.dec.p, st);
+        ck(cudaGetLastError(), "compare");
+        ck(cudaMemcpyAsync(rb_dec(h), Lv.dec.p, Lv.nnodes, cudaMemcpyDeviceToHost, st), "dec d2h");
+    }
+    T.cand = T.act;
+}
+
+void open_finish(OpenTask& T) {
+    if (T.record_stats) T.h->stats.n_dirty_ancestors = T.n_dirty;
+}
+
+// Runs the tasks (distinct indexes of one device) together, stage by stage.
+void run_open_tasks(std::vector<OpenTask>& tasks) {
+    int maxH = -1;
+    for (auto& T : tasks)
+        if (open_has_work(T)) maxH = std::max(maxH, T.h->H);
+    auto wait_all = [&](int l) {
+        for (auto& T : tasks)
+            if (open_has_work(T) && T.h->H >= l) ck(cudaStreamSynchronize(T.h->stream), "open stage");
+    };
+    for (int l = 0; l <= maxH; ++l) {
+        for (auto& T : tasks)
+            if (open_has_work(T) && T.h->H >= l) open_insert(T, l);
+        wait_all(l);
+        for (auto& T : tasks)
+            if (open_has_work(T) && T.h->H >= l) open_close(T, l);
+        wait_all(l);
+    }
+    for (auto& T : tasks)
+        if (open_has_work(T)) open_finish(T);
+}
+
+void do_open(htrip_index* h, const int32_t* rc, int n, const uint8_t* obs, int rows, int cols, bool record_stats) {
+    std::vector<OpenTask> tasks(1);
+    open_prepare(tasks[0], h, rc, n, obs, rows, cols, record_stats);
+    run_open_tasks(tasks);
 }
 
 // ---------------------------------------------------------------------------
@@ -529,7 +662,10 @@ struct QueryPlan {
 // override the default choice per (index shape, viewpoint count) bucket.
 int choose_query_cfg(const htrip_index* h, int ns, int root_group);
 
-void make_plan(const htrip_index* h, const int32_t* vps, const uint8_t* pass_flags, int k, QueryPlan& P) {
+// Plans a query; force_cfg >= 0 imposes the tile configuration (requests
+// that share a launch share one).
+void make_plan(const htrip_index* h, const int32_t* vps, const uint8_t* pass_flags, int k, QueryPlan& P,
+               int force_cfg = -1) {
     const int b = h->b, g = h->g, H = h->H;
     struct V { uint64_t key; int orig; int tx, ty; };
     std::vector<V> v;
@@ -552,6 +688,7 @@ void make_plan(const htrip_index* h, const int32_t* vps, const uint8_t* pass_fla
     const int ns = (int)v.size();
     P.n_sorted = ns;
     P.k = k;
+    P.flags_total = 0;
     P.ldm = std::max(8, (ns + 7) / 8 * 8);
     P.buf.clear();
     P.o_vp0 = 0;
@@ -591,7 +728,7 @@ void make_plan(const htrip_index* h, const int32_t* vps, const uint8_t* pass_fla
         for (const CG& c : cgs[l]) Q.max_group = std::max(Q.max_group, c.cnt);
         Q.n_groups = (int)cgs[l].size();
     }
-    P.cfg = choose_query_cfg(h, ns, H >= 1 ? P.lv[H].max_group : ns);
+    P.cfg = force_cfg >= 0 ? force_cfg : choose_query_cfg(h, ns, H >= 1 ? P.lv[H].max_group : ns);
     const hb::QueryTile tile = hb::query_config_tile(P.cfg);
     const int RW = tile.RW, NC = tile.NCOL;
     // Slot layout: every child group's run starts on an RW boundary.
@@ -688,31 +825,97 @@ void make_plan(const htrip_index* h, const int32_t* vps, const uint8_t* pass_fla
     }
 }
 
-void run_query(htrip_index* h, const QueryPlan& P, uint16_t* out_dev) {
-    cudaStream_t st = h->stream;
-    const int H = h->H, ldv = P.ldv, ldm = P.ldm;
-    if (H > hb::kMaxQueryLevels) throw CudaError{cudaErrorInvalidValue, "hierarchy deeper than the query supports"};
-    for (int l = 1; l <= H; ++l)
+// ---------------------------------------------------------------------------
+// Query launches.  One cooperative launch of the persistent kernel serves
+// any number of planned requests of one device (indexes of any shape, any
+// k).  Device scratch of a launch, every piece 256-byte aligned:
+//   [QueryParams x n][unit prefix, n_phases x (n+1) ints][4 words][plans]
+//       <- one host->device copy of the staged head (words start at zero)
+//   [M of every request]      <- one memset to 0xFF (no pair found yet)
+//   [flags of every request]  <- one memset to 0
+//   [X0 X1 X2 Y0 Y1 of every request][results k*k u16 of every request]
+// ---------------------------------------------------------------------------
+inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+struct QueryReq {
+    const htrip_index* h;
+    const QueryPlan* P;
+    uint16_t* out_dev;  // result on the device; nullptr = in the arena
+};
+
+struct LaunchLayout {
+    int n = 0, n_phases = 0;
+    size_t o_params = 0, o_pre = 0, o_words = 0, head = 0;
+    size_t o_M = 0, M_bytes = 0, o_flags = 0, flags_bytes = 0, o_out = 0, out_bytes = 0, total = 0;
+    std::vector<size_t> plan, M, flags, X[3], Y[2], out;
+};
+
+void check_query_shape(const htrip_index* h) {
+    if (h->H > hb::kMaxQueryLevels) throw CudaError{cudaErrorInvalidValue, "hierarchy deeper than the query supports"};
+    for (int l = 1; l <= h->H; ++l)
         if (h->L[l].nP > hb::query_max_ports())
             throw CudaError{cudaErrorInvalidValue, "child port count above the query kernel's list capacity"};
-    h->qplan.reserve(std::max<size_t>(1, P.buf.size()));
-    ck(cudaMemcpyAsync(h->qplan.p, P.buf.data(), P.buf.size() * sizeof(int), cudaMemcpyHostToDevice, st), "plan");
-    const int* plan = h->qplan.p;
-    int maxExt = 0, maxNP = 64;
-    for (int l = 0; l <= H; ++l) maxExt = std::max(maxExt, h->L[l].nExt);
-    for (int l = 1; l <= H; ++l) maxNP = std::max(maxNP, h->L[l].NP);
-    h->qM.reserve((size_t)ldm * ldm);
-    for (int i = 0; i < 3; ++i) h->qX[i].reserve((size_t)maxExt * ldv);
-    for (int i = 0; i < 2; ++i) h->qY[i].reserve((size_t)maxNP * ldv);
-    h->qflags.reserve(std::max<size_t>(1, P.flags_total));
-    ck(cudaMemsetAsync(h->qM.p, 0xFF, (size_t)ldm * ldm * sizeof(uint32_t), st), "M");
-    if (P.flags_total) ck(cudaMemsetAsync(h->qflags.p, 0, P.flags_total, st), "flags");
+}
+
+LaunchLayout layout_launch(const std::vector<QueryReq>& R) {
+    LaunchLayout L;
+    L.n = (int)R.size();
+    for (const auto& r : R) L.n_phases = std::max(L.n_phases, r.h->H + 3);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off += align256(std::max<size_t>(bytes, 1));
+        return o;
+    };
+    L.o_params = take(R.size() * sizeof(hb::QueryParams));
+    L.o_pre = take((size_t)L.n_phases * (R.size() + 1) * sizeof(int));
+    L.o_words = take(4 * sizeof(unsigned));
+    for (const auto& r : R) L.plan.push_back(take(r.P->buf.size() * sizeof(int)));
+    L.head = off;
+    L.o_M = off;
+    for (const auto& r : R) L.M.push_back(take((size_t)r.P->ldm * r.P->ldm * sizeof(uint32_t)));
+    L.M_bytes = off - L.o_M;
+    L.o_flags = off;
+    for (const auto& r : R) L.flags.push_back(take(r.P->flags_total));
+    L.flags_bytes = off - L.o_flags;
+    for (const auto& r : R) {
+        int maxExt = 0, maxNP = 64;
+        for (int l = 0; l <= r.h->H; ++l) maxExt = std::max(maxExt, r.h->L[l].nExt);
+        for (int l = 1; l <= r.h->H; ++l) maxNP = std::max(maxNP, r.h->L[l].NP);
+        for (int i = 0; i < 3; ++i) L.X[i].push_back(take((size_t)maxExt * r.P->ldv * sizeof(uint16_t)));
+        for (int i = 0; i < 2; ++i) L.Y[i].push_back(take((size_t)maxNP * r.P->ldv * sizeof(uint16_t)));
+    }
+    L.o_out = off;
+    for (const auto& r : R) L.out.push_back(r.out_dev ? 0 : take((size_t)r.P->k * r.P->k * sizeof(uint16_t)));
+    L.out_bytes = off - L.o_out;
+    L.total = off;
+    return L;
+}
+
+// CTA work units of request P in every phase of the launch (the kernel's
+// phase numbering, kernels.cuh QueryLaunch).
+void query_units(const htrip_index* h, const QueryPlan& P, int n_phases, int* units) {
+    const int H = h->H;
+    for (int t = 0; t < n_phases; ++t) units[t] = 0;
+    const long fill = (long)P.n_l0 * h->L[0].nExt;
+    units[0] = (int)((fill + hb::kQueryL0Chunk - 1) / hb::kQueryL0Chunk) +
+               (P.n_sorted + hb::kQueryThreads - 1) / hb::kQueryThreads;
+    for (int t = 1; t <= H + 1; ++t)
+        units[t] = (t <= H ? P.lv[t].n_items : 0) + (t - 1 >= 1 ? P.lv[t - 1].n_meet : 0);
+    units[H + 2] = (int)(((long)P.k * P.k + hb::kQueryFinChunk - 1) / hb::kQueryFinChunk);
+}
+
+hb::QueryParams make_params(const htrip_index* h, const QueryPlan& P, unsigned char* base, const LaunchLayout& L,
+                            int i, uint16_t* out_dev) {
+    const int H = h->H;
+    const int* plan = reinterpret_cast<const int*>(base + L.plan[i]);
+    uint8_t* flags = base + L.flags[i];
     hb::QueryParams Q{};
     Q.H = H;
     Q.k = P.k;
     Q.ns = P.n_sorted;
-    Q.ldv = ldv;
-    Q.ldm = ldm;
+    Q.ldv = P.ldv;
+    Q.ldm = P.ldm;
     Q.n_l0_slots = P.n_l0;
     Q.nExt0 = h->L[0].nExt;
     Q.cfg = P.cfg;
@@ -721,44 +924,133 @@ void run_query(htrip_index* h, const QueryPlan& P, uint16_t* out_dev) {
     Q.l0 = plan + P.o_l0;
     Q.ext0 = h->L[0].d_ext.p;
     Q.leaves = h->L[0].ms();
-    for (int i = 0; i < 3; ++i) Q.X[i] = h->qX[i].p;
-    for (int i = 0; i < 2; ++i) Q.Y[i] = h->qY[i].p;
-    Q.M = h->qM.p;
+    for (int j = 0; j < 3; ++j) Q.X[j] = reinterpret_cast<uint16_t*>(base + L.X[j][i]);
+    for (int j = 0; j < 2; ++j) Q.Y[j] = reinterpret_cast<uint16_t*>(base + L.Y[j][i]);
+    Q.M = reinterpret_cast<uint32_t*>(base + L.M[i]);
     Q.out = out_dev;
-    Q.status = h->qstatus.p;
-    Q.bar = h->qbar.p;
     for (int l = 1; l <= H; ++l) {
         const Level& Lv = h->L[l];
-        const QueryPlan::Lvl& L = P.lv[l];
+        const QueryPlan::Lvl& PL = P.lv[l];
         hb::QueryLevel& q = Q.lv[l];
         q.D = Lv.mat.p;
         q.NP = Lv.NP;
         q.nP = Lv.nP;
         q.ext_inv = Lv.d_ext_inv.p;
-        q.groups = plan + L.o_groups;
-        q.flags = h->qflags.p + L.flags_off;
-        q.items = plan + L.o_items;
-        q.n_items = L.n_items;
-        q.meet = plan + L.o_meet;
-        q.n_meet = L.n_meet;
-        q.s2v = plan + L.o_s2v;
-        q.lift = l < H ? plan + L.o_lift : nullptr;
+        q.groups = plan + PL.o_groups;
+        q.flags = flags + PL.flags_off;
+        q.items = plan + PL.o_items;
+        q.n_items = PL.n_items;
+        q.meet = plan + PL.o_meet;
+        q.n_meet = PL.n_meet;
+        q.s2v = plan + PL.o_s2v;
+        q.lift = l < H ? plan + PL.o_lift : nullptr;
         q.store_y = 1;
     }
-    if (h->qgrid == 0) h->qgrid = hb::query_grid_blocks(h->device);
-    h->qparams.reserve(sizeof(hb::QueryParams));
-    std::memcpy(h->h_qparams, &Q, sizeof(Q));
-    ck(cudaMemcpyAsync(h->qparams.p, h->h_qparams, sizeof(Q), cudaMemcpyHostToDevice, st), "params");
-    h->last_h2d = P.buf.size() * sizeof(int) + sizeof(Q);
-    h->last_d2h = 0;
-    if (!h->qev[0]) {
-        ck(cudaEventCreate(&h->qev[0]), "event");
-        ck(cudaEventCreate(&h->qev[1]), "event");
+    return Q;
+}
+
+// Stages the head of the launch into `stage` (>= L.head bytes of host
+// memory), then issues on `st`: the head copy, the two presets and the
+// kernel, bracketed by ev[0] / ev[1] when given.  Returns the device
+// pointers of the results in `outs`.
+void issue_query_launch(cudaStream_t st, int device, int& grid, int cfg, const std::vector<QueryReq>& R,
+                        const LaunchLayout& L, unsigned char* base, unsigned char* stage, const cudaEvent_t* ev,
+                        std::vector<uint16_t*>& outs) {
+    for (const auto& r : R) check_query_shape(r.h);
+    std::memset(stage, 0, L.head);
+    outs.resize(R.size());
+    auto* params = reinterpret_cast<hb::QueryParams*>(stage + L.o_params);
+    auto* pre = reinterpret_cast<int*>(stage + L.o_pre);
+    std::vector<int> units(L.n_phases);
+    for (int t = 0; t < L.n_phases; ++t) pre[(size_t)t * (L.n + 1)] = 0;
+    for (int i = 0; i < L.n; ++i) {
+        const QueryReq& r = R[i];
+        outs[i] = r.out_dev ? r.out_dev : reinterpret_cast<uint16_t*>(base + L.out[i]);
+        params[i] = make_params(r.h, *r.P, base, L, i, outs[i]);
+        std::memcpy(stage + L.plan[i], r.P->buf.data(), r.P->buf.size() * sizeof(int));
+        query_units(r.h, *r.P, L.n_phases, units.data());
+        for (int t = 0; t < L.n_phases; ++t)
+            pre[(size_t)t * (L.n + 1) + i + 1] = pre[(size_t)t * (L.n + 1) + i] + units[t];
     }
-    ck(cudaEventRecord(h->qev[0], st), "event");
-    ck(hb::launch_query(reinterpret_cast<const hb::QueryParams*>(h->qparams.p), P.cfg, h->qgrid, st), "query kernel");
-    ck(cudaEventRecord(h->qev[1], st), "event");
-    h->qev_valid = true;
+    ck(cudaMemcpyAsync(base, stage, L.head, cudaMemcpyHostToDevice, st), "query launch head");
+    ck(cudaMemsetAsync(base + L.o_M, 0xFF, L.M_bytes, st), "pair matrix preset");
+    ck(cudaMemsetAsync(base + L.o_flags, 0, L.flags_bytes, st), "flag preset");
+    if (grid == 0) grid = hb::query_grid_blocks(device);
+    hb::QueryLaunch QL;
+    QL.n_req = L.n;
+    QL.n_phases = L.n_phases;
+    QL.req = reinterpret_cast<const hb::QueryParams*>(base + L.o_params);
+    QL.unit_pre = reinterpret_cast<const int*>(base + L.o_pre);
+    QL.status = reinterpret_cast<int*>(base + L.o_words);
+    QL.bar = reinterpret_cast<unsigned*>(base + L.o_words) + 1;
+    if (ev) ck(cudaEventRecord(ev[0], st), "event");
+    ck(hb::launch_query(QL, cfg, grid, st), "query kernel");
+    if (ev) ck(cudaEventRecord(ev[1], st), "event");
+}
+
+// Runs the planned requests through the arena `A` on stream `st`.  Results
+// whose out_dev is null are copied into host_out[i] (k*k each).  Returns
+// the kernel's status word (0 ok, 1 grid barrier timeout); synchronous.
+int run_queries(QueryArena& A, int device, cudaStream_t st, const std::vector<QueryReq>& R,
+                const std::vector<uint16_t*>& host_out, bool sync) {
+    int cfg = 0;
+    for (const auto& r : R) cfg = std::max(cfg, r.P->cfg);
+    const LaunchLayout L = layout_launch(R);
+    // A stream-ordered launch (sync == false) may still be reading the
+    // arena or the pinned staging: wait for it before reusing or growing them.
+    if (A.ev_valid) ck(cudaEventSynchronize(A.ev[1]), "previous launch");
+    A.dev.reserve(L.total);
+    A.stage.reserve(L.head);
+    A.outstage.reserve(L.out_bytes + 256);
+    if (!A.ev[0]) {
+        ck(cudaEventCreate(&A.ev[0]), "event");
+        ck(cudaEventCreate(&A.ev[1]), "event");
+    }
+    std::vector<uint16_t*> outs;
+    issue_query_launch(st, device, A.grid, cfg, R, L, A.dev.p, A.stage.p, A.ev, outs);
+    A.ev_valid = true;
+    A.last_h2d = L.head;
+    A.last_d2h = 0;
+    int* status_host = reinterpret_cast<int*>(A.outstage.p + L.out_bytes);
+    bool any_host = false;
+    for (size_t i = 0; i < R.size(); ++i) any_host |= !R[i].out_dev && host_out[i];
+    if (any_host) {
+        ck(cudaMemcpyAsync(A.outstage.p, A.dev.p + L.o_out, L.out_bytes, cudaMemcpyDeviceToHost, st), "results");
+        A.last_d2h += L.out_bytes;
+    }
+    if (!sync) return 0;
+    ck(cudaMemcpyAsync(status_host, A.dev.p + L.o_words, sizeof(int), cudaMemcpyDeviceToHost, st), "status");
+    A.last_d2h += sizeof(int);
+    ck(cudaStreamSynchronize(st), "query sync");
+    if (any_host)
+        for (size_t i = 0; i < R.size(); ++i)
+            if (!R[i].out_dev && host_out[i])
+                std::memcpy(host_out[i], A.outstage.p + (L.out[i] - L.o_out),
+                            (size_t)R[i].P->k * R[i].P->k * sizeof(uint16_t));
+    return *status_host;
+}
+
+// Same-cfg planning for a launch: every request of one launch uses the
+// largest tile configuration any of them would choose on its own.
+void plan_common(std::vector<QueryPlan>& plans, const std::vector<const htrip_index*>& hs,
+                 const std::vector<const int32_t*>& vps, const std::vector<std::vector<uint8_t>>& pf) {
+    int cfg = 0;
+    for (const auto& P : plans) cfg = std::max(cfg, P.cfg);
+    for (size_t i = 0; i < plans.size(); ++i)
+        if (plans[i].cfg != cfg) make_plan(hs[i], vps[i], pf[i].data(), plans[i].k, plans[i], cfg);
+}
+
+// Viewpoint passability as queryAllPairs decides it (minplus_oracle.cpp:961-965,
+// :993-997): Free in `observed` and inside the index.
+std::vector<uint8_t> viewpoint_flags(const htrip_index* h, const int32_t* vps, int k, const uint8_t* observed,
+                                     int rows, int cols) {
+    std::vector<uint8_t> pf(k);
+    for (int i = 0; i < k; ++i) {
+        const int r = vps[2 * i], c = vps[2 * i + 1];
+        pf[i] = (r >= 0 && c >= 0 && r < rows && c < cols && observed[(size_t)r * cols + c] == 1 && r < h->S &&
+                 c < h->S);
+    }
+    return pf;
 }
 
 int choose_query_cfg(const htrip_index* h, int ns, int root_group) {
@@ -801,8 +1093,6 @@ unsigned char* noalloc_scratch(int dev) {
     }
     return g_noalloc_ptr[dev];
 }
-
-inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
 }  // namespace
 
@@ -853,8 +1143,6 @@ htrip_status htrip_destroy(htrip_index* h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->release();
-    for (auto& e : h->qev)
-        if (e) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return HTRIP_OK;
@@ -907,24 +1195,12 @@ htrip_status htrip_query_all_pairs(htrip_index* h, const int32_t* vps, int32_t k
     if (k == 0) return HTRIP_OK;
     HTRIP_GUARD_BEGIN
     ck(cudaSetDevice(h->device), "cudaSetDevice");
-    std::vector<uint8_t> pf(k);
-    for (int i = 0; i < k; ++i) {
-        const int r = vps[2 * i], c = vps[2 * i + 1];
-        pf[i] = (r >= 0 && c >= 0 && r < rows && c < cols && observed[(size_t)r * cols + c] == 1 && r < h->S && c < h->S);
-    }
+    const std::vector<uint8_t> pf = viewpoint_flags(h, vps, k, observed, rows, cols);
     QueryPlan P;
     make_plan(h, vps, pf.data(), k, P);
-    h->qout.reserve((size_t)k * k);
-    run_query(h, P, h->qout.p);
-    int status = 0;
-    ck(cudaMemcpyAsync(out, h->qout.p, (size_t)k * k * sizeof(uint16_t), cudaMemcpyDeviceToHost, h->stream), "out");
-    ck(cudaMemcpyAsync(&status, h->qstatus.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "status");
-    h->last_d2h = (uint64_t)k * k * sizeof(uint16_t) + sizeof(int);
-    ck(cudaStreamSynchronize(h->stream), "query sync");
-    if (status != 0) {
-        cudaMemsetAsync(h->qstatus.p, 0, sizeof(int), h->stream);
+    const std::vector<QueryReq> R{{h, &P, nullptr}};
+    if (run_queries(h->q, h->device, h->stream, R, {out}, true) != 0)
         return fail(HTRIP_ERR_CUDA, "query kernel: grid barrier timed out");
-    }
     return HTRIP_OK;
     HTRIP_GUARD_END
 }
@@ -949,18 +1225,20 @@ htrip_status htrip_query_all_pairs_dev(htrip_index* h, const int32_t* vps_dev, c
     }
     QueryPlan P;
     make_plan(h, vps.data(), pf.data(), k, P);
-    run_query(h, P, out_dev);
-    h->last_d2h = vps.size() * sizeof(int32_t) + pf.size();
+    const std::vector<QueryReq> R{{h, &P, out_dev}};
+    run_queries(h->q, h->device, h->stream, R, {nullptr}, false);
+    h->q.last_d2h = vps.size() * sizeof(int32_t) + pf.size();
     return HTRIP_OK;
     HTRIP_GUARD_END
 }
 
 // Same query as htrip_query_all_pairs, with every piece of device scratch
 // carved from the fixed module-scope array above: no cudaMalloc / cudaFree
-// and no growth of the index's own buffers.  A process-wide lock is held
-// from the first write to the array until the result is back on the host,
-// so calls through this entry point never overlap on the GPU (calls that
-// did overlap would race on the shared array).
+// and no growth of the index's own buffers (host staging is pageable
+// memory).  A process-wide lock is held from the first write to the array
+// until the result is back on the host, so calls through this entry point
+// never overlap on the GPU (calls that did overlap would race on the shared
+// array).
 htrip_status htrip_query_all_pairs_noalloc(htrip_index* h, const int32_t* vps, int32_t k, const uint8_t* observed,
                                            int32_t rows, int32_t cols, uint16_t* out) {
     if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
@@ -974,93 +1252,153 @@ htrip_status htrip_query_all_pairs_noalloc(htrip_index* h, const int32_t* vps, i
             return fail(HTRIP_ERR_UNSUPPORTED, "child port count above the query kernel's list capacity");
     HTRIP_GUARD_BEGIN
     ck(cudaSetDevice(h->device), "cudaSetDevice");
-    std::vector<uint8_t> pf(k);
-    for (int i = 0; i < k; ++i) {
-        const int r = vps[2 * i], c = vps[2 * i + 1];
-        pf[i] = (r >= 0 && c >= 0 && r < rows && c < cols && observed[(size_t)r * cols + c] == 1 && r < h->S && c < h->S);
-    }
+    const std::vector<uint8_t> pf = viewpoint_flags(h, vps, k, observed, rows, cols);
     QueryPlan P;
     make_plan(h, vps, pf.data(), k, P);
-    // Scratch layout (every piece 256-byte aligned).
-    int maxExt = 0, maxNP = 64;
-    for (int l = 0; l <= H; ++l) maxExt = std::max(maxExt, h->L[l].nExt);
-    for (int l = 1; l <= H; ++l) maxNP = std::max(maxNP, h->L[l].NP);
-    size_t off = 0;
-    auto take = [&](size_t bytes) { const size_t o = off; off += align256(std::max<size_t>(bytes, 1)); return o; };
-    const size_t o_params = take(sizeof(hb::QueryParams));
-    const size_t o_words = take(4 * sizeof(unsigned));  // {status, barrier count, barrier generation}
-    const size_t o_plan = take(P.buf.size() * sizeof(int));
-    const size_t o_M = take((size_t)P.ldm * P.ldm * sizeof(uint32_t));
-    const size_t o_flags = take(P.flags_total);
-    size_t o_X[3], o_Y[2];
-    for (auto& o : o_X) o = take((size_t)maxExt * P.ldv * sizeof(uint16_t));
-    for (auto& o : o_Y) o = take((size_t)maxNP * P.ldv * sizeof(uint16_t));
-    const size_t o_out = take((size_t)k * k * sizeof(uint16_t));
-    if (off > kNoAllocScratchBytes)
-        return fail(HTRIP_ERR_UNSUPPORTED, "query needs " + std::to_string(off) +
+    const std::vector<QueryReq> R{{h, &P, nullptr}};
+    const LaunchLayout L = layout_launch(R);
+    if (L.total > kNoAllocScratchBytes)
+        return fail(HTRIP_ERR_UNSUPPORTED, "query needs " + std::to_string(L.total) +
                                                " bytes of device scratch; the allocation-free entry point has " +
                                                std::to_string(kNoAllocScratchBytes) + " (fewer viewpoints or a smaller map)");
+    std::vector<unsigned char> stage(L.head);
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     unsigned char* base = noalloc_scratch(h->device);
     cudaStream_t st = h->stream;
-    int* words = reinterpret_cast<int*>(base + o_words);
-    int* plan = reinterpret_cast<int*>(base + o_plan);
-    uint32_t* M = reinterpret_cast<uint32_t*>(base + o_M);
-    uint8_t* flags = base + o_flags;
-    uint16_t* dout = reinterpret_cast<uint16_t*>(base + o_out);
-    // The array keeps the previous call's contents: reset what must start cleared.
-    ck(cudaMemcpyAsync(plan, P.buf.data(), P.buf.size() * sizeof(int), cudaMemcpyHostToDevice, st), "plan");
-    ck(cudaMemsetAsync(words, 0, 4 * sizeof(unsigned), st), "barrier words");
-    ck(cudaMemsetAsync(M, 0xFF, (size_t)P.ldm * P.ldm * sizeof(uint32_t), st), "M");
-    if (P.flags_total) ck(cudaMemsetAsync(flags, 0, P.flags_total, st), "flags");
-    hb::QueryParams Q{};
-    Q.H = H;
-    Q.k = P.k;
-    Q.ns = P.n_sorted;
-    Q.ldv = P.ldv;
-    Q.ldm = P.ldm;
-    Q.n_l0_slots = P.n_l0;
-    Q.nExt0 = h->L[0].nExt;
-    Q.cfg = P.cfg;
-    Q.vp0 = plan + P.o_vp0;
-    Q.inv = plan + P.o_inv;
-    Q.l0 = plan + P.o_l0;
-    Q.ext0 = h->L[0].d_ext.p;
-    Q.leaves = h->L[0].ms();
-    for (int i = 0; i < 3; ++i) Q.X[i] = reinterpret_cast<uint16_t*>(base + o_X[i]);
-    for (int i = 0; i < 2; ++i) Q.Y[i] = reinterpret_cast<uint16_t*>(base + o_Y[i]);
-    Q.M = M;
-    Q.out = dout;
-    Q.status = words;
-    Q.bar = reinterpret_cast<unsigned*>(words + 1);
-    for (int l = 1; l <= H; ++l) {
-        const Level& Lv = h->L[l];
-        const QueryPlan::Lvl& L = P.lv[l];
-        hb::QueryLevel& q = Q.lv[l];
-        q.D = Lv.mat.p;
-        q.NP = Lv.NP;
-        q.nP = Lv.nP;
-        q.ext_inv = Lv.d_ext_inv.p;
-        q.groups = plan + L.o_groups;
-        q.flags = flags + L.flags_off;
-        q.items = plan + L.o_items;
-        q.n_items = L.n_items;
-        q.meet = plan + L.o_meet;
-        q.n_meet = L.n_meet;
-        q.s2v = plan + L.o_s2v;
-        q.lift = l < H ? plan + L.o_lift : nullptr;
-        q.store_y = 1;
-    }
-    if (h->qgrid == 0) h->qgrid = hb::query_grid_blocks(h->device);
-    // Pageable host -> device: the call returns once the source is staged.
-    ck(cudaMemcpyAsync(base + o_params, &Q, sizeof(Q), cudaMemcpyHostToDevice, st), "params");
-    ck(hb::launch_query(reinterpret_cast<const hb::QueryParams*>(base + o_params), P.cfg, h->qgrid, st),
-       "query kernel");
+    // The array keeps the previous call's contents: the launch head (with
+    // zeroed status / barrier words), the pair matrix and the flags are
+    // rewritten by every call.
+    std::vector<uint16_t*> outs;
+    int grid = h->q.grid;
+    issue_query_launch(st, h->device, grid, P.cfg, R, L, base, stage.data(), nullptr, outs);
+    h->q.grid = grid;
     int status = 0;
-    ck(cudaMemcpyAsync(out, dout, (size_t)k * k * sizeof(uint16_t), cudaMemcpyDeviceToHost, st), "out");
-    ck(cudaMemcpyAsync(&status, words, sizeof(int), cudaMemcpyDeviceToHost, st), "status");
+    ck(cudaMemcpyAsync(out, outs[0], (size_t)k * k * sizeof(uint16_t), cudaMemcpyDeviceToHost, st), "out");
+    ck(cudaMemcpyAsync(&status, base + L.o_words, sizeof(int), cudaMemcpyDeviceToHost, st), "status");
     ck(cudaStreamSynchronize(st), "query sync");
     if (status != 0) return fail(HTRIP_ERR_CUDA, "query kernel: grid barrier timed out");
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_batch_create(int device, htrip_batch** out) {
+    if (!out) return fail(HTRIP_ERR_INVALID, "null out");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(HTRIP_ERR_NO_DEVICE, "no CUDA device");
+    }
+    if (device < 0 || device >= ndev) return fail(HTRIP_ERR_INVALID, "bad device ordinal");
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    auto* b = new htrip_batch();
+    b->device = device;
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete b;
+        return fail(HTRIP_ERR_CUDA, "stream creation failed");
+    }
+    *out = b;
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_batch_destroy(htrip_batch* b) {
+    if (!b) return HTRIP_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    b->q.release();
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return HTRIP_OK;
+}
+
+htrip_status htrip_query_batch(htrip_batch* b, const htrip_query_request* reqs, int32_t n) {
+    if (!b) return fail(HTRIP_ERR_INVALID, "null batch");
+    if (n < 0 || (n > 0 && !reqs)) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    for (int i = 0; i < n; ++i) {
+        const htrip_query_request& r = reqs[i];
+        if (!r.index) return fail(HTRIP_ERR_INVALID, "request " + std::to_string(i) + ": null index");
+        if (!r.index->built) return fail(HTRIP_ERR_NOT_BUILT, "request " + std::to_string(i) + ": index not built");
+        if (r.index->device != b->device)
+            return fail(HTRIP_ERR_INVALID, "request " + std::to_string(i) + ": index on another device");
+        if (r.k < 0 || (r.k > 0 && (!r.vps || !r.out)) || !r.observed)
+            return fail(HTRIP_ERR_INVALID, "request " + std::to_string(i) + ": bad arguments");
+    }
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(b->device), "cudaSetDevice");
+    std::vector<QueryPlan> plans;
+    std::vector<const htrip_index*> hs;
+    std::vector<const int32_t*> vps;
+    std::vector<std::vector<uint8_t>> pf;
+    std::vector<uint16_t*> outs;
+    for (int i = 0; i < n; ++i) {
+        const htrip_query_request& r = reqs[i];
+        if (r.k == 0) continue;
+        hs.push_back(r.index);
+        vps.push_back(r.vps);
+        pf.push_back(viewpoint_flags(r.index, r.vps, r.k, r.observed, r.rows, r.cols));
+        outs.push_back(r.out);
+        plans.emplace_back();
+        make_plan(r.index, r.vps, pf.back().data(), r.k, plans.back());
+    }
+    if (plans.empty()) return HTRIP_OK;
+    plan_common(plans, hs, vps, pf);
+    // Work queued on an index's own stream (a stream-ordered query) ends
+    // before this launch reads the index.
+    for (size_t i = 0; i < hs.size(); ++i) ck(cudaStreamSynchronize(hs[i]->stream), "index stream");
+    std::vector<QueryReq> R;
+    for (size_t i = 0; i < plans.size(); ++i) R.push_back({hs[i], &plans[i], nullptr});
+    if (run_queries(b->q, b->device, b->stream, R, outs, true) != 0)
+        return fail(HTRIP_ERR_CUDA, "query kernel: grid barrier timed out");
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_open_batch(htrip_batch* b, const htrip_open_request* reqs, int32_t n) {
+    if (!b) return fail(HTRIP_ERR_INVALID, "null batch");
+    if (n < 0 || (n > 0 && !reqs)) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    for (int i = 0; i < n; ++i) {
+        const htrip_open_request& r = reqs[i];
+        if (!r.index) return fail(HTRIP_ERR_INVALID, "request " + std::to_string(i) + ": null index");
+        if (!r.index->built) return fail(HTRIP_ERR_NOT_BUILT, "request " + std::to_string(i) + ": index not built");
+        if (r.index->device != b->device)
+            return fail(HTRIP_ERR_INVALID, "request " + std::to_string(i) + ": index on another device");
+        if (r.n < 0 || (r.n > 0 && !r.rc) || !r.observed)
+            return fail(HTRIP_ERR_INVALID, "request " + std::to_string(i) + ": bad arguments");
+    }
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(b->device), "cudaSetDevice");
+    // Requests on the same index are applied in call order: request i goes
+    // into wave w = the number of earlier requests on its index.
+    std::vector<int> wave(n, 0);
+    int n_waves = 0;
+    for (int i = 0; i < n; ++i) {
+        for (int j = 0; j < i; ++j)
+            if (reqs[j].index == reqs[i].index) wave[i] = std::max(wave[i], wave[j] + 1);
+        n_waves = std::max(n_waves, wave[i] + 1);
+    }
+    for (int w = 0; w < n_waves; ++w) {
+        std::vector<OpenTask> tasks;
+        for (int i = 0; i < n; ++i) {
+            if (wave[i] != w) continue;
+            const htrip_open_request& r = reqs[i];
+            ck(cudaStreamSynchronize(r.index->stream), "index stream");
+            tasks.emplace_back();
+            open_prepare(tasks.back(), r.index, r.rc, r.n, r.observed, r.rows, r.cols, true);
+        }
+        run_open_tasks(tasks);
+    }
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_batch_last_kernel_ms(const htrip_batch* b, float* ms) {
+    if (!b || !ms) return fail(HTRIP_ERR_INVALID, "null argument");
+    if (!b->q.ev_valid) return fail(HTRIP_ERR_INVALID, "no launch has run");
+    HTRIP_GUARD_BEGIN
+    ck(cudaEventSynchronize(b->q.ev[1]), "event sync");
+    ck(cudaEventElapsedTime(ms, b->q.ev[0], b->q.ev[1]), "event time");
     return HTRIP_OK;
     HTRIP_GUARD_END
 }
@@ -1150,20 +1488,38 @@ htrip_status htrip_query_work(const htrip_index* h, const int32_t* vps, int32_t 
     return HTRIP_OK;
 }
 
+htrip_status htrip_state_digest(const htrip_index* h, uint64_t* out, int32_t n_out) {
+    if (!h || !out) return fail(HTRIP_ERR_INVALID, "null argument");
+    if (!h->built) return fail(HTRIP_ERR_NOT_BUILT, "index not built");
+    if (n_out < h->H + 1) return fail(HTRIP_ERR_INVALID, "digest needs H + 1 entries");
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    DevBuf<unsigned long long> d;
+    d.reserve(h->H + 1);
+    ck(cudaMemsetAsync(d.p, 0, (h->H + 1) * sizeof(unsigned long long), h->stream), "digest preset");
+    for (int l = 0; l <= h->H; ++l) hb::launch_digest(h->L[l].ms(), h->L[l].nnodes, d.p + l, h->stream);
+    ck(cudaGetLastError(), "digest");
+    ck(cudaMemcpyAsync(out, d.p, (h->H + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream), "digest d2h");
+    ck(cudaStreamSynchronize(h->stream), "digest sync");
+    d.release();
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
 htrip_status htrip_last_query_kernel_ms(const htrip_index* h, float* ms) {
     if (!h || !ms) return fail(HTRIP_ERR_INVALID, "null argument");
-    if (!h->qev_valid) return fail(HTRIP_ERR_INVALID, "no query has run");
+    if (!h->q.ev_valid) return fail(HTRIP_ERR_INVALID, "no query has run");
     HTRIP_GUARD_BEGIN
-    ck(cudaEventSynchronize(h->qev[1]), "event sync");
-    ck(cudaEventElapsedTime(ms, h->qev[0], h->qev[1]), "event time");
+    ck(cudaEventSynchronize(h->q.ev[1]), "event sync");
+    ck(cudaEventElapsedTime(ms, h->q.ev[0], h->q.ev[1]), "event time");
     return HTRIP_OK;
     HTRIP_GUARD_END
 }
 
 htrip_status htrip_last_query_io(const htrip_index* h, uint64_t* h2d_bytes, uint64_t* d2h_bytes) {
     if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
-    if (h2d_bytes) *h2d_bytes = h->last_h2d;
-    if (d2h_bytes) *d2h_bytes = h->last_d2h;
+    if (h2d_bytes) *h2d_bytes = h->q.last_h2d;
+    if (d2h_bytes) *d2h_bytes = h->q.last_d2h;
     return HTRIP_OK;
 }
 
@@ -1205,10 +1561,8 @@ htrip_status htrip_memory_bytes(const htrip_index* h, uint64_t* reference_bytes,
         for (const auto& Lv : h->L)
             dev += (Lv.mat.n + Lv.klist.n * 2 + Lv.kcnt.n * 2) * sizeof(uint16_t) + Lv.kflag.n + Lv.dec.n +
                    (Lv.d_ext.n + Lv.d_seams.n) * sizeof(int);
-        dev += h->pass.n + h->panel.n * 2 + h->pflags.n + h->snap.n * 2 + h->qM.n * 4 + h->qflags.n +
-               h->qkidx.n * 4 + h->qout.n * 2 + h->qplan.n * 4;
-        for (const auto& x : h->qX) dev += x.n * 2;
-        for (const auto& y : h->qY) dev += y.n * 2;
+        dev += h->pass.n + h->panel.n * 2 + h->pflags.n + h->snap.n * 2 + h->q.dev.n + h->upd.n * 4 +
+               h->active.n * 4;
     }
     if (reference_bytes) *reference_bytes = ref;
     if (device_bytes) *device_bytes = dev;

@@ -417,6 +417,36 @@ __global__ void gather_block_kernel(const uint16_t* __restrict__ mat, int NP, co
     out[idx] = mat[(size_t)rows[a] * NP + cols[c]];
 }
 
+// Canonical checksum of a matrix family: the sum (mod 2^64) over matrices m
+// and logical entries (i, j), i, j < n, of splitmix64(((m*n + i)*n + j) << 16
+// | D[i][j]).  Padding is excluded, so the digest depends only on the
+// matrices' contents, never on the layout.
+__device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+__global__ void __launch_bounds__(256) digest_kernel(MatSet M, int count, unsigned long long* out) {
+    const int n = M.n, NP = M.NP;
+    const size_t rows = (size_t)count * n;
+    unsigned long long acc = 0;
+    for (size_t r = blockIdx.x; r < rows; r += gridDim.x) {
+        const size_t m = r / n, i = r % n;
+        const uint16_t* row = M.base + (m * NP + i) * NP;
+        for (int j = threadIdx.x; j < n; j += blockDim.x) acc += mix64(((r * n + j) << 16) | row[j]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
+__global__ void gather_counts_kernel(const int* __restrict__ kcnt, const int* __restrict__ active, int n, int* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = kcnt[active[i]];
+}
+
 __global__ void fill_u16_kernel(uint16_t* p, size_t n, uint16_t v) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
 }
@@ -524,6 +554,18 @@ void launch_gather_block(const uint16_t* mat, int NP, const int* rows, int nr, c
     const size_t n = (size_t)nr * nc;
     if (n == 0) return;
     gather_block_kernel<<<blocks_for(n, 256), 256, 0, st>>>(mat, NP, rows, nr, cols, nc, out);
+}
+
+void launch_digest(MatSet M, int count, unsigned long long* out, cudaStream_t st) {
+    const size_t rows = (size_t)count * M.n;
+    if (rows == 0) return;
+    const unsigned grid = (unsigned)std::min<size_t>(rows, 148 * 8);
+    digest_kernel<<<grid, 256, 0, st>>>(M, count, out);
+}
+
+void launch_gather_counts(const int* kcnt, const int* active, int n, int* out, cudaStream_t st) {
+    if (n == 0) return;
+    gather_counts_kernel<<<blocks_for(n, 256), 256, 0, st>>>(kcnt, active, n, out);
 }
 
 }  // namespace hb

@@ -46,6 +46,9 @@ void launch_closure_round(MatSet M, const int* active, int n_active, const int* 
                           const int* kcnt, int round, uint16_t* panel, uint8_t* flags,
                           cudaStream_t st);
 
+// out[i] = kcnt[active[i]] for i < n (pivot counts of the active matrices).
+void launch_gather_counts(const int* kcnt, const int* active, int n, int* out, cudaStream_t st);
+
 // --- incremental updates -----------------------------------------------------
 // Insert opened in-leaf edges (leaf_tile.cpp:311-330).  edges: per active
 // leaf a range [eoff[i], eoff[i+1]) of (u, v) pairs (2 ints).  Marks pivot
@@ -101,6 +104,7 @@ struct QueryLevel {
     int store_y;
 };
 
+// One queryAllPairs request of a launch.
 struct QueryParams {
     int H, k, ns, ldv, ldm, n_l0_slots, nExt0, cfg;
     const int* vp0;         // per sorted viewpoint {leaf, u, leaf-run start, leaf-run end}
@@ -112,16 +116,38 @@ struct QueryParams {
     uint16_t* Y[2];         // projections Yt_l in P.Y[l & 1] ([column][ldv])
     uint32_t* M;            // sorted-order pair matrix (ldm), preset to 0xFFFFFFFF
     uint16_t* out;          // k x k result
-    int* status;            // 0 ok, 1 grid barrier timeout
-    unsigned* bar;          // grid barrier {count, generation}
     QueryLevel lv[kMaxQueryLevels + 1];
 };
 
-// Cooperative launch of the persistent query kernel on `grid` blocks; the
-// parameter block lives in device memory (P_dev).
+// CTA work units of a request in phase t of the launch (host and device
+// agree on these numbers):
+//   t = 0          level-0 port gathers in chunks of kQueryL0Chunk, then
+//                  same-leaf pair rows in chunks of kQueryThreads
+//   1 <= t <= H+1  project items of level t (t <= H), then meet items of
+//                  level t-1 (t >= 2)
+//   t = H+2        output chunks of kQueryFinChunk entries
+constexpr int kQueryThreads = 512;
+constexpr int kQueryL0Chunk = 4096;
+constexpr int kQueryFinChunk = 4096;
+
+// A launch over n_req requests (any mix of indexes and k on one device).
+struct QueryLaunch {
+    int n_req;
+    int n_phases;              // max over requests of H + 3
+    const QueryParams* req;    // device array of n_req requests
+    const int* unit_pre;       // [n_phases][n_req + 1]: exclusive prefix of units
+    int* status;               // 0 ok, 1 grid barrier timeout
+    unsigned* bar;             // grid barrier {count, generation}
+};
+
+// Cooperative launch of the persistent query kernel on `grid` blocks.
 int query_grid_blocks(int device);
 int query_max_ports();  // largest per-child port count the query kernel handles
-cudaError_t launch_query(const QueryParams* P_dev, int cfg, int grid, cudaStream_t st);
+cudaError_t launch_query(const QueryLaunch& L, int cfg, int grid, cudaStream_t st);
+
+// *out += canonical checksum of the first `count` matrices of M (logical
+// entries only): sum of splitmix64(((m*n + i)*n + j) << 16 | D[i][j]).
+void launch_digest(MatSet M, int count, unsigned long long* out, cudaStream_t st);
 
 // ptr[0 .. n) = value.
 void launch_fill_u16(uint16_t* ptr, size_t n, uint16_t value, cudaStream_t st);

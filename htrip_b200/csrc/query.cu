@@ -79,7 +79,7 @@ __device__ __forceinline__ void ldg_rows(uint32_t (&a)[RW / 2], const uint16_t* 
     }
 }
 
-constexpr int kThreads = 512;
+constexpr int kThreads = kQueryThreads;
 constexpr int kWarps = kThreads / 32;
 
 // Warp w of the CTA streams list entries t = w*U + 16*U*i + u of the
@@ -308,59 +308,78 @@ __device__ void do_meet(const QueryParams& P, const QueryLevel& L, int item, int
     __syncthreads();
 }
 
+// One CTA work unit of request P in phase t (see QueryLaunch).
 template <int RW, int CP>
-__global__ void __launch_bounds__(kThreads, 1) q_persistent_kernel(const QueryParams* __restrict__ Pp) {
-    extern __shared__ __align__(16) int qsm[];
-    int* kl = qsm;
-    uint32_t* red = reinterpret_cast<uint32_t*>(qsm + kMaxList);
-    __shared__ int wsum[kWarps];
-    const QueryParams& P = *Pp;
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int nt = gridDim.x * blockDim.x;
-    // level 0: X0 in level-1 slot order (+ level-1 flags), same-leaf pairs
-    {
+__device__ void run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum, uint32_t* red) {
+    const int tid = threadIdx.x;
+    if (t == 0) {
+        // level 0: X0 in level-1 slot order (+ level-1 flags), same-leaf pairs
         const int S1 = P.n_l0_slots;
         const int total = S1 * P.nExt0;
-        for (int t = gt; t < total; t += nt) {
-            const int p = t / S1, s = t - p * S1;
-            const int j = P.l0[2 * s];
-            if (j < 0) continue;
-            const int* v = P.vp0 + 4 * j;
-            const uint16_t d = P.leaves.base[((size_t)v[0] * P.leaves.NP + v[1]) * P.leaves.NP + P.ext0[p]];
-            P.X[0][(size_t)p * P.ldv + s] = d;
-            if (d < INF && P.H >= 1) P.lv[1].flags[(size_t)P.l0[2 * s + 1] * P.nExt0 + p] = 1;
+        const int n_fill = (total + kQueryL0Chunk - 1) / kQueryL0Chunk;
+        if (u < n_fill) {
+            const int e1 = min(total, (u + 1) * kQueryL0Chunk);
+            for (int e = u * kQueryL0Chunk + tid; e < e1; e += kThreads) {
+                const int p = e / S1, s = e - p * S1;
+                const int j = P.l0[2 * s];
+                if (j < 0) continue;
+                const int* v = P.vp0 + 4 * j;
+                const uint16_t d = P.leaves.base[((size_t)v[0] * P.leaves.NP + v[1]) * P.leaves.NP + P.ext0[p]];
+                P.X[0][(size_t)p * P.ldv + s] = d;
+                if (d < INF && P.H >= 1) P.lv[1].flags[(size_t)P.l0[2 * s + 1] * P.nExt0 + p] = 1;
+            }
+        } else {
+            const int j = (u - n_fill) * kThreads + tid;
+            if (j < P.ns) {
+                const int* v = P.vp0 + 4 * j;
+                const uint16_t* row = P.leaves.base + ((size_t)v[0] * P.leaves.NP + v[1]) * P.leaves.NP;
+                for (int jj = j + 1; jj < v[3]; ++jj) P.M[(size_t)j * P.ldm + jj] = row[P.vp0[4 * jj + 1]];
+            }
         }
-        for (int j = gt; j < P.ns; j += nt) {
-            const int* v = P.vp0 + 4 * j;
-            const uint16_t* row = P.leaves.base + ((size_t)v[0] * P.leaves.NP + v[1]) * P.leaves.NP;
-            for (int jj = j + 1; jj < v[3]; ++jj) P.M[(size_t)j * P.ldm + jj] = row[P.vp0[4 * jj + 1]];
-        }
+        return;
     }
-    if (!grid_barrier(P.bar, P.status)) return;
-    for (int l = 1; l <= P.H + 1; ++l) {
-        const int lp = l <= P.H ? l : 0;  // project level of this phase
-        const int lm = l - 1;              // meet level of this phase
-        const QueryLevel* Lp = lp >= 1 ? &P.lv[lp] : nullptr;
-        const QueryLevel* Lm = lm >= 1 ? &P.lv[lm] : nullptr;
-        const QueryLevel* Ln = (lp >= 1 && lp < P.H) ? &P.lv[lp + 1] : nullptr;
-        const int np = Lp ? Lp->n_items : 0;
-        const int nm = Lm ? Lm->n_meet : 0;
-        for (int w = blockIdx.x; w < np + nm; w += gridDim.x) {
-            if (w < np) do_project<RW, CP>(P, *Lp, Ln, w, lp, kl, wsum, red);
-            else do_meet<RW, CP>(P, *Lm, w - np, lm, kl, wsum, red);
-        }
-        if (!grid_barrier(P.bar, P.status)) return;
+    if (t <= P.H + 1) {
+        const int np = t <= P.H ? P.lv[t].n_items : 0;
+        if (u < np) do_project<RW, CP>(P, P.lv[t], t < P.H ? &P.lv[t + 1] : nullptr, u, t, kl, wsum, red);
+        else do_meet<RW, CP>(P, P.lv[t - 1], u - np, t - 1, kl, wsum, red);
+        return;
     }
-    // finalize: out[a][c]
-    for (int t = gt; t < P.k * P.k; t += nt) {
-        const int a = t / P.k, c = t - a * P.k;
+    // t == H + 2: out[a][c] for one chunk of the k x k output
+    const int kk = P.k * P.k;
+    const int e1 = min(kk, (u + 1) * kQueryFinChunk);
+    for (int e = u * kQueryFinChunk + tid; e < e1; e += kThreads) {
+        const int a = e / P.k, c = e - a * P.k;
         const int ia = P.inv[a], ic = P.inv[c];
         uint32_t v = INF;
         if (ia >= 0 && ic >= 0) {
             if (ia == ic) v = 0;
             else v = min(ia < ic ? P.M[(size_t)ia * P.ldm + ic] : P.M[(size_t)ic * P.ldm + ia], (uint32_t)INF);
         }
-        P.out[t] = (uint16_t)v;
+        P.out[e] = (uint16_t)v;
+    }
+}
+
+// The persistent kernel: phases separated by grid barriers; in each phase
+// the CTAs stride over the units of every request of the launch.
+template <int RW, int CP>
+__global__ void __launch_bounds__(kThreads, 1) q_persistent_kernel(const QueryLaunch B) {
+    extern __shared__ __align__(16) int qsm[];
+    int* kl = qsm;
+    uint32_t* red = reinterpret_cast<uint32_t*>(qsm + kMaxList);
+    __shared__ int wsum[kWarps];
+    for (int t = 0; t < B.n_phases; ++t) {
+        const int* pre = B.unit_pre + (size_t)t * (B.n_req + 1);
+        const int total = pre[B.n_req];
+        for (int w = blockIdx.x; w < total; w += gridDim.x) {
+            int lo = 0, hi = B.n_req;  // pre[lo] <= w < pre[hi]
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (pre[mid] <= w) lo = mid;
+                else hi = mid;
+            }
+            run_unit<RW, CP>(B.req[lo], t, w - pre[lo], kl, wsum, red);
+        }
+        if (t + 1 < B.n_phases && !grid_barrier(B.bar, B.status)) return;
     }
 }
 
@@ -379,7 +398,7 @@ int query_default_config(int NP, int max_group) {
 }
 
 namespace {
-typedef void (*QueryKernel)(const QueryParams*);
+typedef void (*QueryKernel)(const QueryLaunch);
 const QueryKernel kQueryKernels[kNumQueryConfigs] = {q_persistent_kernel<8, 1>, q_persistent_kernel<8, 2>,
                                                      q_persistent_kernel<16, 2>, q_persistent_kernel<8, 4>};
 const size_t kQuerySmem[kNumQueryConfigs] = {query_smem_bytes<8, 1>(), query_smem_bytes<8, 2>(),
@@ -408,9 +427,9 @@ int query_grid_blocks(int device) {
     return sms * std::max(1, per);
 }
 
-cudaError_t launch_query(const QueryParams* P_dev, int cfg, int grid, cudaStream_t st) {
+cudaError_t launch_query(const QueryLaunch& L, int cfg, int grid, cudaStream_t st) {
     configure_query_kernels();
-    void* args[] = {const_cast<QueryParams**>(&P_dev)};
+    void* args[] = {const_cast<QueryLaunch*>(&L)};
     return cudaLaunchCooperativeKernel((const void*)kQueryKernels[cfg], dim3(grid), dim3(kThreads), args,
                                        kQuerySmem[cfg], st);
 }

@@ -41,6 +41,16 @@ class _Config(C.Structure):
     _fields_ = [("tile_size_b", C.c_int32), ("group", C.c_int32)]
 
 
+class _QueryRequest(C.Structure):
+    _fields_ = [("index", C.c_void_p), ("vps", _I32P), ("k", C.c_int32), ("observed", _U8P),
+                ("rows", C.c_int32), ("cols", C.c_int32), ("out", _U16P)]
+
+
+class _OpenRequest(C.Structure):
+    _fields_ = [("index", C.c_void_p), ("rc", _I32P), ("n", C.c_int32), ("observed", _U8P),
+                ("rows", C.c_int32), ("cols", C.c_int32)]
+
+
 class _Stats(C.Structure):
     _fields_ = [("n_touched_leaves", C.c_int32), ("n_dirty_ancestors", C.c_int32), ("n_pivots", C.c_int32)]
 
@@ -53,6 +63,8 @@ EXPORTS = (
     "htrip_shape", "htrip_last_batch_stats", "htrip_memory_bytes", "htrip_read_leaf_D", "htrip_read_leaf_S",
     "htrip_read_node_DU", "htrip_read_node_SU", "htrip_read_node_C2E", "htrip_level_dims", "htrip_query_work",
     "htrip_last_query_kernel_ms", "htrip_last_query_io", "htrip_query_all_pairs_noalloc",
+    "htrip_batch_create", "htrip_batch_destroy", "htrip_query_batch", "htrip_batch_last_kernel_ms",
+    "htrip_state_digest", "htrip_open_batch",
 )
 
 
@@ -92,6 +104,12 @@ def load_library(path: str | None = None):
     lib.htrip_query_work.argtypes = [P, _I32P, I, _U8P, I, I, _U64P, _U64P]
     lib.htrip_last_query_kernel_ms.argtypes = [P, C.POINTER(C.c_float)]
     lib.htrip_last_query_io.argtypes = [P, _U64P, _U64P]
+    lib.htrip_state_digest.argtypes = [P, _U64P, I]
+    lib.htrip_batch_create.argtypes = [C.c_int, C.POINTER(P)]
+    lib.htrip_batch_destroy.argtypes = [P]
+    lib.htrip_query_batch.argtypes = [P, C.POINTER(_QueryRequest), I]
+    lib.htrip_batch_last_kernel_ms.argtypes = [P, C.POINTER(C.c_float)]
+    lib.htrip_open_batch.argtypes = [P, C.POINTER(_OpenRequest), I]
     for f in EXPORTS:
         if f not in ("htrip_last_error", "htrip_stream"):
             getattr(lib, f).restype = C.c_int
@@ -222,6 +240,9 @@ class MinPlusOracle:
         rc = _rc(cells)
         obs, ptr, rows, cols = _grid_args(grid)
         _check(self.lib.htrip_open_cells(self.h, rc.ctypes.data_as(_I32P), len(rc), ptr, rows, cols))
+        self._refresh_stats()
+
+    def _refresh_stats(self):
         st = _Stats()
         _check(self.lib.htrip_last_batch_stats(self.h, C.byref(st)))
         self.last_batch_stats = LastBatchStats(st.n_touched_leaves, st.n_dirty_ancestors, st.n_pivots)
@@ -300,6 +321,13 @@ class MinPlusOracle:
         _check(self.lib.htrip_memory_bytes(self.h, C.byref(ref), C.byref(dev)))
         return dev.value
 
+    def stateDigest(self):
+        """Per-level checksum of every leaf D and node D_U (htrip_state_digest)."""
+        n = self.H + 1
+        out = (C.c_uint64 * n)()
+        _check(self.lib.htrip_state_digest(self.h, out, n))
+        return [int(x) for x in out]
+
     def level_dims(self, lvl: int):
         a = [C.c_int32() for _ in range(4)]
         _check(self.lib.htrip_level_dims(self.h, lvl, *[C.byref(x) for x in a]))
@@ -337,3 +365,57 @@ class MinPlusOracle:
 
 
 HTripOracle = MinPlusOracle
+
+
+class Batch:
+    """Batched calls over many indexes of one device (htrip_batch_*).
+
+    ``query([(oracle, viewpoints, grid), ...])`` answers every request in one
+    launch of the persistent query kernel; each (k, k) result equals the
+    oracle's own ``queryAllPairs`` of that request."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        self.device = device
+        h = C.c_void_p()
+        _check(self.lib.htrip_batch_create(device, C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.lib.htrip_batch_destroy(h)
+            self.h = None
+
+    def query(self, requests):
+        reqs = (_QueryRequest * max(1, len(requests)))()
+        keep, outs = [], []
+        for i, (oracle, vps, grid) in enumerate(requests):
+            rc = _rc(vps)
+            obs, ptr, rows, cols = _grid_args(grid)
+            out = np.empty((len(rc), len(rc)), dtype=np.uint16)
+            keep += [rc, obs]
+            outs.append(out)
+            reqs[i] = _QueryRequest(oracle.h, rc.ctypes.data_as(_I32P), len(rc), ptr, rows, cols,
+                                    out.ctypes.data_as(_U16P))
+        _check(self.lib.htrip_query_batch(self.h, reqs, len(requests)))
+        return outs
+
+    def open(self, requests):
+        """onBatchCellsOpened of every (oracle, cells, grid) request; each
+        oracle's last_batch_stats is refreshed."""
+        reqs = (_OpenRequest * max(1, len(requests)))()
+        keep = []
+        for i, (oracle, cells, grid) in enumerate(requests):
+            rc = _rc(cells)
+            obs, ptr, rows, cols = _grid_args(grid)
+            keep += [rc, obs]
+            reqs[i] = _OpenRequest(oracle.h, rc.ctypes.data_as(_I32P), len(rc), ptr, rows, cols)
+        _check(self.lib.htrip_open_batch(self.h, reqs, len(requests)))
+        for oracle, _, _ in requests:
+            oracle._refresh_stats()
+
+    def lastKernelMs(self) -> float:
+        ms = C.c_float()
+        _check(self.lib.htrip_batch_last_kernel_ms(self.h, C.byref(ms)))
+        return ms.value

@@ -162,3 +162,46 @@ def frontier_cells(observed: np.ndarray, k: int, seed: int) -> np.ndarray:
     idx = rng.choice(cand, size=min(k, cand.size), replace=False)
     cols = observed.shape[1]
     return np.stack([idx // cols, idx % cols], axis=1).astype(np.int32)
+
+
+def batched_mix(n_maps: int, seed: int, sides=(128, 256, 512, 1024), tiles=(8, 16, 32),
+                open_range=(64, 1024), k_range=(8, 512)):
+    """The many-maps workload: per map a side, a generator (street grid with
+    20-40% obstacles or maze with corridor width 1-16), a leaf side b, one
+    opening batch of m cells (withheld from the initial observation and
+    opened in one call) and one all-pairs query of k viewpoints.
+
+    Returns a list of dicts {side, kind, param, b, seed, n_open, k}; grids
+    come from ``mix_grid``."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_maps):
+        side = int(rng.choice(sides))
+        kind = "street" if rng.random() < 0.5 else "maze"
+        param = float(rng.uniform(0.20, 0.40)) if kind == "street" else int(rng.integers(1, 17))
+        out.append(dict(side=side, kind=kind, param=param, b=int(rng.choice(tiles)),
+                        seed=int(rng.integers(0, 2**31 - 1)),
+                        n_open=int(rng.integers(open_range[0], open_range[1] + 1)),
+                        k=int(rng.integers(k_range[0], k_range[1] + 1))))
+    return out
+
+
+def mix_grid(spec) -> np.ndarray:
+    """Ground-truth grid of one ``batched_mix`` entry."""
+    if spec["kind"] == "street":
+        return street_grid(spec["side"], spec["seed"], blocked=spec["param"])
+    return maze_grid(spec["side"], int(spec["param"]), spec["seed"])
+
+
+def withheld_open(truth: np.ndarray, n_open: int, seed: int):
+    """(observed0, cells): n_open Free cells of ``truth`` drawn uniformly and
+    left Unknown in observed0, to be opened in one batch (the reference's
+    update benchmark withholds cells the same way, bench_update_latency.cpp:166-175)."""
+    rng = np.random.default_rng(seed)
+    free = np.flatnonzero(truth.ravel() == FREE)
+    idx = rng.choice(free, size=min(n_open, free.size), replace=False)
+    cols = truth.shape[1]
+    cells = np.stack([idx // cols, idx % cols], axis=1).astype(np.int32)
+    obs = truth.copy()
+    obs[cells[:, 0], cells[:, 1]] = UNKNOWN
+    return obs, cells

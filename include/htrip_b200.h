@@ -125,6 +125,51 @@ htrip_status htrip_query_all_pairs_noalloc(htrip_index* h, const int32_t* vps, i
                                            const uint8_t* observed, int32_t rows, int32_t cols,
                                            uint16_t* out);
 
+/* Batched calls over many indexes (maps) of one device.
+ *
+ * The reference serves one map per call; a host that keeps many maps (one
+ * per robot team or session, robot_simulator.cpp:897-1045 keeps two oracles
+ * per map) calls MinPlusOracle::queryAllPairs / onBatchCellsOpened once per
+ * map.  A batch handle owns a CUDA stream and a scratch arena; one
+ * htrip_query_batch call answers every request in ONE launch of the
+ * persistent query kernel, and each result is bit-identical to the
+ * htrip_query_all_pairs call of the same request alone.                   */
+typedef struct htrip_batch htrip_batch; /* opaque */
+
+typedef struct {
+    htrip_index* index;       /* built index on the batch's device        */
+    const int32_t* vps;       /* k (r, c) pairs, host                     */
+    int32_t k;
+    const uint8_t* observed;  /* rows*cols CellState bytes, host          */
+    int32_t rows, cols;
+    uint16_t* out;            /* k*k host output                          */
+} htrip_query_request;
+
+htrip_status htrip_batch_create(int device, htrip_batch** out);
+htrip_status htrip_batch_destroy(htrip_batch* b);
+
+/* queryAllPairs of every request (minplus_oracle.hpp:337-341 per request).
+ * Several requests may name the same index.  Synchronous on return.       */
+htrip_status htrip_query_batch(htrip_batch* b, const htrip_query_request* reqs, int32_t n);
+
+typedef struct {
+    htrip_index* index;       /* built index on the batch's device        */
+    const int32_t* rc;        /* n (r, c) cells, host, already set Free   */
+    int32_t n;
+    const uint8_t* observed;  /* rows*cols CellState bytes, host          */
+    int32_t rows, cols;
+} htrip_open_request;
+
+/* onBatchCellsOpened of every request (minplus_oracle.hpp:171 per request).
+ * The openings of all indexes advance level by level together (each index
+ * on its own stream, one host wait per stage for all of them); requests on
+ * the same index are applied in call order.  Each index ends in the state,
+ * and with the last_batch_stats, of the same calls made one by one.       */
+htrip_status htrip_open_batch(htrip_batch* b, const htrip_open_request* reqs, int32_t n);
+
+/* Device time of the batch's last query launch.                           */
+htrip_status htrip_batch_last_kernel_ms(const htrip_batch* b, float* ms);
+
 /* Measurement helpers (no reference counterpart).
  * htrip_query_work: the algorithmic HBM bytes and min-plus operations of a
  * queryAllPairs on these viewpoints: k*(4b-4) level-0 gathers; per level and
@@ -174,6 +219,16 @@ htrip_status htrip_read_node_DU(const htrip_index* h, int32_t lvl, int32_t node,
 htrip_status htrip_read_node_SU(const htrip_index* h, int32_t lvl, int32_t node, uint16_t* out);
 htrip_status htrip_read_node_C2E(const htrip_index* h, int32_t lvl, int32_t node, int32_t quad,
                                  uint16_t* out);
+/* Canonical per-level checksum of the whole index (no reference
+ * counterpart; computed on the device, nothing large is copied):
+ *   out[l] = sum mod 2^64 over the level's matrices m (leaves[m].D for
+ *   l = 0, levels[l-1][m].D_U above) and logical entries (i, j) of
+ *   splitmix64(((m*n + i)*n + j) << 16 | value),  n = b^2 or nV.
+ * Two indexes with equal digests hold equal matrices (up to 64-bit hash
+ * collisions); the reference's members give the same numbers when summed
+ * the same way.  n_out >= H + 1.                                          */
+htrip_status htrip_state_digest(const htrip_index* h, uint64_t* out, int32_t n_out);
+
 /* nV, nExt and per-child port count nP of level `lvl` (0 = leaves: n=b^2). */
 htrip_status htrip_level_dims(const htrip_index* h, int32_t lvl, int32_t* n, int32_t* n_ext,
                               int32_t* n_child_ports, int32_t* n_nodes);

@@ -77,6 +77,8 @@ def _load_ref():
         lib.ref_node_DU.argtypes = [_P, _I, _I, _U16P]
         lib.ref_node_SU.restype = _I
         lib.ref_node_SU.argtypes = [_P, _I, _I, _U16P]
+        lib.ref_digest.restype = _I
+        lib.ref_digest.argtypes = [_P, C.POINTER(C.c_uint64)]
         lib.ref_node_C2E.restype = _I
         lib.ref_node_C2E.argtypes = [_P, _I, _I, _I, _U16P]
         lib.ref_node_geometry.restype = _I
@@ -159,6 +161,13 @@ class RefOracle:
         out = np.zeros(3, dtype=np.int32)
         self.lib.ref_stats(self.h, _p(out, _I32P))
         return tuple(int(x) for x in out)
+
+    def digest(self):
+        """Per-level checksum of leaves[m].D / levels[l][m].D_U (the device
+        library's htrip_state_digest formula)."""
+        out = (C.c_uint64 * 64)()
+        n = self.lib.ref_digest(self.h, out)
+        return [int(out[i]) for i in range(n)]
 
     def leaf_D(self, i):
         n = self.b * self.b

@@ -186,4 +186,36 @@ int ref_node_geometry(void* p, int lvl, int n, int32_t* vu, int32_t* ext_idx, in
     return static_cast<int>(N.seam_candidates.size());
 }
 
+// Per-level checksum of the reference's matrices in the form the device
+// library's htrip_state_digest uses: out[l] = sum mod 2^64 over matrices m
+// (leaves[m].D for l = 0, levels[l-1][m].D_U above) and entries (i, j) of
+// splitmix64(((m*n + i)*n + j) << 16 | value).  Returns H + 1 (the number of
+// entries written).
+int ref_digest(void* p, uint64_t* out) {
+    auto& o = static_cast<RefHandle*>(p)->oracle;
+    auto mix = [](uint64_t x) {
+        x += 0x9E3779B97F4A7C15ull;
+        x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+        x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+        return x ^ (x >> 31);
+    };
+    auto sum = [&](const std::vector<dist_t>& D, uint64_t m, uint64_t n) {
+        uint64_t acc = 0;
+        for (uint64_t i = 0; i < n; ++i)
+            for (uint64_t j = 0; j < n; ++j) acc += mix((((m * n + i) * n + j) << 16) | D[i * n + j]);
+        return acc;
+    };
+    out[0] = 0;
+    for (size_t m = 0; m < o.leaves.size(); ++m) {
+        const uint64_t n = static_cast<uint64_t>(o.leaves[m].b) * o.leaves[m].b;
+        out[0] += sum(o.leaves[m].D, m, n);
+    }
+    for (size_t l = 0; l < o.levels.size(); ++l) {
+        out[l + 1] = 0;
+        for (size_t m = 0; m < o.levels[l].size(); ++m)
+            out[l + 1] += sum(o.levels[l][m].D_U, m, o.levels[l][m].V_U.size());
+    }
+    return static_cast<int>(o.levels.size()) + 1;
+}
+
 }  // extern "C"
