@@ -190,6 +190,244 @@ def run_reference(args, rank, world):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Further workloads (1 GPU): incremental opening, many maps batched, served
+# ---------------------------------------------------------------------------
+def _pct(xs, q):
+    return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
+
+
+def bench_opening(device, steps=400):
+    """Incremental opening on a 1024x1024 street grid, b=8: radius-40 disks
+    around 16 robots observed, then `steps` onBatchCellsOpened calls of 256
+    cells in BFS-ring order, each followed by queryAllPairs over 16 robot
+    poses + 48 frontier cells.  Each call is synchronous, timed on the host
+    (submit to host-visible completion).  The reference's own CPU path is
+    timed on the same stream shape at 256x256 (its 1024x1024 update takes
+    tens of seconds per call), beside ours on that same 256x256 stream."""
+    from htrip_b200 import workloads as W
+    from htrip_b200.minplus_oracle import HierarchyConfig, MinPlusOracle
+    truth = W.street_grid(1024, 3)
+    obs, starts, batches = W.exploration_stream(truth, 16, 40, 256, steps, 3)
+    dev = MinPlusOracle(HierarchyConfig(8, 2, 2), device=device)
+    t = time.perf_counter()
+    assert dev.build(obs)
+    build_s = time.perf_counter() - t
+    open_ms, query_ms, cells, entries = [], [], 0, 0
+    for step, c in enumerate(batches):
+        obs[c[:, 0], c[:, 1]] = W.FREE
+        t = time.perf_counter()
+        dev.onBatchCellsOpened(c, obs)
+        open_ms.append(1e3 * (time.perf_counter() - t))
+        cells += len(c)
+        vps = np.concatenate([starts, W.frontier_cells(obs, 48, 1000 + step)]).astype(np.int32)
+        t = time.perf_counter()
+        dev.queryAllPairs(vps, obs)
+        query_ms.append(1e3 * (time.perf_counter() - t))
+        entries += len(vps) ** 2
+    fresh = MinPlusOracle(HierarchyConfig(8, 2, 2), device=device)
+    assert fresh.build(obs)
+    parity = "bit-exact" if fresh.stateDigest() == dev.stateDigest() else "MISMATCH"
+    out = {"workload": f"1024x1024 street, b=8, {len(batches)} onBatchCellsOpened x 256 cells (BFS rings), "
+                       "each + queryAllPairs k=64",
+           "cells_per_s": cells / (1e-3 * sum(open_ms)), "unit": "cells/s",
+           "open_ms_p50": _pct(open_ms, 50), "open_ms_p99": _pct(open_ms, 99),
+           "query_entries_per_s": entries / (1e-3 * sum(query_ms)), "query_ms_p50": _pct(query_ms, 50),
+           "build_s": round(build_s, 4), "parity_vs_rebuild": parity}
+    del dev, fresh
+    # like-for-like reference comparison on a 256x256 stream of the same shape
+    from oracle.ref import RefOracle, ref_available
+    truth = W.street_grid(256, 4)
+    obs0, starts, batches = W.exploration_stream(truth, 4, 20, 256, 24, 4)
+    dev = MinPlusOracle(HierarchyConfig(8, 2, 2), device=device)
+    obs = obs0.copy()
+    assert dev.build(obs)
+    ours = []
+    for c in batches:
+        obs[c[:, 0], c[:, 1]] = W.FREE
+        t = time.perf_counter()
+        dev.onBatchCellsOpened(c, obs)
+        ours.append(time.perf_counter() - t)
+    n_cells = sum(len(c) for c in batches)
+    small = {"workload": f"256x256 street, b=8, {len(batches)} x 256 cells", "gpu_cells_per_s": n_cells / sum(ours)}
+    if ref_available():
+        ref = RefOracle(8)
+        ref.set_grid(obs0)
+        assert ref.build()
+        ref_s = []
+        for c in batches:
+            ref.set_cells(c, W.FREE)
+            t = time.perf_counter()
+            ref.open_batch(c)
+            ref_s.append(time.perf_counter() - t)
+        small.update({"reference_cells_per_s": n_cells / sum(ref_s), "reference_cores": 1,
+                      "reference_kind": "reference", "parity": "bit-exact" if ref.digest() == dev.stateDigest()
+                      else "MISMATCH"})
+    out["small_stream_vs_reference"] = small
+    return out
+
+
+_GRID_CACHE = {}
+
+
+def _palette_grid(side, kind, param):
+    from htrip_b200 import workloads as W
+    key = (side, kind, param)
+    if key not in _GRID_CACHE:
+        _GRID_CACHE[key] = (W.street_grid(side, 17, blocked=param) if kind == "street"
+                            else W.maze_grid(side, int(param), 17))
+    return _GRID_CACHE[key]
+
+
+def _mix_maps(n, seed, budget_bytes=None):
+    """Map specs of the many-maps workloads: side from {128, 256, 512, 1024},
+    street (20/30/40% obstacles) or maze (corridor 1/4/16), b from {8, 16, 32};
+    grids come from a small seeded palette (maps sharing a grid are still
+    independent indexes with their own openings)."""
+    from htrip_b200.minplus_oracle import HierarchyConfig, estimate_bytes
+    rng = np.random.default_rng(seed)
+    out, total = [], 0
+    while len(out) < n:
+        side = int(rng.choice([128, 256, 512, 1024]))
+        kind = "street" if rng.random() < 0.5 else "maze"
+        param = float(rng.choice([0.2, 0.3, 0.4])) if kind == "street" else int(rng.choice([1, 4, 16]))
+        b = int(rng.choice([8, 16, 32]))
+        est = estimate_bytes(HierarchyConfig(b, 2, 2), side, side)
+        if budget_bytes is not None and total + est > budget_bytes:
+            if side == 128:
+                break
+            continue
+        total += est
+        out.append(dict(side=side, kind=kind, param=param, b=b, seed=int(rng.integers(0, 2**31 - 1)), est=est))
+    return out, total
+
+
+def bench_batched(device, n_maps=64):
+    """64 independent maps: one opening batch (64-1024 withheld cells) and one
+    queryAllPairs (k uniform in [8, 512]) per map.  Batched path: ONE
+    htrip_open_batch and ONE htrip_query_batch (one launch of the persistent
+    query kernel over all 64 requests).  Plain path: per map
+    htrip_open_cells then htrip_query_all_pairs.  Same inputs; every matrix
+    and every index state compared between the two (bit-exact)."""
+    from htrip_b200 import workloads as W
+    from htrip_b200.minplus_oracle import Batch, HierarchyConfig, MinPlusOracle
+    specs, total = _mix_maps(n_maps, 5)
+    rng = np.random.default_rng(6)
+    maps = []
+    for sp in specs:
+        truth = _palette_grid(sp["side"], sp["kind"], sp["param"])
+        obs, cells = W.withheld_open(truth, int(rng.integers(64, 1025)), sp["seed"])
+        k = int(rng.integers(8, 513))
+        full = obs.copy()
+        full[cells[:, 0], cells[:, 1]] = W.FREE
+        vps = W.sample_free(full, k, sp["seed"] + 1)
+        maps.append((sp, obs, cells, full, vps))
+    def build_all():
+        out = []
+        for sp, obs, _, _, _ in maps:
+            d = MinPlusOracle(HierarchyConfig(sp["b"], 2, 2), device=device)
+            assert d.build(obs)
+            out.append(d)
+        return out
+    plain = build_all()
+    t0 = time.perf_counter()
+    t_open = 0.0
+    plain_out = []
+    for d, (sp, obs, cells, full, vps) in zip(plain, maps):
+        t = time.perf_counter()
+        d.onBatchCellsOpened(cells, full)
+        t_open += time.perf_counter() - t
+        plain_out.append(d.queryAllPairs(vps, full))
+    t_plain = time.perf_counter() - t0
+    digests = [d.stateDigest() for d in plain]
+    del plain
+    batched = build_all()
+    bt = Batch(device)
+    t0 = time.perf_counter()
+    bt.open([(d, cells, full) for d, (sp, obs, cells, full, vps) in zip(batched, maps)])
+    t_bopen = time.perf_counter() - t0
+    outs = bt.query([(d, vps, full) for d, (sp, obs, cells, full, vps) in zip(batched, maps)])
+    t_batched = time.perf_counter() - t0
+    kern_ms = bt.lastKernelMs()
+    ok = all(np.array_equal(a, b) for a, b in zip(outs, plain_out)) and \
+        all(d.stateDigest() == g for d, g in zip(batched, digests))
+    n_cells = sum(len(m[2]) for m in maps)
+    n_entries = sum(len(m[4]) ** 2 for m in maps)
+    del batched
+    return {"workload": f"{len(maps)} maps (sides 128-1024, street/maze, b 8/16/32, "
+                        f"{total / 2**30:.1f} GiB of indexes): one opening batch (64-1024 cells) + one "
+                        "queryAllPairs (k 8-512) per map",
+            "batched_s": t_batched, "plain_s": t_plain, "speedup_vs_plain": t_plain / t_batched,
+            "batched_cells_per_s": n_cells / t_bopen, "plain_cells_per_s": n_cells / t_open,
+            "batched_entries_per_s": n_entries / (t_batched - t_bopen),
+            "plain_entries_per_s": n_entries / (t_plain - t_open),
+            "query_launch_kernel_ms": kern_ms, "query_launches": 1,
+            "parity_vs_plain": "bit-exact" if ok else "MISMATCH"}
+
+
+def bench_served(device, rates=(5000.0, 20000.0, 50000.0), max_requests=10000, plain_requests=2500,
+                 budget_gb=120.0, n_sessions=256):
+    """256 resident map sessions (128^2-1024^2, about 120 GB of indexes) under
+    open-loop Poisson arrivals: 70% queryAllPairs with k log-uniform in
+    [4, 512], 30% onBatchCellsOpened of 1-512 cells.  Each session explores
+    its map: it starts with radius-40 disks around 4 robots observed and
+    opens cells in BFS-ring order from there (the exploration stream of the
+    incremental-opening workload).  The batched server (htrip_server,
+    continuous batching) at several rates (one second of arrivals, at most
+    `max_requests`), beside the plain per-call server (one request at a time,
+    no batching) on the first `plain_requests` requests of the lowest-rate
+    trace.  Latency = submission to host-visible result."""
+    from htrip_b200 import workloads as W
+    from htrip_b200.minplus_oracle import HierarchyConfig, Server
+    specs, total = _mix_maps(n_sessions, 9, budget_bytes=int(budget_gb * 2**30))
+    pools, streams = [], {}
+    for sp in specs:
+        key = (sp["side"], sp["kind"], sp["param"], sp["seed"] % 2)
+        truth = _palette_grid(sp["side"], sp["kind"], sp["param"])
+        if key not in streams:
+            obs, starts, batches = W.exploration_stream(truth, 4, 40, 512, 64, key[3])
+            streams[key] = (obs, np.concatenate(batches) if batches else np.zeros((0, 2), np.int32))
+        obs, cells = streams[key]
+        pools.append((truth, obs, cells, sp["b"]))
+
+    def run(rate, n_req, plain, trace=None):
+        srv = Server(device=device, plain=plain)
+        sids = [srv.add_session(HierarchyConfig(b, 2, 2), obs) for _, obs, _, b in pools]
+        reqs, arrival = trace if trace is not None else \
+            W.served_trace([(t, c) for t, _, c, _ in pools], n_req, rate, int(rate) + 1)
+        outs, lat, wall = srv.run_trace([(sids[s], k, rc) for s, k, rc in reqs], arrival)
+        st = srv.stats()
+        srv.close()
+        q = [l for (s, k, rc), l in zip(reqs, lat) if k == 0]
+        o = [l for (s, k, rc), l in zip(reqs, lat) if k == 1]
+        entries = sum(len(rc) ** 2 for s, k, rc in reqs if k == 0)
+        cells = sum(len(rc) for s, k, rc in reqs if k == 1)
+        return {"rate_req_s": rate, "requests": n_req, "wall_s": wall,
+                "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99),
+                "query_p50_ms": _pct(q, 50), "query_p99_ms": _pct(q, 99),
+                "open_p50_ms": _pct(o, 50), "open_p99_ms": _pct(o, 99),
+                "entries_per_s": entries / wall, "cells_per_s": cells / wall,
+                "launches": int(st["launches_query"] + st["launches_open"])}, reqs, outs
+
+    served = []
+    first = None
+    for r in rates:
+        res, reqs, outs = run(r, min(max_requests, int(r)), False)
+        served.append(res)
+        if first is None:
+            first = (reqs, outs)
+    # the plain per-call path on a prefix of the same trace
+    reqs0, arrival0 = W.served_trace([(t, c) for t, _, c, _ in pools], min(max_requests, int(rates[0])), rates[0],
+                                     int(rates[0]) + 1)
+    n = min(plain_requests, len(reqs0))
+    plain, preqs, pouts = run(rates[0], n, True, trace=(reqs0[:n], arrival0[:n]))
+    same = all(a is None or np.array_equal(a, b) for a, b in zip(first[1][:n], pouts[:n]))
+    return {"workload": f"{len(specs)} sessions (sides 128-1024, b 8/16/32, {total / 2**30:.0f} GiB of indexes), "
+                        "Poisson arrivals, 70% queryAllPairs (k log-uniform 4-512), 30% openings (1-512 cells)",
+            "served": served, "plain_per_call": plain,
+            "parity_served_vs_plain": "bit-exact" if same else "MISMATCH"}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -282,6 +520,16 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": args.steps,
         "parity": parity,
     }
+    if world == 1 and not args.headline_only:
+        for name, fn in (("cells_opened", lambda: bench_opening(local_rank)),
+                         ("batched", lambda: bench_batched(local_rank)),
+                         ("served", lambda: bench_served(local_rank))):
+            t = time.perf_counter()
+            try:
+                line[name] = fn()
+            except Exception as e:  # a failing section is reported, the headline line still prints
+                line[name] = {"error": f"{type(e).__name__}: {e}"}
+            log(f"{name}: {time.perf_counter() - t:.1f} s")
     print(json.dumps(line), flush=True)
     return 0
 
@@ -292,6 +540,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--headline-only", action="store_true",
+                    help="only the queryAllPairs headline (skip the opening / batched / served workloads)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))

@@ -153,6 +153,10 @@ struct htrip_index {
     cudaStream_t stream = nullptr;
     int b = 16, g = 2;
     bool built = false;
+    bool offloaded = false;  // matrices parked in host memory (htrip_offload)
+    std::vector<std::vector<uint16_t>> parked;  // per level matrices, then the passability mirror
+    size_t parked_pass = 0;
+    uint64_t ref_bytes = 0;  // the reference's totalMemoryBytes accounting of this index
     int S = 0, H = 0, rows = 0, cols = 0, leaves_x = 0;
     std::vector<Level> L;
     DevBuf<uint8_t> pass;
@@ -267,6 +271,19 @@ void make_levels(htrip_index* h) {
     }
 }
 
+// The reference's accounting of an index of this geometry: D and S of
+// every leaf, D_U, S_U and child_to_ext of every node
+// (MinPlusOracle::totalMemoryBytes, minplus_oracle.cpp:2116-2134).
+uint64_t reference_bytes(const htrip_index* h) {
+    const Level& L0 = h->L[0];
+    uint64_t ref = (uint64_t)L0.nnodes * ((uint64_t)L0.n * L0.n + (uint64_t)L0.nExt * L0.nExt) * 2;
+    for (int l = 1; l <= h->H; ++l) {
+        const Level& Lv = h->L[l];
+        ref += (uint64_t)Lv.nnodes * ((uint64_t)Lv.n * Lv.n + (uint64_t)Lv.nExt * Lv.nExt + (uint64_t)Lv.n * Lv.nExt) * 2;
+    }
+    return ref;
+}
+
 void alloc_levels(htrip_index* h) {
     for (auto& Lv : h->L) {
         Lv.mat.reserve((size_t)Lv.nnodes * Lv.NP * Lv.NP);
@@ -336,12 +353,15 @@ void do_build(htrip_index* h, const uint8_t* observed, int rows, int cols) {
     for (int t = S / b; t > 1; t /= g) ++H;
     h->release();
     h->built = false;
+    h->offloaded = false;
+    h->parked.clear();
     h->S = S;
     h->H = H;
     h->rows = rows;
     h->cols = cols;
     h->leaves_x = S / b;
     make_levels(h);
+    h->ref_bytes = reference_bytes(h);
     alloc_levels(h);
     cudaStream_t st = h->stream;
     // Passability mirror, padded to S x S (outside the grid = not passable).
@@ -1113,6 +1133,13 @@ unsigned char* noalloc_scratch(int dev) {
         return fail(HTRIP_ERR_OOM, "host allocation failed");                               \
     }
 
+// OK when the index can serve calls: built and resident on the device.
+static htrip_status ready(const htrip_index* h) {
+    if (!h->built) return fail(HTRIP_ERR_NOT_BUILT, "index not built");
+    if (h->offloaded) return fail(HTRIP_ERR_INVALID, "index is offloaded to host memory (htrip_restore first)");
+    return HTRIP_OK;
+}
+
 extern "C" {
 
 const char* htrip_last_error(void) { return g_err.c_str(); }
@@ -1166,7 +1193,7 @@ htrip_status htrip_build(htrip_index* h, const uint8_t* observed, int32_t rows, 
 htrip_status htrip_open_cells(htrip_index* h, const int32_t* rc, int32_t n, const uint8_t* observed, int32_t rows,
                               int32_t cols) {
     if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
-    if (!h->built) return fail(HTRIP_ERR_NOT_BUILT, "index not built");
+    if (const htrip_status rs = ready(h)) return rs;
     if (n < 0 || (n > 0 && !rc) || !observed) return fail(HTRIP_ERR_INVALID, "bad arguments");
     HTRIP_GUARD_BEGIN
     ck(cudaSetDevice(h->device), "cudaSetDevice");
@@ -1177,7 +1204,7 @@ htrip_status htrip_open_cells(htrip_index* h, const int32_t* rc, int32_t n, cons
 
 htrip_status htrip_open_cell(htrip_index* h, int32_t r, int32_t c, const uint8_t* observed, int32_t rows, int32_t cols) {
     if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
-    if (!h->built) return fail(HTRIP_ERR_NOT_BUILT, "index not built");
+    if (const htrip_status rs = ready(h)) return rs;
     if (!observed) return fail(HTRIP_ERR_INVALID, "bad arguments");
     HTRIP_GUARD_BEGIN
     ck(cudaSetDevice(h->device), "cudaSetDevice");
@@ -1190,7 +1217,7 @@ htrip_status htrip_open_cell(htrip_index* h, int32_t r, int32_t c, const uint8_t
 htrip_status htrip_query_all_pairs(htrip_index* h, const int32_t* vps, int32_t k, const uint8_t* observed, int32_t rows,
                                    int32_t cols, uint16_t* out) {
     if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
-    if (!h->built) return fail(HTRIP_ERR_NOT_BUILT, "index not built");
+    if (const htrip_status rs = ready(h)) return rs;
     if (k < 0 || (k > 0 && (!vps || !out)) || !observed) return fail(HTRIP_ERR_INVALID, "bad arguments");
     if (k == 0) return HTRIP_OK;
     HTRIP_GUARD_BEGIN
@@ -1208,7 +1235,7 @@ htrip_status htrip_query_all_pairs(htrip_index* h, const int32_t* vps, int32_t k
 htrip_status htrip_query_all_pairs_dev(htrip_index* h, const int32_t* vps_dev, const uint8_t* passable_dev, int32_t k,
                                        uint16_t* out_dev) {
     if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
-    if (!h->built) return fail(HTRIP_ERR_NOT_BUILT, "index not built");
+    if (const htrip_status rs = ready(h)) return rs;
     if (k < 0 || (k > 0 && (!vps_dev || !passable_dev || !out_dev))) return fail(HTRIP_ERR_INVALID, "bad arguments");
     if (k == 0) return HTRIP_OK;
     HTRIP_GUARD_BEGIN
@@ -1242,7 +1269,7 @@ htrip_status htrip_query_all_pairs_dev(htrip_index* h, const int32_t* vps_dev, c
 htrip_status htrip_query_all_pairs_noalloc(htrip_index* h, const int32_t* vps, int32_t k, const uint8_t* observed,
                                            int32_t rows, int32_t cols, uint16_t* out) {
     if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
-    if (!h->built) return fail(HTRIP_ERR_NOT_BUILT, "index not built");
+    if (const htrip_status rs = ready(h)) return rs;
     if (k < 0 || (k > 0 && (!vps || !out)) || !observed) return fail(HTRIP_ERR_INVALID, "bad arguments");
     if (k == 0) return HTRIP_OK;
     const int H = h->H;
@@ -1320,6 +1347,7 @@ htrip_status htrip_query_batch(htrip_batch* b, const htrip_query_request* reqs, 
         const htrip_query_request& r = reqs[i];
         if (!r.index) return fail(HTRIP_ERR_INVALID, "request " + std::to_string(i) + ": null index");
         if (!r.index->built) return fail(HTRIP_ERR_NOT_BUILT, "request " + std::to_string(i) + ": index not built");
+        if (r.index->offloaded) return fail(HTRIP_ERR_INVALID, "request " + std::to_string(i) + ": index offloaded");
         if (r.index->device != b->device)
             return fail(HTRIP_ERR_INVALID, "request " + std::to_string(i) + ": index on another device");
         if (r.k < 0 || (r.k > 0 && (!r.vps || !r.out)) || !r.observed)
@@ -1362,6 +1390,7 @@ htrip_status htrip_open_batch(htrip_batch* b, const htrip_open_request* reqs, in
         const htrip_open_request& r = reqs[i];
         if (!r.index) return fail(HTRIP_ERR_INVALID, "request " + std::to_string(i) + ": null index");
         if (!r.index->built) return fail(HTRIP_ERR_NOT_BUILT, "request " + std::to_string(i) + ": index not built");
+        if (r.index->offloaded) return fail(HTRIP_ERR_INVALID, "request " + std::to_string(i) + ": index offloaded");
         if (r.index->device != b->device)
             return fail(HTRIP_ERR_INVALID, "request " + std::to_string(i) + ": index on another device");
         if (r.n < 0 || (r.n > 0 && !r.rc) || !r.observed)
@@ -1408,6 +1437,7 @@ htrip_status htrip_clone(const htrip_index* src, htrip_index** out) {
     *out = nullptr;
     HTRIP_GUARD_BEGIN
     ck(cudaSetDevice(src->device), "cudaSetDevice");
+    if (src->offloaded) return fail(HTRIP_ERR_INVALID, "index is offloaded to host memory (htrip_restore first)");
     ck(cudaStreamSynchronize(src->stream), "sync");
     auto* h = new htrip_index();
     h->device = src->device;
@@ -1427,6 +1457,7 @@ htrip_status htrip_clone(const htrip_index* src, htrip_index** out) {
             ck(cudaStreamSynchronize(h->stream), "clone sync");
             h->built = true;
             h->stats = src->stats;
+            h->ref_bytes = src->ref_bytes;
         }
     } catch (...) {
         htrip_destroy(h);
@@ -1490,7 +1521,7 @@ htrip_status htrip_query_work(const htrip_index* h, const int32_t* vps, int32_t 
 
 htrip_status htrip_state_digest(const htrip_index* h, uint64_t* out, int32_t n_out) {
     if (!h || !out) return fail(HTRIP_ERR_INVALID, "null argument");
-    if (!h->built) return fail(HTRIP_ERR_NOT_BUILT, "index not built");
+    if (const htrip_status rs = ready(h)) return rs;
     if (n_out < h->H + 1) return fail(HTRIP_ERR_INVALID, "digest needs H + 1 entries");
     HTRIP_GUARD_BEGIN
     ck(cudaSetDevice(h->device), "cudaSetDevice");
@@ -1502,6 +1533,19 @@ htrip_status htrip_state_digest(const htrip_index* h, uint64_t* out, int32_t n_o
     ck(cudaMemcpyAsync(out, d.p, (h->H + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream), "digest d2h");
     ck(cudaStreamSynchronize(h->stream), "digest sync");
     d.release();
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_measure_minplus_rate(int device, int variant, double* entries_per_s) {
+    if (!entries_per_s || variant < 0 || variant > 3) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    int sms = 0;
+    ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "attribute");
+    const double r = hb::measure_minplus_rate(variant, sms);
+    if (r <= 0) return fail(HTRIP_ERR_CUDA, "min-plus rate kernel failed");
+    *entries_per_s = r;
     return HTRIP_OK;
     HTRIP_GUARD_END
 }
@@ -1547,22 +1591,99 @@ htrip_status htrip_last_batch_stats(const htrip_index* h, htrip_batch_stats* out
     return HTRIP_OK;
 }
 
+htrip_status htrip_offload(htrip_index* h) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    if (const htrip_status rs = ready(h)) return rs;
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    ck(cudaStreamSynchronize(h->stream), "sync");
+    std::vector<std::vector<uint16_t>> parked(h->H + 2);
+    for (int l = 0; l <= h->H; ++l) {
+        parked[l].resize(h->L[l].mat.n);
+        ck(cudaMemcpyAsync(parked[l].data(), h->L[l].mat.p, h->L[l].mat.n * sizeof(uint16_t), cudaMemcpyDeviceToHost,
+                           h->stream), "offload");
+    }
+    parked[h->H + 1].resize((h->pass.n + 1) / 2);
+    ck(cudaMemcpyAsync(parked[h->H + 1].data(), h->pass.p, h->pass.n, cudaMemcpyDeviceToHost, h->stream), "offload");
+    ck(cudaStreamSynchronize(h->stream), "offload sync");
+    const size_t pass_n = h->pass.n;
+    h->release();  // every device buffer of the index (geometry is rebuilt on restore)
+    h->parked = std::move(parked);
+    h->parked_pass = pass_n;
+    h->offloaded = true;
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_restore(htrip_index* h) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    if (!h->built) return fail(HTRIP_ERR_NOT_BUILT, "index not built");
+    if (!h->offloaded) return HTRIP_OK;
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    try {
+        make_levels(h);
+        alloc_levels(h);
+        for (int l = 0; l <= h->H; ++l)
+            ck(cudaMemcpyAsync(h->L[l].mat.p, h->parked[l].data(), h->L[l].mat.n * sizeof(uint16_t),
+                               cudaMemcpyHostToDevice, h->stream), "restore");
+        h->pass.reserve(h->parked_pass);
+        ck(cudaMemcpyAsync(h->pass.p, h->parked[h->H + 1].data(), h->parked_pass, cudaMemcpyHostToDevice, h->stream),
+           "restore");
+        ck(cudaStreamSynchronize(h->stream), "restore sync");
+    } catch (const CudaError&) {
+        h->release();  // still offloaded: the parked copy is intact
+        throw;
+    }
+    h->parked.clear();
+    h->parked.shrink_to_fit();
+    h->offloaded = false;
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_is_resident(const htrip_index* h, int32_t* resident) {
+    if (!h || !resident) return fail(HTRIP_ERR_INVALID, "null argument");
+    *resident = h->built && !h->offloaded;
+    return HTRIP_OK;
+}
+
+htrip_status htrip_estimate_bytes(htrip_config cfg, int32_t rows, int32_t cols, uint64_t* device_bytes) {
+    if (!device_bytes) return fail(HTRIP_ERR_INVALID, "null argument");
+    const int b = cfg.tile_size_b, g = cfg.group;
+    if (!(b >= 2 && b <= 32 && g >= 2 && g * g <= 256) || std::max(rows, cols) <= 0)
+        return fail(HTRIP_ERR_INVALID, "invalid config or grid");
+    htrip_index tmp;
+    tmp.b = b;
+    tmp.g = g;
+    int S = b;
+    while (S < std::max(rows, cols)) S *= g;
+    int H = 0;
+    for (int t = S / b; t > 1; t /= g) ++H;
+    tmp.S = S;
+    tmp.H = H;
+    tmp.leaves_x = S / b;
+    make_levels(&tmp);
+    uint64_t bytes = (uint64_t)S * S;  // passability mirror
+    for (const auto& Lv : tmp.L) {
+        const uint64_t mats = (uint64_t)Lv.nnodes * Lv.NP;
+        bytes += mats * Lv.NP * sizeof(uint16_t) + mats /* pivot flags */ + mats * sizeof(int) /* pivot lists */ +
+                 (uint64_t)Lv.nnodes * (2 * sizeof(int) + 1) + (uint64_t)(Lv.nExt + Lv.NP + Lv.seams.size()) * sizeof(int);
+    }
+    *device_bytes = bytes;
+    return HTRIP_OK;
+    }
+
 htrip_status htrip_memory_bytes(const htrip_index* h, uint64_t* reference_bytes, uint64_t* device_bytes) {
     if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
     uint64_t ref = 0, dev = 0;
     if (h->built) {
-        const Level& L0 = h->L[0];
-        ref += (uint64_t)L0.nnodes * ((uint64_t)L0.n * L0.n + (uint64_t)L0.nExt * L0.nExt) * 2;
-        for (int l = 1; l <= h->H; ++l) {
-            const Level& Lv = h->L[l];
-            ref += (uint64_t)Lv.nnodes *
-                   ((uint64_t)Lv.n * Lv.n + (uint64_t)Lv.nExt * Lv.nExt + (uint64_t)Lv.n * Lv.nExt) * 2;
-        }
+        ref = h->ref_bytes;
         for (const auto& Lv : h->L)
             dev += (Lv.mat.n + Lv.klist.n * 2 + Lv.kcnt.n * 2) * sizeof(uint16_t) + Lv.kflag.n + Lv.dec.n +
                    (Lv.d_ext.n + Lv.d_seams.n) * sizeof(int);
         dev += h->pass.n + h->panel.n * 2 + h->pflags.n + h->snap.n * 2 + h->q.dev.n + h->upd.n * 4 +
-               h->active.n * 4;
+               h->active.n * 4 + h->rb_dev.n * 4;
     }
     if (reference_bytes) *reference_bytes = ref;
     if (device_bytes) *device_bytes = dev;
@@ -1589,7 +1710,7 @@ static htrip_status read_block(const htrip_index* h, int lvl, int node, const in
 }
 
 static bool valid_node(const htrip_index* h, int lvl, int node) {
-    return h && h->built && lvl >= 0 && lvl <= h->H && node >= 0 && node < h->L[lvl].nnodes;
+    return h && h->built && !h->offloaded && lvl >= 0 && lvl <= h->H && node >= 0 && node < h->L[lvl].nnodes;
 }
 
 htrip_status htrip_read_leaf_D(const htrip_index* h, int32_t leaf, uint16_t* out) {

@@ -442,6 +442,40 @@ __global__ void __launch_bounds__(256) digest_kernel(MatSet M, int count, unsign
     if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
 }
 
+// Register-only rate of the packed-u16 min-plus update, 16 entries per
+// thread per iteration on 8 independent accumulators.  Variants:
+//   0  clamped: min2(add2(min2(b, INF - a), a), c)      (any a <= INF)
+//   1  clamped with the fused add+min (__viaddmin_u16x2)
+//   2  fast:    min2(add2(b, a), c)                      (a <= 5535)
+//   3  fast with the fused add+min
+// Operands stay below 16384, so no variant wraps.
+template <int V>
+__global__ void __launch_bounds__(512) minplus_rate_kernel(int iters, uint32_t seed, uint32_t* sink) {
+    uint32_t acc[8], bv[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        acc[c] = INF2 - (threadIdx.x + c);
+        bv[c] = ((seed * (c + 1) + threadIdx.x) & 0x3FFFu) * 0x10001u;
+    }
+    uint32_t a = (threadIdx.x * 7u + seed) & 0x3FFFu;
+    for (int i = 0; i < iters; ++i) {
+        const uint32_t aa = splat(a);
+        const uint32_t tt = INF2 - aa;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            if constexpr (V == 0) acc[c] = min2(add2(min2(bv[c], tt), aa), acc[c]);
+            else if constexpr (V == 1) acc[c] = __viaddmin_u16x2(min2(bv[c], tt), aa, acc[c]);
+            else if constexpr (V == 2) acc[c] = min2(add2(bv[c], aa), acc[c]);
+            else acc[c] = __viaddmin_u16x2(bv[c], aa, acc[c]);
+        }
+        a = (a + 5u) & 0x3FFFu;
+    }
+    uint32_t x = 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) x ^= acc[c];
+    if (x == seed) sink[0] = x;
+}
+
 __global__ void gather_counts_kernel(const int* __restrict__ kcnt, const int* __restrict__ active, int n, int* out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = kcnt[active[i]];
@@ -566,6 +600,35 @@ void launch_digest(MatSet M, int count, unsigned long long* out, cudaStream_t st
 void launch_gather_counts(const int* kcnt, const int* active, int n, int* out, cudaStream_t st) {
     if (n == 0) return;
     gather_counts_kernel<<<blocks_for(n, 256), 256, 0, st>>>(kcnt, active, n, out);
+}
+
+double measure_minplus_rate(int variant, int sms) {
+    const int iters = 4096, threads = 512, blocks = sms * 4;
+    uint32_t* sink = nullptr;
+    if (cudaMalloc(&sink, sizeof(uint32_t)) != cudaSuccess) return -1.0;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto launch = [&](int it) {
+        switch (variant) {
+            case 0: minplus_rate_kernel<0><<<blocks, threads>>>(it, 12345u, sink); break;
+            case 1: minplus_rate_kernel<1><<<blocks, threads>>>(it, 12345u, sink); break;
+            case 2: minplus_rate_kernel<2><<<blocks, threads>>>(it, 12345u, sink); break;
+            default: minplus_rate_kernel<3><<<blocks, threads>>>(it, 12345u, sink); break;
+        }
+    };
+    launch(64);  // warm-up
+    cudaEventRecord(e0);
+    launch(iters);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    if (cudaGetLastError() != cudaSuccess || ms <= 0.f) return -1.0;
+    return (double)blocks * threads * iters * 16.0 / (ms * 1e-3);
 }
 
 }  // namespace hb

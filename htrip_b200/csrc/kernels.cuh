@@ -149,6 +149,10 @@ cudaError_t launch_query(const QueryLaunch& L, int cfg, int grid, cudaStream_t s
 // entries only): sum of splitmix64(((m*n + i)*n + j) << 16 | D[i][j]).
 void launch_digest(MatSet M, int count, unsigned long long* out, cudaStream_t st);
 
+// Entries per second of the register-only packed-u16 min-plus update
+// (variant 0..3, see minplus_rate_kernel) on `sms` SMs x 4 CTAs; -1 on error.
+double measure_minplus_rate(int variant, int sms);
+
 // ptr[0 .. n) = value.
 void launch_fill_u16(uint16_t* ptr, size_t n, uint16_t value, cudaStream_t st);
 

@@ -51,6 +51,21 @@ class _OpenRequest(C.Structure):
                 ("rows", C.c_int32), ("cols", C.c_int32)]
 
 
+class _ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64), ("max_requests_per_launch", C.c_int32),
+                ("plain_per_call", C.c_int32)]
+
+
+class _ServerStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in (
+        "launches_query", "launches_open", "requests_query", "requests_open", "evictions", "restores",
+        "sessions", "resident_sessions", "resident_bytes", "budget_bytes")]
+
+
+class _ServerRequest(C.Structure):
+    _fields_ = [("session", C.c_int64), ("kind", C.c_int32), ("rc", _I32P), ("n", C.c_int32), ("out", _U16P)]
+
+
 class _Stats(C.Structure):
     _fields_ = [("n_touched_leaves", C.c_int32), ("n_dirty_ancestors", C.c_int32), ("n_pivots", C.c_int32)]
 
@@ -64,7 +79,11 @@ EXPORTS = (
     "htrip_read_node_DU", "htrip_read_node_SU", "htrip_read_node_C2E", "htrip_level_dims", "htrip_query_work",
     "htrip_last_query_kernel_ms", "htrip_last_query_io", "htrip_query_all_pairs_noalloc",
     "htrip_batch_create", "htrip_batch_destroy", "htrip_query_batch", "htrip_batch_last_kernel_ms",
-    "htrip_state_digest", "htrip_open_batch",
+    "htrip_state_digest", "htrip_open_batch", "htrip_offload", "htrip_restore", "htrip_is_resident",
+    "htrip_estimate_bytes", "htrip_server_last_error", "htrip_server_create", "htrip_server_destroy",
+    "htrip_server_add_session", "htrip_server_remove_session", "htrip_server_submit_query",
+    "htrip_server_submit_open", "htrip_server_wait", "htrip_server_get_stats", "htrip_server_run_trace",
+    "htrip_measure_minplus_rate",
 )
 
 
@@ -110,8 +129,24 @@ def load_library(path: str | None = None):
     lib.htrip_query_batch.argtypes = [P, C.POINTER(_QueryRequest), I]
     lib.htrip_batch_last_kernel_ms.argtypes = [P, C.POINTER(C.c_float)]
     lib.htrip_open_batch.argtypes = [P, C.POINTER(_OpenRequest), I]
+    lib.htrip_measure_minplus_rate.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
+    lib.htrip_offload.argtypes = [P]
+    lib.htrip_restore.argtypes = [P]
+    lib.htrip_is_resident.argtypes = [P, _I32P]
+    lib.htrip_estimate_bytes.argtypes = [_Config, I, I, _U64P]
+    lib.htrip_server_last_error.restype = C.c_char_p
+    lib.htrip_server_create.argtypes = [C.POINTER(_ServerConfig), C.POINTER(P)]
+    lib.htrip_server_destroy.argtypes = [P]
+    lib.htrip_server_add_session.argtypes = [P, _Config, _U8P, I, I, C.POINTER(C.c_int64)]
+    lib.htrip_server_remove_session.argtypes = [P, C.c_int64]
+    lib.htrip_server_submit_query.argtypes = [P, C.c_int64, _I32P, I, _U16P, _U64P]
+    lib.htrip_server_submit_open.argtypes = [P, C.c_int64, _I32P, I, _U64P]
+    lib.htrip_server_wait.argtypes = [P, C.c_uint64, C.POINTER(C.c_double)]
+    lib.htrip_server_get_stats.argtypes = [P, C.POINTER(_ServerStats)]
+    lib.htrip_server_run_trace.argtypes = [P, C.POINTER(_ServerRequest), C.POINTER(C.c_double), I,
+                                           C.POINTER(C.c_double), C.POINTER(C.c_double)]
     for f in EXPORTS:
-        if f not in ("htrip_last_error", "htrip_stream"):
+        if f not in ("htrip_last_error", "htrip_stream", "htrip_server_last_error"):
             getattr(lib, f).restype = C.c_int
     _lib = lib
     return lib
@@ -120,6 +155,11 @@ def load_library(path: str | None = None):
 def _check(status: int):
     if status != 0:
         raise HtripError(status, _lib.htrip_last_error().decode())
+
+
+def _check_server(status: int):
+    if status != 0:
+        raise HtripError(status, _lib.htrip_server_last_error().decode())
 
 
 @dataclass
@@ -321,6 +361,18 @@ class MinPlusOracle:
         _check(self.lib.htrip_memory_bytes(self.h, C.byref(ref), C.byref(dev)))
         return dev.value
 
+    def offload(self):
+        """Park the index in host memory and free its device memory (htrip_offload)."""
+        _check(self.lib.htrip_offload(self.h))
+
+    def restore(self):
+        _check(self.lib.htrip_restore(self.h))
+
+    def isResident(self) -> bool:
+        r = C.c_int32()
+        _check(self.lib.htrip_is_resident(self.h, C.byref(r)))
+        return bool(r.value)
+
     def stateDigest(self):
         """Per-level checksum of every leaf D and node D_U (htrip_state_digest)."""
         n = self.H + 1
@@ -419,3 +471,102 @@ class Batch:
         ms = C.c_float()
         _check(self.lib.htrip_batch_last_kernel_ms(self.h, C.byref(ms)))
         return ms.value
+
+
+
+def minplus_rate(device: int = 0, variant: int = 0) -> float:
+    """Measured register-only packed-u16 min-plus rate (entries/s) of the device."""
+    lib = load_library()
+    out = C.c_double()
+    _check(lib.htrip_measure_minplus_rate(device, variant, C.byref(out)))
+    return out.value
+
+
+def estimate_bytes(config: HierarchyConfig, rows: int, cols: int) -> int:
+    """Device bytes an index of this config and grid holds after build."""
+    lib = load_library()
+    out = C.c_uint64()
+    _check(lib.htrip_estimate_bytes(_Config(config.tile_size_b, config.group_w), rows, cols, C.byref(out)))
+    return out.value
+
+
+class Server:
+    """Request server over many resident map sessions (htrip_server_*)."""
+
+    QUERY, OPEN = 0, 1
+
+    def __init__(self, device: int = 0, budget_bytes: int = 0, max_per_launch: int = 0, plain: bool = False):
+        self.lib = load_library()
+        h = C.c_void_p()
+        cfg = _ServerConfig(device, budget_bytes, max_per_launch, 1 if plain else 0)
+        _check_server(self.lib.htrip_server_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self._pending = {}
+
+    def close(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.lib.htrip_server_destroy(h)
+            self.h = None
+
+    __del__ = close
+
+    def add_session(self, config: HierarchyConfig, grid) -> int:
+        obs, ptr, rows, cols = _grid_args(grid)
+        sid = C.c_int64()
+        _check_server(self.lib.htrip_server_add_session(self.h, _Config(config.tile_size_b, config.group_w), ptr,
+                                                        rows, cols, C.byref(sid)))
+        return sid.value
+
+    def remove_session(self, sid: int):
+        _check_server(self.lib.htrip_server_remove_session(self.h, sid))
+
+    def submit_query(self, sid: int, vps):
+        rc = _rc(vps)
+        out = np.empty((len(rc), len(rc)), dtype=np.uint16)
+        t = C.c_uint64()
+        _check_server(self.lib.htrip_server_submit_query(self.h, sid, rc.ctypes.data_as(_I32P), len(rc),
+                                                         out.ctypes.data_as(_U16P), C.byref(t)))
+        self._pending[t.value] = (rc, out)
+        return t.value, out
+
+    def submit_open(self, sid: int, cells):
+        rc = _rc(cells)
+        t = C.c_uint64()
+        _check_server(self.lib.htrip_server_submit_open(self.h, sid, rc.ctypes.data_as(_I32P), len(rc), C.byref(t)))
+        self._pending[t.value] = (rc, None)
+        return t.value
+
+    def wait(self, ticket: int) -> float:
+        lat = C.c_double()
+        try:
+            _check_server(self.lib.htrip_server_wait(self.h, ticket, C.byref(lat)))
+        finally:
+            self._pending.pop(ticket, None)
+        return lat.value
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        _check_server(self.lib.htrip_server_get_stats(self.h, C.byref(st)))
+        return {n: getattr(st, n) for n, _ in _ServerStats._fields_}
+
+    def run_trace(self, requests, arrival_s):
+        """requests: list of (session, kind, rc); open-loop submission at
+        arrival_s[i] seconds.  Returns (outs, latency_ms array, wall_s);
+        outs[i] is the (k, k) matrix of a query, None for an opening."""
+        n = len(requests)
+        arr = (_ServerRequest * max(1, n))()
+        keep, outs = [], []
+        for i, (sid, kind, rc) in enumerate(requests):
+            rc = _rc(rc)
+            out = np.empty((len(rc), len(rc)), dtype=np.uint16) if kind == self.QUERY else None
+            keep.append(rc)
+            outs.append(out)
+            arr[i] = _ServerRequest(sid, kind, rc.ctypes.data_as(_I32P), len(rc),
+                                    out.ctypes.data_as(_U16P) if out is not None else None)
+        t = np.ascontiguousarray(arrival_s, dtype=np.float64)
+        lat = np.empty(n, dtype=np.float64)
+        wall = C.c_double()
+        _check_server(self.lib.htrip_server_run_trace(self.h, arr, t.ctypes.data_as(C.POINTER(C.c_double)), n,
+                                                      lat.ctypes.data_as(C.POINTER(C.c_double)), C.byref(wall)))
+        return outs, lat, wall.value

@@ -133,7 +133,8 @@ def exploration_stream(truth: np.ndarray, n_robots: int, radius: int, batch: int
     seen = observed == FREE
     q = deque(zip(*np.nonzero(seen)))
     order = []
-    while q:
+    need = batch * n_batches
+    while q and len(order) < need:
         r, c = q.popleft()
         for dr, dc in ((-1, 0), (1, 0), (0, -1), (0, 1)):
             nr, nc = r + dr, c + dc
@@ -205,3 +206,39 @@ def withheld_open(truth: np.ndarray, n_open: int, seed: int):
     obs = truth.copy()
     obs[cells[:, 0], cells[:, 1]] = UNKNOWN
     return obs, cells
+
+
+def served_trace(pools, n_req: int, rate: float, seed: int, q_frac: float = 0.7,
+                 k_range=(4, 512), open_range=(1, 512)):
+    """Open-loop request stream over map sessions.
+
+    ``pools``: per session ``(truth, withheld)`` - the ground-truth grid and
+    the cells still to be opened, in opening order.  Arrivals are Poisson at
+    ``rate`` requests/s; a request is an all-pairs query with probability
+    ``q_frac`` (k log-uniform in ``k_range``, viewpoints uniform on the
+    session's ground-truth Free cells, so some may still be unobserved and
+    answer INF) and otherwise an opening of the session's next m cells, m
+    uniform in ``open_range`` (a query once the session has none left).
+
+    Returns ``(requests, arrival_s)``: requests are ``(session_index, kind,
+    rc)`` with kind 0 = query, 1 = opening."""
+    rng = np.random.default_rng(seed)
+    arrival = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
+    arrival -= arrival[0]
+    cursor = [0] * len(pools)
+    frees = [np.flatnonzero(t.ravel() == FREE) for t, _ in pools]
+    out = []
+    for _ in range(n_req):
+        s = int(rng.integers(0, len(pools)))
+        truth, withheld = pools[s]
+        if rng.random() >= q_frac and cursor[s] < len(withheld):
+            m = int(rng.integers(open_range[0], open_range[1] + 1))
+            cells = withheld[cursor[s]:cursor[s] + m]
+            cursor[s] += len(cells)
+            out.append((s, 1, cells.astype(np.int32)))
+            continue
+        k = int(round(np.exp(rng.uniform(np.log(k_range[0]), np.log(k_range[1])))))
+        idx = rng.choice(frees[s], size=min(k, frees[s].size), replace=False)
+        cols = truth.shape[1]
+        out.append((s, 0, np.stack([idx // cols, idx % cols], axis=1).astype(np.int32)))
+    return out, arrival

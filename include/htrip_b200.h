@@ -170,6 +170,75 @@ htrip_status htrip_open_batch(htrip_batch* b, const htrip_open_request* reqs, in
 /* Device time of the batch's last query launch.                           */
 htrip_status htrip_batch_last_kernel_ms(const htrip_batch* b, float* ms);
 
+/* Request server over many resident map sessions (no reference
+ * counterpart; it generalises the reference simulator's double-buffered
+ * update / query threads, robot_simulator.cpp:897-1045, to many maps).
+ *  - A session is one map: the server builds its index (MinPlusOracle::
+ *    build) and keeps its own copy of the observed grid.
+ *  - Requests are asynchronous: a query (queryAllPairs, result written to
+ *    the caller's k*k buffer) or an opening (onBatchCellsOpened; the server
+ *    marks the cells Free in its grid first).  Requests of one session run
+ *    in submission order; requests of different sessions are batched: all
+ *    ready queries go into one launch of the query kernel and all ready
+ *    openings advance together, while new requests queue for the next
+ *    launch (continuous batching).  Every result equals the same request
+ *    run alone on a session that saw the same earlier requests.
+ *  - Sessions are admitted against an HBM budget by their estimated
+ *    footprint; idle sessions are offloaded to host memory (least recently
+ *    used first) to make room, and brought back when a request needs them.
+ *    A session that cannot fit is refused with HTRIP_ERR_OOM.
+ *  - Latency = submission to result in host memory.                       */
+typedef struct htrip_server htrip_server; /* opaque */
+
+typedef struct {
+    int32_t device;
+    uint64_t hbm_budget_bytes;        /* 0: 80% of the device's free memory   */
+    int32_t max_requests_per_launch;  /* 0: 128                               */
+    int32_t plain_per_call;           /* 1: no batching - one worker serves one
+                                         request at a time in arrival order
+                                         through the single-index calls (the
+                                         baseline the batched server is
+                                         measured against)                     */
+} htrip_server_config;
+
+typedef struct {
+    uint64_t launches_query, launches_open;   /* batched launches issued       */
+    uint64_t requests_query, requests_open;   /* requests submitted            */
+    uint64_t evictions, restores;             /* offloads to / returns from host */
+    uint64_t sessions, resident_sessions;
+    uint64_t resident_bytes, budget_bytes;
+} htrip_server_stats;
+
+typedef struct {
+    int64_t session;
+    int32_t kind;       /* 0 = query (rc = viewpoints, out = k*k), 1 = opening */
+    const int32_t* rc;  /* n (r, c) pairs, host                                */
+    int32_t n;
+    uint16_t* out;
+} htrip_server_request;
+
+/* Last error message of a server call on the calling thread.              */
+const char* htrip_server_last_error(void);
+htrip_status htrip_server_create(const htrip_server_config* cfg, htrip_server** out);
+/* Waits for every queued request, then frees all sessions.                */
+htrip_status htrip_server_destroy(htrip_server* s);
+htrip_status htrip_server_add_session(htrip_server* s, htrip_config cfg, const uint8_t* observed, int32_t rows,
+                                      int32_t cols, int64_t* session);
+/* Waits for the session's queued requests, then frees it.                 */
+htrip_status htrip_server_remove_session(htrip_server* s, int64_t session);
+htrip_status htrip_server_submit_query(htrip_server* s, int64_t session, const int32_t* vps, int32_t k,
+                                       uint16_t* out, uint64_t* ticket);
+htrip_status htrip_server_submit_open(htrip_server* s, int64_t session, const int32_t* rc, int32_t n,
+                                      uint64_t* ticket);
+/* Blocks until the request is done; returns its status and latency.      */
+htrip_status htrip_server_wait(htrip_server* s, uint64_t ticket, double* latency_ms);
+htrip_status htrip_server_get_stats(htrip_server* s, htrip_server_stats* out);
+/* Open-loop load: request i is submitted arrival_s[i] seconds after the
+ * call starts, by the calling thread; then every request is waited for.
+ * latency_ms[i] = its latency (-1 if it failed); wall_s = whole call.     */
+htrip_status htrip_server_run_trace(htrip_server* s, const htrip_server_request* reqs, const double* arrival_s,
+                                    int32_t n, double* latency_ms, double* wall_s);
+
 /* Measurement helpers (no reference counterpart).
  * htrip_query_work: the algorithmic HBM bytes and min-plus operations of a
  * queryAllPairs on these viewpoints: k*(4b-4) level-0 gathers; per level and
@@ -184,6 +253,13 @@ htrip_status htrip_query_work(const htrip_index* h, const int32_t* vps, int32_t 
                               int32_t rows, int32_t cols, uint64_t* alg_bytes, uint64_t* alg_ops);
 htrip_status htrip_last_query_kernel_ms(const htrip_index* h, float* ms);
 htrip_status htrip_last_query_io(const htrip_index* h, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
+
+/* Register-only rate (entries/s) of the packed-u16 clamped min-plus update
+ * on every SM of `device`: the integer-issue peak the kernels are measured
+ * against.  variant 0: add.u16x2 / min.u16x2 clamped form (any a <= INF);
+ * 1: the same with the fused add+min intrinsic; 2, 3: the unclamped forms
+ * (a <= 5535).                                                            */
+htrip_status htrip_measure_minplus_rate(int device, int variant, double* entries_per_s);
 
 /* Wait for all work queued on the index's stream.                         */
 htrip_status htrip_sync(htrip_index* h);
@@ -219,6 +295,19 @@ htrip_status htrip_read_node_DU(const htrip_index* h, int32_t lvl, int32_t node,
 htrip_status htrip_read_node_SU(const htrip_index* h, int32_t lvl, int32_t node, uint16_t* out);
 htrip_status htrip_read_node_C2E(const htrip_index* h, int32_t lvl, int32_t node, int32_t quad,
                                  uint16_t* out);
+/* Residency (no reference counterpart; the reference keeps every oracle in
+ * host RAM).  htrip_offload copies the index's matrices to host memory and
+ * frees all of its device memory; every call except htrip_restore,
+ * htrip_destroy, htrip_shape, htrip_memory_bytes and htrip_is_resident then
+ * fails with HTRIP_ERR_INVALID.  htrip_restore brings it back unchanged
+ * (on HTRIP_ERR_OOM it stays offloaded).  htrip_estimate_bytes: the device
+ * bytes an index of this config and grid holds after build (matrices,
+ * pivot lists and tables; query and update scratch excluded).            */
+htrip_status htrip_offload(htrip_index* h);
+htrip_status htrip_restore(htrip_index* h);
+htrip_status htrip_is_resident(const htrip_index* h, int32_t* resident);
+htrip_status htrip_estimate_bytes(htrip_config cfg, int32_t rows, int32_t cols, uint64_t* device_bytes);
+
 /* Canonical per-level checksum of the whole index (no reference
  * counterpart; computed on the device, nothing large is copied):
  *   out[l] = sum mod 2^64 over the level's matrices m (leaves[m].D for
