@@ -135,6 +135,8 @@ struct QueryArena {
     cudaEvent_t ev[2] = {nullptr, nullptr};
     bool ev_valid = false;
     uint64_t last_h2d = 0, last_d2h = 0;
+    size_t last_words = 0;  // arena offset of the last launch's words
+    int last_phases = 0;
     void release() {
         dev.release();
         stage.release();
@@ -863,6 +865,11 @@ struct QueryReq {
     uint16_t* out_dev;  // result on the device; nullptr = in the arena
 };
 
+// Launch words: {status, barrier count, barrier generation, pad}, then the
+// phase time stamps at byte kTraceOffset.
+constexpr size_t kTraceOffset = 64;
+constexpr size_t kWordsBytes = kTraceOffset + (hb::kMaxQueryPhases + 1) * sizeof(unsigned long long);
+
 struct LaunchLayout {
     int n = 0, n_phases = 0;
     size_t o_params = 0, o_pre = 0, o_words = 0, head = 0;
@@ -889,7 +896,7 @@ LaunchLayout layout_launch(const std::vector<QueryReq>& R) {
     };
     L.o_params = take(R.size() * sizeof(hb::QueryParams));
     L.o_pre = take((size_t)L.n_phases * (R.size() + 1) * sizeof(int));
-    L.o_words = take(4 * sizeof(unsigned));
+    L.o_words = take(kWordsBytes);
     for (const auto& r : R) L.plan.push_back(take(r.P->buf.size() * sizeof(int)));
     L.head = off;
     L.o_M = off;
@@ -1003,6 +1010,7 @@ void issue_query_launch(cudaStream_t st, int device, int& grid, int cfg, const s
     QL.unit_pre = reinterpret_cast<const int*>(base + L.o_pre);
     QL.status = reinterpret_cast<int*>(base + L.o_words);
     QL.bar = reinterpret_cast<unsigned*>(base + L.o_words) + 1;
+    QL.trace = reinterpret_cast<unsigned long long*>(base + L.o_words + kTraceOffset);
     if (ev) ck(cudaEventRecord(ev[0], st), "event");
     ck(hb::launch_query(QL, cfg, grid, st), "query kernel");
     if (ev) ck(cudaEventRecord(ev[1], st), "event");
@@ -1029,6 +1037,8 @@ int run_queries(QueryArena& A, int device, cudaStream_t st, const std::vector<Qu
     std::vector<uint16_t*> outs;
     issue_query_launch(st, device, A.grid, cfg, R, L, A.dev.p, A.stage.p, A.ev, outs);
     A.ev_valid = true;
+    A.last_words = L.o_words;
+    A.last_phases = L.n_phases;
     A.last_h2d = L.head;
     A.last_d2h = 0;
     int* status_host = reinterpret_cast<int*>(A.outstage.p + L.out_bytes);
@@ -1558,6 +1568,31 @@ htrip_status htrip_last_query_kernel_ms(const htrip_index* h, float* ms) {
     ck(cudaEventElapsedTime(ms, h->q.ev[0], h->q.ev[1]), "event time");
     return HTRIP_OK;
     HTRIP_GUARD_END
+}
+
+static htrip_status arena_phases(const QueryArena& A, cudaStream_t st, uint64_t* ns, int32_t max_n, int32_t* n) {
+    if (!ns || !n || max_n < 0) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    if (!A.ev_valid) return fail(HTRIP_ERR_INVALID, "no query has run");
+    HTRIP_GUARD_BEGIN
+    unsigned long long t[hb::kMaxQueryPhases + 1];
+    ck(cudaEventSynchronize(A.ev[1]), "event sync");
+    ck(cudaMemcpyAsync(t, A.dev.p + A.last_words + kTraceOffset, (A.last_phases + 1) * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, st), "trace d2h");
+    ck(cudaStreamSynchronize(st), "trace sync");
+    *n = std::min<int32_t>(max_n, A.last_phases);
+    for (int i = 0; i < *n; ++i) ns[i] = t[i + 1] - t[i];
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_last_query_phases(const htrip_index* h, uint64_t* ns, int32_t max_n, int32_t* n) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    return arena_phases(h->q, h->stream, ns, max_n, n);
+}
+
+htrip_status htrip_batch_last_phases(const htrip_batch* b, uint64_t* ns, int32_t max_n, int32_t* n) {
+    if (!b) return fail(HTRIP_ERR_INVALID, "null batch");
+    return arena_phases(b->q, b->stream, ns, max_n, n);
 }
 
 htrip_status htrip_last_query_io(const htrip_index* h, uint64_t* h2d_bytes, uint64_t* d2h_bytes) {

@@ -126,9 +126,12 @@ struct QueryParams {
 //   1 <= t <= H+1  project items of level t (t <= H), then meet items of
 //                  level t-1 (t >= 2)
 //   t = H+2        output chunks of kQueryFinChunk entries
-constexpr int kQueryThreads = 512;
-constexpr int kQueryL0Chunk = 4096;
-constexpr int kQueryFinChunk = 4096;
+#ifndef HB_QUERY_THREADS
+#define HB_QUERY_THREADS 256
+#endif
+constexpr int kQueryThreads = HB_QUERY_THREADS;
+constexpr int kQueryL0Chunk = 512;
+constexpr int kQueryFinChunk = 1024;
 
 // A launch over n_req requests (any mix of indexes and k on one device).
 struct QueryLaunch {
@@ -138,7 +141,9 @@ struct QueryLaunch {
     const int* unit_pre;       // [n_phases][n_req + 1]: exclusive prefix of units
     int* status;               // 0 ok, 1 grid barrier timeout
     unsigned* bar;             // grid barrier {count, generation}
+    unsigned long long* trace; // n_phases + 1 global-timer stamps (CTA 0), or null
 };
+constexpr int kMaxQueryPhases = kMaxQueryLevels + 3;
 
 // Cooperative launch of the persistent query kernel on `grid` blocks.
 int query_grid_blocks(int device);

@@ -40,6 +40,11 @@ __device__ __forceinline__ u32 min2(u32 a, u32 b) {
     asm("min.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
     return r;
 }
+__device__ __forceinline__ u32 max2(u32 a, u32 b) {
+    u32 r;
+    asm("max.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
 // a (low 16 bits) replicated into both halves.
 __device__ __forceinline__ u32 splat(u32 a) { return __byte_perm(a, 0, 0x1010); }
 

@@ -8,10 +8,15 @@
 // X_{l-1} (ports x slots) and the projections Yt_l (node columns x slots) are
 // stored in level-l slot order.
 //
-// Work is cut into warp-sized items (no shared memory, no CTA barriers): a
-// warp keeps RW rows x 64*CP columns of packed u16 accumulators and streams
-// its operand rows from L2/HBM.  The rows of a warp are warp-uniform, the
-// columns are spread over the lanes.
+// Work is cut into CTA items: a tile of RW rows x 64*CP columns of packed
+// u16 accumulators.  The CTA's warps split the item's list of operand rows
+// (split-K inside the CTA), each streaming its rows from L2/HBM through a
+// cp.async ring in shared memory, then the partial tiles are min-reduced in
+// shared memory and the epilogue is spread over the warps.  The rows of a
+// warp are warp-uniform, the columns are spread over the lanes; per operand
+// row the tile's RW values decide, uniformly for the warp, between skipping
+// (all INF), the unclamped 2-op update (all <= 5535) and the clamped one.
+// Two 256-thread CTAs per SM keep two items in flight.
 //
 //   level 0  X0[p][s] = leaf D[u][port p] for every viewpoint (+ finite-port
 //            flags of its level-1 child group) and same-leaf pairs
@@ -56,65 +61,123 @@ __device__ __forceinline__ void row_update(uint32_t (&acc)[CP], const uint32_t (
     for (int c = 0; c < CP; ++c) acc[c] = min2(add2(min2(bv[c], tt), aa), acc[c]);
 }
 
-template <int CP>
-__device__ __forceinline__ void ldg_pairs(uint32_t (&bv)[CP], const uint16_t* p) {
-    if constexpr (CP == 4) {
-        const uint4 v = __ldcg(reinterpret_cast<const uint4*>(p));
-        bv[0] = v.x; bv[1] = v.y; bv[2] = v.z; bv[3] = v.w;
-    } else if constexpr (CP == 2) {
-        const uint2 v = __ldcg(reinterpret_cast<const uint2*>(p));
-        bv[0] = v.x; bv[1] = v.y;
-    } else {
-        bv[0] = __ldcg(reinterpret_cast<const unsigned int*>(p));
-    }
-}
-
-// RW consecutive u16 row values (16-byte aligned) -> RW/2 packed pairs.
-template <int RW>
-__device__ __forceinline__ void ldg_rows(uint32_t (&a)[RW / 2], const uint16_t* p) {
-#pragma unroll
-    for (int h = 0; h < RW / 8; ++h) {
-        const uint4 v = __ldcg(reinterpret_cast<const uint4*>(p) + h);
-        a[4 * h] = v.x; a[4 * h + 1] = v.y; a[4 * h + 2] = v.z; a[4 * h + 3] = v.w;
-    }
-}
-
 constexpr int kThreads = kQueryThreads;
 constexpr int kWarps = kThreads / 32;
 
-// Warp w of the CTA streams list entries t = w*U + 16*U*i + u of the
-// compacted row list kl[0..n):
+// Operand staging: every warp keeps kPipeStages x kPipeRows operand rows in
+// flight through cp.async into its own shared-memory ring, so an item's
+// rows arrive at L2 / HBM throughput rather than one round trip per row.
+constexpr int kPipeStages = 4;
+constexpr int kPipeRows = 4;
+
+// Words of one staged row: the lane-major B pairs (32 lanes x CP), then RW
+// u16 of the A row.
+template <int RW, int CP>
+constexpr int pipe_slot_words() {
+    return CP * 32 + RW / 2;
+}
+template <int RW, int CP>
+constexpr int pipe_warp_words() {
+    return kPipeStages * kPipeRows * pipe_slot_words<RW, CP>();
+}
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async(uint32_t saddr, const void* g) {
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(g) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(saddr), "l"(g), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Warp w of the CTA streams list entries t = w*U + 16*U*i + u (U =
+// kPipeRows) of the compacted row list kl[0..n):
 //   acc[r][c] = min over its rows p of A[p*lda + r] (+) B[p*ldb + lane pair c].
-// U rows per warp are in flight (their loads precede the arithmetic), so a CTA
-// keeps 16*U operand rows in flight.
-template <int RW, int CP, int U = (RW * CP >= 32 ? 4 : 8)>
+// A rows are RW consecutive u16 (16-byte aligned); B is already offset to the
+// lane's CP pairs (4*CP-byte aligned).  `pipe` is the warp's staging ring.
+template <int RW, int CP>
 __device__ __forceinline__ void warp_minplus_list(uint32_t (&acc)[RW][CP], const int* kl, int n, int warp,
                                                   const uint16_t* __restrict__ A, int lda,
-                                                  const uint16_t* __restrict__ B, int ldb) {
-    for (int t0 = warp * U; t0 < n; t0 += kWarps * U) {
-        int rows[U];
+                                                  const uint16_t* __restrict__ B, int ldb, uint32_t* pipe) {
+    constexpr int U = kPipeRows, NS = kPipeStages, SW = pipe_slot_words<RW, CP>();
+    const int lane = threadIdx.x & 31;
+    const int stride = kWarps * U;
+    const int first = warp * U;
+    const int n_it = first < n ? (n - first + stride - 1) / stride : 0;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(pipe);
+    auto issue = [&](int it) {
+        if (it < n_it) {
+            const int st = it % NS;
 #pragma unroll
-        for (int u = 0; u < U; ++u) rows[u] = t0 + u < n ? kl[t0 + u] : -1;
-        uint32_t bv[U][CP];
-        uint32_t av[U][RW / 2];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            if (rows[u] >= 0) {
-                ldg_pairs<CP>(bv[u], B + (size_t)rows[u] * ldb);
-                ldg_rows<RW>(av[u], A + (size_t)rows[u] * lda);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            if (rows[u] >= 0) {
-#pragma unroll
-                for (int r2 = 0; r2 < RW / 2; ++r2) {
-                    row_update<CP>(acc[2 * r2], bv[u], __byte_perm(av[u][r2], 0, 0x1010));
-                    row_update<CP>(acc[2 * r2 + 1], bv[u], __byte_perm(av[u][r2], 0, 0x3232));
+            for (int u = 0; u < U; ++u) {
+                const int t = first + it * stride + u;
+                if (t < n) {
+                    const int row = kl[t];
+                    const uint32_t slot = sbase + (uint32_t)((st * U + u) * SW) * 4u;
+                    cp_async<CP * 4>(slot + lane * CP * 4, B + (size_t)row * ldb);
+                    if (lane < RW / 8) cp_async<16>(slot + CP * 128 + lane * 16, A + (size_t)row * lda + lane * 8);
                 }
             }
         }
+        cp_commit();
+    };
+#pragma unroll
+    for (int st = 0; st < NS - 1; ++st) issue(st);
+    for (int it = 0; it < n_it; ++it) {
+        issue(it + NS - 1);
+        cp_wait<NS - 1>();
+        __syncwarp();
+        const int st = it % NS;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (first + it * stride + u < n) {
+                const uint32_t* slot = pipe + (st * U + u) * SW;
+                uint32_t bv[CP];
+#pragma unroll
+                for (int c = 0; c < CP; ++c) bv[c] = slot[lane * CP + c];
+                const uint32_t* a = slot + CP * 32;
+                uint32_t aw[RW / 2];
+#pragma unroll
+                for (int r2 = 0; r2 < RW / 2; ++r2) aw[r2] = a[r2];
+                // The row's RW values are warp-uniform: all INF -> nothing to
+                // do; all <= INF_HEADROOM -> the unclamped 2-op form is exact
+                // (a + b <= 65535 never wraps, and a sum >= INF loses to c);
+                // otherwise the clamped form (exact for any a <= INF).
+                uint32_t mx = aw[0], mn = aw[0];
+#pragma unroll
+                for (int r2 = 1; r2 < RW / 2; ++r2) {
+                    mx = max2(mx, aw[r2]);
+                    mn = min2(mn, aw[r2]);
+                }
+                mn = min2(mn, mn >> 16) & 0xffffu;
+                mx = max2(mx, mx >> 16) & 0xffffu;
+                if (mn >= INF) continue;
+                if (mx <= INF_HEADROOM) {
+#pragma unroll
+                    for (int r2 = 0; r2 < RW / 2; ++r2) {
+                        const uint32_t lo = __byte_perm(aw[r2], 0, 0x1010), hi = __byte_perm(aw[r2], 0, 0x3232);
+#pragma unroll
+                        for (int c = 0; c < CP; ++c) {
+                            acc[2 * r2][c] = acc_fast(acc[2 * r2][c], bv[c], lo);
+                            acc[2 * r2 + 1][c] = acc_fast(acc[2 * r2 + 1][c], bv[c], hi);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int r2 = 0; r2 < RW / 2; ++r2) {
+                        row_update<CP>(acc[2 * r2], bv, __byte_perm(aw[r2], 0, 0x1010));
+                        row_update<CP>(acc[2 * r2 + 1], bv, __byte_perm(aw[r2], 0, 0x3232));
+                    }
+                }
+            }
+        }
+        __syncwarp();
     }
+    cp_wait<0>();
 }
 
 // Compacts the set flags of rows [kb, ke) into kl (ascending); returns the
@@ -147,12 +210,13 @@ __device__ __forceinline__ int compact_flags(const uint8_t* __restrict__ flags, 
     return total;
 }
 
-// Min-reduction of the 16 warps' accumulators through shared memory; the
+// Min-reduction of the warps' accumulators through shared memory; the
 // reduced tile ends up in every warp's acc (warp 0 uses it).
 template <int RW, int CP>
 __device__ __forceinline__ void cta_reduce(uint32_t (&acc)[RW][CP], uint32_t* red) {
     constexpr int E = RW * CP * 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __syncthreads();  // the staging rings alias `red`: every warp is done reading them
 #pragma unroll
     for (int r = 0; r < RW; ++r)
 #pragma unroll
@@ -202,27 +266,57 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* status) {
     return ok && *(volatile int*)status == 0;
 }
 
+__device__ __forceinline__ unsigned long long global_timer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // ---------------------------------------------------------------------------
 // Work item bodies.
 // ---------------------------------------------------------------------------
 // Shared memory of the persistent kernel: compacted row list (nP <= 4096
 // ports), scan partials and the split-K reduction buffer.
 constexpr int kMaxList = 4096 + 64;
+// The staging rings (during an item's k-loop) and the split-K reduction
+// buffer (after it) share one region.
 template <int RW, int CP>
 constexpr size_t query_smem_bytes() {
-    return (size_t)kMaxList * sizeof(int) + (size_t)kWarps * RW * CP * 32 * sizeof(uint32_t);
+    return (size_t)kMaxList * sizeof(int) +
+           std::max((size_t)kWarps * RW * CP * 32, (size_t)kWarps * pipe_warp_words<RW, CP>()) * sizeof(uint32_t);
 }
 
+// Per-item metadata staged in shared memory at the start of an item (its
+// global loads overlap the k-loop): the exterior index / viewpoint of each
+// tile column and the lift slot / viewpoint of each tile row.
+struct ItemMeta {
+    int col[256];
+    int row[2][16];
+};
+
 // project item {group, m0, n0}: tile of RW slots x 64*CP node columns; the
-// 16 warps split the group's finite ports.
+// CTA's warps split the group's finite ports.  After the reduction the
+// epilogue (Y stores and lift scatters) is spread over the warps.
 template <int RW, int CP>
 __device__ void do_project(const QueryParams& P, const QueryLevel& L, const QueryLevel* Ln, int item, int l,
-                           int* kl, int* wsum, uint32_t* red) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+                           int* kl, int* wsum, uint32_t* red, ItemMeta& im) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, tid = threadIdx.x;
     const int* it = L.items + 3 * item;
     const int gi = it[0], m0 = it[1], n0 = it[2];
     const int* G = L.groups + 5 * gi;
     const int node = G[0], q = G[1], slot0 = G[2], cnt = G[3];
+    if (Ln) {
+        for (int t = tid; t < 64 * CP + RW; t += kThreads) {
+            if (t < 64 * CP) {
+                im.col[t] = n0 + t < L.NP ? L.ext_inv[n0 + t] : -1;
+            } else {
+                const int r = t - 64 * CP;
+                const bool ok = m0 + r < cnt;
+                im.row[0][r] = ok ? L.lift[2 * (slot0 + m0 + r)] : -1;
+                im.row[1][r] = ok ? L.lift[2 * (slot0 + m0 + r) + 1] : -1;
+            }
+        }
+    }
     const int nA = compact_flags(L.flags + (size_t)gi * L.nP, 0, L.nP, kl, wsum);
     const uint16_t* D = L.D + (size_t)node * L.NP * L.NP + (size_t)q * L.nP * L.NP;
     const int col = n0 + lane * 2 * CP;
@@ -233,55 +327,62 @@ __device__ void do_project(const QueryParams& P, const QueryLevel& L, const Quer
     for (int r = 0; r < RW; ++r)
 #pragma unroll
         for (int c = 0; c < CP; ++c) acc[r][c] = INF2;
-    warp_minplus_list<RW, CP>(acc, kl, nA, warp, Xp, P.ldv, D + (live_col ? col : n0), L.NP);
+    warp_minplus_list<RW, CP>(acc, kl, nA, warp, Xp, P.ldv, D + (live_col ? col : n0), L.NP,
+                              red + warp * pipe_warp_words<RW, CP>());
     cta_reduce<RW, CP>(acc, red);
-    if (warp == 0 && live_col) {
-        uint16_t* Y = P.Y[l & 1];
+    uint16_t* Y = P.Y[l & 1];
 #pragma unroll
-        for (int cc = 0; cc < 2 * CP; ++cc) {
-            uint16_t v[RW];
+    for (int cc = 0; cc < 2 * CP; ++cc) {
+        const bool do_y = L.store_y && (cc % kWarps) == warp;
+        const bool do_lift = Ln && ((2 * CP + cc) % kWarps) == warp;
+        if (!live_col || (!do_y && !do_lift)) continue;
+        uint16_t v[RW];
 #pragma unroll
-            for (int r = 0; r < RW; ++r)
-                v[r] = (uint16_t)((cc & 1) ? (acc[r][cc >> 1] >> 16) : (acc[r][cc >> 1] & 0xffffu));
-            if (L.store_y) {
-                uint16_t* y = Y + (size_t)(col + cc) * P.ldv + slot0 + m0;
+        for (int r = 0; r < RW; ++r)
+            v[r] = (uint16_t)((cc & 1) ? (acc[r][cc >> 1] >> 16) : (acc[r][cc >> 1] & 0xffffu));
+        if (do_y) {
+            uint16_t* y = Y + (size_t)(col + cc) * P.ldv + slot0 + m0;
 #pragma unroll
-                for (int r8 = 0; r8 < RW / 8; ++r8) {
-                    uint4 o;
-                    o.x = v[8 * r8] | ((uint32_t)v[8 * r8 + 1] << 16);
-                    o.y = v[8 * r8 + 2] | ((uint32_t)v[8 * r8 + 3] << 16);
-                    o.z = v[8 * r8 + 4] | ((uint32_t)v[8 * r8 + 5] << 16);
-                    o.w = v[8 * r8 + 6] | ((uint32_t)v[8 * r8 + 7] << 16);
-                    reinterpret_cast<uint4*>(y)[r8] = o;
-                }
+            for (int r8 = 0; r8 < RW / 8; ++r8) {
+                uint4 o;
+                o.x = v[8 * r8] | ((uint32_t)v[8 * r8 + 1] << 16);
+                o.y = v[8 * r8 + 2] | ((uint32_t)v[8 * r8 + 3] << 16);
+                o.z = v[8 * r8 + 4] | ((uint32_t)v[8 * r8 + 5] << 16);
+                o.w = v[8 * r8 + 6] | ((uint32_t)v[8 * r8 + 7] << 16);
+                reinterpret_cast<uint4*>(y)[r8] = o;
             }
-            if (Ln) {  // lift: exterior column e of this node -> X_l[e][level-(l+1) slot]
-                const int e = L.ext_inv[col + cc];
-                if (e >= 0) {
-                    uint16_t* Xn = P.X[l % 3] + (size_t)e * P.ldv;
+        }
+        if (do_lift) {  // exterior column e of this node -> X_l[e][level-(l+1) slot]
+            const int e = im.col[lane * 2 * CP + cc];
+            if (e >= 0) {
+                uint16_t* Xn = P.X[l % 3] + (size_t)e * P.ldv;
 #pragma unroll
-                    for (int r = 0; r < RW; ++r) {
-                        if (m0 + r < cnt) {
-                            const int* ls = L.lift + 2 * (slot0 + m0 + r);
-                            Xn[ls[0]] = v[r];
-                            if (v[r] < INF) Ln->flags[(size_t)ls[1] * Ln->nP + e] = 1;
-                        }
+                for (int r = 0; r < RW; ++r) {
+                    const int slot = im.row[0][r];
+                    if (slot >= 0) {
+                        Xn[slot] = v[r];
+                        if (v[r] < INF) Ln->flags[(size_t)im.row[1][r] * Ln->nP + e] = 1;
                     }
                 }
             }
         }
     }
-    __syncthreads();  // kl / red are reused by the next item
+    __syncthreads();  // kl / red / im are reused by the next item
 }
 
 // meet item {i0, j0, nj, g2, coloff, kb, ke}: rows = RW viewpoints j of
 // child group g2 (slots j0..), lanes = 64*CP viewpoint slots i (from i0).
+// After the reduction warp w combines rows r = w (mod warps) into M.
 template <int RW, int CP>
 __device__ void do_meet(const QueryParams& P, const QueryLevel& L, int item, int l, int* kl, int* wsum,
-                        uint32_t* red) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+                        uint32_t* red, ItemMeta& im) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, tid = threadIdx.x;
     const int* it = L.meet + 7 * item;
     const int i0 = it[0], j0 = it[1], nj = it[2], g2 = it[3], coloff = it[4], kb = it[5], ke = it[6];
+    for (int t = tid; t < 64 * CP + RW; t += kThreads) {
+        if (t < 64 * CP) im.col[t] = L.s2v[i0 + t];
+        else im.row[0][t - 64 * CP] = t - 64 * CP < nj ? L.s2v[j0 + t - 64 * CP] : -1;
+    }
     const int nA = compact_flags(L.flags + (size_t)g2 * L.nP, kb, ke, kl, wsum);
     const uint16_t* Xp = P.X[(l - 1) % 3] + j0;
     const uint16_t* Y = P.Y[l & 1] + (size_t)coloff * P.ldv + i0 + lane * 2 * CP;
@@ -290,19 +391,18 @@ __device__ void do_meet(const QueryParams& P, const QueryLevel& L, int item, int
     for (int r = 0; r < RW; ++r)
 #pragma unroll
         for (int c = 0; c < CP; ++c) acc[r][c] = INF2;
-    warp_minplus_list<RW, CP>(acc, kl, nA, warp, Xp, P.ldv, Y, P.ldv);
+    warp_minplus_list<RW, CP>(acc, kl, nA, warp, Xp, P.ldv, Y, P.ldv, red + warp * pipe_warp_words<RW, CP>());
     cta_reduce<RW, CP>(acc, red);
-    if (warp == 0) {
 #pragma unroll
-        for (int r = 0; r < RW; ++r) {
-            if (r >= nj) break;
-            const int vj = L.s2v[j0 + r];
+    for (int r = 0; r < RW; ++r) {
+        if ((r % kWarps) != warp) continue;
+        const int vj = im.row[0][r];
+        if (vj < 0) continue;
 #pragma unroll
-            for (int cc = 0; cc < 2 * CP; ++cc) {
-                const int vi = L.s2v[i0 + lane * 2 * CP + cc];
-                const uint32_t v = (cc & 1) ? (acc[r][cc >> 1] >> 16) : (acc[r][cc >> 1] & 0xffffu);
-                if (vi >= 0 && vi < vj && v < INF) atomicMin(&P.M[(size_t)vi * P.ldm + vj], v);
-            }
+        for (int cc = 0; cc < 2 * CP; ++cc) {
+            const int vi = im.col[lane * 2 * CP + cc];
+            const uint32_t v = (cc & 1) ? (acc[r][cc >> 1] >> 16) : (acc[r][cc >> 1] & 0xffffu);
+            if (vi >= 0 && vi < vj && v < INF) atomicMin(&P.M[(size_t)vi * P.ldm + vj], v);
         }
     }
     __syncthreads();
@@ -310,7 +410,7 @@ __device__ void do_meet(const QueryParams& P, const QueryLevel& L, int item, int
 
 // One CTA work unit of request P in phase t (see QueryLaunch).
 template <int RW, int CP>
-__device__ void run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum, uint32_t* red) {
+__device__ void run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum, uint32_t* red, ItemMeta& im) {
     const int tid = threadIdx.x;
     if (t == 0) {
         // level 0: X0 in level-1 slot order (+ level-1 flags), same-leaf pairs
@@ -340,8 +440,8 @@ __device__ void run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum,
     }
     if (t <= P.H + 1) {
         const int np = t <= P.H ? P.lv[t].n_items : 0;
-        if (u < np) do_project<RW, CP>(P, P.lv[t], t < P.H ? &P.lv[t + 1] : nullptr, u, t, kl, wsum, red);
-        else do_meet<RW, CP>(P, P.lv[t - 1], u - np, t - 1, kl, wsum, red);
+        if (u < np) do_project<RW, CP>(P, P.lv[t], t < P.H ? &P.lv[t + 1] : nullptr, u, t, kl, wsum, red, im);
+        else do_meet<RW, CP>(P, P.lv[t - 1], u - np, t - 1, kl, wsum, red, im);
         return;
     }
     // t == H + 2: out[a][c] for one chunk of the k x k output
@@ -362,11 +462,14 @@ __device__ void run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum,
 // The persistent kernel: phases separated by grid barriers; in each phase
 // the CTAs stride over the units of every request of the launch.
 template <int RW, int CP>
-__global__ void __launch_bounds__(kThreads, 1) q_persistent_kernel(const QueryLaunch B) {
+__global__ void __launch_bounds__(kThreads, 512 / kThreads) q_persistent_kernel(const QueryLaunch B) {
     extern __shared__ __align__(16) int qsm[];
     int* kl = qsm;
     uint32_t* red = reinterpret_cast<uint32_t*>(qsm + kMaxList);
     __shared__ int wsum[kWarps];
+    __shared__ ItemMeta im;
+    const bool stamp = B.trace && blockIdx.x == 0 && threadIdx.x == 0;
+    if (stamp) B.trace[0] = global_timer();
     for (int t = 0; t < B.n_phases; ++t) {
         const int* pre = B.unit_pre + (size_t)t * (B.n_req + 1);
         const int total = pre[B.n_req];
@@ -377,9 +480,10 @@ __global__ void __launch_bounds__(kThreads, 1) q_persistent_kernel(const QueryLa
                 if (pre[mid] <= w) lo = mid;
                 else hi = mid;
             }
-            run_unit<RW, CP>(B.req[lo], t, w - pre[lo], kl, wsum, red);
+            run_unit<RW, CP>(B.req[lo], t, w - pre[lo], kl, wsum, red, im);
         }
         if (t + 1 < B.n_phases && !grid_barrier(B.bar, B.status)) return;
+        if (stamp) B.trace[t + 1] = global_timer();
     }
 }
 

@@ -83,7 +83,7 @@ EXPORTS = (
     "htrip_estimate_bytes", "htrip_server_last_error", "htrip_server_create", "htrip_server_destroy",
     "htrip_server_add_session", "htrip_server_remove_session", "htrip_server_submit_query",
     "htrip_server_submit_open", "htrip_server_wait", "htrip_server_get_stats", "htrip_server_run_trace",
-    "htrip_measure_minplus_rate",
+    "htrip_measure_minplus_rate", "htrip_last_query_phases", "htrip_batch_last_phases",
 )
 
 
@@ -130,6 +130,8 @@ def load_library(path: str | None = None):
     lib.htrip_batch_last_kernel_ms.argtypes = [P, C.POINTER(C.c_float)]
     lib.htrip_open_batch.argtypes = [P, C.POINTER(_OpenRequest), I]
     lib.htrip_measure_minplus_rate.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
+    lib.htrip_last_query_phases.argtypes = [P, _U64P, I, _I32P]
+    lib.htrip_batch_last_phases.argtypes = [P, _U64P, I, _I32P]
     lib.htrip_offload.argtypes = [P]
     lib.htrip_restore.argtypes = [P]
     lib.htrip_is_resident.argtypes = [P, _I32P]
@@ -338,6 +340,13 @@ class MinPlusOracle:
         _check(self.lib.htrip_last_query_kernel_ms(self.h, C.byref(ms)))
         return ms.value
 
+    def lastQueryPhases(self):
+        """Per-phase nanoseconds of the last query launch (htrip_last_query_phases)."""
+        buf = (C.c_uint64 * 32)()
+        n = C.c_int32()
+        _check(self.lib.htrip_last_query_phases(self.h, buf, 32, C.byref(n)))
+        return [int(buf[i]) for i in range(n.value)]
+
     def lastQueryIO(self):
         """(host->device, device->host) bytes copied by the last query call."""
         a, b = C.c_uint64(), C.c_uint64()
@@ -471,6 +480,12 @@ class Batch:
         ms = C.c_float()
         _check(self.lib.htrip_batch_last_kernel_ms(self.h, C.byref(ms)))
         return ms.value
+
+    def lastPhases(self):
+        buf = (C.c_uint64 * 32)()
+        n = C.c_int32()
+        _check(self.lib.htrip_batch_last_phases(self.h, buf, 32, C.byref(n)))
+        return [int(buf[i]) for i in range(n.value)]
 
 
 

@@ -261,6 +261,13 @@ htrip_status htrip_last_query_io(const htrip_index* h, uint64_t* h2d_bytes, uint
  * (a <= 5535).                                                            */
 htrip_status htrip_measure_minplus_rate(int device, int variant, double* entries_per_s);
 
+/* Phase trace of the last query launch of an index / a batch: ns[i] =
+ * global-timer nanoseconds of phase i of the persistent query kernel
+ * (0: level-0 gathers; 1..H+1: projections of level i with the meets of
+ * level i-1; H+2: output), as seen by its first CTA.  *n = phases written. */
+htrip_status htrip_last_query_phases(const htrip_index* h, uint64_t* ns, int32_t max_n, int32_t* n);
+htrip_status htrip_batch_last_phases(const htrip_batch* b, uint64_t* ns, int32_t max_n, int32_t* n);
+
 /* Wait for all work queued on the index's stream.                         */
 htrip_status htrip_sync(htrip_index* h);
 
