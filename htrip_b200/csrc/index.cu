@@ -334,7 +334,7 @@ void close_matrices(htrip_index* h, Level& Lv, const std::vector<int>& act) {
         int maxk = 0;
         for (int i = 0; i < na; ++i) maxk = std::max(maxk, kc[act[c0 + i]]);
         if (maxk == 0) continue;
-        h->panel.reserve(per * na);
+        h->panel.reserve(hb::closure_scratch_elems(Lv.NP, na));
         h->pflags.reserve((size_t)na * (Lv.NP / hb::kFlagTile));
         const int rounds = (maxk + hb::kPivotChunk - 1) / hb::kPivotChunk;
         for (int r = 0; r < rounds; ++r) {
@@ -607,7 +607,7 @@ void open_close(OpenTask& T, int l) {
         int maxk = 0;
         for (int i = 0; i < nc; ++i) maxk = std::max(maxk, kc[c0 + i]);
         if (maxk == 0) continue;
-        h->panel.reserve(per * nc);
+        h->panel.reserve(hb::closure_scratch_elems(Lv.NP, nc));
         h->pflags.reserve((size_t)nc * (Lv.NP / hb::kFlagTile));
         const int rounds = (maxk + hb::kPivotChunk - 1) / hb::kPivotChunk;
         for (int r = 0; r < rounds; ++r) {

@@ -173,24 +173,30 @@ __global__ void compact_pivots_kernel(uint8_t* kflag, int NP, const int* __restr
 
 // ---------------------------------------------------------------------------
 // Blocked pivot-set Kleene closure, one round over pivots Kc (|Kc| = mk <= B):
-//   T  = D[Kc, Kc], closed in shared memory (Floyd-Warshall over Kc),
-//   R' = T* (x) D[Kc, :]                (panel kernel, B x NP per matrix)
-//   D  = min(D, R'^T (x) R')            (syrk kernel; D is symmetric, so
+//   T  = D[Kc, Kc], closed once per matrix in shared memory
+//        (pivot_close_kernel, Floyd-Warshall over Kc),
+//   R' = T* (x) D[Kc, :]                (closure_gemm_kernel<.., true>,
+//                                        B x NP per matrix)
+//   D  = min(D, R'^T (x) R')            (closure_gemm_kernel<.., false>; D
+//                                        is symmetric, so
 //                                        R'[k][i] = (D[:,Kc] (x) T*)[i][k])
 // This is exactly the reference's sequential relaxation over the same pivots
 // (leaf_tile.cpp:348-371, internal_node.cpp:201-231, :372-399): both give
 // the unique shortest-path closure through the pivot set.
 // ---------------------------------------------------------------------------
-constexpr int kPanelSlab = 256;
-
+// Closure of the round's pivot block T = D[Kc, Kc] (mk <= B) of every
+// active matrix, once per matrix: Floyd-Warshall over Kc in shared memory
+// (the reference's sequential relaxation restricted to the pivots).  tstar
+// receives T* as a B x B block (identity beyond mk); T is symmetric, so T*
+// is too.
 __global__ void __launch_bounds__(256)
-closure_panel_kernel(MatSet M, const int* __restrict__ active, const int* __restrict__ klist,
-                     const int* __restrict__ kcnt, int round, uint16_t* panel, uint8_t* flags) {
-    constexpr int B = kPivotChunk;
-    __shared__ uint16_t T[B][B + 2];
-    __shared__ __align__(16) uint16_t Dk[B][kPanelSlab];
+pivot_close_kernel(MatSet M, const int* __restrict__ active, const int* __restrict__ klist,
+                   const int* __restrict__ kcnt, int round, uint16_t* tstar) {
+    constexpr int B = kPivotChunk;   // 64: 256 threads x 16 entries
+    constexpr int LD = B + 8;        // padded row (144 bytes): column reads hit distinct banks
+    __shared__ __align__(16) uint16_t T[B][LD];
     __shared__ int kc[B];
-    const int slot = blockIdx.y;
+    const int slot = blockIdx.x;
     const int m = active[slot];
     const int NP = M.NP;
     const int mk = min(B, kcnt[m] - round * B);
@@ -205,90 +211,106 @@ closure_panel_kernel(MatSet M, const int* __restrict__ active, const int* __rest
         T[a][c] = (a < mk && c < mk) ? D[(size_t)kc[a] * NP + kc[c]] : (a == c ? 0 : INF);
     }
     __syncthreads();
+    // Thread t owns row a = t / 4, columns c0 .. c0 + 15 (8 packed pairs).
+    const int a = tid >> 2, c0 = (tid & 3) * 16;
+    uint32_t v[8];
+    {
+        const uint4 x = *reinterpret_cast<const uint4*>(&T[a][c0]);
+        const uint4 y = *reinterpret_cast<const uint4*>(&T[a][c0 + 8]);
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w; v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
+    }
+    // Step kk reads only row kk and column kk, which step kk leaves unchanged
+    // (T[kk][kk] = 0), so one barrier per step orders the writes of step kk
+    // before the reads of step kk + 1.
     for (int kk = 0; kk < mk; ++kk) {
-        for (int idx = tid; idx < mk * mk; idx += blockDim.x) {
-            const int a = idx / mk, c = idx % mk;
-            const uint32_t alt = sat_add(T[a][kk], T[kk][c]);
-            if (alt < T[a][c]) T[a][c] = (uint16_t)alt;
+        const uint32_t t = T[a][kk];
+        const uint4 x = *reinterpret_cast<const uint4*>(&T[kk][c0]);
+        const uint4 y = *reinterpret_cast<const uint4*>(&T[kk][c0 + 8]);
+        if (t < INF) {
+            const uint32_t r[8] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
+            const uint32_t aa = splat(t), tt = splat(INF - t);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = acc_clamp(v[i], r[i], aa, tt);
+            *reinterpret_cast<uint4*>(&T[a][c0]) = make_uint4(v[0], v[1], v[2], v[3]);
+            *reinterpret_cast<uint4*>(&T[a][c0 + 8]) = make_uint4(v[4], v[5], v[6], v[7]);
         }
         __syncthreads();
     }
-    const int slab0 = blockIdx.x * kPanelSlab;
-    const int w = min(kPanelSlab, NP - slab0);
-    for (int idx = tid; idx < mk * (w / 8); idx += blockDim.x) {
-        const int a = idx / (w / 8), c8 = idx % (w / 8);
-        reinterpret_cast<uint4*>(&Dk[a][0])[c8] =
-            reinterpret_cast<const uint4*>(D + (size_t)kc[a] * NP + slab0)[c8];
-    }
-    __syncthreads();
-    uint16_t* P = panel + (size_t)slot * B * NP;
-    // Each thread: one pivot row a and a run of column pairs.
-    __shared__ int tile_any[kPanelSlab / kFlagTile];
-    if (tid < kPanelSlab / kFlagTile) tile_any[tid] = 0;
-    __syncthreads();
-    const int pairs = w / 2;
-    for (int idx = tid; idx < B * pairs; idx += blockDim.x) {
-        const int a = idx / pairs, cp = idx % pairs;
-        uint32_t acc = INF2;
-        if (a < mk) {
-            const uint32_t* dk = reinterpret_cast<const uint32_t*>(&Dk[0][0]) + cp;
-            for (int c = 0; c < mk; ++c) {
-                const uint32_t t = T[a][c];
-                if (t >= INF) continue;
-                acc = acc_clamp(acc, dk[c * (kPanelSlab / 2)], splat(t), splat(INF - t));
-            }
-            if (acc != INF2) tile_any[(2 * cp) / kFlagTile] = 1;
-        }
-        reinterpret_cast<uint32_t*>(P + (size_t)a * NP + slab0)[cp] = acc;
-    }
-    __syncthreads();
-    if (tid < w / kFlagTile) flags[(size_t)slot * (NP / kFlagTile) + slab0 / kFlagTile + tid] = tile_any[tid] ? 1 : 0;
+    uint4* out = reinterpret_cast<uint4*>(tstar + (size_t)slot * B * B + (size_t)a * B + c0);
+    out[0] = make_uint4(v[0], v[1], v[2], v[3]);
+    out[1] = make_uint4(v[4], v[5], v[6], v[7]);
 }
 
 // Register-tiled symmetric rank-|Kc| min-plus update.  Warp w owns RW rows
 // of the CTA tile; all 32 lanes of a warp share those rows, so the pivot
 // value a = R'[k][row] is warp-uniform and the fast / clamped / skip choice
 // never diverges.  Each lane owns CP packed column pairs.
-template <int RW, int CP>
+//
+// PANEL = true computes the round's panel with the same tiling instead:
+//   R'[a][j] = min_c T*[c][a] (+) D[Kc[c]][j]      (T* symmetric, so
+// T*[c][a] = T*[a][c]), one CTA per 64*CP columns and all B pivot rows,
+// and marks the 64-column tiles of R' holding any finite value.
+template <int RW, int CP, bool PANEL>
 __global__ void __launch_bounds__(256)
-closure_syrk_kernel(MatSet M, const int* __restrict__ active, const int* __restrict__ kcnt, int round,
-                    const uint16_t* __restrict__ panel, const uint8_t* __restrict__ flags) {
+closure_gemm_kernel(MatSet M, const int* __restrict__ active, const int* __restrict__ klist,
+                    const int* __restrict__ kcnt, int round, uint16_t* panel, uint8_t* flags,
+                    const uint16_t* __restrict__ tstar) {
     constexpr int B = kPivotChunk;
     constexpr int MT = 8 * RW;
     constexpr int NT = 64 * CP;
+    static_assert(!PANEL || MT == B, "the panel tile covers all pivot rows");
     extern __shared__ __align__(16) uint16_t sm[];
     uint16_t* As = sm;            // [B][MT]
     uint16_t* Bs = sm + B * MT;   // [B][NT]
+    __shared__ int kc[B];
+    __shared__ int tile_any[NT / kFlagTile];
     const int slot = blockIdx.z;
     const int m = active[slot];
     const int NP = M.NP;
     const int mk = min(B, kcnt[m] - round * B);
     if (mk <= 0) return;
     const int i0 = blockIdx.y * MT, j0 = blockIdx.x * NT;
-    const uint8_t* fl = flags + (size_t)slot * (NP / kFlagTile);
-    bool any_i = false, any_j = false;
-    for (int t = 0; t < MT / kFlagTile + (MT % kFlagTile ? 1 : 0); ++t) any_i |= fl[(i0 + t * kFlagTile) / kFlagTile] != 0;
-    for (int t = 0; t < NT / kFlagTile + (NT % kFlagTile ? 1 : 0); ++t) any_j |= fl[(j0 + t * kFlagTile) / kFlagTile] != 0;
-    if (!any_i || !any_j) return;
-    const uint16_t* P = panel + (size_t)slot * B * NP;
+    uint16_t* P = panel + (size_t)slot * B * NP;
+    uint16_t* D = mat_ptr(M, m);
     const int tid = threadIdx.x;
-    for (int idx = tid; idx < mk * (MT / 8); idx += blockDim.x) {
-        const int a = idx / (MT / 8), c8 = idx % (MT / 8);
-        reinterpret_cast<uint4*>(As + a * MT)[c8] = reinterpret_cast<const uint4*>(P + (size_t)a * NP + i0)[c8];
-    }
-    for (int idx = tid; idx < mk * (NT / 8); idx += blockDim.x) {
-        const int a = idx / (NT / 8), c8 = idx % (NT / 8);
-        reinterpret_cast<uint4*>(Bs + a * NT)[c8] = reinterpret_cast<const uint4*>(P + (size_t)a * NP + j0)[c8];
+    if constexpr (PANEL) {
+        const int* K = klist + (size_t)m * NP + round * B;
+        if (tid < mk) kc[tid] = K[tid];
+        if (tid < NT / kFlagTile) tile_any[tid] = 0;
+        __syncthreads();
+        const uint16_t* Ts = tstar + (size_t)slot * B * B;
+        for (int idx = tid; idx < mk * (MT / 8); idx += blockDim.x) {
+            const int a = idx / (MT / 8), c8 = idx % (MT / 8);
+            reinterpret_cast<uint4*>(As + a * MT)[c8] = reinterpret_cast<const uint4*>(Ts + (size_t)a * B)[c8];
+        }
+        for (int idx = tid; idx < mk * (NT / 8); idx += blockDim.x) {
+            const int a = idx / (NT / 8), c8 = idx % (NT / 8);
+            reinterpret_cast<uint4*>(Bs + a * NT)[c8] =
+                reinterpret_cast<const uint4*>(D + (size_t)kc[a] * NP + j0)[c8];
+        }
+    } else {
+        const uint8_t* fl = flags + (size_t)slot * (NP / kFlagTile);
+        bool any_i = false, any_j = false;
+        for (int t = 0; t < MT / kFlagTile + (MT % kFlagTile ? 1 : 0); ++t) any_i |= fl[(i0 + t * kFlagTile) / kFlagTile] != 0;
+        for (int t = 0; t < NT / kFlagTile + (NT % kFlagTile ? 1 : 0); ++t) any_j |= fl[(j0 + t * kFlagTile) / kFlagTile] != 0;
+        if (!any_i || !any_j) return;
+        for (int idx = tid; idx < mk * (MT / 8); idx += blockDim.x) {
+            const int a = idx / (MT / 8), c8 = idx % (MT / 8);
+            reinterpret_cast<uint4*>(As + a * MT)[c8] = reinterpret_cast<const uint4*>(P + (size_t)a * NP + i0)[c8];
+        }
+        for (int idx = tid; idx < mk * (NT / 8); idx += blockDim.x) {
+            const int a = idx / (NT / 8), c8 = idx % (NT / 8);
+            reinterpret_cast<uint4*>(Bs + a * NT)[c8] = reinterpret_cast<const uint4*>(P + (size_t)a * NP + j0)[c8];
+        }
     }
     const int warp = tid >> 5, lane = tid & 31;
-    uint16_t* D = mat_ptr(M, m);
     uint32_t acc[RW][CP];
     const int col = j0 + lane * 2 * CP;
 #pragma unroll
     for (int r = 0; r < RW; ++r) {
         const uint32_t* src = reinterpret_cast<const uint32_t*>(D + (size_t)(i0 + warp * RW + r) * NP + col);
 #pragma unroll
-        for (int c = 0; c < CP; ++c) acc[r][c] = src[c];
+        for (int c = 0; c < CP; ++c) acc[r][c] = PANEL ? INF2 : src[c];
     }
     __syncthreads();
     for (int k = 0; k < mk; ++k) {
@@ -310,11 +332,27 @@ closure_syrk_kernel(MatSet M, const int* __restrict__ active, const int* __restr
             }
         }
     }
+    if constexpr (PANEL) {
+        bool any = false;
 #pragma unroll
-    for (int r = 0; r < RW; ++r) {
-        uint32_t* dst = reinterpret_cast<uint32_t*>(D + (size_t)(i0 + warp * RW + r) * NP + col);
+        for (int r = 0; r < RW; ++r) {
+            uint32_t* dst = reinterpret_cast<uint32_t*>(P + (size_t)(warp * RW + r) * NP + col);
 #pragma unroll
-        for (int c = 0; c < CP; ++c) dst[c] = acc[r][c];
+            for (int c = 0; c < CP; ++c) {
+                dst[c] = acc[r][c];
+                any |= acc[r][c] != INF2;
+            }
+        }
+        if (any) tile_any[(lane * 2 * CP) / kFlagTile] = 1;
+        __syncthreads();
+        if (tid < NT / kFlagTile) flags[(size_t)slot * (NP / kFlagTile) + j0 / kFlagTile + tid] = tile_any[tid] ? 1 : 0;
+    } else {
+#pragma unroll
+        for (int r = 0; r < RW; ++r) {
+            uint32_t* dst = reinterpret_cast<uint32_t*>(D + (size_t)(i0 + warp * RW + r) * NP + col);
+#pragma unroll
+            for (int c = 0; c < CP; ++c) dst[c] = acc[r][c];
+        }
     }
 }
 
@@ -519,28 +557,41 @@ void launch_compact_pivots(uint8_t* kflag, int NP, const int* active, int n_acti
     compact_pivots_kernel<<<n_active, 256, 0, st>>>(kflag, NP, active, klist, kcnt);
 }
 
-template <int RW, int CP>
-static void launch_syrk_t(MatSet M, const int* active, int n_active, const int* kcnt, int round,
-                          const uint16_t* panel, const uint8_t* flags, cudaStream_t st) {
+template <int RW, int CP, bool PANEL>
+static void launch_gemm_t(MatSet M, const int* active, int n_active, const int* klist, const int* kcnt, int round,
+                          uint16_t* panel, uint8_t* flags, const uint16_t* tstar, cudaStream_t st) {
     constexpr int MT = 8 * RW, NT = 64 * CP;
     const size_t smem = (size_t)kPivotChunk * (MT + NT) * sizeof(uint16_t);
     static bool configured = false;
     if (!configured) {
-        cudaFuncSetAttribute(closure_syrk_kernel<RW, CP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(closure_gemm_kernel<RW, CP, PANEL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
         configured = true;
     }
-    dim3 grid(M.NP / NT, M.NP / MT, n_active);
-    closure_syrk_kernel<RW, CP><<<grid, 256, smem, st>>>(M, active, kcnt, round, panel, flags);
+    dim3 grid(M.NP / NT, PANEL ? 1 : M.NP / MT, n_active);
+    closure_gemm_kernel<RW, CP, PANEL><<<grid, 256, smem, st>>>(M, active, klist, kcnt, round, panel, flags, tstar);
+}
+
+size_t closure_scratch_elems(int NP, int n_active) {
+    return (size_t)n_active * kPivotChunk * NP + (size_t)n_active * kPivotChunk * kPivotChunk;
 }
 
 void launch_closure_round(MatSet M, const int* active, int n_active, const int* klist, const int* kcnt,
                           int round, uint16_t* panel, uint8_t* flags, cudaStream_t st) {
     if (n_active == 0) return;
-    dim3 pgrid(blocks_for(M.NP, kPanelSlab), n_active);
-    closure_panel_kernel<<<pgrid, 256, 0, st>>>(M, active, klist, kcnt, round, panel, flags);
-    if (M.NP >= 256) launch_syrk_t<16, 4>(M, active, n_active, kcnt, round, panel, flags, st);
-    else if (M.NP >= 128) launch_syrk_t<16, 2>(M, active, n_active, kcnt, round, panel, flags, st);
-    else launch_syrk_t<8, 1>(M, active, n_active, kcnt, round, panel, flags, st);
+    uint16_t* tstar = panel + (size_t)n_active * kPivotChunk * M.NP;
+    pivot_close_kernel<<<n_active, 256, 0, st>>>(M, active, klist, kcnt, round, tstar);
+    // Panel tiles: the widest whose grid still has two CTAs per SM (148 SMs).
+    const size_t ctas = (size_t)(M.NP / 64) * n_active;
+    if (M.NP >= 256 && ctas >= 4 * 296)
+        launch_gemm_t<8, 4, true>(M, active, n_active, klist, kcnt, round, panel, flags, tstar, st);
+    else if (M.NP >= 128 && ctas >= 2 * 296)
+        launch_gemm_t<8, 2, true>(M, active, n_active, klist, kcnt, round, panel, flags, tstar, st);
+    else
+        launch_gemm_t<8, 1, true>(M, active, n_active, klist, kcnt, round, panel, flags, tstar, st);
+    if (M.NP >= 256) launch_gemm_t<16, 4, false>(M, active, n_active, klist, kcnt, round, panel, flags, tstar, st);
+    else if (M.NP >= 128) launch_gemm_t<16, 2, false>(M, active, n_active, klist, kcnt, round, panel, flags, tstar, st);
+    else launch_gemm_t<8, 1, false>(M, active, n_active, klist, kcnt, round, panel, flags, tstar, st);
 }
 
 void launch_leaf_edges(MatSet leaves, const int* active, int n_active, const int* eoff, const int* edges,

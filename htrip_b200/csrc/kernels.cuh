@@ -41,7 +41,9 @@ void launch_compact_pivots(uint8_t* kflag, int NP, const int* active, int n_acti
                            int* kcnt, cudaStream_t st);
 
 // One round of the blocked pivot-set Kleene closure: pivots
-// klist[m][round*B .. round*B+B).  panel/flags: scratch for n_active mats.
+// klist[m][round*B .. round*B+B).  panel: closure_scratch_elems(NP,
+// n_active) u16 of scratch; flags: n_active * NP / kFlagTile bytes.
+size_t closure_scratch_elems(int NP, int n_active);
 void launch_closure_round(MatSet M, const int* active, int n_active, const int* klist,
                           const int* kcnt, int round, uint16_t* panel, uint8_t* flags,
                           cudaStream_t st);
