@@ -214,11 +214,15 @@ def bench_opening(device, steps=400):
     assert dev.build(obs)
     build_s = time.perf_counter() - t
     open_ms, query_ms, cells, entries = [], [], 0, 0
+    ops = nbytes = 0
     for step, c in enumerate(batches):
         obs[c[:, 0], c[:, 1]] = W.FREE
         t = time.perf_counter()
         dev.onBatchCellsOpened(c, obs)
         open_ms.append(1e3 * (time.perf_counter() - t))
+        b_, o_ = dev.lastOpenWork()
+        ops += o_
+        nbytes += b_
         cells += len(c)
         vps = np.concatenate([starts, W.frontier_cells(obs, 48, 1000 + step)]).astype(np.int32)
         t = time.perf_counter()
@@ -231,6 +235,9 @@ def bench_opening(device, steps=400):
     out = {"workload": f"1024x1024 street, b=8, {len(batches)} onBatchCellsOpened x 256 cells (BFS rings), "
                        "each + queryAllPairs k=64",
            "cells_per_s": cells / (1e-3 * sum(open_ms)), "unit": "cells/s",
+           "alg_minplus_ops_per_call": ops / len(batches), "alg_bytes_per_call": nbytes / len(batches),
+           "achieved_t_minplus_per_s": ops / (1e-3 * sum(open_ms)) / 1e12,
+           "achieved_gb_per_s": nbytes / (1e-3 * sum(open_ms)) / 1e9,
            "open_ms_p50": _pct(open_ms, 50), "open_ms_p99": _pct(open_ms, 99),
            "query_entries_per_s": entries / (1e-3 * sum(query_ms)), "query_ms_p50": _pct(query_ms, 50),
            "build_s": round(build_s, 4), "parity_vs_rebuild": parity}
@@ -533,6 +540,8 @@ def run_ours(args, rank, world, local_rank):
         for name, fn in (("cells_opened", lambda: bench_opening(local_rank)),
                          ("batched", lambda: bench_batched(local_rank)),
                          ("served", lambda: bench_served(local_rank))):
+            if args.section and args.section != name:
+                continue
             t = time.perf_counter()
             try:
                 line[name] = fn()
@@ -551,6 +560,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--headline-only", action="store_true",
                     help="only the queryAllPairs headline (skip the opening / batched / served workloads)")
+    ap.add_argument("--section", choices=["cells_opened", "batched", "served"],
+                    help="run only this one of the further workloads after the headline")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))

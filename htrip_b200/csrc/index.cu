@@ -66,12 +66,16 @@ int pad_order(int n) {
     return (n + 255) / 256 * 256;
 }
 
+// Device buffer.  A buffer that has to grow grows by at least half its size,
+// so scratch that creeps up call by call is reallocated (a device-wide
+// synchronisation) only a few times; a first reservation is exact.
 template <class T>
 struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
     void reserve(size_t m) {
         if (m <= n) return;
+        if (n) m = std::max(m, n + n / 2);
         if (p) cudaFree(p);
         p = nullptr;
         n = 0;
@@ -112,6 +116,7 @@ struct HostBuf {
     size_t n = 0;
     void reserve(size_t m) {
         if (m <= n) return;
+        if (n) m = std::max(m, n + n / 2);
         if (p) cudaFreeHost(p);
         p = nullptr;
         n = 0;
@@ -159,6 +164,7 @@ struct htrip_index {
     std::vector<std::vector<uint16_t>> parked;  // per level matrices, then the passability mirror
     size_t parked_pass = 0;
     uint64_t ref_bytes = 0;  // the reference's totalMemoryBytes accounting of this index
+    uint64_t open_ops = 0, open_bytes = 0;  // algorithmic work of the last opening call
     int S = 0, H = 0, rows = 0, cols = 0, leaves_x = 0;
     std::vector<Level> L;
     DevBuf<uint8_t> pass;
@@ -499,6 +505,7 @@ void open_prepare(OpenTask& T, htrip_index* h, const int32_t* rc, int n, const u
         }
     }
     if (record_stats) h->stats = {0, 0, 0};
+    h->open_ops = h->open_bytes = 0;
 }
 
 bool open_has_work(const OpenTask& T) { return !T.leaves.empty(); }
@@ -600,6 +607,14 @@ void open_close(OpenTask& T, int l) {
     Level& Lv = h->L[l];
     const int na = (int)T.act.size();
     const int* kc = rb_kcnt(h);
+    // algorithmic work of this level (per dirty matrix of order n with pivot
+    // set K: n^2 |K| min-plus ops, 2 n^2 2 + |K| n 2 2 bytes)
+    for (int i = 0; i < na; ++i) {
+        if (kc[i] == 0) continue;
+        const uint64_t n = (uint64_t)Lv.n, k = (uint64_t)kc[i];
+        h->open_ops += n * n * k;
+        h->open_bytes += 4 * n * n + 4 * k * n;
+    }
     const size_t per = (size_t)hb::kPivotChunk * Lv.NP;
     const size_t cap = std::max<size_t>(1, (size_t)(128u << 20) / (per * sizeof(uint16_t)));
     for (size_t c0 = 0; c0 < (size_t)na; c0 += cap) {
@@ -1593,6 +1608,13 @@ htrip_status htrip_last_query_phases(const htrip_index* h, uint64_t* ns, int32_t
 htrip_status htrip_batch_last_phases(const htrip_batch* b, uint64_t* ns, int32_t max_n, int32_t* n) {
     if (!b) return fail(HTRIP_ERR_INVALID, "null batch");
     return arena_phases(b->q, b->stream, ns, max_n, n);
+}
+
+htrip_status htrip_last_open_work(const htrip_index* h, uint64_t* alg_bytes, uint64_t* alg_ops) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    if (alg_bytes) *alg_bytes = h->open_bytes;
+    if (alg_ops) *alg_ops = h->open_ops;
+    return HTRIP_OK;
 }
 
 htrip_status htrip_last_query_io(const htrip_index* h, uint64_t* h2d_bytes, uint64_t* d2h_bytes) {

@@ -83,7 +83,7 @@ EXPORTS = (
     "htrip_estimate_bytes", "htrip_server_last_error", "htrip_server_create", "htrip_server_destroy",
     "htrip_server_add_session", "htrip_server_remove_session", "htrip_server_submit_query",
     "htrip_server_submit_open", "htrip_server_wait", "htrip_server_get_stats", "htrip_server_run_trace",
-    "htrip_measure_minplus_rate", "htrip_last_query_phases", "htrip_batch_last_phases",
+    "htrip_measure_minplus_rate", "htrip_last_query_phases", "htrip_batch_last_phases", "htrip_last_open_work",
 )
 
 
@@ -131,6 +131,7 @@ def load_library(path: str | None = None):
     lib.htrip_open_batch.argtypes = [P, C.POINTER(_OpenRequest), I]
     lib.htrip_measure_minplus_rate.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
     lib.htrip_last_query_phases.argtypes = [P, _U64P, I, _I32P]
+    lib.htrip_last_open_work.argtypes = [P, _U64P, _U64P]
     lib.htrip_batch_last_phases.argtypes = [P, _U64P, I, _I32P]
     lib.htrip_offload.argtypes = [P]
     lib.htrip_restore.argtypes = [P]
@@ -339,6 +340,12 @@ class MinPlusOracle:
         ms = C.c_float()
         _check(self.lib.htrip_last_query_kernel_ms(self.h, C.byref(ms)))
         return ms.value
+
+    def lastOpenWork(self):
+        """(algorithmic bytes, min-plus ops) of the last opening call."""
+        b, o = C.c_uint64(), C.c_uint64()
+        _check(self.lib.htrip_last_open_work(self.h, C.byref(b), C.byref(o)))
+        return b.value, o.value
 
     def lastQueryPhases(self):
         """Per-phase nanoseconds of the last query launch (htrip_last_query_phases)."""

@@ -261,6 +261,12 @@ htrip_status htrip_last_query_io(const htrip_index* h, uint64_t* h2d_bytes, uint
  * (a <= 5535).                                                            */
 htrip_status htrip_measure_minplus_rate(int device, int variant, double* entries_per_s);
 
+/* Algorithmic work of the index's last opening call (htrip_open_cells,
+ * htrip_open_cell or its part of htrip_open_batch): per dirty matrix of
+ * order n (b^2 or nV) closed over the pivot set K, n^2 |K| min-plus
+ * operations and 2 n^2 2 + |K| n 2 2 bytes, summed over leaves and nodes.  */
+htrip_status htrip_last_open_work(const htrip_index* h, uint64_t* alg_bytes, uint64_t* alg_ops);
+
 /* Phase trace of the last query launch of an index / a batch: ns[i] =
  * global-timer nanoseconds of phase i of the persistent query kernel
  * (0: level-0 gathers; 1..H+1: projections of level i with the meets of
