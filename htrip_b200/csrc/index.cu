@@ -13,6 +13,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <tuple>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -1098,9 +1100,40 @@ std::vector<uint8_t> viewpoint_flags(const htrip_index* h, const int32_t* vps, i
     return pf;
 }
 
+// ---------------------------------------------------------------------------
+// Query tile autotuner.  A process-wide table maps a request bucket - the
+// index's depth H and root matrix order, and the base-2 logarithms of the
+// viewpoint count and of the largest root child group - to the tile
+// configuration (hb::query_config_tile) measured fastest for a sample of
+// that bucket (htrip_autotune_query).  Buckets without an entry use the
+// fixed rule.  The table is exported / imported as text lines
+// "H NP log2_k log2_group cfg" (htrip_autotune_export / _import).
+// ---------------------------------------------------------------------------
+struct TuneKey {
+    int H, NP, kb, gb;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(H, NP, kb, gb) < std::tie(o.H, o.NP, o.kb, o.gb);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, int> g_tune;
+
+int log2_bucket(int x) {
+    int b = 0;
+    while ((1 << (b + 1)) <= std::max(x, 1)) ++b;
+    return b;
+}
+
+TuneKey tune_key(const htrip_index* h, int ns, int root_group) {
+    return TuneKey{h->H, h->L[h->H].NP, log2_bucket(ns), log2_bucket(root_group)};
+}
+
 int choose_query_cfg(const htrip_index* h, int ns, int root_group) {
-    (void)h;
-    (void)ns;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(tune_key(h, ns, root_group));
+        if (it != g_tune.end()) return it->second;
+    }
     return root_group >= 24 ? 2 : 1;
 }
 
@@ -1608,6 +1641,90 @@ htrip_status htrip_last_query_phases(const htrip_index* h, uint64_t* ns, int32_t
 htrip_status htrip_batch_last_phases(const htrip_batch* b, uint64_t* ns, int32_t max_n, int32_t* n) {
     if (!b) return fail(HTRIP_ERR_INVALID, "null batch");
     return arena_phases(b->q, b->stream, ns, max_n, n);
+}
+
+htrip_status htrip_autotune_query(htrip_index* h, const int32_t* vps, int32_t k, const uint8_t* observed,
+                                  int32_t rows, int32_t cols, int32_t reps, int32_t* best_cfg, float* best_ms) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    if (const htrip_status rs = ready(h)) return rs;
+    if (k <= 0 || !vps || !observed || reps <= 0) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    const std::vector<uint8_t> pf = viewpoint_flags(h, vps, k, observed, rows, cols);
+    QueryPlan P0;
+    make_plan(h, vps, pf.data(), k, P0);
+    const TuneKey key = tune_key(h, P0.n_sorted, h->H >= 1 ? P0.lv[h->H].max_group : P0.n_sorted);
+    int best = -1;
+    float best_t = 0.f;
+    for (int cfg = 0; cfg < hb::kNumQueryConfigs; ++cfg) {
+        QueryPlan P;
+        make_plan(h, vps, pf.data(), k, P, cfg);
+        const std::vector<QueryReq> R{{h, &P, nullptr}};
+        float t = 0.f;
+        for (int r = 0; r <= reps; ++r) {  // the first launch warms up and is not counted
+            if (run_queries(h->q, h->device, h->stream, R, {nullptr}, true) != 0)
+                return fail(HTRIP_ERR_CUDA, "query kernel: grid barrier timed out");
+            float ms = 0.f;
+            ck(cudaEventElapsedTime(&ms, h->q.ev[0], h->q.ev[1]), "event time");
+            if (r > 0) t = (r == 1) ? ms : std::min(t, ms);
+        }
+        if (best < 0 || t < best_t) {
+            best = cfg;
+            best_t = t;
+        }
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune[key] = best;
+    }
+    if (best_cfg) *best_cfg = best;
+    if (best_ms) *best_ms = best_t;
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_autotune_export(char* buf, size_t cap, size_t* len) {
+    std::string out;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        for (const auto& kv : g_tune)
+            out += std::to_string(kv.first.H) + " " + std::to_string(kv.first.NP) + " " + std::to_string(kv.first.kb) +
+                   " " + std::to_string(kv.first.gb) + " " + std::to_string(kv.second) + "\n";
+    }
+    if (len) *len = out.size();
+    if (buf && cap > 0) {
+        const size_t n = std::min(cap - 1, out.size());
+        std::memcpy(buf, out.data(), n);
+        buf[n] = 0;
+        if (out.size() + 1 > cap) return fail(HTRIP_ERR_INVALID, "buffer too small");
+    }
+    return HTRIP_OK;
+}
+
+htrip_status htrip_autotune_import(const char* text) {
+    if (!text) return fail(HTRIP_ERR_INVALID, "null text");
+    std::map<TuneKey, int> add;
+    const char* p = text;
+    while (*p) {
+        int v[5], used = 0;
+        if (std::sscanf(p, "%d %d %d %d %d%n", &v[0], &v[1], &v[2], &v[3], &v[4], &used) != 5) {
+            while (*p == ' ' || *p == '\n' || *p == '\r' || *p == '\t') ++p;
+            if (!*p) break;
+            return fail(HTRIP_ERR_INVALID, "malformed tuning line");
+        }
+        if (v[4] < 0 || v[4] >= hb::kNumQueryConfigs) return fail(HTRIP_ERR_INVALID, "tile configuration out of range");
+        add[TuneKey{v[0], v[1], v[2], v[3]}] = v[4];
+        p += used;
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (const auto& kv : add) g_tune[kv.first] = kv.second;
+    return HTRIP_OK;
+}
+
+htrip_status htrip_autotune_clear(void) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune.clear();
+    return HTRIP_OK;
 }
 
 htrip_status htrip_last_open_work(const htrip_index* h, uint64_t* alg_bytes, uint64_t* alg_ops) {

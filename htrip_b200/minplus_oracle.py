@@ -84,6 +84,7 @@ EXPORTS = (
     "htrip_server_add_session", "htrip_server_remove_session", "htrip_server_submit_query",
     "htrip_server_submit_open", "htrip_server_wait", "htrip_server_get_stats", "htrip_server_run_trace",
     "htrip_measure_minplus_rate", "htrip_last_query_phases", "htrip_batch_last_phases", "htrip_last_open_work",
+    "htrip_autotune_query", "htrip_autotune_export", "htrip_autotune_import", "htrip_autotune_clear",
 )
 
 
@@ -132,6 +133,10 @@ def load_library(path: str | None = None):
     lib.htrip_measure_minplus_rate.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
     lib.htrip_last_query_phases.argtypes = [P, _U64P, I, _I32P]
     lib.htrip_last_open_work.argtypes = [P, _U64P, _U64P]
+    lib.htrip_autotune_query.argtypes = [P, _I32P, I, _U8P, I, I, I, _I32P, C.POINTER(C.c_float)]
+    lib.htrip_autotune_export.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
+    lib.htrip_autotune_import.argtypes = [C.c_char_p]
+    lib.htrip_autotune_clear.argtypes = []
     lib.htrip_batch_last_phases.argtypes = [P, _U64P, I, _I32P]
     lib.htrip_offload.argtypes = [P]
     lib.htrip_restore.argtypes = [P]
@@ -341,6 +346,16 @@ class MinPlusOracle:
         _check(self.lib.htrip_last_query_kernel_ms(self.h, C.byref(ms)))
         return ms.value
 
+    def autotuneQuery(self, viewpoints, grid, reps: int = 5):
+        """Time every query tile shape on this request; the fastest becomes the
+        shape of its bucket (htrip_autotune_query).  Returns (cfg, ms)."""
+        rc = _rc(viewpoints)
+        obs, ptr, rows, cols = _grid_args(grid)
+        cfg, ms = C.c_int32(), C.c_float()
+        _check(self.lib.htrip_autotune_query(self.h, rc.ctypes.data_as(_I32P), len(rc), ptr, rows, cols, reps,
+                                             C.byref(cfg), C.byref(ms)))
+        return cfg.value, ms.value
+
     def lastOpenWork(self):
         """(algorithmic bytes, min-plus ops) of the last opening call."""
         b, o = C.c_uint64(), C.c_uint64()
@@ -494,6 +509,24 @@ class Batch:
         _check(self.lib.htrip_batch_last_phases(self.h, buf, 32, C.byref(n)))
         return [int(buf[i]) for i in range(n.value)]
 
+
+
+def autotune_export() -> str:
+    """The tuning table as text lines "H NP log2_k log2_group cfg"."""
+    lib = load_library()
+    n = C.c_size_t()
+    _check(lib.htrip_autotune_export(None, 0, C.byref(n)))
+    buf = C.create_string_buffer(n.value + 1)
+    _check(lib.htrip_autotune_export(buf, n.value + 1, C.byref(n)))
+    return buf.value.decode()
+
+
+def autotune_import(text: str):
+    _check(load_library().htrip_autotune_import(text.encode()))
+
+
+def autotune_clear():
+    _check(load_library().htrip_autotune_clear())
 
 
 def minplus_rate(device: int = 0, variant: int = 0) -> float:

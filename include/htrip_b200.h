@@ -261,6 +261,21 @@ htrip_status htrip_last_query_io(const htrip_index* h, uint64_t* h2d_bytes, uint
  * (a <= 5535).                                                            */
 htrip_status htrip_measure_minplus_rate(int device, int variant, double* entries_per_s);
 
+/* Query tile autotuner (no reference counterpart).  The query kernel has
+ * hb::kNumQueryConfigs tile shapes; a process-wide table maps a request
+ * bucket (H, root matrix order, log2 of the viewpoint count, log2 of the
+ * largest root child group) to the shape to use, falling back to a fixed
+ * rule.  htrip_autotune_query times every shape on this request (reps
+ * timed launches each, minimum kept), stores the fastest for its bucket and
+ * returns it.  Results do not depend on the shape (the kernel is exact for
+ * all of them).  The table is exported / imported as text lines
+ * "H NP log2_k log2_group cfg"; htrip_autotune_clear empties it.           */
+htrip_status htrip_autotune_query(htrip_index* h, const int32_t* vps, int32_t k, const uint8_t* observed,
+                                  int32_t rows, int32_t cols, int32_t reps, int32_t* best_cfg, float* best_ms);
+htrip_status htrip_autotune_export(char* buf, size_t cap, size_t* len);
+htrip_status htrip_autotune_import(const char* text);
+htrip_status htrip_autotune_clear(void);
+
 /* Algorithmic work of the index's last opening call (htrip_open_cells,
  * htrip_open_cell or its part of htrip_open_batch): per dirty matrix of
  * order n (b^2 or nV) closed over the pivot set K, n^2 |K| min-plus
