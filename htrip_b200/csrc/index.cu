@@ -167,6 +167,8 @@ struct htrip_index {
     size_t parked_pass = 0;
     uint64_t ref_bytes = 0;  // the reference's totalMemoryBytes accounting of this index
     uint64_t open_ops = 0, open_bytes = 0;  // algorithmic work of the last opening call
+    uint64_t epoch = 0;           // build / root growth count (reference MinPlusOracle::epoch)
+    uint64_t update_counter = 0;  // opening calls since creation
     int S = 0, H = 0, rows = 0, cols = 0, leaves_x = 0;
     std::vector<Level> L;
     DevBuf<uint8_t> pass;
@@ -198,6 +200,17 @@ struct htrip_index {
         snap.release(); pivots.release(); rb.release(); rb_dev.release();
         q.release();
     }
+};
+
+// Cached result of queryAllPairsIncremental (reference HTripIncrementalState,
+// minplus_oracle.hpp:262-273): the viewpoints, the index's build / root-growth
+// epoch and update count when the matrix was computed, and the matrix.
+struct htrip_incremental {
+    bool initialized = false;
+    const htrip_index* index = nullptr;
+    uint64_t epoch = 0, updates = 0;
+    std::vector<int32_t> vps;
+    std::vector<uint16_t> matrix;
 };
 
 // A launch context for batched calls over many indexes of one device
@@ -397,6 +410,99 @@ void do_build(htrip_index* h, const uint8_t* observed, int rows, int cols) {
     }
     ck(cudaStreamSynchronize(st), "build sync");
     h->built = true;
+    h->epoch++;
+}
+
+// ---------------------------------------------------------------------------
+// Root growth (reference MinPlusOracle::liftRoot, minplus_oracle.cpp:2008-2114):
+// S -> S*g, H -> H+1.  Every existing leaf and node keeps its matrix (moved to
+// its index in the wider level); leaves and nodes of the new area are built
+// from `observed` (leaf BFS, child summaries + seams, closure), and a new
+// root closes the old root and its new siblings over their seams.
+// ---------------------------------------------------------------------------
+void do_lift_root(htrip_index* h, const uint8_t* observed, int rows, int cols) {
+    const int g = h->g, b = h->b;
+    const int old_S = h->S, old_H = h->H;
+    cudaStream_t st = h->stream;
+    ck(cudaStreamSynchronize(st), "sync");
+    std::vector<Level> old = std::move(h->L);
+    h->L.clear();
+    const int old_rows = h->rows, old_cols = h->cols, old_max_nodes = h->max_nodes;
+    const uint64_t old_ref = h->ref_bytes;
+    h->S = old_S * g;
+    h->H = old_H + 1;
+    h->leaves_x = h->S / b;
+    h->rows = rows;
+    h->cols = cols;
+    try {
+        make_levels(h);
+        h->ref_bytes = reference_bytes(h);
+        alloc_levels(h);
+        // move the old matrices to their places in the wider levels
+        for (int l = 0; l <= old_H; ++l) {
+            Level& Ln = h->L[l];
+            const Level& Lo = old[l];
+            const size_t mat = (size_t)Ln.NP * Ln.NP * sizeof(uint16_t);
+            ck(cudaMemcpy2DAsync(Ln.mat.p, Ln.nodes_x * mat, Lo.mat.p, Lo.nodes_x * mat, Lo.nodes_x * mat, Lo.nodes_x,
+                                 cudaMemcpyDeviceToDevice, st), "move matrices");
+        }
+    } catch (...) {
+        for (auto& l : h->L) { l.d_ext.release(); l.d_seams.release(); l.d_ext_inv.release(); l.mat.release();
+                               l.kflag.release(); l.klist.release(); l.kcnt.release(); l.dec.release(); }
+        h->L = std::move(old);  // the old matrices are intact
+        h->S = old_S;
+        h->H = old_H;
+        h->leaves_x = old_S / b;
+        h->rows = old_rows;
+        h->cols = old_cols;
+        h->max_nodes = old_max_nodes;  // the read-back buffers only ever grow
+        h->ref_bytes = old_ref;
+        throw;
+    }
+    for (auto& l : old) { l.d_ext.release(); l.d_seams.release(); l.d_ext_inv.release(); l.mat.release();
+                          l.kflag.release(); l.klist.release(); l.kcnt.release(); l.dec.release(); }
+    old.clear();
+    const int S = h->S;
+    std::vector<uint8_t> pass((size_t)S * S, 0);
+    for (int r = 0; r < std::min(rows, S); ++r)
+        for (int c = 0; c < std::min(cols, S); ++c) pass[(size_t)r * S + c] = observed[(size_t)r * cols + c] == 1;
+    h->pass.reserve(pass.size());
+    ck(cudaMemcpyAsync(h->pass.p, pass.data(), pass.size(), cudaMemcpyHostToDevice, st), "pass");
+    // the new area of every level below the new root
+    auto fresh = [&](int nodes_x, int old_nodes_x) {
+        std::vector<int> v;
+        for (int ty = 0; ty < nodes_x; ++ty)
+            for (int tx = 0; tx < nodes_x; ++tx)
+                if (tx >= old_nodes_x || ty >= old_nodes_x) v.push_back(ty * nodes_x + tx);
+        return v;
+    };
+    DevBuf<int> list;
+    {
+        Level& L0 = h->L[0];
+        const std::vector<int> nl = fresh(L0.nodes_x, old_S / b);
+        list.reserve(nl.size());
+        ck(cudaMemcpyAsync(list.p, nl.data(), nl.size() * sizeof(int), cudaMemcpyHostToDevice, st), "list");
+        hb::launch_leaf_bfs(h->pass.p, S, b, h->leaves_x, (int)nl.size(), L0.ms(), st, list.p);
+        ck(cudaGetLastError(), "leaf bfs");
+        ck(cudaStreamSynchronize(st), "sync");
+    }
+    for (int l = 1; l <= h->H; ++l) {
+        Level& Lv = h->L[l];
+        Level& Lc = h->L[l - 1];
+        const std::vector<int> nn = l < h->H ? fresh(Lv.nodes_x, old_S / Lv.side) : std::vector<int>{0};
+        list.reserve(nn.size());
+        ck(cudaMemcpyAsync(list.p, nn.data(), nn.size() * sizeof(int), cudaMemcpyHostToDevice, st), "list");
+        hb::launch_node_init(Lv.ms(), Lc.ms(), Lc.d_ext.p, Lv.nP, g, Lv.nodes_x, Lc.nodes_x, (int)nn.size(), st,
+                             list.p);
+        ck(cudaGetLastError(), "node init");
+        hb::launch_seams_build(Lv.ms(), Lv.d_seams.p, Lv.nseams, h->pass.p, S, Lv.side, Lv.nodes_x, (int)nn.size(),
+                               Lv.kflag.p, st, list.p);
+        ck(cudaGetLastError(), "seams build");
+        close_matrices(h, Lv, nn);
+        ck(cudaStreamSynchronize(st), "sync");
+    }
+    list.release();
+    h->epoch++;
 }
 
 // ---------------------------------------------------------------------------
@@ -671,6 +777,7 @@ void run_open_tasks(std::vector<OpenTask>& tasks) {
 }
 
 void do_open(htrip_index* h, const int32_t* rc, int n, const uint8_t* obs, int rows, int cols, bool record_stats) {
+    h->update_counter++;
     std::vector<OpenTask> tasks(1);
     open_prepare(tasks[0], h, rc, n, obs, rows, cols, record_stats);
     run_open_tasks(tasks);
@@ -1248,6 +1355,18 @@ htrip_status htrip_build(htrip_index* h, const uint8_t* observed, int32_t rows, 
     HTRIP_GUARD_END
 }
 
+htrip_status htrip_lift_root(htrip_index* h, const uint8_t* observed, int32_t rows, int32_t cols) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    if (const htrip_status rs = ready(h)) return rs;
+    if (rows < 0 || cols < 0 || ((rows > 0 && cols > 0) && !observed)) return fail(HTRIP_ERR_INVALID, "bad grid");
+    if ((int64_t)h->S * h->g > (1 << 20)) return fail(HTRIP_ERR_UNSUPPORTED, "grid side above 2^20");
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    do_lift_root(h, observed, rows > 0 && cols > 0 ? rows : 0, rows > 0 && cols > 0 ? cols : 0);
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
 htrip_status htrip_open_cells(htrip_index* h, const int32_t* rc, int32_t n, const uint8_t* observed, int32_t rows,
                               int32_t cols) {
     if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
@@ -1286,6 +1405,74 @@ htrip_status htrip_query_all_pairs(htrip_index* h, const int32_t* vps, int32_t k
     const std::vector<QueryReq> R{{h, &P, nullptr}};
     if (run_queries(h->q, h->device, h->stream, R, {out}, true) != 0)
         return fail(HTRIP_ERR_CUDA, "query kernel: grid barrier timed out");
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_query_distance(htrip_index* h, int32_t r1, int32_t c1, int32_t r2, int32_t c2,
+                                  const uint8_t* observed, int32_t rows, int32_t cols, uint16_t* out) {
+    if (!h || !out || !observed) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    if (const htrip_status rs = ready(h)) return rs;
+    const int32_t vps[4] = {r1, c1, r2, c2};
+    const std::vector<uint8_t> pf = viewpoint_flags(h, vps, 2, observed, rows, cols);
+    // queryDistance (minplus_oracle.cpp:834-849): INF unless both cells are
+    // passable and inside the index, 0 for s == t.
+    if (!pf[0] || !pf[1]) {
+        *out = HTRIP_INF;
+        return HTRIP_OK;
+    }
+    if (r1 == r2 && c1 == c2) {
+        *out = 0;
+        return HTRIP_OK;
+    }
+    uint16_t m[4];
+    const htrip_status st = htrip_query_all_pairs(h, vps, 2, observed, rows, cols, m);
+    if (st != HTRIP_OK) return st;
+    *out = m[1];
+    return HTRIP_OK;
+}
+
+htrip_status htrip_incremental_create(htrip_incremental** out) {
+    if (!out) return fail(HTRIP_ERR_INVALID, "null out");
+    *out = new (std::nothrow) htrip_incremental();
+    return *out ? HTRIP_OK : fail(HTRIP_ERR_OOM, "host allocation failed");
+}
+
+htrip_status htrip_incremental_destroy(htrip_incremental* s) {
+    delete s;
+    return HTRIP_OK;
+}
+
+htrip_status htrip_query_all_pairs_incremental(htrip_index* h, htrip_incremental* s, const int32_t* vps, int32_t k,
+                                               const uint8_t* observed, int32_t rows, int32_t cols, uint16_t* out,
+                                               int32_t* recomputed) {
+    if (!h || !s) return fail(HTRIP_ERR_INVALID, "null argument");
+    if (const htrip_status rs = ready(h)) return rs;
+    if (k < 0 || (k > 0 && (!vps || !out)) || !observed) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    if (recomputed) *recomputed = 0;
+    if (k == 0) {  // minplus_oracle.cpp:1450-1454
+        s->initialized = false;
+        return HTRIP_OK;
+    }
+    const bool same_vps = s->vps.size() == 2 * (size_t)k && std::equal(vps, vps + 2 * (size_t)k, s->vps.begin());
+    if (s->initialized && s->index == h && s->epoch == h->epoch && same_vps && s->updates == h->update_counter) {
+        std::memcpy(out, s->matrix.data(), (size_t)k * k * sizeof(uint16_t));  // no update since: the cached matrix
+        return HTRIP_OK;
+    }
+    HTRIP_GUARD_BEGIN
+    s->matrix.resize((size_t)k * k);
+    const htrip_status st = htrip_query_all_pairs(h, vps, k, observed, rows, cols, s->matrix.data());
+    if (st != HTRIP_OK) {
+        s->initialized = false;
+        return st;
+    }
+    s->vps.assign(vps, vps + 2 * (size_t)k);
+    s->index = h;
+    s->epoch = h->epoch;
+    s->updates = h->update_counter;
+    s->initialized = true;
+    std::memcpy(out, s->matrix.data(), (size_t)k * k * sizeof(uint16_t));
+    if (recomputed) *recomputed = 1;
     return HTRIP_OK;
     HTRIP_GUARD_END
 }
@@ -1471,6 +1658,7 @@ htrip_status htrip_open_batch(htrip_batch* b, const htrip_open_request* reqs, in
             if (wave[i] != w) continue;
             const htrip_open_request& r = reqs[i];
             ck(cudaStreamSynchronize(r.index->stream), "index stream");
+            r.index->update_counter++;
             tasks.emplace_back();
             open_prepare(tasks.back(), r.index, r.rc, r.n, r.observed, r.rows, r.cols, true);
         }

@@ -29,9 +29,10 @@ __device__ __forceinline__ uint16_t* mat_ptr(const MatSet& M, int m) {
 constexpr int kBfsWarps = 8;
 
 __global__ void __launch_bounds__(kBfsWarps * 32)
-leaf_bfs_kernel(const uint8_t* __restrict__ pass, int S, int b, int leaves_x, MatSet L) {
+leaf_bfs_kernel(const uint8_t* __restrict__ pass, int S, int b, int leaves_x, MatSet L, const int* __restrict__ list,
+                int y0) {
     extern __shared__ __align__(16) uint16_t sm_rows[];
-    const int leaf = blockIdx.y;
+    const int leaf = list ? list[y0 + blockIdx.y] : y0 + blockIdx.y;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int src = blockIdx.x * kBfsWarps + warp;
     const int NP = L.NP, n = b * b;
@@ -85,8 +86,8 @@ leaf_bfs_kernel(const uint8_t* __restrict__ pass, int S, int b, int leaves_x, Ma
 // matrix restricted to its exterior ports: child[ext[p]][ext[p']].
 // ---------------------------------------------------------------------------
 __global__ void node_init_kernel(MatSet N, MatSet Cm, const int* __restrict__ cext, int nP, int g,
-                                 int nodes_x, int child_nodes_x) {
-    const int node = blockIdx.y;
+                                 int nodes_x, int child_nodes_x, const int* __restrict__ list, int y0) {
+    const int node = list ? list[y0 + blockIdx.y] : y0 + blockIdx.y;
     const int NP = N.NP, nV = N.n;
     const size_t chunk = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // 8 entries
     const size_t per_row = NP / 8;
@@ -120,8 +121,8 @@ __global__ void node_init_kernel(MatSet N, MatSet Cm, const int* __restrict__ ce
 // Build-time seams: both cells Free -> unit edge, both endpoints are pivots.
 __global__ void seams_build_kernel(MatSet N, const int* __restrict__ seams, int n_seams,
                                    const uint8_t* __restrict__ pass, int S, int side, int nodes_x,
-                                   uint8_t* kflag) {
-    const int node = blockIdx.y;
+                                   uint8_t* kflag, const int* __restrict__ list, int y0) {
+    const int node = list ? list[y0 + blockIdx.y] : y0 + blockIdx.y;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_seams) return;
     const int* e = seams + 6 * s;
@@ -530,25 +531,34 @@ inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1)
 // ---------------------------------------------------------------------------
 // Launch wrappers
 // ---------------------------------------------------------------------------
+// grid.y is limited to 65535: per-matrix launches go in slices of that many.
+constexpr int kMaxGridY = 65535;
+
 void launch_leaf_bfs(const uint8_t* pass, int S, int b, int leaves_x, int n_leaves, MatSet leaves,
-                     cudaStream_t st) {
-    dim3 grid(blocks_for(leaves.NP, kBfsWarps), n_leaves);
+                     cudaStream_t st, const int* list) {
     const size_t smem = (size_t)kBfsWarps * leaves.NP * sizeof(uint16_t);
-    leaf_bfs_kernel<<<grid, kBfsWarps * 32, smem, st>>>(pass, S, b, leaves_x, leaves);
+    for (int y0 = 0; y0 < n_leaves; y0 += kMaxGridY) {
+        dim3 grid(blocks_for(leaves.NP, kBfsWarps), std::min(kMaxGridY, n_leaves - y0));
+        leaf_bfs_kernel<<<grid, kBfsWarps * 32, smem, st>>>(pass, S, b, leaves_x, leaves, list, y0);
+    }
 }
 
 void launch_node_init(MatSet node, MatSet child, const int* child_ext, int nP, int g, int nodes_x,
-                      int child_nodes_x, int n_nodes, cudaStream_t st) {
+                      int child_nodes_x, int n_nodes, cudaStream_t st, const int* list) {
     const size_t chunks = (size_t)node.NP * (node.NP / 8);
-    dim3 grid(blocks_for(chunks, 256), n_nodes);
-    node_init_kernel<<<grid, 256, 0, st>>>(node, child, child_ext, nP, g, nodes_x, child_nodes_x);
+    for (int y0 = 0; y0 < n_nodes; y0 += kMaxGridY) {
+        dim3 grid(blocks_for(chunks, 256), std::min(kMaxGridY, n_nodes - y0));
+        node_init_kernel<<<grid, 256, 0, st>>>(node, child, child_ext, nP, g, nodes_x, child_nodes_x, list, y0);
+    }
 }
 
 void launch_seams_build(MatSet node, const int* seams, int n_seams, const uint8_t* pass, int S, int side,
-                        int nodes_x, int n_nodes, uint8_t* kflag, cudaStream_t st) {
+                        int nodes_x, int n_nodes, uint8_t* kflag, cudaStream_t st, const int* list) {
     if (n_seams == 0) return;
-    dim3 grid(blocks_for(n_seams, 128), n_nodes);
-    seams_build_kernel<<<grid, 128, 0, st>>>(node, seams, n_seams, pass, S, side, nodes_x, kflag);
+    for (int y0 = 0; y0 < n_nodes; y0 += kMaxGridY) {
+        dim3 grid(blocks_for(n_seams, 128), std::min(kMaxGridY, n_nodes - y0));
+        seams_build_kernel<<<grid, 128, 0, st>>>(node, seams, n_seams, pass, S, side, nodes_x, kflag, list, y0);
+    }
 }
 
 void launch_compact_pivots(uint8_t* kflag, int NP, const int* active, int n_active, int* klist, int* kcnt,

@@ -21,19 +21,21 @@ constexpr int kFlagTile = 64;     // column granularity of panel "finite" flags
 // --- build ------------------------------------------------------------------
 // Leaf APSP by bit-parallel BFS (reference LeafTile::recomputeFromGrid,
 // leaf_tile.cpp:96-153).  pass: S*S bytes, 1 = Free.
+// With `list`, the n_leaves leaves list[0..n_leaves) instead of 0..n_leaves.
 void launch_leaf_bfs(const uint8_t* pass, int S, int b, int leaves_x, int n_leaves, MatSet leaves,
-                     cudaStream_t st);
+                     cudaStream_t st, const int* list = nullptr);
 
 // Internal-node initial D_U: block diagonal of child summaries, INF
 // elsewhere (internal_node.cpp:98-145).  child_ext: the child level's
 // port -> matrix-index table (nP entries).
 void launch_node_init(MatSet node, MatSet child, const int* child_ext, int nP, int g, int nodes_x,
-                      int child_nodes_x, int n_nodes, cudaStream_t st);
+                      int child_nodes_x, int n_nodes, cudaStream_t st, const int* list = nullptr);
 
 // Seam edges of the build (internal_node.cpp:155-173): seams = 6 ints per
 // candidate {u, v, ur, uc, vr, vc} (node-relative coordinates).
 void launch_seams_build(MatSet node, const int* seams, int n_seams, const uint8_t* pass, int S,
-                        int side, int nodes_x, int n_nodes, uint8_t* kflag, cudaStream_t st);
+                        int side, int nodes_x, int n_nodes, uint8_t* kflag, cudaStream_t st,
+                        const int* list = nullptr);
 
 // --- closure over pivot sets -------------------------------------------------
 // Compact per-matrix pivot flags into sorted lists (clears the flags).

@@ -177,6 +177,46 @@ std::vector<dist_t> MinPlusOracle::queryAllPairs(const std::vector<Point>& viewp
     return m;
 }
 
+void MinPlusOracle::queryAllPairsIncremental(const std::vector<Point>& viewpoints, const GridMap& grid,
+                                             std::vector<dist_t>& out_matrix, HTripQueryScratch& scratch,
+                                             HTripIncrementalState& state) const {
+    const size_t k = viewpoints.size();
+    if (k == 0) {  // reference minplus_oracle.cpp:1450-1454
+        out_matrix.clear();
+        state.initialized = false;
+        return;
+    }
+    const bool same = state.initialized && state.epoch_seen == epoch && state.vp_pts == viewpoints;
+    if (same && state.last_update_counter == update_counter) {
+        out_matrix = state.matrix;
+        return;
+    }
+    queryAllPairs(viewpoints, grid, state.matrix, scratch);
+    state.vp_pts = viewpoints;
+    state.epoch_seen = epoch;
+    state.last_update_counter = update_counter;
+    state.initialized = true;
+    out_matrix = state.matrix;
+}
+
+dist_t MinPlusOracle::queryDistance(Point s, Point t, const GridMap& grid) const {
+    if (!grid.isPassable(s) || !grid.isPassable(t)) return INF;  // reference minplus_oracle.cpp:836-837
+    if (s == t) return 0;
+    if (!built_) return INF;
+    dist_t d = INF;
+    check(htrip_query_distance(h_, s.r, s.c, t.r, t.c, grid.observedBytes(), grid.rows, grid.cols, &d),
+          "queryDistance");
+    return d;
+}
+
+void MinPlusOracle::liftRoot(const GridMap& grid) {
+    if (!built_) return;
+    check(htrip_lift_root(h_, grid.rows > 0 && grid.cols > 0 ? grid.observedBytes() : nullptr, grid.rows, grid.cols),
+          "liftRoot");
+    refreshShape();
+    ++epoch;
+}
+
 size_t MinPlusOracle::totalMemoryBytes() const noexcept {
     uint64_t ref = 0, dev = 0;
     if (htrip_memory_bytes(h_, &ref, &dev) != HTRIP_OK) return 0;

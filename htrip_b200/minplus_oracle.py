@@ -85,6 +85,8 @@ EXPORTS = (
     "htrip_server_submit_open", "htrip_server_wait", "htrip_server_get_stats", "htrip_server_run_trace",
     "htrip_measure_minplus_rate", "htrip_last_query_phases", "htrip_batch_last_phases", "htrip_last_open_work",
     "htrip_autotune_query", "htrip_autotune_export", "htrip_autotune_import", "htrip_autotune_clear",
+    "htrip_lift_root", "htrip_query_distance", "htrip_incremental_create", "htrip_incremental_destroy",
+    "htrip_query_all_pairs_incremental",
 )
 
 
@@ -137,6 +139,11 @@ def load_library(path: str | None = None):
     lib.htrip_autotune_export.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
     lib.htrip_autotune_import.argtypes = [C.c_char_p]
     lib.htrip_autotune_clear.argtypes = []
+    lib.htrip_lift_root.argtypes = [P, _U8P, I, I]
+    lib.htrip_query_distance.argtypes = [P, I, I, I, I, _U8P, I, I, _U16P]
+    lib.htrip_incremental_create.argtypes = [C.POINTER(P)]
+    lib.htrip_incremental_destroy.argtypes = [P]
+    lib.htrip_query_all_pairs_incremental.argtypes = [P, P, _I32P, I, _U8P, I, I, _U16P, _I32P]
     lib.htrip_batch_last_phases.argtypes = [P, _U64P, I, _I32P]
     lib.htrip_offload.argtypes = [P]
     lib.htrip_restore.argtypes = [P]
@@ -299,6 +306,15 @@ class MinPlusOracle:
         obs, ptr, rows, cols = _grid_args(grid)
         _check(self.lib.htrip_open_cell(self.h, int(p[0]), int(p[1]), ptr, rows, cols))
 
+    def liftRoot(self, grid=None):
+        """Grow the index to S*g, H+1 (reference liftRoot); grid None = the
+        reference's default empty GridMap."""
+        if grid is None:
+            _check(self.lib.htrip_lift_root(self.h, None, 0, 0))
+            return
+        obs, ptr, rows, cols = _grid_args(grid)
+        _check(self.lib.htrip_lift_root(self.h, ptr, rows, cols))
+
     # -- queries ----------------------------------------------------------
     def queryAllPairs(self, viewpoints, grid, out: np.ndarray | None = None, scratch=None) -> np.ndarray:
         rc = _rc(viewpoints)
@@ -310,6 +326,29 @@ class MinPlusOracle:
         obs, ptr, rows, cols = _grid_args(grid)
         _check(self.lib.htrip_query_all_pairs(self.h, rc.ctypes.data_as(_I32P), k, ptr, rows, cols,
                                               out.ctypes.data_as(_U16P)))
+        return out
+
+    def queryDistance(self, s, t, grid) -> int:
+        """Reference queryDistance (minplus_oracle.hpp:312)."""
+        obs, ptr, rows, cols = _grid_args(grid)
+        out = C.c_uint16()
+        _check(self.lib.htrip_query_distance(self.h, int(s[0]), int(s[1]), int(t[0]), int(t[1]), ptr, rows, cols,
+                                             C.byref(out)))
+        return out.value
+
+    def queryAllPairsIncremental(self, viewpoints, grid, state: "IncrementalState",
+                                 out: np.ndarray | None = None) -> np.ndarray:
+        """Reference queryAllPairsIncremental: the cached matrix when nothing
+        changed since `state` was filled, else a fresh full query."""
+        rc = _rc(viewpoints)
+        k = len(rc)
+        if out is None or out.shape != (k, k) or out.dtype != np.uint16 or not out.flags.c_contiguous:
+            out = np.empty((k, k), dtype=np.uint16)
+        obs, ptr, rows, cols = _grid_args(grid)
+        rec = C.c_int32()
+        _check(self.lib.htrip_query_all_pairs_incremental(self.h, state.h, rc.ctypes.data_as(_I32P), k, ptr, rows,
+                                                          cols, out.ctypes.data_as(_U16P), C.byref(rec)))
+        state.last_recomputed = bool(rec.value)
         return out
 
     def queryAllPairsNoAlloc(self, viewpoints, grid, out: np.ndarray | None = None) -> np.ndarray:
@@ -448,6 +487,23 @@ class MinPlusOracle:
 
 
 HTripOracle = MinPlusOracle
+
+
+class IncrementalState:
+    """Reference HTripIncrementalState (cache of the last incremental query)."""
+
+    def __init__(self):
+        self.lib = load_library()
+        h = C.c_void_p()
+        _check(self.lib.htrip_incremental_create(C.byref(h)))
+        self.h = h
+        self.last_recomputed = False
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.lib.htrip_incremental_destroy(h)
+            self.h = None
 
 
 class Batch:

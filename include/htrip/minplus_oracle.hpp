@@ -16,6 +16,10 @@
 //   struct LastBatchStats / last_batch_stats             :251-256
 //   void queryAllPairs(vps, grid, out, scratch) const    :337-341
 //   std::vector<dist_t> queryAllPairs(vps, grid) const   :348-349
+//   void queryAllPairsIncremental(vps, grid, out, scratch,
+//                                 HTripIncrementalState&) const :290-294
+//   dist_t queryDistance(Point, Point, const GridMap&) const    :312
+//   void liftRoot(const GridMap& = GridMap())            :380
 //   size_t totalMemoryBytes() const                      :385
 //   copy construction / assignment (deep copy, as the reference's
 //   value-type oracle: bench_update_latency.cpp:178,186)
@@ -81,6 +85,17 @@ public:
     };
     mutable HTripQueryScratch query_scratch;  // used by the 2-argument queryAllPairs
 
+    // Cache of queryAllPairsIncremental (the reference's field names for the
+    // fields a caller reads).  The matrix is reused while the viewpoints,
+    // the epoch and the update counter stay as they were.
+    struct HTripIncrementalState {
+        bool initialized = false;
+        uint64_t epoch_seen = 0;
+        uint32_t last_update_counter = 0;
+        std::vector<Point> vp_pts;
+        std::vector<dist_t> matrix;
+    };
+
     // Index on CUDA device 0 with the default config (b = 16, 2 x 2 groups).
     MinPlusOracle();
     // Index on CUDA device `device`.  Throws DeviceError when no CUDA device
@@ -113,6 +128,18 @@ public:
                        HTripQueryScratch& scratch) const;
     [[nodiscard]] std::vector<dist_t> queryAllPairs(const std::vector<Point>& viewpoints,
                                                     const GridMap& grid) const;
+    // Same matrix as queryAllPairs; without any update since `state` was
+    // filled for the same viewpoints it is the cached one (no device work),
+    // otherwise the full query runs again.
+    void queryAllPairsIncremental(const std::vector<Point>& viewpoints, const GridMap& grid,
+                                  std::vector<dist_t>& out_matrix, HTripQueryScratch& scratch,
+                                  HTripIncrementalState& state) const;
+    // Exact distance between two cells (INF if either is not passable).
+    [[nodiscard]] dist_t queryDistance(Point s, Point t, const GridMap& grid) const;
+
+    // Grows the index to S * g, H + 1: existing tiles keep their tables, the
+    // new area and the new root are built from `grid`.
+    void liftRoot(const GridMap& grid = GridMap());
 
     // The reference's accounting of the same index: bytes of every D, S,
     // D_U, S_U and child_to_ext table.

@@ -87,6 +87,13 @@ htrip_status htrip_open_cells(htrip_index* h, const int32_t* rc, int32_t n,
 htrip_status htrip_open_cell(htrip_index* h, int32_t r, int32_t c,
                              const uint8_t* observed, int32_t rows, int32_t cols);
 
+/* void liftRoot(const GridMap& grid)          minplus_oracle.hpp:380
+ * Grows the index: S -> S*g, H -> H+1.  Existing leaves and nodes keep
+ * their matrices; leaves and nodes of the new area, and the new root, are
+ * built from `observed` (rows x cols; rows = cols = 0 stands for the
+ * reference's default empty GridMap, where nothing is passable).          */
+htrip_status htrip_lift_root(htrip_index* h, const uint8_t* observed, int32_t rows, int32_t cols);
+
 /* void queryAllPairs(vps, grid, out, HTripQueryScratch&) const
  *                                              minplus_oracle.hpp:337-341
  * out: k*k uint16 row-major.  Diagonal 0 for Free viewpoints, INF rows and
@@ -94,6 +101,28 @@ htrip_status htrip_open_cell(htrip_index* h, int32_t r, int32_t c,
 htrip_status htrip_query_all_pairs(htrip_index* h, const int32_t* vps, int32_t k,
                                    const uint8_t* observed, int32_t rows, int32_t cols,
                                    uint16_t* out);
+
+/* dist_t queryDistance(Point s, Point t, const GridMap&) const
+ *                                              minplus_oracle.hpp:312
+ * INF unless both cells are Free and inside the index, 0 for s == t, else
+ * the exact distance (one query of the two cells).                        */
+htrip_status htrip_query_distance(htrip_index* h, int32_t r1, int32_t c1, int32_t r2, int32_t c2,
+                                  const uint8_t* observed, int32_t rows, int32_t cols, uint16_t* out);
+
+/* void queryAllPairsIncremental(vps, grid, out, scratch, state) const
+ *                                              minplus_oracle.hpp:290-294
+ * `state` caches the last matrix with the index's build / root-growth epoch
+ * and its count of opening calls.  Same viewpoints, same epoch and no
+ * opening since: the cached matrix is returned without device work (the
+ * reference's fast path).  Otherwise the whole matrix is recomputed by one
+ * query launch (the reference re-lifts only viewpoints under changed nodes;
+ * both give the full query's matrix).  *recomputed (optional) tells which. */
+typedef struct htrip_incremental htrip_incremental; /* opaque */
+htrip_status htrip_incremental_create(htrip_incremental** out);
+htrip_status htrip_incremental_destroy(htrip_incremental* s);
+htrip_status htrip_query_all_pairs_incremental(htrip_index* h, htrip_incremental* s, const int32_t* vps, int32_t k,
+                                               const uint8_t* observed, int32_t rows, int32_t cols, uint16_t* out,
+                                               int32_t* recomputed);
 
 /* Same query with the per-viewpoint passability already decided by the
  * caller (passable[i] != 0 iff viewpoint i is Free).  vps/passable/out are

@@ -57,6 +57,10 @@ def _load_ref():
         lib.ref_build.argtypes = [_P]
         lib.ref_open_batch.argtypes = [_P, _I32P, _I]
         lib.ref_open_cell.argtypes = [_P, _I, _I]
+        lib.ref_lift_root.argtypes = [_P]
+        lib.ref_query_distance.restype = _I
+        lib.ref_query_distance.argtypes = [_P, _I, _I, _I, _I]
+        lib.ref_query_incremental.argtypes = [_P, _I32P, _I, _U16P]
         lib.ref_query.argtypes = [_P, _I32P, _I, _U16P]
         lib.ref_time_query.restype = C.c_double
         lib.ref_time_query.argtypes = [_P, _I32P, _I, _I, _I, _U16P]
@@ -121,6 +125,19 @@ class RefOracle:
 
     def open_cell(self, r: int, c: int):
         self.lib.ref_open_cell(self.h, r, c)
+
+    def query_distance(self, s, t) -> int:
+        return self.lib.ref_query_distance(self.h, int(s[0]), int(s[1]), int(t[0]), int(t[1]))
+
+    def query_incremental(self, vps) -> np.ndarray:
+        rc = _rc(vps)
+        out = np.empty((len(rc), len(rc)), dtype=np.uint16)
+        self.lib.ref_query_incremental(self.h, _p(rc, _I32P), len(rc), _p(out, _U16P))
+        return out
+
+    def lift_root(self):
+        """MinPlusOracle::liftRoot with the handle's current grid."""
+        self.lib.ref_lift_root(self.h)
 
     def query(self, vps) -> np.ndarray:
         rc = _rc(vps)

@@ -32,6 +32,8 @@ namespace {
 struct RefHandle {
     MinPlusOracle oracle;
     GridMap grid;
+    MinPlusOracle::HTripQueryScratch scratch;
+    MinPlusOracle::HTripIncrementalState inc;
 };
 
 std::vector<Point> toPoints(const int32_t* rc, int n) {
@@ -83,6 +85,28 @@ int ref_build(void* p) {
 void ref_open_batch(void* p, const int32_t* rc, int n) {
     auto* h = static_cast<RefHandle*>(p);
     h->oracle.onBatchCellsOpened(toPoints(rc, n), h->grid);
+}
+
+// MinPlusOracle::queryDistance(s, t, grid) (minplus_oracle.hpp:312).
+int ref_query_distance(void* p, int r1, int c1, int r2, int c2) {
+    auto* h = static_cast<RefHandle*>(p);
+    return h->oracle.queryDistance(Point{r1, c1}, Point{r2, c2}, h->grid);
+}
+
+// MinPlusOracle::queryAllPairsIncremental with the handle's persistent state
+// (minplus_oracle.hpp:290-294).
+void ref_query_incremental(void* p, const int32_t* rc, int k, uint16_t* out) {
+    auto* h = static_cast<RefHandle*>(p);
+    std::vector<dist_t> m;
+    h->oracle.queryAllPairsIncremental(toPoints(rc, k), h->grid, m, h->scratch, h->inc);
+    std::memcpy(out, m.data(), m.size() * sizeof(dist_t));
+}
+
+// MinPlusOracle::liftRoot(grid) with the handle's current grid
+// (minplus_oracle.hpp:380); an empty grid stands for the default argument.
+void ref_lift_root(void* p) {
+    auto* h = static_cast<RefHandle*>(p);
+    h->oracle.liftRoot(h->grid);
 }
 
 void ref_open_cell(void* p, int r, int c) {
