@@ -992,7 +992,7 @@ struct QueryReq {
 // Launch words: {status, barrier count, barrier generation, pad}, then the
 // phase time stamps at byte kTraceOffset.
 constexpr size_t kTraceOffset = 64;
-constexpr size_t kWordsBytes = kTraceOffset + (hb::kMaxQueryPhases + 1) * sizeof(unsigned long long);
+constexpr size_t kWordsBytes = kTraceOffset + (2 * hb::kMaxQueryPhases + 1) * sizeof(unsigned long long);
 
 struct LaunchLayout {
     int n = 0, n_phases = 0;
@@ -1553,7 +1553,9 @@ htrip_status htrip_query_all_pairs_noalloc(htrip_index* h, const int32_t* vps, i
     HTRIP_GUARD_END
 }
 
-htrip_status htrip_batch_create(int device, htrip_batch** out) {
+htrip_status htrip_batch_create(int device, htrip_batch** out) { return htrip_batch_create_priority(device, 0, out); }
+
+htrip_status htrip_batch_create_priority(int device, int32_t high_priority, htrip_batch** out) {
     if (!out) return fail(HTRIP_ERR_INVALID, "null out");
     *out = nullptr;
     int ndev = 0;
@@ -1564,9 +1566,11 @@ htrip_status htrip_batch_create(int device, htrip_batch** out) {
     if (device < 0 || device >= ndev) return fail(HTRIP_ERR_INVALID, "bad device ordinal");
     HTRIP_GUARD_BEGIN
     ck(cudaSetDevice(device), "cudaSetDevice");
+    int lo = 0, hi = 0;  // numerically lower = higher priority
+    ck(cudaDeviceGetStreamPriorityRange(&lo, &hi), "stream priority range");
     auto* b = new htrip_batch();
     b->device = device;
-    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithPriority(&b->stream, cudaStreamNonBlocking, high_priority ? hi : lo) != cudaSuccess) {
         delete b;
         return fail(HTRIP_ERR_CUDA, "stream creation failed");
     }
@@ -1806,17 +1810,27 @@ htrip_status htrip_last_query_kernel_ms(const htrip_index* h, float* ms) {
     HTRIP_GUARD_END
 }
 
+// ns[i] = duration of phase i; with max_n >= 2 * phases, ns[phases + i] =
+// the part of it until the last CTA finished its work (the rest is the wait
+// in the grid barrier).
 static htrip_status arena_phases(const QueryArena& A, cudaStream_t st, uint64_t* ns, int32_t max_n, int32_t* n) {
     if (!ns || !n || max_n < 0) return fail(HTRIP_ERR_INVALID, "bad arguments");
     if (!A.ev_valid) return fail(HTRIP_ERR_INVALID, "no query has run");
     HTRIP_GUARD_BEGIN
-    unsigned long long t[hb::kMaxQueryPhases + 1];
+    unsigned long long t[2 * hb::kMaxQueryPhases + 1];
     ck(cudaEventSynchronize(A.ev[1]), "event sync");
-    ck(cudaMemcpyAsync(t, A.dev.p + A.last_words + kTraceOffset, (A.last_phases + 1) * sizeof(unsigned long long),
-                       cudaMemcpyDeviceToHost, st), "trace d2h");
+    ck(cudaMemcpyAsync(t, A.dev.p + A.last_words + kTraceOffset, sizeof(t), cudaMemcpyDeviceToHost, st), "trace d2h");
     ck(cudaStreamSynchronize(st), "trace sync");
-    *n = std::min<int32_t>(max_n, A.last_phases);
+    const int P = A.last_phases;
+    *n = std::min<int32_t>(max_n, P);
     for (int i = 0; i < *n; ++i) ns[i] = t[i + 1] - t[i];
+    if (max_n >= 2 * P) {
+        for (int i = 0; i < P; ++i) {
+            const unsigned long long e = t[hb::kMaxQueryPhases + 1 + i];
+            ns[P + i] = e > t[i] ? e - t[i] : 0;
+        }
+        *n = 2 * P;
+    }
     return HTRIP_OK;
     HTRIP_GUARD_END
 }

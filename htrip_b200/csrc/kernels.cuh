@@ -145,7 +145,9 @@ struct QueryLaunch {
     const int* unit_pre;       // [n_phases][n_req + 1]: exclusive prefix of units
     int* status;               // 0 ok, 1 grid barrier timeout
     unsigned* bar;             // grid barrier {count, generation}
-    unsigned long long* trace; // n_phases + 1 global-timer stamps (CTA 0), or null
+    unsigned long long* trace; // [0, n_phases]: phase starts as CTA 0 sees them; then from
+                               // [kMaxQueryPhases + 1 + t]: the latest end of work of phase t
+                               // over all CTAs; or null
 };
 constexpr int kMaxQueryPhases = kMaxQueryLevels + 3;
 

@@ -482,6 +482,8 @@ __global__ void __launch_bounds__(kThreads, 512 / kThreads) q_persistent_kernel(
             }
             run_unit<RW, CP>(B.req[lo], t, w - pre[lo], kl, wsum, red, im);
         }
+        if (B.trace && threadIdx.x == 0)  // the phase's last CTA to finish its units
+            atomicMax(B.trace + kMaxQueryPhases + 1 + t, global_timer());
         if (t + 1 < B.n_phases && !grid_barrier(B.bar, B.status)) return;
         if (stamp) B.trace[t + 1] = global_timer();
     }

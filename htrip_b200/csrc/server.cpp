@@ -358,7 +358,9 @@ htrip_status htrip_server_create(const htrip_server_config* cfg, htrip_server** 
         S->budget = (uint64_t)(fr * 0.80);
     }
     for (int k = 0; k < 2; ++k) {
-        const htrip_status r = htrip_batch_create(S->device, &S->batch[k]);
+        // queries on a high-priority stream: the cooperative query launch gets
+        // the SMs ahead of the openings' many small kernels
+        const htrip_status r = htrip_batch_create_priority(S->device, k == kQuery ? 1 : 0, &S->batch[k]);
         if (r != HTRIP_OK) {
             const std::string e = htrip_last_error();
             for (auto* b : S->batch) htrip_batch_destroy(b);

@@ -86,7 +86,7 @@ EXPORTS = (
     "htrip_measure_minplus_rate", "htrip_last_query_phases", "htrip_batch_last_phases", "htrip_last_open_work",
     "htrip_autotune_query", "htrip_autotune_export", "htrip_autotune_import", "htrip_autotune_clear",
     "htrip_lift_root", "htrip_query_distance", "htrip_incremental_create", "htrip_incremental_destroy",
-    "htrip_query_all_pairs_incremental",
+    "htrip_query_all_pairs_incremental", "htrip_batch_create_priority",
 )
 
 
@@ -128,6 +128,7 @@ def load_library(path: str | None = None):
     lib.htrip_last_query_io.argtypes = [P, _U64P, _U64P]
     lib.htrip_state_digest.argtypes = [P, _U64P, I]
     lib.htrip_batch_create.argtypes = [C.c_int, C.POINTER(P)]
+    lib.htrip_batch_create_priority.argtypes = [C.c_int, I, C.POINTER(P)]
     lib.htrip_batch_destroy.argtypes = [P]
     lib.htrip_query_batch.argtypes = [P, C.POINTER(_QueryRequest), I]
     lib.htrip_batch_last_kernel_ms.argtypes = [P, C.POINTER(C.c_float)]

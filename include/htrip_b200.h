@@ -175,6 +175,10 @@ typedef struct {
 } htrip_query_request;
 
 htrip_status htrip_batch_create(int device, htrip_batch** out);
+/* The same with the batch's stream at the device's highest stream priority
+ * (high_priority != 0): its kernels' CTAs are scheduled before those of
+ * default-priority streams (e.g. queries ahead of concurrent openings).    */
+htrip_status htrip_batch_create_priority(int device, int32_t high_priority, htrip_batch** out);
 htrip_status htrip_batch_destroy(htrip_batch* b);
 
 /* queryAllPairs of every request (minplus_oracle.hpp:337-341 per request).
@@ -314,7 +318,10 @@ htrip_status htrip_last_open_work(const htrip_index* h, uint64_t* alg_bytes, uin
 /* Phase trace of the last query launch of an index / a batch: ns[i] =
  * global-timer nanoseconds of phase i of the persistent query kernel
  * (0: level-0 gathers; 1..H+1: projections of level i with the meets of
- * level i-1; H+2: output), as seen by its first CTA.  *n = phases written. */
+ * level i-1; H+2: output), as seen by its first CTA.  With max_n >= 2 *
+ * phases, ns[phases + i] is the part of phase i until its last CTA finished
+ * its work (the rest of the phase is the grid-barrier wait).  *n = entries
+ * written.                                                                */
 htrip_status htrip_last_query_phases(const htrip_index* h, uint64_t* ns, int32_t max_n, int32_t* n);
 htrip_status htrip_batch_last_phases(const htrip_batch* b, uint64_t* ns, int32_t max_n, int32_t* n);
 

@@ -264,6 +264,47 @@ void non_square() {
     EXPECT(o.tileIndexAtLevel(1, 1, 1) == 5 && o.leafIndex(3, 2) == 19, "tile index");
 }
 
+// queryDistance (Suite 15, test_exactness.cpp:989-1023: equals the matrix
+// entry), queryAllPairsIncremental (test_property_based.cpp: incremental ==
+// full across openings) and liftRoot (the grown index still answers exactly).
+void next_members() {
+    GridMap truth = rooms_grid(32, 32, 8, 91);
+    GridMap obs = truth;
+    std::vector<Point> cells;
+    for (int c = 1; c < 31; c += 2) cells.push_back(Point(20, c));
+    for (auto& p : cells) obs.setObserved(p, CellState::Unknown);
+    MinPlusOracle o(HierarchyConfig{8, 2, 2, 0});
+    EXPECT(o.build(obs), "build");
+    const auto vps = sample_points(truth, 14, 9, 1);
+    MinPlusOracle::HTripQueryScratch scratch;
+    MinPlusOracle::HTripIncrementalState state;
+    std::vector<dist_t> inc, full;
+    o.queryAllPairsIncremental(vps, obs, inc, scratch, state);
+    expect_matrix(inc, bfs_matrix(obs, vps), "incremental first call");
+    const size_t k = vps.size();
+    for (size_t i = 0; i < k; ++i)
+        for (size_t j = 0; j < k; ++j)
+            EXPECT(o.queryDistance(vps[i], vps[j], obs) == inc[i * k + j], "queryDistance %zu %zu", i, j);
+    for (auto& p : cells) obs.setObserved(p, CellState::Free);
+    o.onBatchCellsOpened(cells, obs);
+    o.queryAllPairsIncremental(vps, obs, inc, scratch, state);
+    o.queryAllPairs(vps, obs, full, scratch);
+    expect_matrix(inc, full, "incremental == full after an opening");
+    expect_matrix(inc, bfs_matrix(obs, vps), "incremental vs BFS");
+    EXPECT(state.initialized && state.last_update_counter == o.update_counter, "incremental state");
+    // grow the root over a 64 x 64 grid whose old quadrant is unchanged
+    GridMap big = rooms_grid(64, 64, 8, 92);
+    for (int r = 0; r < 32; ++r)
+        for (int c = 0; c < 32; ++c) big.setObserved(r, c, obs.getObserved(r, c));
+    const uint64_t epoch = o.epoch;
+    o.liftRoot(big);
+    EXPECT(o.S == 64 && o.H == 3 && o.epoch == epoch + 1, "liftRoot shape S=%d H=%d", o.S, o.H);
+    const auto vps2 = sample_points(big, 16, 10, 1);
+    expect_matrix(o.queryAllPairs(vps2, big), bfs_matrix(big, vps2), "query after liftRoot");
+    o.queryAllPairsIncremental(vps2, big, inc, scratch, state);
+    expect_matrix(inc, bfs_matrix(big, vps2), "incremental after liftRoot (epoch changed)");
+}
+
 int host_only() {
     static_assert(add_dist(INF, 0) == INF && add_dist(59999, 1) == INF && add_dist(59998, 1) == 59999);
     static_assert(add_dist(1, 2, 3) == 6 && add_dist(30000, 30000, 1) == INF);
@@ -302,6 +343,7 @@ int main(int argc, char** argv) {
     random_openings("rooms", 16, 16, 16, 2, 15, 2, 6);  // H = 0
     copy_semantics();
     non_square();
+    next_members();
     std::printf("%s (%d failures)\n", g_fail ? "drop-in suite FAILED" : "drop-in suite passed", g_fail);
     return g_fail ? 1 : 0;
 }
