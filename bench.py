@@ -418,7 +418,10 @@ def bench_served(device, rates=(5000.0, 20000.0, 50000.0), max_requests=10000, p
                 "query_p50_ms": _pct(q, 50), "query_p99_ms": _pct(q, 99),
                 "open_p50_ms": _pct(o, 50), "open_p99_ms": _pct(o, 99),
                 "entries_per_s": entries / wall, "cells_per_s": cells / wall,
-                "launches": int(st["launches_query"] + st["launches_open"])}, reqs, outs
+                "launches": int(st["launches_query"] + st["launches_open"]),
+                "query_launches": int(st["launches_query"]), "open_launches": int(st["launches_open"]),
+                "query_worker_busy_s": st["busy_query_us"] / 1e6,
+                "open_worker_busy_s": st["busy_open_us"] / 1e6}, reqs, outs
 
     served = []
     first = None

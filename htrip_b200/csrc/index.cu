@@ -18,6 +18,10 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <exception>
+#include <condition_variable>
+#include <thread>
+#include <functional>
 #include <new>
 #include <numeric>
 #include <string>
@@ -697,11 +701,9 @@ void open_insert(OpenTask& T, int l) {
         ck(cudaGetLastError(), "node insert");
     }
     const int na = (int)T.act.size();
-    hb::launch_compact_pivots(Lv.kflag.p, Lv.NP, h->active.p, na, Lv.klist.p, Lv.kcnt.p, st);
+    // pivot lists, and the pivot counts of the active matrices in act order
+    hb::launch_compact_pivots(Lv.kflag.p, Lv.NP, h->active.p, na, Lv.klist.p, Lv.kcnt.p, st, h->rb_dev.p);
     ck(cudaGetLastError(), "compact");
-    // pivot counts of the active matrices, in act order
-    hb::launch_gather_counts(Lv.kcnt.p, h->active.p, na, h->rb_dev.p, st);
-    ck(cudaGetLastError(), "gather counts");
     ck(cudaMemcpyAsync(rb_kcnt(h), h->rb_dev.p, na * sizeof(int), cudaMemcpyDeviceToHost, st), "kcnt d2h");
 }
 
@@ -755,7 +757,13 @@ void open_finish(OpenTask& T) {
     if (T.record_stats) T.h->stats.n_dirty_ancestors = T.n_dirty;
 }
 
-// Runs the tasks (distinct indexes of one device) together, stage by stage.
+// Runs the tasks (distinct indexes of one device) together, stage by stage:
+// every task's insert(l) is issued on its index's stream, one wait covers
+// them all, then every task's close(l), one wait.  Issuing from one thread
+// with shared waits keeps gaps between stages in which other work (a
+// cooperative query launch, which needs every SM) gets the device; tasks
+// issued from several threads at once kept the device busy with small
+// kernels and held such launches back.
 void run_open_tasks(std::vector<OpenTask>& tasks) {
     int maxH = -1;
     for (auto& T : tasks)

@@ -140,7 +140,7 @@ __global__ void seams_build_kernel(MatSet N, const int* __restrict__ seams, int 
 // Pivot compaction: flags -> ascending index list, one CTA per matrix.
 // ---------------------------------------------------------------------------
 __global__ void compact_pivots_kernel(uint8_t* kflag, int NP, const int* __restrict__ active,
-                                      int* klist, int* kcnt) {
+                                      int* klist, int* kcnt, int* slot_cnt) {
     __shared__ int warp_tot[32];
     __shared__ int base;
     const int m = active[blockIdx.x];
@@ -169,7 +169,10 @@ __global__ void compact_pivots_kernel(uint8_t* kflag, int NP, const int* __restr
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) kcnt[m] = base;
+    if (threadIdx.x == 0) {
+        kcnt[m] = base;
+        if (slot_cnt) slot_cnt[blockIdx.x] = base;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -515,10 +518,6 @@ __global__ void __launch_bounds__(512) minplus_rate_kernel(int iters, uint32_t s
     if (x == seed) sink[0] = x;
 }
 
-__global__ void gather_counts_kernel(const int* __restrict__ kcnt, const int* __restrict__ active, int n, int* out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = kcnt[active[i]];
-}
 
 __global__ void fill_u16_kernel(uint16_t* p, size_t n, uint16_t v) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
@@ -562,9 +561,9 @@ void launch_seams_build(MatSet node, const int* seams, int n_seams, const uint8_
 }
 
 void launch_compact_pivots(uint8_t* kflag, int NP, const int* active, int n_active, int* klist, int* kcnt,
-                           cudaStream_t st) {
+                           cudaStream_t st, int* slot_cnt) {
     if (n_active == 0) return;
-    compact_pivots_kernel<<<n_active, 256, 0, st>>>(kflag, NP, active, klist, kcnt);
+    compact_pivots_kernel<<<n_active, 256, 0, st>>>(kflag, NP, active, klist, kcnt, slot_cnt);
 }
 
 template <int RW, int CP, bool PANEL>
@@ -658,10 +657,6 @@ void launch_digest(MatSet M, int count, unsigned long long* out, cudaStream_t st
     digest_kernel<<<grid, 256, 0, st>>>(M, count, out);
 }
 
-void launch_gather_counts(const int* kcnt, const int* active, int n, int* out, cudaStream_t st) {
-    if (n == 0) return;
-    gather_counts_kernel<<<blocks_for(n, 256), 256, 0, st>>>(kcnt, active, n, out);
-}
 
 double measure_minplus_rate(int variant, int sms) {
     const int iters = 4096, threads = 512, blocks = sms * 4;

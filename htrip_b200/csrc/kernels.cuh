@@ -38,9 +38,10 @@ void launch_seams_build(MatSet node, const int* seams, int n_seams, const uint8_
                         const int* list = nullptr);
 
 // --- closure over pivot sets -------------------------------------------------
-// Compact per-matrix pivot flags into sorted lists (clears the flags).
+// Compact per-matrix pivot flags into sorted lists (clears the flags);
+// slot_cnt (optional) receives the counts in active order as well.
 void launch_compact_pivots(uint8_t* kflag, int NP, const int* active, int n_active, int* klist,
-                           int* kcnt, cudaStream_t st);
+                           int* kcnt, cudaStream_t st, int* slot_cnt = nullptr);
 
 // One round of the blocked pivot-set Kleene closure: pivots
 // klist[m][round*B .. round*B+B).  panel: closure_scratch_elems(NP,
@@ -49,9 +50,6 @@ size_t closure_scratch_elems(int NP, int n_active);
 void launch_closure_round(MatSet M, const int* active, int n_active, const int* klist,
                           const int* kcnt, int round, uint16_t* panel, uint8_t* flags,
                           cudaStream_t st);
-
-// out[i] = kcnt[active[i]] for i < n (pivot counts of the active matrices).
-void launch_gather_counts(const int* kcnt, const int* active, int n, int* out, cudaStream_t st);
 
 // --- incremental updates -----------------------------------------------------
 // Insert opened in-leaf edges (leaf_tile.cpp:311-330).  edges: per active

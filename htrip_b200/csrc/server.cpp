@@ -204,6 +204,7 @@ void worker_loop(htrip_server* S, int kind) {
         lk.unlock();
         htrip_status rs = HTRIP_OK;
         std::string err;
+        const auto tb = Clock::now();
         if (!ready.empty()) {
             if (kind == kQuery) {
                 std::vector<htrip_query_request> qr;
@@ -245,8 +246,14 @@ void worker_loop(htrip_server* S, int kind) {
             it.s->busy = false;
             it.s->last_use = ++S->tick;
         }
-        if (kind == kQuery) S->st.launches_query++;
-        else S->st.launches_open++;
+        const double busy = std::chrono::duration<double>(t1 - tb).count();
+        if (kind == kQuery) {
+            S->st.launches_query++;
+            S->st.busy_query_us += (uint64_t)(busy * 1e6);
+        } else {
+            S->st.launches_open++;
+            S->st.busy_open_us += (uint64_t)(busy * 1e6);
+        }
         S->completions++;
         S->cv_done.notify_all();
         S->cv_work.notify_all();

@@ -59,7 +59,7 @@ class _ServerConfig(C.Structure):
 class _ServerStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "launches_query", "launches_open", "requests_query", "requests_open", "evictions", "restores",
-        "sessions", "resident_sessions", "resident_bytes", "budget_bytes")]
+        "sessions", "resident_sessions", "resident_bytes", "budget_bytes", "busy_query_us", "busy_open_us")]
 
 
 class _ServerRequest(C.Structure):

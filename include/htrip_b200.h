@@ -240,6 +240,7 @@ typedef struct {
     uint64_t evictions, restores;             /* offloads to / returns from host */
     uint64_t sessions, resident_sessions;
     uint64_t resident_bytes, budget_bytes;
+    uint64_t busy_query_us, busy_open_us;     /* time the workers spent in their calls */
 } htrip_server_stats;
 
 typedef struct {
