@@ -116,6 +116,8 @@ struct Level {
     MatSet ms() const { return MatSet{mat.p, n, NP}; }
 };
 
+inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
 // Pinned host buffer (grows, never shrinks).
 struct HostBuf {
     unsigned char* p = nullptr;
@@ -159,6 +161,26 @@ struct QueryArena {
     }
 };
 
+// Scratch of update launches (build closures and openings): the device
+// array of matrix descriptors with the launch's edge / seam lists and
+// per-slot / per-task read-back words, exterior snapshots, closure panels
+// and tile flags; pinned staging for the upload and the read-backs.
+struct UpdateArena {
+    DevBuf<unsigned char> dev;
+    DevBuf<uint16_t> snap;
+    DevBuf<uint16_t> panel;
+    DevBuf<uint8_t> pflags;
+    HostBuf stage, rb;
+    void release() {
+        dev.release();
+        snap.release();
+        panel.release();
+        pflags.release();
+        stage.release();
+        rb.release();
+    }
+};
+
 }  // namespace
 
 struct htrip_index {
@@ -176,18 +198,8 @@ struct htrip_index {
     int S = 0, H = 0, rows = 0, cols = 0, leaves_x = 0;
     std::vector<Level> L;
     DevBuf<uint8_t> pass;
-    // closure scratch
-    DevBuf<uint16_t> panel;
-    DevBuf<uint8_t> pflags;
-    DevBuf<int> active;
-    DevBuf<int> upd;        // uploaded per-update lists
-    DevBuf<uint16_t> snap;
-    DevBuf<int> pivots;
-    // opening read-back: pinned host words (pivots, pivot counts, decrease
-    // flags) and the device array the counts are gathered into
-    int max_nodes = 0;
-    HostBuf rb;
-    DevBuf<int> rb_dev;
+    // scratch of the index's own build / opening launches
+    UpdateArena u;
     // query scratch: one device arena per launch (QueryArena) plus pinned
     // host staging for its parameter block / plans and for the result
     QueryArena q;
@@ -200,8 +212,8 @@ struct htrip_index {
             l.klist.release(); l.kcnt.release(); l.dec.release();
         }
         L.clear();
-        pass.release(); panel.release(); pflags.release(); active.release(); upd.release();
-        snap.release(); pivots.release(); rb.release(); rb_dev.release();
+        pass.release();
+        u.release();
         q.release();
     }
 };
@@ -223,7 +235,8 @@ struct htrip_batch {
     int device = 0;
     cudaStream_t stream = nullptr;
     QueryArena q;
-    ~htrip_batch() { q.release(); }
+    UpdateArena u;
+    ~htrip_batch() { q.release(); u.release(); }
 };
 
 namespace {
@@ -333,40 +346,73 @@ void alloc_levels(htrip_index* h) {
         Lv.klist.reserve((size_t)Lv.nnodes * Lv.NP);
         Lv.kcnt.reserve(Lv.nnodes);
         Lv.dec.reserve(Lv.nnodes);
+        // decrease flags are zero outside an opening call (each level's flags
+        // are cleared by the level above once it has read them)
+        ck(cudaMemsetAsync(Lv.dec.p, 0, Lv.nnodes, h->stream), "dec");
     }
-    h->pivots.reserve(1);
-    h->max_nodes = 1;
-    for (auto& Lv : h->L) h->max_nodes = std::max(h->max_nodes, Lv.nnodes);
-    h->rb.reserve(sizeof(int) * (1 + (size_t)h->max_nodes) + h->max_nodes);
-    h->rb_dev.reserve(h->max_nodes);
 }
 
-// Closure of the listed matrices of level `Lv` over their pivot flags.
-void close_matrices(htrip_index* h, Level& Lv, const std::vector<int>& act) {
-    if (act.empty()) return;
-    cudaStream_t st = h->stream;
-    const size_t per = (size_t)hb::kPivotChunk * Lv.NP;
+// Descriptor of matrix m of level Lv (an index's own level arrays).
+hb::Slot level_slot(Level& Lv, Level* child, int m, int task, int root) {
+    hb::Slot sl{};
+    sl.mat = Lv.mat.p + (size_t)m * Lv.NP * Lv.NP;
+    sl.kflag = Lv.kflag.p + (size_t)m * Lv.NP;
+    sl.klist = Lv.klist.p + (size_t)m * Lv.NP;
+    sl.kcnt = Lv.kcnt.p + m;
+    sl.dec = Lv.dec.p + m;
+    sl.child_mat = child ? child->mat.p : nullptr;
+    sl.child_dec = child ? child->dec.p : nullptr;
+    sl.node = m;
+    sl.nodes_x = Lv.nodes_x;
+    sl.child_nodes_x = child ? child->nodes_x : 0;
+    sl.task = task;
+    sl.root = root;
+    return sl;
+}
+
+// Closure rounds of `n` slots (already uploaded at d_slots, pivots already
+// compacted, counts cnt[] on the host) of order NP, in chunks that bound the
+// panel scratch.  Issued on `st`, not waited for.
+void close_slots(UpdateArena& A, const hb::Slot* d_slots, const int* cnt, int n, int NP, cudaStream_t st) {
+    const size_t per = (size_t)hb::kPivotChunk * NP;
     const size_t cap = std::max<size_t>(1, (size_t)(128u << 20) / (per * sizeof(uint16_t)));
-    std::vector<int> kc(Lv.nnodes);
-    for (size_t c0 = 0; c0 < act.size(); c0 += cap) {
-        const int na = (int)std::min(cap, act.size() - c0);
-        h->active.reserve(na);
-        ck(cudaMemcpyAsync(h->active.p, act.data() + c0, na * sizeof(int), cudaMemcpyHostToDevice, st), "active");
-        hb::launch_compact_pivots(Lv.kflag.p, Lv.NP, h->active.p, na, Lv.klist.p, Lv.kcnt.p, st);
-        ck(cudaGetLastError(), "compact");
-        ck(cudaMemcpyAsync(kc.data(), Lv.kcnt.p, Lv.nnodes * sizeof(int), cudaMemcpyDeviceToHost, st), "kcnt");
-        ck(cudaStreamSynchronize(st), "sync kcnt");
+    for (size_t c0 = 0; c0 < (size_t)n; c0 += cap) {
+        const int nc = (int)std::min(cap, (size_t)n - c0);
         int maxk = 0;
-        for (int i = 0; i < na; ++i) maxk = std::max(maxk, kc[act[c0 + i]]);
+        for (int i = 0; i < nc; ++i) maxk = std::max(maxk, cnt[c0 + i]);
         if (maxk == 0) continue;
-        h->panel.reserve(hb::closure_scratch_elems(Lv.NP, na));
-        h->pflags.reserve((size_t)na * (Lv.NP / hb::kFlagTile));
+        A.panel.reserve(hb::closure_scratch_elems(NP, nc));
+        A.pflags.reserve((size_t)nc * (NP / hb::kFlagTile));
         const int rounds = (maxk + hb::kPivotChunk - 1) / hb::kPivotChunk;
         for (int r = 0; r < rounds; ++r) {
-            hb::launch_closure_round(Lv.ms(), h->active.p, na, Lv.klist.p, Lv.kcnt.p, r, h->panel.p, h->pflags.p, st);
+            hb::launch_closure_round(d_slots + c0, nc, NP, r, A.panel.p, A.pflags.p, st);
             ck(cudaGetLastError(), "closure round");
         }
     }
+}
+
+// Closure of the listed matrices of level `Lv` over their pivot flags
+// (build and root growth).
+void close_matrices(htrip_index* h, Level& Lv, const std::vector<int>& act) {
+    if (act.empty()) return;
+    cudaStream_t st = h->stream;
+    UpdateArena& A = h->u;
+    const int n = (int)act.size();
+    const size_t slots_b = align256(n * sizeof(hb::Slot));
+    A.stage.reserve(slots_b);
+    A.rb.reserve(n * sizeof(int));
+    A.dev.reserve(slots_b + n * sizeof(int));
+    auto* hs = reinterpret_cast<hb::Slot*>(A.stage.p);
+    for (int i = 0; i < n; ++i) hs[i] = level_slot(Lv, nullptr, act[i], 0, 0);
+    ck(cudaMemcpyAsync(A.dev.p, A.stage.p, n * sizeof(hb::Slot), cudaMemcpyHostToDevice, st), "slots");
+    const auto* ds = reinterpret_cast<const hb::Slot*>(A.dev.p);
+    int* dcnt = reinterpret_cast<int*>(A.dev.p + slots_b);
+    hb::launch_compact_pivots(ds, n, Lv.NP, dcnt, st);
+    ck(cudaGetLastError(), "compact");
+    int* cnt = reinterpret_cast<int*>(A.rb.p);
+    ck(cudaMemcpyAsync(cnt, dcnt, n * sizeof(int), cudaMemcpyDeviceToHost, st), "counts");
+    ck(cudaStreamSynchronize(st), "sync counts");
+    close_slots(A, ds, cnt, n, Lv.NP, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -431,7 +477,7 @@ void do_lift_root(htrip_index* h, const uint8_t* observed, int rows, int cols) {
     ck(cudaStreamSynchronize(st), "sync");
     std::vector<Level> old = std::move(h->L);
     h->L.clear();
-    const int old_rows = h->rows, old_cols = h->cols, old_max_nodes = h->max_nodes;
+    const int old_rows = h->rows, old_cols = h->cols;
     const uint64_t old_ref = h->ref_bytes;
     h->S = old_S * g;
     h->H = old_H + 1;
@@ -459,7 +505,6 @@ void do_lift_root(htrip_index* h, const uint8_t* observed, int rows, int cols) {
         h->leaves_x = old_S / b;
         h->rows = old_rows;
         h->cols = old_cols;
-        h->max_nodes = old_max_nodes;  // the read-back buffers only ever grow
         h->ref_bytes = old_ref;
         throw;
     }
@@ -531,36 +576,34 @@ int vertex_index(const Level& Lv, int g, int r, int c) {
     return p < 0 ? -1 : q * Lv.nP + p;
 }
 
-// One onBatchCellsOpened call as a staged task.  Every level l = 0..H takes
-// two stages, each ending in a small device->host read into pinned memory:
-//   insert(l): leaves: in-leaf edges (pivots marked); nodes: the parents of
-//              children whose summary decreased plus the nodes holding new
-//              seams get the decreased child entries and the seams inserted;
-//              then the pivot flags are compacted  -> pivot counts to host
-//   close(l):  blocked closure over the pivots, then the exterior block is
-//              compared with its snapshot       -> decrease flags to host
-// A host wait separates the stages.  htrip_open_cells runs one task alone;
-// htrip_open_batch advances the tasks of many indexes stage by stage, each
-// on its index's own stream, with one wait per stage for all of them.
+// One onBatchCellsOpened call of one index.  Host bucketing first
+// (minplus_oracle.cpp:539-598), then the levels l = 0..H in order, each in
+// two stages:
+//   insert(l): leaves: the opened in-leaf edges (pivots marked); nodes: the
+//              parents of children whose summary decreased plus the nodes
+//              holding new seams get the decreased child entries and the seams
+//              inserted; the exterior blocks are snapshotted first; the pivot
+//              flags are compacted                 -> pivot counts to host
+//   close(l):  blocked closure over the pivots, then the exterior blocks are
+//              compared with their snapshots       -> decrease flags to host
+// run_open_tasks runs any number of tasks (distinct indexes of one device)
+// together: at each stage the matrices of all tasks with the same leaf side
+// b (hence the same order, padding and port tables at this level) form ONE
+// launch of each kernel, over a device array of matrix descriptors.
 struct OpenTask {
     htrip_index* h = nullptr;
     bool record_stats = true;
-    // host bucketing (minplus_oracle.cpp:539-598)
     std::vector<int> leaves;                             // touched leaves, first-touch order
     std::vector<std::vector<int>> edges;                 // per touched leaf: (u, v) pairs
     std::vector<std::vector<std::vector<int>>> seams;    // [lvl][slot]: (u, v) V_U pairs
     std::vector<std::vector<int>> seam_nodes, seam_slot;
     // progress
-    std::vector<int> act, cand;  // active matrices of this level / the level below
+    std::vector<int> act, cand;    // active matrices of this level / of the level below
+    std::vector<uint8_t> cand_dec; // decrease flags of `cand` (read back after its close)
     int n_dirty = 0;
-    bool skip = false;           // nothing changes at the current level
-    size_t cap = 0;              // closure chunk (matrices) of the current level
+    int slot0 = 0;                 // the task's first slot in this stage's launch
+    int task = 0;                  // the task's index in the launch
 };
-
-// Pinned read-back words of a task: [pivots][kcnt of every node][dec bytes].
-inline int* rb_kcnt(htrip_index* h) { return reinterpret_cast<int*>(h->rb.p) + 1; }
-inline int* rb_pivots(htrip_index* h) { return reinterpret_cast<int*>(h->rb.p); }
-inline uint8_t* rb_dec(htrip_index* h) { return h->rb.p + sizeof(int) * (1 + (size_t)h->max_nodes); }
 
 void open_prepare(OpenTask& T, htrip_index* h, const int32_t* rc, int n, const uint8_t* obs, int rows, int cols,
                   bool record_stats) {
@@ -622,173 +665,183 @@ void open_prepare(OpenTask& T, htrip_index* h, const int32_t* rc, int n, const u
 
 bool open_has_work(const OpenTask& T) { return !T.leaves.empty(); }
 
-// Stage insert(l) of T (issued on the index's stream, not waited for).
-void open_insert(OpenTask& T, int l) {
+// Active matrices of level l >= 1: parents of the children whose summary
+// decreased (in first-seen order), then the nodes holding new seams.
+void open_active(OpenTask& T, int l) {
     htrip_index* h = T.h;
-    cudaStream_t st = h->stream;
-    const int g = h->g, H = h->H;
+    const int g = h->g;
     Level& Lv = h->L[l];
-    T.skip = false;
-    if (l == 0) {
-        T.act = T.leaves;
-        std::vector<int> buf;
-        std::vector<int> eoff(T.leaves.size() + 1, 0);
-        for (size_t i = 0; i < T.leaves.size(); ++i) eoff[i + 1] = eoff[i] + (int)T.edges[i].size() / 2;
-        buf.insert(buf.end(), eoff.begin(), eoff.end());
-        for (auto& e : T.edges) buf.insert(buf.end(), e.begin(), e.end());
-        const int na = (int)T.act.size();
-        h->upd.reserve(buf.size());
-        h->active.reserve(na);
-        ck(cudaMemcpyAsync(h->active.p, T.act.data(), na * sizeof(int), cudaMemcpyHostToDevice, st), "act");
-        ck(cudaMemcpyAsync(h->upd.p, buf.data(), buf.size() * sizeof(int), cudaMemcpyHostToDevice, st), "upd");
-        ck(cudaMemsetAsync(h->pivots.p, 0, sizeof(int), st), "piv");
-        ck(cudaMemsetAsync(Lv.dec.p, 0, Lv.nnodes, st), "dec0");
-        if (H > 0) {
-            h->snap.reserve((size_t)na * Lv.nExt * Lv.nExt);
-            hb::launch_ext_snapshot(Lv.ms(), Lv.d_ext.p, Lv.nExt, h->active.p, na, h->snap.p, st);
-        }
-        hb::launch_leaf_edges(Lv.ms(), h->active.p, na, h->upd.p, h->upd.p + eoff.size(), Lv.kflag.p, h->pivots.p,
-                              st);
-        ck(cudaGetLastError(), "leaf edges");
-        ck(cudaMemcpyAsync(rb_pivots(h), h->pivots.p, sizeof(int), cudaMemcpyDeviceToHost, st), "piv d2h");
-    } else {
-        // candidates: parents of children whose summary decreased, plus seam nodes
-        Level& Lc = h->L[l - 1];
-        const uint8_t* child_dec = rb_dec(h);
-        std::vector<int> slot_of(Lv.nnodes, -1);
-        T.act.clear();
-        for (int c : T.cand) {
-            if (!child_dec[c]) continue;
-            const int cx = c % Lc.nodes_x, cy = c / Lc.nodes_x;
-            const int p = (cy / g) * Lv.nodes_x + (cx / g);
-            if (slot_of[p] < 0) { slot_of[p] = (int)T.act.size(); T.act.push_back(p); }
-        }
-        for (int node : T.seam_nodes[l])
-            if (slot_of[node] < 0) { slot_of[node] = (int)T.act.size(); T.act.push_back(node); }
-        T.n_dirty += (int)T.act.size();
-        if (T.act.empty()) {
-            // nothing changes at this level; higher levels only see seams
-            T.skip = true;
-            T.cand.clear();
-            std::memset(rb_dec(h), 0, Lv.nnodes);
-            ck(cudaMemsetAsync(Lv.dec.p, 0, Lv.nnodes, st), "dec");
-            return;
-        }
-        const int na = (int)T.act.size();
-        std::vector<int> buf(na + 1, 0);
-        for (int i = 0; i < na; ++i) {
-            const int sl = T.seam_slot[l][T.act[i]];
-            buf[i + 1] = buf[i] + (sl >= 0 ? (int)T.seams[l][sl].size() / 2 : 0);
-        }
-        for (int i = 0; i < na; ++i) {
-            const int sl = T.seam_slot[l][T.act[i]];
-            if (sl >= 0) buf.insert(buf.end(), T.seams[l][sl].begin(), T.seams[l][sl].end());
-        }
-        // The decrease flags of the level below are consumed on the device
-        // (child insert) before Lv.dec is cleared for this level.
-        h->active.reserve(na);
-        h->upd.reserve(buf.size());
-        ck(cudaMemcpyAsync(h->active.p, T.act.data(), na * sizeof(int), cudaMemcpyHostToDevice, st), "act");
-        ck(cudaMemcpyAsync(h->upd.p, buf.data(), buf.size() * sizeof(int), cudaMemcpyHostToDevice, st), "upd");
-        ck(cudaMemsetAsync(Lv.dec.p, 0, Lv.nnodes, st), "dec");
-        if (l < H) {
-            h->snap.reserve((size_t)na * Lv.nExt * Lv.nExt);
-            hb::launch_ext_snapshot(Lv.ms(), Lv.d_ext.p, Lv.nExt, h->active.p, na, h->snap.p, st);
-        }
-        hb::launch_node_child_insert(Lv.ms(), Lc.ms(), Lc.d_ext.p, Lv.nP, g, Lv.nodes_x, Lc.nodes_x, h->active.p,
-                                     na, Lc.dec.p, Lv.kflag.p, st);
-        hb::launch_node_seams(Lv.ms(), h->active.p, na, h->upd.p, h->upd.p + na + 1, Lv.kflag.p, st);
-        ck(cudaGetLastError(), "node insert");
+    Level& Lc = h->L[l - 1];
+    std::vector<int> slot_of(Lv.nnodes, -1);
+    T.act.clear();
+    for (size_t i = 0; i < T.cand.size(); ++i) {
+        if (!T.cand_dec[i]) continue;
+        const int c = T.cand[i];
+        const int cx = c % Lc.nodes_x, cy = c / Lc.nodes_x;
+        const int p = (cy / g) * Lv.nodes_x + (cx / g);
+        if (slot_of[p] < 0) { slot_of[p] = (int)T.act.size(); T.act.push_back(p); }
     }
-    const int na = (int)T.act.size();
-    // pivot lists, and the pivot counts of the active matrices in act order
-    hb::launch_compact_pivots(Lv.kflag.p, Lv.NP, h->active.p, na, Lv.klist.p, Lv.kcnt.p, st, h->rb_dev.p);
-    ck(cudaGetLastError(), "compact");
-    ck(cudaMemcpyAsync(rb_kcnt(h), h->rb_dev.p, na * sizeof(int), cudaMemcpyDeviceToHost, st), "kcnt d2h");
+    for (int node : T.seam_nodes[l])
+        if (slot_of[node] < 0) { slot_of[node] = (int)T.act.size(); T.act.push_back(node); }
+    T.n_dirty += (int)T.act.size();
 }
 
-// Stage close(l) of T: closure rounds over the pivot counts read back by
-// insert(l), then the summary comparison whose flags insert(l+1) reads.
-void open_close(OpenTask& T, int l) {
-    htrip_index* h = T.h;
-    if (T.skip) return;
-    cudaStream_t st = h->stream;
-    const int H = h->H;
-    Level& Lv = h->L[l];
-    const int na = (int)T.act.size();
-    const int* kc = rb_kcnt(h);
-    // algorithmic work of this level (per dirty matrix of order n with pivot
-    // set K: n^2 |K| min-plus ops, 2 n^2 2 + |K| n 2 2 bytes)
-    for (int i = 0; i < na; ++i) {
-        if (kc[i] == 0) continue;
-        const uint64_t n = (uint64_t)Lv.n, k = (uint64_t)kc[i];
-        h->open_ops += n * n * k;
-        h->open_bytes += 4 * n * n + 4 * k * n;
-    }
-    const size_t per = (size_t)hb::kPivotChunk * Lv.NP;
-    const size_t cap = std::max<size_t>(1, (size_t)(128u << 20) / (per * sizeof(uint16_t)));
-    for (size_t c0 = 0; c0 < (size_t)na; c0 += cap) {
-        const int nc = (int)std::min(cap, (size_t)na - c0);
-        int maxk = 0;
-        for (int i = 0; i < nc; ++i) maxk = std::max(maxk, kc[c0 + i]);
-        if (maxk == 0) continue;
-        h->panel.reserve(hb::closure_scratch_elems(Lv.NP, nc));
-        h->pflags.reserve((size_t)nc * (Lv.NP / hb::kFlagTile));
-        const int rounds = (maxk + hb::kPivotChunk - 1) / hb::kPivotChunk;
-        for (int r = 0; r < rounds; ++r) {
-            hb::launch_closure_round(Lv.ms(), h->active.p + c0, nc, Lv.klist.p, Lv.kcnt.p, r, h->panel.p,
-                                     h->pflags.p, st);
-            ck(cudaGetLastError(), "closure round");
-        }
-    }
-    if (l == 0 && T.record_stats) {
-        h->stats.n_touched_leaves = na;
-        h->stats.n_pivots = *rb_pivots(h);
-    }
-    if (l < H) {
-        hb::launch_ext_compare(Lv.ms(), Lv.d_ext.p, Lv.nExt, h->active.p, na, h->snap.p, Lv.dec.p, st);
-        ck(cudaGetLastError(), "compare");
-        ck(cudaMemcpyAsync(rb_dec(h), Lv.dec.p, Lv.nnodes, cudaMemcpyDeviceToHost, st), "dec d2h");
-    }
-    T.cand = T.act;
-}
-
-void open_finish(OpenTask& T) {
-    if (T.record_stats) T.h->stats.n_dirty_ancestors = T.n_dirty;
-}
-
-// Runs the tasks (distinct indexes of one device) together, stage by stage:
-// every task's insert(l) is issued on its index's stream, one wait covers
-// them all, then every task's close(l), one wait.  Issuing from one thread
-// with shared waits keeps gaps between stages in which other work (a
-// cooperative query launch, which needs every SM) gets the device; tasks
-// issued from several threads at once kept the device busy with small
-// kernels and held such launches back.
-void run_open_tasks(std::vector<OpenTask>& tasks) {
+// Runs the tasks (distinct indexes of one device, each with work) on stream
+// `st` with scratch arena A.
+void run_open_tasks(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t st) {
     int maxH = -1;
-    for (auto& T : tasks)
-        if (open_has_work(T)) maxH = std::max(maxH, T.h->H);
-    auto wait_all = [&](int l) {
-        for (auto& T : tasks)
-            if (open_has_work(T) && T.h->H >= l) ck(cudaStreamSynchronize(T.h->stream), "open stage");
-    };
-    for (int l = 0; l <= maxH; ++l) {
-        for (auto& T : tasks)
-            if (open_has_work(T) && T.h->H >= l) open_insert(T, l);
-        wait_all(l);
-        for (auto& T : tasks)
-            if (open_has_work(T) && T.h->H >= l) open_close(T, l);
-        wait_all(l);
+    for (size_t t = 0; t < tasks.size(); ++t) {
+        tasks[t]->task = (int)t;
+        maxH = std::max(maxH, tasks[t]->h->H);
     }
-    for (auto& T : tasks)
-        if (open_has_work(T)) open_finish(T);
+    const int n_tasks = (int)tasks.size();
+    for (int l = 0; l <= maxH; ++l) {
+        // ---- active matrices and the groups of this stage (one per leaf side b)
+        std::vector<OpenTask*> live;
+        for (OpenTask* T : tasks) {
+            if (T->h->H < l) continue;
+            if (l == 0) T->act = T->leaves;
+            else open_active(*T, l);
+            if (!T->act.empty()) live.push_back(T);
+            else {  // nothing changes at this level; higher levels only see seams
+                T->cand.clear();
+                T->cand_dec.clear();
+            }
+        }
+        if (live.empty()) continue;
+        // tasks of equal (b, g) share this level's geometry: one launch per group
+        auto key = [](const OpenTask* t) { return t->h->b * 1024 + t->h->g; };
+        std::stable_sort(live.begin(), live.end(), [&](const OpenTask* a, const OpenTask* c) { return key(a) < key(c); });
+        struct Group { int t0, t1, s0, s1; size_t snap_off; };
+        std::vector<Group> groups;
+        int n_slots = 0;
+        size_t list_ints = 0, snap_elems = 0;
+        for (size_t i = 0; i < live.size();) {
+            size_t j = i;
+            Group G{(int)i, 0, n_slots, 0, snap_elems};
+            const Level& Lv0 = live[i]->h->L[l];
+            while (j < live.size() && key(live[j]) == key(live[i])) {
+                live[j]->slot0 = n_slots;
+                n_slots += (int)live[j]->act.size();
+                ++j;
+            }
+            G.t1 = (int)j;
+            G.s1 = n_slots;
+            snap_elems += (size_t)(G.s1 - G.s0) * Lv0.nExt * Lv0.nExt;
+            groups.push_back(G);
+            i = j;
+        }
+        for (OpenTask* T : live) {
+            if (l == 0)
+                for (auto& e : T->edges) list_ints += e.size();
+            else
+                for (int m : T->act) {
+                    const int sl = T->seam_slot[l][m];
+                    if (sl >= 0) list_ints += T->seams[l][sl].size();
+                }
+        }
+        // ---- staged upload: [slots][lists][slot counts][slot dec][task pivots]
+        const size_t o_list = align256(n_slots * sizeof(hb::Slot));
+        const size_t o_cnt = o_list + align256(std::max<size_t>(1, list_ints) * sizeof(int));
+        const size_t o_dec = o_cnt + align256(n_slots * sizeof(int));
+        const size_t o_piv = o_dec + align256(n_slots);
+        const size_t total = o_piv + align256(n_tasks * sizeof(int));
+        A.stage.reserve(total);
+        A.dev.reserve(total);
+        A.rb.reserve(total - o_cnt);
+        std::memset(A.stage.p + o_cnt, 0, total - o_cnt);
+        auto* hs = reinterpret_cast<hb::Slot*>(A.stage.p);
+        int* hl = reinterpret_cast<int*>(A.stage.p + o_list);
+        int li = 0;  // in (u, v) pairs
+        for (OpenTask* T : live) {
+            Level& Lv = T->h->L[l];
+            Level* child = l >= 1 ? &T->h->L[l - 1] : nullptr;
+            for (size_t i = 0; i < T->act.size(); ++i) {
+                const int m = T->act[i];
+                hb::Slot sl = level_slot(Lv, child, m, T->task, l == T->h->H);
+                sl.list_begin = li;
+                const std::vector<int>* lst = nullptr;
+                if (l == 0) lst = &T->edges[i];
+                else if (T->seam_slot[l][m] >= 0) lst = &T->seams[l][T->seam_slot[l][m]];
+                if (lst) {
+                    std::memcpy(hl + 2 * li, lst->data(), lst->size() * sizeof(int));
+                    li += (int)lst->size() / 2;
+                }
+                sl.list_end = li;
+                hs[T->slot0 + i] = sl;
+            }
+        }
+        ck(cudaMemcpyAsync(A.dev.p, A.stage.p, total, cudaMemcpyHostToDevice, st), "open stage upload");
+        const auto* ds = reinterpret_cast<const hb::Slot*>(A.dev.p);
+        const int* dl = reinterpret_cast<const int*>(A.dev.p + o_list);
+        int* dcnt = reinterpret_cast<int*>(A.dev.p + o_cnt);
+        uint8_t* ddec = A.dev.p + o_dec;
+        int* dpiv = reinterpret_cast<int*>(A.dev.p + o_piv);
+        A.snap.reserve(std::max<size_t>(1, snap_elems));
+        // ---- insert stage, one launch per kernel and group
+        for (const Group& G : groups) {
+            const htrip_index* h0 = live[G.t0]->h;
+            const Level& Lv = h0->L[l];
+            const int n = G.s1 - G.s0;
+            hb::launch_ext_snapshot(ds + G.s0, n, Lv.d_ext.p, Lv.nExt, Lv.NP, A.snap.p + G.snap_off, st);
+            if (l == 0) {
+                hb::launch_leaf_edges(ds + G.s0, n, dl, Lv.NP, dpiv, st);
+            } else {
+                const Level& Lc = h0->L[l - 1];
+                hb::launch_node_child_insert(ds + G.s0, n, Lc.d_ext.p, Lv.nP, h0->g, Lv.NP, Lc.NP, st);
+                hb::launch_node_seams(ds + G.s0, n, dl, Lv.NP, st);
+            }
+            hb::launch_compact_pivots(ds + G.s0, n, Lv.NP, dcnt + G.s0, st);
+            ck(cudaGetLastError(), "open insert");
+        }
+        int* hcnt = reinterpret_cast<int*>(A.rb.p);
+        int* hpiv = reinterpret_cast<int*>(A.rb.p + (o_piv - o_cnt));
+        uint8_t* hdec = A.rb.p + (o_dec - o_cnt);
+        ck(cudaMemcpyAsync(A.rb.p, A.dev.p + o_cnt, o_dec - o_cnt, cudaMemcpyDeviceToHost, st), "counts");
+        if (l == 0)
+            ck(cudaMemcpyAsync(hpiv, dpiv, n_tasks * sizeof(int), cudaMemcpyDeviceToHost, st), "pivots");
+        ck(cudaStreamSynchronize(st), "open insert stage");
+        // ---- close stage
+        for (const Group& G : groups) {
+            const htrip_index* h0 = live[G.t0]->h;
+            const Level& Lv = h0->L[l];
+            const int n = G.s1 - G.s0;
+            close_slots(A, ds + G.s0, hcnt + G.s0, n, Lv.NP, st);
+            hb::launch_ext_compare(ds + G.s0, n, Lv.d_ext.p, Lv.nExt, Lv.NP, A.snap.p + G.snap_off, ddec + G.s0,
+                                   h0->g, st);
+            ck(cudaGetLastError(), "open close");
+        }
+        ck(cudaMemcpyAsync(hdec, ddec, n_slots, cudaMemcpyDeviceToHost, st), "decreases");
+        ck(cudaStreamSynchronize(st), "open close stage");
+        // ---- per task: work accounting, stats, the next level's candidates
+        for (OpenTask* T : live) {
+            htrip_index* h = T->h;
+            const uint64_t n = (uint64_t)h->L[l].n;
+            for (size_t i = 0; i < T->act.size(); ++i) {
+                const uint64_t k = (uint64_t)hcnt[T->slot0 + i];
+                if (!k) continue;
+                h->open_ops += n * n * k;
+                h->open_bytes += 4 * n * n + 4 * k * n;
+            }
+            if (l == 0 && T->record_stats) {
+                h->stats.n_touched_leaves = (int)T->act.size();
+                h->stats.n_pivots = hpiv[T->task];
+            }
+            T->cand = T->act;
+            T->cand_dec.assign(hdec + T->slot0, hdec + T->slot0 + T->act.size());
+        }
+    }
+    for (OpenTask* T : tasks)
+        if (T->record_stats) T->h->stats.n_dirty_ancestors = T->n_dirty;
 }
 
 void do_open(htrip_index* h, const int32_t* rc, int n, const uint8_t* obs, int rows, int cols, bool record_stats) {
     h->update_counter++;
-    std::vector<OpenTask> tasks(1);
-    open_prepare(tasks[0], h, rc, n, obs, rows, cols, record_stats);
-    run_open_tasks(tasks);
+    OpenTask T;
+    open_prepare(T, h, rc, n, obs, rows, cols, record_stats);
+    if (!open_has_work(T)) return;
+    std::vector<OpenTask*> tasks{&T};
+    run_open_tasks(tasks, h->u, h->stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -989,7 +1042,6 @@ void make_plan(const htrip_index* h, const int32_t* vps, const uint8_t* pass_fla
 //   [flags of every request]  <- one memset to 0
 //   [X0 X1 X2 Y0 Y1 of every request][results k*k u16 of every request]
 // ---------------------------------------------------------------------------
-inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
 struct QueryReq {
     const htrip_index* h;
@@ -1666,6 +1718,7 @@ htrip_status htrip_open_batch(htrip_batch* b, const htrip_open_request* reqs, in
     }
     for (int w = 0; w < n_waves; ++w) {
         std::vector<OpenTask> tasks;
+        tasks.reserve(n);
         for (int i = 0; i < n; ++i) {
             if (wave[i] != w) continue;
             const htrip_open_request& r = reqs[i];
@@ -1674,7 +1727,10 @@ htrip_status htrip_open_batch(htrip_batch* b, const htrip_open_request* reqs, in
             tasks.emplace_back();
             open_prepare(tasks.back(), r.index, r.rc, r.n, r.observed, r.rows, r.cols, true);
         }
-        run_open_tasks(tasks);
+        std::vector<OpenTask*> work;
+        for (auto& T : tasks)
+            if (open_has_work(T)) work.push_back(&T);
+        if (!work.empty()) run_open_tasks(work, b->u, b->stream);
     }
     return HTRIP_OK;
     HTRIP_GUARD_END
@@ -2066,8 +2122,7 @@ htrip_status htrip_memory_bytes(const htrip_index* h, uint64_t* reference_bytes,
         for (const auto& Lv : h->L)
             dev += (Lv.mat.n + Lv.klist.n * 2 + Lv.kcnt.n * 2) * sizeof(uint16_t) + Lv.kflag.n + Lv.dec.n +
                    (Lv.d_ext.n + Lv.d_seams.n) * sizeof(int);
-        dev += h->pass.n + h->panel.n * 2 + h->pflags.n + h->snap.n * 2 + h->q.dev.n + h->upd.n * 4 +
-               h->active.n * 4 + h->rb_dev.n * 4;
+        dev += h->pass.n + h->u.dev.n + h->u.snap.n * 2 + h->u.panel.n * 2 + h->u.pflags.n + h->q.dev.n;
     }
     if (reference_bytes) *reference_bytes = ref;
     if (device_bytes) *device_bytes = dev;

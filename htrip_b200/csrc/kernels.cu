@@ -16,6 +16,9 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 
+// grid.y / grid.z are limited to 65535: per-matrix launches go in slices.
+constexpr int kMaxGridY = 65535;
+
 __device__ __forceinline__ uint16_t* mat_ptr(const MatSet& M, int m) {
     return M.base + (size_t)m * M.NP * M.NP;
 }
@@ -139,13 +142,12 @@ __global__ void seams_build_kernel(MatSet N, const int* __restrict__ seams, int 
 // ---------------------------------------------------------------------------
 // Pivot compaction: flags -> ascending index list, one CTA per matrix.
 // ---------------------------------------------------------------------------
-__global__ void compact_pivots_kernel(uint8_t* kflag, int NP, const int* __restrict__ active,
-                                      int* klist, int* kcnt, int* slot_cnt) {
+__global__ void compact_pivots_kernel(const Slot* __restrict__ S, int NP, int* slot_cnt) {
     __shared__ int warp_tot[32];
     __shared__ int base;
-    const int m = active[blockIdx.x];
-    uint8_t* f = kflag + (size_t)m * NP;
-    int* out = klist + (size_t)m * NP;
+    const Slot& sl = S[blockIdx.x];
+    uint8_t* f = sl.kflag;
+    int* out = sl.klist;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     if (threadIdx.x == 0) base = 0;
     __syncthreads();
@@ -170,7 +172,7 @@ __global__ void compact_pivots_kernel(uint8_t* kflag, int NP, const int* __restr
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        kcnt[m] = base;
+        *sl.kcnt = base;
         if (slot_cnt) slot_cnt[blockIdx.x] = base;
     }
 }
@@ -194,19 +196,17 @@ __global__ void compact_pivots_kernel(uint8_t* kflag, int NP, const int* __restr
 // receives T* as a B x B block (identity beyond mk); T is symmetric, so T*
 // is too.
 __global__ void __launch_bounds__(256)
-pivot_close_kernel(MatSet M, const int* __restrict__ active, const int* __restrict__ klist,
-                   const int* __restrict__ kcnt, int round, uint16_t* tstar) {
+pivot_close_kernel(const Slot* __restrict__ S, int NP, int round, uint16_t* tstar) {
     constexpr int B = kPivotChunk;   // 64: 256 threads x 16 entries
     constexpr int LD = B + 8;        // padded row (144 bytes): column reads hit distinct banks
     __shared__ __align__(16) uint16_t T[B][LD];
     __shared__ int kc[B];
     const int slot = blockIdx.x;
-    const int m = active[slot];
-    const int NP = M.NP;
-    const int mk = min(B, kcnt[m] - round * B);
+    const Slot& sl = S[slot];
+    const int mk = min(B, *sl.kcnt - round * B);
     if (mk <= 0) return;
-    const int* K = klist + (size_t)m * NP + round * B;
-    const uint16_t* D = mat_ptr(M, m);
+    const int* K = sl.klist + round * B;
+    const uint16_t* D = sl.mat;
     const int tid = threadIdx.x;
     if (tid < mk) kc[tid] = K[tid];
     __syncthreads();
@@ -256,8 +256,7 @@ pivot_close_kernel(MatSet M, const int* __restrict__ active, const int* __restri
 // and marks the 64-column tiles of R' holding any finite value.
 template <int RW, int CP, bool PANEL>
 __global__ void __launch_bounds__(256)
-closure_gemm_kernel(MatSet M, const int* __restrict__ active, const int* __restrict__ klist,
-                    const int* __restrict__ kcnt, int round, uint16_t* panel, uint8_t* flags,
+closure_gemm_kernel(const Slot* __restrict__ S, int NP, int round, uint16_t* panel, uint8_t* flags,
                     const uint16_t* __restrict__ tstar) {
     constexpr int B = kPivotChunk;
     constexpr int MT = 8 * RW;
@@ -269,16 +268,15 @@ closure_gemm_kernel(MatSet M, const int* __restrict__ active, const int* __restr
     __shared__ int kc[B];
     __shared__ int tile_any[NT / kFlagTile];
     const int slot = blockIdx.z;
-    const int m = active[slot];
-    const int NP = M.NP;
-    const int mk = min(B, kcnt[m] - round * B);
+    const Slot& sl = S[slot];
+    const int mk = min(B, *sl.kcnt - round * B);
     if (mk <= 0) return;
     const int i0 = blockIdx.y * MT, j0 = blockIdx.x * NT;
     uint16_t* P = panel + (size_t)slot * B * NP;
-    uint16_t* D = mat_ptr(M, m);
+    uint16_t* D = sl.mat;
     const int tid = threadIdx.x;
     if constexpr (PANEL) {
-        const int* K = klist + (size_t)m * NP + round * B;
+        const int* K = sl.klist + round * B;
         if (tid < mk) kc[tid] = K[tid];
         if (tid < NT / kFlagTile) tile_any[tid] = 0;
         __syncthreads();
@@ -365,16 +363,15 @@ closure_gemm_kernel(MatSet M, const int* __restrict__ active, const int* __restr
 // ---------------------------------------------------------------------------
 // In-leaf edges, processed sequentially per leaf like the reference loop
 // (leaf_tile.cpp:311-330): an edge counts (and its endpoints become pivots)
-// only if it shortens D[u][v].
-__global__ void leaf_edges_kernel(MatSet L, const int* __restrict__ active, const int* __restrict__ eoff,
-                                  const int* __restrict__ edges, uint8_t* kflag, int* pivots) {
+// only if it shortens D[u][v].  Edges of slot s: list[list_begin .. list_end).
+__global__ void leaf_edges_kernel(const Slot* __restrict__ S, const int* __restrict__ edges, int NP,
+                                  int* task_pivots) {
     if (threadIdx.x != 0) return;
-    const int m = active[blockIdx.x];
-    uint16_t* D = mat_ptr(L, m);
-    const int NP = L.NP;
-    uint8_t* f = kflag + (size_t)m * NP;
+    const Slot& sl = S[blockIdx.x];
+    uint16_t* D = sl.mat;
+    uint8_t* f = sl.kflag;
     int np = 0;
-    for (int e = eoff[blockIdx.x]; e < eoff[blockIdx.x + 1]; ++e) {
+    for (int e = sl.list_begin; e < sl.list_end; ++e) {
         const int u = edges[2 * e], v = edges[2 * e + 1];
         if (1 < D[(size_t)u * NP + v]) {
             D[(size_t)u * NP + v] = 1;
@@ -383,72 +380,87 @@ __global__ void leaf_edges_kernel(MatSet L, const int* __restrict__ active, cons
             if (!f[v]) { f[v] = 1; ++np; }
         }
     }
-    atomicAdd(pivots, np);
+    atomicAdd(task_pivots + sl.task, np);
 }
 
 // Child-summary decreases (internal_node.cpp:343-353).  Inserting every child
 // summary entry that is smaller than the parent's is the same as inserting
 // the reference's decrease list: entries that did not decrease can never be
 // smaller than the parent's (the parent block is <= the old summary).
-__global__ void node_child_insert_kernel(MatSet N, MatSet Cm, const int* __restrict__ cext, int nP, int g,
-                                         int nodes_x, int child_nodes_x, const int* __restrict__ active,
-                                         const uint8_t* __restrict__ child_dec, uint8_t* kflag) {
-    const int node = active[blockIdx.z];
+__global__ void node_child_insert_kernel(const Slot* __restrict__ S, const int* __restrict__ cext, int nP, int g,
+                                         int NP, int childNP) {
+    const Slot& sl = S[blockIdx.z];
     const int q = blockIdx.y;
-    const int tx = node % nodes_x, ty = node / nodes_x;
-    const int child = (ty * g + q / g) * child_nodes_x + (tx * g + q % g);
-    if (!child_dec[child]) return;
+    const int tx = sl.node % sl.nodes_x, ty = sl.node / sl.nodes_x;
+    const int child = (ty * g + q / g) * sl.child_nodes_x + (tx * g + q % g);
+    if (!sl.child_dec[child]) return;
     const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (size_t)nP * nP) return;
     const int p = (int)(idx / nP), pp = (int)(idx % nP);
-    const uint16_t w = mat_ptr(Cm, child)[(size_t)cext[p] * Cm.NP + cext[pp]];
-    uint16_t* D = mat_ptr(N, node);
+    const uint16_t w = sl.child_mat[((size_t)child * childNP + cext[p]) * childNP + cext[pp]];
+    uint16_t* D = sl.mat;
     const int u = q * nP + p, v = q * nP + pp;
-    if (w < D[(size_t)u * N.NP + v]) {
-        D[(size_t)u * N.NP + v] = w;  // (v, u) is written by its own thread
-        kflag[(size_t)node * N.NP + u] = 1;
-        kflag[(size_t)node * N.NP + v] = 1;
+    if (w < D[(size_t)u * NP + v]) {
+        D[(size_t)u * NP + v] = w;  // (v, u) is written by its own thread
+        sl.kflag[u] = 1;
+        sl.kflag[v] = 1;
     }
 }
 
-// Update-time seams (internal_node.cpp:356-365), sequential per node.
-__global__ void node_seams_kernel(MatSet N, const int* __restrict__ active, const int* __restrict__ soff,
-                                  const int* __restrict__ seams, uint8_t* kflag) {
+// Update-time seams (internal_node.cpp:356-365), sequential per node; seams
+// of slot s: list[list_begin .. list_end).
+__global__ void node_seams_kernel(const Slot* __restrict__ S, const int* __restrict__ seams, int NP) {
     if (threadIdx.x != 0) return;
-    const int node = active[blockIdx.x];
-    uint16_t* D = mat_ptr(N, node);
-    const int NP = N.NP;
-    for (int s = soff[blockIdx.x]; s < soff[blockIdx.x + 1]; ++s) {
+    const Slot& sl = S[blockIdx.x];
+    uint16_t* D = sl.mat;
+    for (int s = sl.list_begin; s < sl.list_end; ++s) {
         const int u = seams[2 * s], v = seams[2 * s + 1];
         if (1 < D[(size_t)u * NP + v]) {
             D[(size_t)u * NP + v] = 1;
             D[(size_t)v * NP + u] = 1;
-            kflag[(size_t)node * NP + u] = 1;
-            kflag[(size_t)node * NP + v] = 1;
+            sl.kflag[u] = 1;
+            sl.kflag[v] = 1;
         }
     }
 }
 
-__global__ void ext_snapshot_kernel(MatSet M, const int* __restrict__ ext, int nExt, const int* __restrict__ active,
+// Exterior block snapshot of every non-root slot (summary S / S_U before the
+// update).
+__global__ void ext_snapshot_kernel(const Slot* __restrict__ S, const int* __restrict__ ext, int nExt, int NP,
                                     uint16_t* snap) {
     const int slot = blockIdx.y;
+    if (S[slot].root) return;
     const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (size_t)nExt * nExt) return;
     const int a = (int)(idx / nExt), c = (int)(idx % nExt);
-    snap[(size_t)slot * nExt * nExt + idx] = mat_ptr(M, active[slot])[(size_t)ext[a] * M.NP + ext[c]];
+    snap[(size_t)slot * nExt * nExt + idx] = S[slot].mat[(size_t)ext[a] * NP + ext[c]];
 }
 
-__global__ void ext_compare_kernel(MatSet M, const int* __restrict__ ext, int nExt, const int* __restrict__ active,
-                                   const uint16_t* __restrict__ snap, uint8_t* dec) {
+// After the update: a non-root slot whose exterior block decreased anywhere
+// gets its decrease flag (and slot_dec[slot]) set (refreshBoundarySummary,
+// leaf_tile.cpp:253-273, internal_node.cpp:415-433).  Every node slot also
+// clears its children's decrease flags, which its insert stage has consumed:
+// outside an opening call all decrease flags are zero.
+__global__ void ext_compare_kernel(const Slot* __restrict__ S, const int* __restrict__ ext, int nExt, int NP,
+                                   const uint16_t* __restrict__ snap, uint8_t* slot_dec, int g) {
     const int slot = blockIdx.y;
+    const Slot& sl = S[slot];
+    if (sl.child_dec && blockIdx.x == 0 && threadIdx.x < g * g) {
+        const int q = threadIdx.x;
+        const int tx = sl.node % sl.nodes_x, ty = sl.node / sl.nodes_x;
+        sl.child_dec[(ty * g + q / g) * sl.child_nodes_x + (tx * g + q % g)] = 0;
+    }
+    if (sl.root) return;
     const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int m = active[slot];
     bool d = false;
     if (idx < (size_t)nExt * nExt) {
         const int a = (int)(idx / nExt), c = (int)(idx % nExt);
-        d = mat_ptr(M, m)[(size_t)ext[a] * M.NP + ext[c]] < snap[(size_t)slot * nExt * nExt + idx];
+        d = sl.mat[(size_t)ext[a] * NP + ext[c]] < snap[(size_t)slot * nExt * nExt + idx];
     }
-    if (__any_sync(FULL, d) && (threadIdx.x & 31) == 0) dec[m] = 1;
+    if (__any_sync(FULL, d) && (threadIdx.x & 31) == 0) {
+        *sl.dec = 1;
+        slot_dec[slot] = 1;
+    }
 }
 
 __global__ void gather_block_kernel(const uint16_t* __restrict__ mat, int NP, const int* __restrict__ rows, int nr,
@@ -530,8 +542,6 @@ inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1)
 // ---------------------------------------------------------------------------
 // Launch wrappers
 // ---------------------------------------------------------------------------
-// grid.y is limited to 65535: per-matrix launches go in slices of that many.
-constexpr int kMaxGridY = 65535;
 
 void launch_leaf_bfs(const uint8_t* pass, int S, int b, int leaves_x, int n_leaves, MatSet leaves,
                      cudaStream_t st, const int* list) {
@@ -560,15 +570,14 @@ void launch_seams_build(MatSet node, const int* seams, int n_seams, const uint8_
     }
 }
 
-void launch_compact_pivots(uint8_t* kflag, int NP, const int* active, int n_active, int* klist, int* kcnt,
-                           cudaStream_t st, int* slot_cnt) {
-    if (n_active == 0) return;
-    compact_pivots_kernel<<<n_active, 256, 0, st>>>(kflag, NP, active, klist, kcnt, slot_cnt);
+void launch_compact_pivots(const Slot* S, int n, int NP, int* slot_cnt, cudaStream_t st) {
+    if (n == 0) return;
+    compact_pivots_kernel<<<n, 256, 0, st>>>(S, NP, slot_cnt);
 }
 
 template <int RW, int CP, bool PANEL>
-static void launch_gemm_t(MatSet M, const int* active, int n_active, const int* klist, const int* kcnt, int round,
-                          uint16_t* panel, uint8_t* flags, const uint16_t* tstar, cudaStream_t st) {
+static void launch_gemm_t(const Slot* S, int n, int NP, int round, uint16_t* panel, uint8_t* flags,
+                          const uint16_t* tstar, cudaStream_t st) {
     constexpr int MT = 8 * RW, NT = 64 * CP;
     const size_t smem = (size_t)kPivotChunk * (MT + NT) * sizeof(uint16_t);
     static bool configured = false;
@@ -577,65 +586,64 @@ static void launch_gemm_t(MatSet M, const int* active, int n_active, const int* 
                              (int)smem);
         configured = true;
     }
-    dim3 grid(M.NP / NT, PANEL ? 1 : M.NP / MT, n_active);
-    closure_gemm_kernel<RW, CP, PANEL><<<grid, 256, smem, st>>>(M, active, klist, kcnt, round, panel, flags, tstar);
+    dim3 grid(NP / NT, PANEL ? 1 : NP / MT, n);
+    closure_gemm_kernel<RW, CP, PANEL><<<grid, 256, smem, st>>>(S, NP, round, panel, flags, tstar);
 }
 
 size_t closure_scratch_elems(int NP, int n_active) {
     return (size_t)n_active * kPivotChunk * NP + (size_t)n_active * kPivotChunk * kPivotChunk;
 }
 
-void launch_closure_round(MatSet M, const int* active, int n_active, const int* klist, const int* kcnt,
-                          int round, uint16_t* panel, uint8_t* flags, cudaStream_t st) {
-    if (n_active == 0) return;
-    uint16_t* tstar = panel + (size_t)n_active * kPivotChunk * M.NP;
-    pivot_close_kernel<<<n_active, 256, 0, st>>>(M, active, klist, kcnt, round, tstar);
+void launch_closure_round(const Slot* S, int n, int NP, int round, uint16_t* panel, uint8_t* flags,
+                          cudaStream_t st) {
+    if (n == 0) return;
+    uint16_t* tstar = panel + (size_t)n * kPivotChunk * NP;
+    pivot_close_kernel<<<n, 256, 0, st>>>(S, NP, round, tstar);
     // Panel tiles: the widest whose grid still has two CTAs per SM (148 SMs).
-    const size_t ctas = (size_t)(M.NP / 64) * n_active;
-    if (M.NP >= 256 && ctas >= 4 * 296)
-        launch_gemm_t<8, 4, true>(M, active, n_active, klist, kcnt, round, panel, flags, tstar, st);
-    else if (M.NP >= 128 && ctas >= 2 * 296)
-        launch_gemm_t<8, 2, true>(M, active, n_active, klist, kcnt, round, panel, flags, tstar, st);
+    const size_t ctas = (size_t)(NP / 64) * n;
+    if (NP >= 256 && ctas >= 4 * 296)
+        launch_gemm_t<8, 4, true>(S, n, NP, round, panel, flags, tstar, st);
+    else if (NP >= 128 && ctas >= 2 * 296)
+        launch_gemm_t<8, 2, true>(S, n, NP, round, panel, flags, tstar, st);
     else
-        launch_gemm_t<8, 1, true>(M, active, n_active, klist, kcnt, round, panel, flags, tstar, st);
-    if (M.NP >= 256) launch_gemm_t<16, 4, false>(M, active, n_active, klist, kcnt, round, panel, flags, tstar, st);
-    else if (M.NP >= 128) launch_gemm_t<16, 2, false>(M, active, n_active, klist, kcnt, round, panel, flags, tstar, st);
-    else launch_gemm_t<8, 1, false>(M, active, n_active, klist, kcnt, round, panel, flags, tstar, st);
+        launch_gemm_t<8, 1, true>(S, n, NP, round, panel, flags, tstar, st);
+    if (NP >= 256) launch_gemm_t<16, 4, false>(S, n, NP, round, panel, flags, tstar, st);
+    else if (NP >= 128) launch_gemm_t<16, 2, false>(S, n, NP, round, panel, flags, tstar, st);
+    else launch_gemm_t<8, 1, false>(S, n, NP, round, panel, flags, tstar, st);
 }
 
-void launch_leaf_edges(MatSet leaves, const int* active, int n_active, const int* eoff, const int* edges,
-                       uint8_t* kflag, int* pivots, cudaStream_t st) {
-    if (n_active == 0) return;
-    leaf_edges_kernel<<<n_active, 32, 0, st>>>(leaves, active, eoff, edges, kflag, pivots);
+void launch_leaf_edges(const Slot* S, int n, const int* edges, int NP, int* task_pivots, cudaStream_t st) {
+    if (n == 0) return;
+    leaf_edges_kernel<<<n, 32, 0, st>>>(S, edges, NP, task_pivots);
 }
 
-void launch_node_child_insert(MatSet node, MatSet child, const int* child_ext, int nP, int g, int nodes_x,
-                              int child_nodes_x, const int* active, int n_active, const uint8_t* child_dec,
-                              uint8_t* kflag, cudaStream_t st) {
-    if (n_active == 0) return;
-    dim3 grid(blocks_for((size_t)nP * nP, 256), g * g, n_active);
-    node_child_insert_kernel<<<grid, 256, 0, st>>>(node, child, child_ext, nP, g, nodes_x, child_nodes_x, active,
-                                                   child_dec, kflag);
+void launch_node_child_insert(const Slot* S, int n, const int* child_ext, int nP, int g, int NP, int childNP,
+                              cudaStream_t st) {
+    for (int z0 = 0; z0 < n; z0 += kMaxGridY) {
+        dim3 grid(blocks_for((size_t)nP * nP, 256), g * g, std::min(kMaxGridY, n - z0));
+        node_child_insert_kernel<<<grid, 256, 0, st>>>(S + z0, child_ext, nP, g, NP, childNP);
+    }
 }
 
-void launch_node_seams(MatSet node, const int* active, int n_active, const int* soff, const int* seams,
-                       uint8_t* kflag, cudaStream_t st) {
-    if (n_active == 0) return;
-    node_seams_kernel<<<n_active, 32, 0, st>>>(node, active, soff, seams, kflag);
+void launch_node_seams(const Slot* S, int n, const int* seams, int NP, cudaStream_t st) {
+    if (n == 0) return;
+    node_seams_kernel<<<n, 32, 0, st>>>(S, seams, NP);
 }
 
-void launch_ext_snapshot(MatSet M, const int* ext, int nExt, const int* active, int n_active, uint16_t* snap,
-                         cudaStream_t st) {
-    if (n_active == 0) return;
-    dim3 grid(blocks_for((size_t)nExt * nExt, 256), n_active);
-    ext_snapshot_kernel<<<grid, 256, 0, st>>>(M, ext, nExt, active, snap);
+void launch_ext_snapshot(const Slot* S, int n, const int* ext, int nExt, int NP, uint16_t* snap, cudaStream_t st) {
+    for (int y0 = 0; y0 < n; y0 += kMaxGridY) {
+        dim3 grid(blocks_for((size_t)nExt * nExt, 256), std::min(kMaxGridY, n - y0));
+        ext_snapshot_kernel<<<grid, 256, 0, st>>>(S + y0, ext, nExt, NP, snap + (size_t)y0 * nExt * nExt);
+    }
 }
 
-void launch_ext_compare(MatSet M, const int* ext, int nExt, const int* active, int n_active, const uint16_t* snap,
-                        uint8_t* dec, cudaStream_t st) {
-    if (n_active == 0) return;
-    dim3 grid(blocks_for((size_t)nExt * nExt, 256), n_active);
-    ext_compare_kernel<<<grid, 256, 0, st>>>(M, ext, nExt, active, snap, dec);
+void launch_ext_compare(const Slot* S, int n, const int* ext, int nExt, int NP, const uint16_t* snap,
+                        uint8_t* slot_dec, int g, cudaStream_t st) {
+    for (int y0 = 0; y0 < n; y0 += kMaxGridY) {
+        dim3 grid(blocks_for((size_t)nExt * nExt, 256), std::min(kMaxGridY, n - y0));
+        ext_compare_kernel<<<grid, 256, 0, st>>>(S + y0, ext, nExt, NP, snap + (size_t)y0 * nExt * nExt,
+                                                 slot_dec + y0, g);
+    }
 }
 
 void launch_fill_u16(uint16_t* ptr, size_t n, uint16_t value, cudaStream_t st) {

@@ -37,47 +37,58 @@ void launch_seams_build(MatSet node, const int* seams, int n_seams, const uint8_
                         int side, int nodes_x, int n_nodes, uint8_t* kflag, cudaStream_t st,
                         const int* list = nullptr);
 
-// --- closure over pivot sets -------------------------------------------------
-// Compact per-matrix pivot flags into sorted lists (clears the flags);
-// slot_cnt (optional) receives the counts in active order as well.
-void launch_compact_pivots(uint8_t* kflag, int NP, const int* active, int n_active, int* klist,
-                           int* kcnt, cudaStream_t st, int* slot_cnt = nullptr);
+// One matrix of an update launch (any index, any map size: the launch's
+// matrices share b, g and level, hence order, padding and port tables).
+struct Slot {
+    uint16_t* mat;              // the matrix (NP x NP)
+    uint8_t* kflag;             // its pivot flags (NP)
+    int* klist;                 // its pivot list (NP)
+    int* kcnt;                  // its pivot count
+    uint8_t* dec;               // its summary-decreased flag
+    const uint16_t* child_mat;  // node slots: the child level's matrices (null for leaves)
+    uint8_t* child_dec;         // node slots: the child level's decrease flags (null for leaves)
+    int node, nodes_x, child_nodes_x;
+    int list_begin, list_end;   // the slot's range of the launch's edge / seam list
+    int task;                   // the slot's opening task within the launch
+    int root;                   // 1: the index's root (no summary above it)
+};
 
-// One round of the blocked pivot-set Kleene closure: pivots
-// klist[m][round*B .. round*B+B).  panel: closure_scratch_elems(NP,
-// n_active) u16 of scratch; flags: n_active * NP / kFlagTile bytes.
+// --- closure over pivot sets -------------------------------------------------
+// Compact every slot's pivot flags into its sorted list (clears the flags);
+// slot_cnt (optional) receives the counts in slot order as well.
+void launch_compact_pivots(const Slot* S, int n, int NP, int* slot_cnt, cudaStream_t st);
+
+// One round of the blocked pivot-set Kleene closure of every slot: pivots
+// klist[round*B .. round*B+B).  panel: closure_scratch_elems(NP, n) u16 of
+// scratch; flags: n * NP / kFlagTile bytes.
 size_t closure_scratch_elems(int NP, int n_active);
-void launch_closure_round(MatSet M, const int* active, int n_active, const int* klist,
-                          const int* kcnt, int round, uint16_t* panel, uint8_t* flags,
+void launch_closure_round(const Slot* S, int n, int NP, int round, uint16_t* panel, uint8_t* flags,
                           cudaStream_t st);
 
 // --- incremental updates -----------------------------------------------------
-// Insert opened in-leaf edges (leaf_tile.cpp:311-330).  edges: per active
-// leaf a range [eoff[i], eoff[i+1]) of (u, v) pairs (2 ints).  Marks pivot
-// flags, counts pivots into *pivots.
-void launch_leaf_edges(MatSet leaves, const int* active, int n_active, const int* eoff,
-                       const int* edges, uint8_t* kflag, int* pivots, cudaStream_t st);
+// Insert opened in-leaf edges (leaf_tile.cpp:311-330): slot s's (u, v)
+// pairs are edges[list_begin .. list_end); marks pivot flags and adds the
+// new pivots to task_pivots[task].
+void launch_leaf_edges(const Slot* S, int n, const int* edges, int NP, int* task_pivots, cudaStream_t st);
 
-// Child-summary decreases into parent D_U (internal_node.cpp:343-353):
-// for each active node and each child whose flag is set, insert every
-// child summary entry smaller than the parent's and mark both endpoints.
-void launch_node_child_insert(MatSet node, MatSet child, const int* child_ext, int nP, int g,
-                              int nodes_x, int child_nodes_x, const int* active, int n_active,
-                              const uint8_t* child_dec, uint8_t* kflag, cudaStream_t st);
+// Child-summary decreases into parent D_U (internal_node.cpp:343-353): for
+// each slot and each child whose decrease flag is set, insert every child
+// summary entry smaller than the parent's and mark both endpoints.
+void launch_node_child_insert(const Slot* S, int n, const int* child_ext, int nP, int g, int NP, int childNP,
+                              cudaStream_t st);
 
-// Seam edges of an update (internal_node.cpp:356-365): per active node a
-// range [soff[i], soff[i+1]) of (u, v) V_U-index pairs.
-void launch_node_seams(MatSet node, const int* active, int n_active, const int* soff,
-                       const int* seams, uint8_t* kflag, cudaStream_t st);
+// Seam edges of an update (internal_node.cpp:356-365): slot s's (u, v) V_U
+// pairs are seams[list_begin .. list_end).
+void launch_node_seams(const Slot* S, int n, const int* seams, int NP, cudaStream_t st);
 
-// Snapshot / compare of a matrix's exterior block (summary S or S_U):
-// snap[i] holds nExt*nExt entries per active matrix.  compare sets
-// dec[active[i]] = 1 when any entry decreased (refreshBoundarySummary,
-// leaf_tile.cpp:253-273, internal_node.cpp:415-433).
-void launch_ext_snapshot(MatSet M, const int* ext, int nExt, const int* active, int n_active,
-                         uint16_t* snap, cudaStream_t st);
-void launch_ext_compare(MatSet M, const int* ext, int nExt, const int* active, int n_active,
-                        const uint16_t* snap, uint8_t* dec, cudaStream_t st);
+// Snapshot / compare of the non-root slots' exterior block (summary S or
+// S_U): snap holds nExt*nExt entries per slot; compare sets *dec and
+// slot_dec[slot] when any entry decreased (refreshBoundarySummary,
+// leaf_tile.cpp:253-273, internal_node.cpp:415-433) and clears the node
+// slots' children's decrease flags.
+void launch_ext_snapshot(const Slot* S, int n, const int* ext, int nExt, int NP, uint16_t* snap, cudaStream_t st);
+void launch_ext_compare(const Slot* S, int n, const int* ext, int nExt, int NP, const uint16_t* snap,
+                        uint8_t* slot_dec, int g, cudaStream_t st);
 
 // --- query (query.cu) -------------------------------------------------------
 constexpr int kMaxQueryLevels = 16;
