@@ -1852,7 +1852,7 @@ htrip_status htrip_state_digest(const htrip_index* h, uint64_t* out, int32_t n_o
 }
 
 htrip_status htrip_measure_minplus_rate(int device, int variant, double* entries_per_s) {
-    if (!entries_per_s || variant < 0 || variant > 3) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    if (!entries_per_s || variant < 0 || variant > 4) return fail(HTRIP_ERR_INVALID, "bad arguments");
     HTRIP_GUARD_BEGIN
     ck(cudaSetDevice(device), "cudaSetDevice");
     int sms = 0;

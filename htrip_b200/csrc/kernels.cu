@@ -502,6 +502,8 @@ __global__ void __launch_bounds__(256) digest_kernel(MatSet M, int count, unsign
 //   1  clamped with the fused add+min (__viaddmin_u16x2)
 //   2  fast:    min2(add2(b, a), c)                      (a <= 5535)
 //   3  fast with the fused add+min
+//   4  saturating: min2(vaddus2(b, a), c) (any a <= INF: a sum above 65535
+//      saturates, and min with c <= INF gives the clamped result)
 // Operands stay below 16384, so no variant wraps.
 template <int V>
 __global__ void __launch_bounds__(512) minplus_rate_kernel(int iters, uint32_t seed, uint32_t* sink) {
@@ -520,7 +522,8 @@ __global__ void __launch_bounds__(512) minplus_rate_kernel(int iters, uint32_t s
             if constexpr (V == 0) acc[c] = min2(add2(min2(bv[c], tt), aa), acc[c]);
             else if constexpr (V == 1) acc[c] = __viaddmin_u16x2(min2(bv[c], tt), aa, acc[c]);
             else if constexpr (V == 2) acc[c] = min2(add2(bv[c], aa), acc[c]);
-            else acc[c] = __viaddmin_u16x2(bv[c], aa, acc[c]);
+            else if constexpr (V == 3) acc[c] = __viaddmin_u16x2(bv[c], aa, acc[c]);
+            else acc[c] = min2(__vaddus2(bv[c], aa), acc[c]);
         }
         a = (a + 5u) & 0x3FFFu;
     }
@@ -678,7 +681,8 @@ double measure_minplus_rate(int variant, int sms) {
             case 0: minplus_rate_kernel<0><<<blocks, threads>>>(it, 12345u, sink); break;
             case 1: minplus_rate_kernel<1><<<blocks, threads>>>(it, 12345u, sink); break;
             case 2: minplus_rate_kernel<2><<<blocks, threads>>>(it, 12345u, sink); break;
-            default: minplus_rate_kernel<3><<<blocks, threads>>>(it, 12345u, sink); break;
+            case 3: minplus_rate_kernel<3><<<blocks, threads>>>(it, 12345u, sink); break;
+            default: minplus_rate_kernel<4><<<blocks, threads>>>(it, 12345u, sink); break;
         }
     };
     launch(64);  // warm-up

@@ -292,7 +292,7 @@ htrip_status htrip_last_query_io(const htrip_index* h, uint64_t* h2d_bytes, uint
  * on every SM of `device`: the integer-issue peak the kernels are measured
  * against.  variant 0: add.u16x2 / min.u16x2 clamped form (any a <= INF);
  * 1: the same with the fused add+min intrinsic; 2, 3: the unclamped forms
- * (a <= 5535).                                                            */
+ * (a <= 5535); 4: min with a saturating packed add (any a <= INF).        */
 htrip_status htrip_measure_minplus_rate(int device, int variant, double* entries_per_s);
 
 /* Query tile autotuner (no reference counterpart).  The query kernel has
