@@ -457,6 +457,11 @@ def run_ours(args, rank, world, local_rank):
     out_host = np.empty((k, k), dtype=np.uint16)
     # the project's autotuner picks the query tile shape for this request bucket
     tile_cfg, _ = idx.autotuneQuery(vps, grid, reps=5)
+    if args.tile_config is not None:  # impose a shape on the bucket (e.g. for a profiler run)
+        from htrip_b200.minplus_oracle import autotune_export, autotune_import
+        key = " ".join(autotune_export().strip().splitlines()[-1].split()[:4])
+        autotune_import(f"{key} {args.tile_config}\n")
+        tile_cfg = args.tile_config
     idx.queryAllPairs(vps, grid, out_host)
 
     # parity of this rank's matrix against the CPU checker (rank 0 also times it)
@@ -566,6 +571,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--headline-only", action="store_true",
                     help="only the queryAllPairs headline (skip the opening / batched / served workloads)")
+    ap.add_argument("--tile-config", type=int, choices=[0, 1, 2, 3],
+                    help="query tile shape to use for the headline instead of the autotuner's choice")
     ap.add_argument("--section", choices=["cells_opened", "batched", "served"],
                     help="run only this one of the further workloads after the headline")
     args = ap.parse_args()
