@@ -555,6 +555,95 @@ void do_lift_root(htrip_index* h, const uint8_t* observed, int rows, int cols) {
 }
 
 // ---------------------------------------------------------------------------
+// Non-monotone updates (reference onCellBlocked, minplus_oracle.cpp:247-302,
+// and onBatchLeavesChanged, :507-527 with propagateBatchUpward, :427-505):
+// the listed leaves are rebuilt from the grid (leaf BFS) and every ancestor of
+// a rebuilt tile is rebuilt from its children's summaries and its seams
+// (node init + seams + closure), level by level up to the root.  Each rebuilt
+// matrix is the unique closure of its region, so the index equals the one a
+// full build of the same grid gives on those tiles.
+// ---------------------------------------------------------------------------
+// propagate_all: every ancestor of a rebuilt tile is rebuilt (onCellBlocked);
+// otherwise a rebuilt node's parent is rebuilt only if the node's exterior
+// summary S_U changed (propagateBatchUpward, minplus_oracle.cpp:479-498);
+// the listed leaves' parents are always rebuilt.
+void do_rebuild_leaves(htrip_index* h, const std::vector<int>& leaves_in, const uint8_t* observed, int rows,
+                       int cols, bool propagate_all) {
+    cudaStream_t st = h->stream;
+    const int S = h->S, g = h->g;
+    std::vector<int> cur;
+    {
+        std::vector<uint8_t> seen(h->L[0].nnodes, 0);
+        for (int l : leaves_in)
+            if (l >= 0 && l < h->L[0].nnodes && !seen[l]) { seen[l] = 1; cur.push_back(l); }
+    }
+    if (cur.empty()) return;
+    h->update_counter++;
+    // the passability mirror follows the caller's grid (leaf BFS and seams read it)
+    std::vector<uint8_t> pass((size_t)S * S, 0);
+    for (int r = 0; r < std::min(rows, S); ++r)
+        for (int c = 0; c < std::min(cols, S); ++c) pass[(size_t)r * S + c] = observed[(size_t)r * cols + c] == 1;
+    ck(cudaMemcpyAsync(h->pass.p, pass.data(), pass.size(), cudaMemcpyHostToDevice, st), "pass");
+    DevBuf<int> list;
+    DevBuf<hb::Slot> slots;
+    DevBuf<uint8_t> changed;
+    list.reserve(cur.size());
+    ck(cudaMemcpyAsync(list.p, cur.data(), cur.size() * sizeof(int), cudaMemcpyHostToDevice, st), "list");
+    hb::launch_leaf_bfs(h->pass.p, S, h->b, h->leaves_x, (int)cur.size(), h->L[0].ms(), st, list.p);
+    ck(cudaGetLastError(), "leaf bfs");
+    ck(cudaStreamSynchronize(st), "sync");
+    for (int l = 1; l <= h->H && !cur.empty(); ++l) {
+        Level& Lv = h->L[l];
+        Level& Lc = h->L[l - 1];
+        std::vector<int> parents;
+        std::vector<uint8_t> seen(Lv.nnodes, 0);
+        for (int c : cur) {
+            const int p = (c / Lc.nodes_x / g) * Lv.nodes_x + (c % Lc.nodes_x) / g;
+            if (!seen[p]) { seen[p] = 1; parents.push_back(p); }
+        }
+        const int n = (int)parents.size();
+        const bool track = !propagate_all && l < h->H;  // does the next level depend on S_U changes?
+        std::vector<hb::Slot> hs;
+        if (track) {
+            hs.resize(n);
+            for (int i = 0; i < n; ++i) hs[i] = level_slot(Lv, nullptr, parents[i], 0, 0);
+            slots.reserve(n);
+            ck(cudaMemcpyAsync(slots.p, hs.data(), n * sizeof(hb::Slot), cudaMemcpyHostToDevice, st), "slots");
+            h->u.snap.reserve((size_t)n * Lv.nExt * Lv.nExt);
+            hb::launch_ext_snapshot(slots.p, n, Lv.d_ext.p, Lv.nExt, Lv.NP, h->u.snap.p, st);
+            ck(cudaGetLastError(), "snapshot");
+        }
+        list.reserve(n);
+        ck(cudaMemcpyAsync(list.p, parents.data(), n * sizeof(int), cudaMemcpyHostToDevice, st), "list");
+        hb::launch_node_init(Lv.ms(), Lc.ms(), Lc.d_ext.p, Lv.nP, g, Lv.nodes_x, Lc.nodes_x, n, st, list.p);
+        ck(cudaGetLastError(), "node init");
+        hb::launch_seams_build(Lv.ms(), Lv.d_seams.p, Lv.nseams, h->pass.p, S, Lv.side, Lv.nodes_x, n, Lv.kflag.p,
+                               st, list.p);
+        ck(cudaGetLastError(), "seams build");
+        close_matrices(h, Lv, parents);
+        if (track) {
+            changed.reserve(n);
+            ck(cudaMemsetAsync(changed.p, 0, n, st), "changed");
+            hb::launch_ext_compare(slots.p, n, Lv.d_ext.p, Lv.nExt, Lv.NP, h->u.snap.p, changed.p, g, st, 1);
+            ck(cudaGetLastError(), "compare");
+            std::vector<uint8_t> ch(n);
+            ck(cudaMemcpyAsync(ch.data(), changed.p, n, cudaMemcpyDeviceToHost, st), "changed d2h");
+            ck(cudaStreamSynchronize(st), "sync");
+            std::vector<int> next;
+            for (int i = 0; i < n; ++i)
+                if (ch[i]) next.push_back(parents[i]);
+            cur = std::move(next);
+        } else {
+            ck(cudaStreamSynchronize(st), "sync");
+            cur = std::move(parents);
+        }
+    }
+    list.release();
+    slots.release();
+    changed.release();
+}
+
+// ---------------------------------------------------------------------------
 // Batched opening (reference onBatchCellsOpened, minplus_oracle.cpp:530-729)
 // ---------------------------------------------------------------------------
 int find_lca_level(const htrip_index* h, int r1, int c1, int r2, int c2) {
@@ -1411,6 +1500,31 @@ htrip_status htrip_build(htrip_index* h, const uint8_t* observed, int32_t rows, 
     HTRIP_GUARD_BEGIN
     ck(cudaSetDevice(h->device), "cudaSetDevice");
     do_build(h, observed, rows, cols);
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_cell_blocked(htrip_index* h, int32_t r, int32_t c, const uint8_t* observed, int32_t rows,
+                                int32_t cols) {
+    if (!h || !observed) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    if (const htrip_status rs = ready(h)) return rs;
+    if (r < 0 || c < 0 || r >= h->S || c >= h->S) return HTRIP_OK;  // minplus_oracle.cpp:251 (outside: ignored)
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    do_rebuild_leaves(h, {(r / h->b) * h->leaves_x + c / h->b}, observed, rows, cols, true);
+    h->epoch++;  // minplus_oracle.cpp:300-301
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_leaves_changed(htrip_index* h, const int32_t* leaves, int32_t n, const uint8_t* observed,
+                                  int32_t rows, int32_t cols) {
+    if (!h || !observed || n < 0 || (n > 0 && !leaves)) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    if (const htrip_status rs = ready(h)) return rs;
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    do_rebuild_leaves(h, std::vector<int>(leaves, leaves + n), observed, rows, cols, false);
+    h->epoch++;  // propagateBatchUpward ends with epoch++ (minplus_oracle.cpp:504)
     return HTRIP_OK;
     HTRIP_GUARD_END
 }

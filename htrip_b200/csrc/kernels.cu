@@ -442,9 +442,19 @@ __global__ void ext_snapshot_kernel(const Slot* __restrict__ S, const int* __res
 // clears its children's decrease flags, which its insert stage has consumed:
 // outside an opening call all decrease flags are zero.
 __global__ void ext_compare_kernel(const Slot* __restrict__ S, const int* __restrict__ ext, int nExt, int NP,
-                                   const uint16_t* __restrict__ snap, uint8_t* slot_dec, int g) {
+                                   const uint16_t* __restrict__ snap, uint8_t* slot_dec, int g, int any_change) {
     const int slot = blockIdx.y;
     const Slot& sl = S[slot];
+    if (any_change) {  // rebuilds: slot_dec[slot] = 1 when any exterior entry differs, nothing else
+        const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+        bool d = false;
+        if (idx < (size_t)nExt * nExt) {
+            const int a = (int)(idx / nExt), c = (int)(idx % nExt);
+            d = sl.mat[(size_t)ext[a] * NP + ext[c]] != snap[(size_t)slot * nExt * nExt + idx];
+        }
+        if (__any_sync(FULL, d) && (threadIdx.x & 31) == 0) slot_dec[slot] = 1;
+        return;
+    }
     if (sl.child_dec && blockIdx.x == 0 && threadIdx.x < g * g) {
         const int q = threadIdx.x;
         const int tx = sl.node % sl.nodes_x, ty = sl.node / sl.nodes_x;
@@ -641,11 +651,11 @@ void launch_ext_snapshot(const Slot* S, int n, const int* ext, int nExt, int NP,
 }
 
 void launch_ext_compare(const Slot* S, int n, const int* ext, int nExt, int NP, const uint16_t* snap,
-                        uint8_t* slot_dec, int g, cudaStream_t st) {
+                        uint8_t* slot_dec, int g, cudaStream_t st, int any_change) {
     for (int y0 = 0; y0 < n; y0 += kMaxGridY) {
         dim3 grid(blocks_for((size_t)nExt * nExt, 256), std::min(kMaxGridY, n - y0));
         ext_compare_kernel<<<grid, 256, 0, st>>>(S + y0, ext, nExt, NP, snap + (size_t)y0 * nExt * nExt,
-                                                 slot_dec + y0, g);
+                                                 slot_dec + y0, g, any_change);
     }
 }
 

@@ -85,10 +85,11 @@ void launch_node_seams(const Slot* S, int n, const int* seams, int NP, cudaStrea
 // S_U): snap holds nExt*nExt entries per slot; compare sets *dec and
 // slot_dec[slot] when any entry decreased (refreshBoundarySummary,
 // leaf_tile.cpp:253-273, internal_node.cpp:415-433) and clears the node
-// slots' children's decrease flags.
+// slots' children's decrease flags.  With any_change != 0 (rebuilds) it only
+// sets slot_dec[slot] when any exterior entry differs from the snapshot.
 void launch_ext_snapshot(const Slot* S, int n, const int* ext, int nExt, int NP, uint16_t* snap, cudaStream_t st);
 void launch_ext_compare(const Slot* S, int n, const int* ext, int nExt, int NP, const uint16_t* snap,
-                        uint8_t* slot_dec, int g, cudaStream_t st);
+                        uint8_t* slot_dec, int g, cudaStream_t st, int any_change = 0);
 
 // --- query (query.cu) -------------------------------------------------------
 constexpr int kMaxQueryLevels = 16;

@@ -149,6 +149,22 @@ void MinPlusOracle::onBatchCellsOpened(const std::vector<Point>& newly_opened, c
     last_batch_stats = {st.n_touched_leaves, st.n_dirty_ancestors, st.n_pivots};
 }
 
+void MinPlusOracle::onCellBlocked(Point p, const GridMap& grid) {
+    if (!built_) return;
+    ++update_counter;
+    check(htrip_cell_blocked(h_, p.r, p.c, grid.observedBytes(), grid.rows, grid.cols), "onCellBlocked");
+    ++epoch;  // reference minplus_oracle.cpp:300-301
+}
+
+void MinPlusOracle::onBatchLeavesChanged(const std::vector<int>& leaf_indices, const GridMap& grid) {
+    if (!built_ || leaf_indices.empty()) return;
+    ++update_counter;
+    std::vector<int32_t> li(leaf_indices.begin(), leaf_indices.end());
+    check(htrip_leaves_changed(h_, li.data(), int32_t(li.size()), grid.observedBytes(), grid.rows, grid.cols),
+          "onBatchLeavesChanged");
+    ++epoch;  // reference propagateBatchUpward, minplus_oracle.cpp:504
+}
+
 void MinPlusOracle::queryAllPairs(const std::vector<Point>& viewpoints, const GridMap& grid,
                                   std::vector<dist_t>& out_matrix, HTripQueryScratch& scratch) const {
     const size_t k = viewpoints.size();

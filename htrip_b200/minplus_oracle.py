@@ -86,7 +86,8 @@ EXPORTS = (
     "htrip_measure_minplus_rate", "htrip_last_query_phases", "htrip_batch_last_phases", "htrip_last_open_work",
     "htrip_autotune_query", "htrip_autotune_export", "htrip_autotune_import", "htrip_autotune_clear",
     "htrip_lift_root", "htrip_query_distance", "htrip_incremental_create", "htrip_incremental_destroy",
-    "htrip_query_all_pairs_incremental", "htrip_batch_create_priority",
+    "htrip_query_all_pairs_incremental", "htrip_batch_create_priority", "htrip_cell_blocked",
+    "htrip_leaves_changed",
 )
 
 
@@ -141,6 +142,8 @@ def load_library(path: str | None = None):
     lib.htrip_autotune_import.argtypes = [C.c_char_p]
     lib.htrip_autotune_clear.argtypes = []
     lib.htrip_lift_root.argtypes = [P, _U8P, I, I]
+    lib.htrip_cell_blocked.argtypes = [P, I, I, _U8P, I, I]
+    lib.htrip_leaves_changed.argtypes = [P, _I32P, I, _U8P, I, I]
     lib.htrip_query_distance.argtypes = [P, I, I, I, I, _U8P, I, I, _U16P]
     lib.htrip_incremental_create.argtypes = [C.POINTER(P)]
     lib.htrip_incremental_destroy.argtypes = [P]
@@ -306,6 +309,17 @@ class MinPlusOracle:
     def onCellOpened(self, p, grid):
         obs, ptr, rows, cols = _grid_args(grid)
         _check(self.lib.htrip_open_cell(self.h, int(p[0]), int(p[1]), ptr, rows, cols))
+
+    def onCellBlocked(self, p, grid):
+        """Reference onCellBlocked (the caller has made p non-Free in grid)."""
+        obs, ptr, rows, cols = _grid_args(grid)
+        _check(self.lib.htrip_cell_blocked(self.h, int(p[0]), int(p[1]), ptr, rows, cols))
+
+    def onBatchLeavesChanged(self, leaf_indices, grid):
+        """Reference onBatchLeavesChanged: rebuild these leaves and their ancestors."""
+        li = np.ascontiguousarray(np.asarray(leaf_indices, dtype=np.int32).ravel())
+        obs, ptr, rows, cols = _grid_args(grid)
+        _check(self.lib.htrip_leaves_changed(self.h, li.ctypes.data_as(_I32P), len(li), ptr, rows, cols))
 
     def liftRoot(self, grid=None):
         """Grow the index to S*g, H+1 (reference liftRoot); grid None = the

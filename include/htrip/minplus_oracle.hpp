@@ -12,6 +12,9 @@
 //   void onCellOpened(Point, const GridMap&)             :109
 //   void onBatchCellsOpened(const std::vector<Point>&,
 //                           const GridMap&)              :171
+//   void onCellBlocked(Point, const GridMap&)            :123
+//   void onBatchLeavesChanged(const std::vector<int>&,
+//                             const GridMap&)            :157
 //   struct HTripQueryScratch (caller-owned, reused)      :189-238
 //   struct LastBatchStats / last_batch_stats             :251-256
 //   void queryAllPairs(vps, grid, out, scratch) const    :337-341
@@ -121,6 +124,10 @@ public:
     // reference's single-cell path does.
     void onCellOpened(Point p, const GridMap& grid);
     void onBatchCellsOpened(const std::vector<Point>& newly_opened, const GridMap& grid);
+    // Non-monotone updates: the caller has made the cell(s) non-Free in
+    // grid.observed; the leaf (leaves) and every ancestor are rebuilt.
+    void onCellBlocked(Point p, const GridMap& grid);
+    void onBatchLeavesChanged(const std::vector<int>& leaf_indices, const GridMap& grid);
 
     // k x k row-major matrix of exact 4-connected distances (INF when
     // unreachable), resized and filled by the call.

@@ -87,6 +87,21 @@ htrip_status htrip_open_cells(htrip_index* h, const int32_t* rc, int32_t n,
 htrip_status htrip_open_cell(htrip_index* h, int32_t r, int32_t c,
                              const uint8_t* observed, int32_t rows, int32_t cols);
 
+/* void onCellBlocked(Point, const GridMap&)    minplus_oracle.hpp:123
+ * The caller has already made the cell non-Free in `observed`.  Its leaf is
+ * rebuilt from the grid and every ancestor from its children and seams, up
+ * to the root (distances may grow: a non-monotone update).  Cells outside
+ * the index are ignored.                                                  */
+htrip_status htrip_cell_blocked(htrip_index* h, int32_t r, int32_t c, const uint8_t* observed, int32_t rows,
+                                int32_t cols);
+
+/* void onBatchLeavesChanged(const std::vector<int>& leaves, const GridMap&)
+ *                                              minplus_oracle.hpp:157
+ * Rebuilds the listed leaves (row-major leaf indices; others ignored) from
+ * the grid and their ancestors, each dirty ancestor once per level.       */
+htrip_status htrip_leaves_changed(htrip_index* h, const int32_t* leaves, int32_t n, const uint8_t* observed,
+                                  int32_t rows, int32_t cols);
+
 /* void liftRoot(const GridMap& grid)          minplus_oracle.hpp:380
  * Grows the index: S -> S*g, H -> H+1.  Existing leaves and nodes keep
  * their matrices; leaves and nodes of the new area, and the new root, are

@@ -58,6 +58,8 @@ def _load_ref():
         lib.ref_open_batch.argtypes = [_P, _I32P, _I]
         lib.ref_open_cell.argtypes = [_P, _I, _I]
         lib.ref_lift_root.argtypes = [_P]
+        lib.ref_cell_blocked.argtypes = [_P, _I, _I]
+        lib.ref_leaves_changed.argtypes = [_P, _I32P, _I]
         lib.ref_query_distance.restype = _I
         lib.ref_query_distance.argtypes = [_P, _I, _I, _I, _I]
         lib.ref_query_incremental.argtypes = [_P, _I32P, _I, _U16P]
@@ -134,6 +136,13 @@ class RefOracle:
         out = np.empty((len(rc), len(rc)), dtype=np.uint16)
         self.lib.ref_query_incremental(self.h, _p(rc, _I32P), len(rc), _p(out, _U16P))
         return out
+
+    def cell_blocked(self, r: int, c: int):
+        self.lib.ref_cell_blocked(self.h, int(r), int(c))
+
+    def leaves_changed(self, leaves):
+        li = np.ascontiguousarray(np.asarray(leaves, dtype=np.int32).ravel())
+        self.lib.ref_leaves_changed(self.h, _p(li, _I32P), len(li))
 
     def lift_root(self):
         """MinPlusOracle::liftRoot with the handle's current grid."""

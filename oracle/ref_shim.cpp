@@ -102,6 +102,17 @@ void ref_query_incremental(void* p, const int32_t* rc, int k, uint16_t* out) {
     std::memcpy(out, m.data(), m.size() * sizeof(dist_t));
 }
 
+// MinPlusOracle::onCellBlocked(p, grid) (minplus_oracle.hpp:123) and
+// onBatchLeavesChanged(leaves, grid) (:157) with the handle's current grid.
+void ref_cell_blocked(void* p, int r, int c) {
+    auto* h = static_cast<RefHandle*>(p);
+    h->oracle.onCellBlocked(Point{r, c}, h->grid);
+}
+void ref_leaves_changed(void* p, const int32_t* leaves, int n) {
+    auto* h = static_cast<RefHandle*>(p);
+    h->oracle.onBatchLeavesChanged(std::vector<int>(leaves, leaves + n), h->grid);
+}
+
 // MinPlusOracle::liftRoot(grid) with the handle's current grid
 // (minplus_oracle.hpp:380); an empty grid stands for the default argument.
 void ref_lift_root(void* p) {

@@ -123,3 +123,50 @@ def test_incremental_query_equals_reference_and_full(gpu):
     m = dev.queryAllPairsIncremental(vps2, obs, state)
     assert state.last_recomputed
     np.testing.assert_array_equal(m, ref.query_incremental(vps2))
+
+
+BLOCK_CASES = [("rooms", 32, 8, 2, 21), ("street", 64, 16, 2, 22), ("noise", 64, 4, 4, 23), ("maze", 64, 8, 2, 24),
+               ("noise", 16, 16, 2, 25)]
+
+
+@pytest.mark.parametrize("kind,side,b,g,seed", BLOCK_CASES)
+def test_blockages_match_reference(gpu, kind, side, b, g, seed):
+    """onCellBlocked (Suite 6, test_exactness.cpp:473-497, blockages) and
+    onBatchLeavesChanged against the reference: state, queries, BFS."""
+    truth = make_grid(kind, side, side, seed)
+    obs, cells = W.withheld_open(truth, side * side // 10, seed)
+    ref, dev = _both(obs, b, g)
+    obs[cells[:, 0], cells[:, 1]] = W.FREE          # open first, then block some cells
+    ref.set_cells(cells, W.FREE)
+    ref.open_batch(cells)
+    dev.onBatchCellsOpened(cells, obs)
+    rng = np.random.default_rng(seed)
+    free = np.argwhere(obs == W.FREE)
+    for p in free[rng.choice(len(free), size=4, replace=False)]:
+        obs[p[0], p[1]] = W.OBSTACLE
+        ref.set_cells([p], W.OBSTACLE)
+        ref.cell_blocked(p[0], p[1])
+        dev.onCellBlocked(p, obs)
+        assert dev.stateDigest() == ref.digest()
+        vps = viewpoints(obs, 16, int(p[0]) * 7 + 1, include_blocked=1)
+        np.testing.assert_array_equal(dev.queryAllPairs(vps, obs), ref.query(vps))
+        np.testing.assert_array_equal(dev.queryAllPairs(vps, obs), ref.bfs(vps))
+    # several leaves at once
+    lx = dev.num_leaf_tiles_x
+    picks = free[rng.choice(len(free), size=6, replace=False)]
+    obs[picks[:, 0], picks[:, 1]] = W.OBSTACLE
+    ref.set_cells(picks, W.OBSTACLE)
+    leaves = sorted({int(r) // b * lx + int(c) // b for r, c in picks})
+    ref.leaves_changed(leaves)
+    dev.onBatchLeavesChanged(leaves, obs)
+    assert dev.stateDigest() == ref.digest()
+    vps = viewpoints(obs, 16, seed + 5)
+    np.testing.assert_array_equal(dev.queryAllPairs(vps, obs), ref.bfs(vps))
+    # openings after blockages still match
+    reopen = picks[:3]
+    obs[reopen[:, 0], reopen[:, 1]] = W.FREE
+    ref.set_cells(reopen, W.FREE)
+    ref.open_batch(reopen)
+    dev.onBatchCellsOpened(reopen, obs)
+    assert dev.stateDigest() == ref.digest()
+    np.testing.assert_array_equal(dev.queryAllPairs(vps, obs), ref.query(vps))
