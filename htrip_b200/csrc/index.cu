@@ -1965,6 +1965,20 @@ htrip_status htrip_state_digest(const htrip_index* h, uint64_t* out, int32_t n_o
     HTRIP_GUARD_END
 }
 
+htrip_status htrip_selftest_barrier_timeout(int device, int32_t* status, int32_t* ctas_returned, float* ms) {
+    if (!status || !ctas_returned || !ms) return fail(HTRIP_ERR_INVALID, "null argument");
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    int st = 0, ret = 0;
+    float t = 0.f;
+    ck(hb::barrier_timeout_selftest(&st, &ret, &t), "barrier self-test");
+    *status = st;
+    *ctas_returned = ret;
+    *ms = t;
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
 htrip_status htrip_measure_minplus_rate(int device, int variant, double* entries_per_s) {
     if (!entries_per_s || variant < 0 || variant > 4) return fail(HTRIP_ERR_INVALID, "bad arguments");
     HTRIP_GUARD_BEGIN

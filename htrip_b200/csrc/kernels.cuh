@@ -164,6 +164,10 @@ constexpr int kMaxQueryPhases = kMaxQueryLevels + 3;
 // Cooperative launch of the persistent query kernel on `grid` blocks.
 int query_grid_blocks(int device);
 int query_max_ports();  // largest per-child port count the query kernel handles
+// Runs a 4-CTA launch whose grid barrier can never complete (it expects a
+// fifth CTA) with a short poll limit: *status is the status word the
+// timeout sets (1), *returned the number of CTAs that returned (4).
+cudaError_t barrier_timeout_selftest(int* status, int* returned, float* ms);
 cudaError_t launch_query(const QueryLaunch& L, int cfg, int grid, cudaStream_t st);
 
 // *out += canonical checksum of the first `count` matrices of M (logical

@@ -235,9 +235,10 @@ __device__ __forceinline__ void cta_reduce(uint32_t (&acc)[RW][CP], uint32_t* re
         for (int c = 0; c < CP; ++c) acc[r][c] = red[(r * CP + c) * 32 + lane];
 }
 
-// Grid barrier with a bounded spin; a timeout sets *status and the kernel
-// finishes without waiting further (the host reports the error).
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* status) {
+// Grid barrier over `expected` CTAs with a bounded spin (`limit` polls); a
+// timeout sets *status and the kernel finishes without waiting further (the
+// host reports the error).
+__device__ __forceinline__ bool grid_barrier_n(unsigned* bar, int* status, unsigned expected, unsigned limit) {
     __syncthreads();
     bool ok = true;
     if (threadIdx.x == 0) {
@@ -245,14 +246,14 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* status) {
         const unsigned gen = *vgen;
         __threadfence();
         const unsigned arrived = atomicAdd(bar, 1u);
-        if (arrived == gridDim.x - 1) {
+        if (arrived == expected - 1) {
             atomicExch(bar, 0u);
             __threadfence();
             atomicAdd(bar + 1, 1u);
         } else {
             unsigned it = 0;
             while (*vgen == gen) {
-                if (++it > (1u << 24)) {
+                if (++it > limit) {
                     atomicExch(status, 1);
                     ok = false;
                     break;
@@ -264,6 +265,18 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* status) {
     }
     __syncthreads();
     return ok && *(volatile int*)status == 0;
+}
+
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* status) {
+    return grid_barrier_n(bar, status, gridDim.x, 1u << 24);
+}
+
+// Self-test of the bounded wait: a barrier that expects one CTA more than the
+// launch has can never complete, so every CTA gives up after `limit` polls,
+// records the timeout in *status and returns.
+__global__ void barrier_timeout_probe_kernel(unsigned* bar, int* status, unsigned limit, int* returned) {
+    grid_barrier_n(bar, status, gridDim.x + 1, limit);
+    if (threadIdx.x == 0) atomicAdd(returned, 1);
 }
 
 __device__ __forceinline__ unsigned long long global_timer() {
@@ -520,6 +533,30 @@ void configure_query_kernels() {
 }  // namespace
 
 int query_max_ports() { return kMaxList - 64; }
+
+cudaError_t barrier_timeout_selftest(int* status, int* returned, float* ms) {
+    // words: {status, barrier count, barrier generation, CTAs returned}
+    unsigned* w = nullptr;
+    cudaError_t e = cudaMalloc(&w, 4 * sizeof(unsigned));
+    if (e != cudaSuccess) return e;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaMemset(w, 0, 4 * sizeof(unsigned));
+    cudaEventRecord(e0);
+    barrier_timeout_probe_kernel<<<4, 64>>>(w + 1, reinterpret_cast<int*>(w), 1u << 14, reinterpret_cast<int*>(w + 3));
+    cudaEventRecord(e1);
+    e = cudaEventSynchronize(e1);
+    unsigned h[4] = {0, 0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpy(h, w, sizeof(h), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) cudaEventElapsedTime(ms, e0, e1);
+    *status = (int)h[0];
+    *returned = (int)h[3];
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(w);
+    return e;
+}
 
 int query_grid_blocks(int device) {
     configure_query_kernels();

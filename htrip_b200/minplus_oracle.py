@@ -87,7 +87,7 @@ EXPORTS = (
     "htrip_autotune_query", "htrip_autotune_export", "htrip_autotune_import", "htrip_autotune_clear",
     "htrip_lift_root", "htrip_query_distance", "htrip_incremental_create", "htrip_incremental_destroy",
     "htrip_query_all_pairs_incremental", "htrip_batch_create_priority", "htrip_cell_blocked",
-    "htrip_leaves_changed",
+    "htrip_leaves_changed", "htrip_selftest_barrier_timeout",
 )
 
 
@@ -143,6 +143,7 @@ def load_library(path: str | None = None):
     lib.htrip_autotune_clear.argtypes = []
     lib.htrip_lift_root.argtypes = [P, _U8P, I, I]
     lib.htrip_cell_blocked.argtypes = [P, I, I, _U8P, I, I]
+    lib.htrip_selftest_barrier_timeout.argtypes = [C.c_int, _I32P, _I32P, C.POINTER(C.c_float)]
     lib.htrip_leaves_changed.argtypes = [P, _I32P, I, _U8P, I, I]
     lib.htrip_query_distance.argtypes = [P, I, I, I, I, _U8P, I, I, _U16P]
     lib.htrip_incremental_create.argtypes = [C.POINTER(P)]
@@ -598,6 +599,14 @@ def autotune_import(text: str):
 
 def autotune_clear():
     _check(load_library().htrip_autotune_clear())
+
+
+def selftest_barrier_timeout(device: int = 0):
+    """(status, CTAs returned, ms) of a grid barrier that cannot complete."""
+    lib = load_library()
+    st, ret, ms = C.c_int32(), C.c_int32(), C.c_float()
+    _check(lib.htrip_selftest_barrier_timeout(device, C.byref(st), C.byref(ret), C.byref(ms)))
+    return st.value, ret.value, ms.value
 
 
 def minplus_rate(device: int = 0, variant: int = 0) -> float:

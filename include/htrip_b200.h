@@ -341,6 +341,15 @@ htrip_status htrip_last_open_work(const htrip_index* h, uint64_t* alg_bytes, uin
 htrip_status htrip_last_query_phases(const htrip_index* h, uint64_t* ns, int32_t max_n, int32_t* n);
 htrip_status htrip_batch_last_phases(const htrip_batch* b, uint64_t* ns, int32_t max_n, int32_t* n);
 
+/* Failure-detection self-test (no reference counterpart).  Every wait in
+ * the query kernel's grid barrier is bounded: after a poll limit the CTA
+ * records a timeout in the launch's status word and returns, and the host
+ * call fails with HTRIP_ERR_CUDA while the context stays usable.  This runs
+ * a 4-CTA launch of the same barrier that can never complete (it expects a
+ * fifth CTA) with a short limit: *status = 1 (timeout recorded),
+ * *ctas_returned = 4, *ms = the launch's duration.                        */
+htrip_status htrip_selftest_barrier_timeout(int device, int32_t* status, int32_t* ctas_returned, float* ms);
+
 /* Wait for all work queued on the index's stream.                         */
 htrip_status htrip_sync(htrip_index* h);
 
