@@ -215,27 +215,32 @@ def bench_opening(device, steps=400):
     build_s = time.perf_counter() - t
     open_ms, query_ms, cells, entries = [], [], 0, 0
     ops = nbytes = 0
+    warm = 10  # the stream's first calls grow the scratch arenas and load the kernels: untimed
     for step, c in enumerate(batches):
         obs[c[:, 0], c[:, 1]] = W.FREE
         t = time.perf_counter()
         dev.onBatchCellsOpened(c, obs)
-        open_ms.append(1e3 * (time.perf_counter() - t))
+        ms = 1e3 * (time.perf_counter() - t)
+        vps = np.concatenate([starts, W.frontier_cells(obs, 48, 1000 + step)]).astype(np.int32)
+        t = time.perf_counter()
+        dev.queryAllPairs(vps, obs)
+        qms = 1e3 * (time.perf_counter() - t)
+        if step < warm:
+            continue
+        open_ms.append(ms)
+        query_ms.append(qms)
         b_, o_ = dev.lastOpenWork()
         ops += o_
         nbytes += b_
         cells += len(c)
-        vps = np.concatenate([starts, W.frontier_cells(obs, 48, 1000 + step)]).astype(np.int32)
-        t = time.perf_counter()
-        dev.queryAllPairs(vps, obs)
-        query_ms.append(1e3 * (time.perf_counter() - t))
         entries += len(vps) ** 2
     fresh = MinPlusOracle(HierarchyConfig(8, 2, 2), device=device)
     assert fresh.build(obs)
     parity = "bit-exact" if fresh.stateDigest() == dev.stateDigest() else "MISMATCH"
     out = {"workload": f"1024x1024 street, b=8, {len(batches)} onBatchCellsOpened x 256 cells (BFS rings), "
-                       "each + queryAllPairs k=64",
+                       f"each + queryAllPairs k=64; the first {warm} calls untimed",
            "cells_per_s": cells / (1e-3 * sum(open_ms)), "unit": "cells/s",
-           "alg_minplus_ops_per_call": ops / len(batches), "alg_bytes_per_call": nbytes / len(batches),
+           "alg_minplus_ops_per_call": ops / len(open_ms), "alg_bytes_per_call": nbytes / len(open_ms),
            "achieved_t_minplus_per_s": ops / (1e-3 * sum(open_ms)) / 1e12,
            "achieved_gb_per_s": nbytes / (1e-3 * sum(open_ms)) / 1e9,
            "open_ms_p50": _pct(open_ms, 50), "open_ms_p99": _pct(open_ms, 99),
@@ -559,7 +564,7 @@ def run_ours(args, rank, world, local_rank):
                                "peak_source": "measured (htrip_measure_minplus_rate, clamped packed-u16 update)"}},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
-        "gpu_launches": args.steps,
+        "gpu_launches": 2 * args.steps,  # per step: the planner (with the presets) and the query kernel
         "parity": parity,
     }
     if world == 1 and not args.headline_only:

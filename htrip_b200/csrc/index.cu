@@ -15,7 +15,9 @@
 #include <algorithm>
 #include <map>
 #include <tuple>
+#include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <exception>
@@ -150,10 +152,27 @@ struct QueryArena {
     uint64_t last_h2d = 0, last_d2h = 0;
     size_t last_words = 0;  // arena offset of the last launch's words
     int last_phases = 0;
+    // device-planned queries: host-mapped record the planner writes (one
+    // 8-byte word: seq << 32 | status << 26 | viewpoints << 13 | largest root
+    // child group), the sequence number of the last planned call and the
+    // tile hint taken from it
+    int* info = nullptr;
+    int* info_dev = nullptr;
+    int plan_seq = 0, info_k_last = 0;
+    int hint_k = 0, hint_ns = 0, hint_group = 0;
+    // ticket counter of the planner's blocks and its value after the last
+    // planned launch
+    DevBuf<unsigned> ticket;
+    unsigned ticket_next = 0;
     void release() {
         dev.release();
         stage.release();
         outstage.release();
+        ticket.release();
+        ticket_next = 0;
+        if (info) cudaFreeHost(info);
+        info = info_dev = nullptr;
+        plan_seq = hint_k = 0;
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         ev[0] = ev[1] = nullptr;
@@ -1394,6 +1413,300 @@ int choose_query_cfg(const htrip_index* h, int ns, int root_group) {
 }
 
 // ---------------------------------------------------------------------------
+// Device-planned queries (plan.cu).  A single request on an index's own
+// stream is planned by the device from its viewpoints, so nothing on the host
+// waits for the GPU before the launch: a query with device-resident inputs
+// is two launches (planner, query kernel) and no copy.  Arena layout, every
+// piece 256-byte aligned:
+//   [QueryParams][unit prefix][launch words][viewpoints 8k + flags k]
+//   [plan ints][M][flags][X0 X1 X2 Y0 Y1][result k*k u16, host-bound calls]
+// The plan capacities are worst cases for k viewpoints, so the planner's
+// overflow status (2) is a guard, not a path: a synchronous call that sees
+// it replans on the host.
+// ---------------------------------------------------------------------------
+struct DevPlanLayout {
+    hb::PlanGeom G{};
+    hb::PlanLayout O{};
+    size_t o_params = 0, o_pre = 0, o_words = 0, o_in = 0, o_plan = 0, o_M = 0, o_flags = 0, o_out = 0;
+    size_t X[3] = {}, Y[2] = {}, total = 0;
+    int n_phases = 0, fill_blocks = 1;
+};
+
+// Whether the device planner takes a request.  It can: k within its
+// shared-memory sort, Morton codes below 2^52 (they carry the viewpoint index
+// in the low 12 bits), and the query kernel's depth and port limits.  It
+// does, by default, when the viewpoints are already on the device (the host
+// would otherwise wait for their copy); with host viewpoints the host plans
+// (its plan goes out with the viewpoints' copy anyway, and measured faster).
+// HTRIP_QUERY_PLANNER=host plans every query on the host, =device every
+// query it can on the device.
+bool devplan_supported(const htrip_index* h, int k, bool host_inputs) {
+    if (k < 1 || k > hb::plan_max_k() || h->H > hb::kMaxQueryLevels) return false;
+    static const int mode = [] {
+        const char* e = std::getenv("HTRIP_QUERY_PLANNER");
+        if (e && std::strcmp(e, "host") == 0) return 1;
+        if (e && std::strcmp(e, "device") == 0) return 2;
+        return 0;
+    }();
+    if (mode == 1 || (mode == 0 && host_inputs)) return false;
+    double codes = 1;
+    for (int l = 0; l < std::max(h->H, 1); ++l) codes *= (double)h->g * h->g;
+    if (codes >= 4503599627370496.0) return false;  // 2^52
+    for (int l = 1; l <= h->H; ++l)
+        if (h->L[l].nP > hb::query_max_ports()) return false;
+    return true;
+}
+
+DevPlanLayout devplan_layout(const htrip_index* h, int k, int cfg, bool out_in_arena) {
+    DevPlanLayout D;
+    const hb::QueryTile tile = hb::query_config_tile(cfg);
+    const long RW = tile.RW, NC = tile.NCOL;
+    const int H = h->H, g = h->g;
+    hb::PlanGeom& G = D.G;
+    hb::PlanLayout& O = D.O;
+    G.H = H;
+    G.g = g;
+    G.b = h->b;
+    G.S = h->S;
+    G.leaves_x = h->leaves_x;
+    G.RW = (int)RW;
+    G.NC = (int)NC;
+    G.nExt0 = h->L[0].nExt;
+    auto log2_exact = [](int v) {
+        int sh = 0;
+        while ((1 << sh) < v) ++sh;
+        return (1 << sh) == v ? sh : -1;
+    };
+    G.g_shift = log2_exact(g);
+    G.b_shift = log2_exact(h->b);
+    for (int l = 0; l <= H; ++l) {
+        G.side[l] = h->L[l].side;
+        G.nodes_x[l] = h->L[l].nodes_x;
+        G.nP[l] = h->L[l].nP;
+        G.NP[l] = h->L[l].NP;
+    }
+    O.k = k;
+    O.kpow = hb::plan_kpow(k);
+    O.sort_bytes = hb::plan_sort_bytes(O.kpow);
+    // plan ints; pieces start on 64-int boundaries
+    size_t n = 0;
+    auto take = [&](size_t ints) {
+        const size_t o = n;
+        n += (ints + 63) / 64 * 64;
+        return (int)o;
+    };
+    long max_slots = k;
+    size_t flags = 0;
+    for (int l = 1; l <= H; ++l) {
+        O.flags_off[l] = (long long)flags;
+        // groups: distinct level-(l-1) nodes holding a viewpoint; slots: each
+        // group's run padded to RW; a node's run spans at most g^2 groups
+        const long ngr = std::min<long>(k, h->L[l - 1].nnodes);
+        const long slots = k + ngr * (RW - 1);
+        const long rows = (slots + RW - 1) / RW;
+        const long span = std::min<long>(slots, k + (long)g * g * (RW - 1));
+        const long NP = h->L[l].NP;
+        O.cap_groups[l] = (int)ngr;
+        O.cap_slots[l] = (int)slots;
+        O.cap_items[l] = (int)(rows * ((NP + NC - 1) / NC));
+        // meet base items: per group, ceil(span / NC) slot tiles x its row
+        // tiles; the port split adds at most kPlanTargetItems
+        O.cap_meet[l] = (int)(((span + NC - 1) / NC + 1) * rows + hb::kPlanTargetItems);
+        max_slots = std::max(max_slots, slots);
+        flags += (size_t)ngr * h->L[l].nP;
+    }
+    O.o_vp0 = take(4 * (size_t)k);
+    O.o_inv = take(k);
+    O.o_rec = take(hb::plan_record_ints());
+    O.o_l0 = take(H >= 1 ? 2 * (size_t)O.cap_slots[1] : 0);
+    for (int l = 1; l <= H; ++l) {
+        O.o_groups[l] = take(5 * (size_t)O.cap_groups[l]);
+        O.o_items[l] = take(3 * (size_t)O.cap_items[l]);
+        O.o_meet[l] = take(7 * (size_t)O.cap_meet[l]);
+        O.o_s2v[l] = take((size_t)O.cap_slots[l] + NC);
+        O.o_lift[l] = l < H ? take(2 * (size_t)O.cap_slots[l]) : 0;
+    }
+    if (n > (size_t)INT32_MAX) throw CudaError{cudaErrorInvalidValue, "device plan larger than 2^31 ints"};
+    O.cap_ldv = (int)((max_slots + 256 + 7) / 8 * 8);
+    size_t off = 0;
+    auto takeb = [&](size_t bytes) {
+        const size_t o = off;
+        off += align256(std::max<size_t>(bytes, 1));
+        return o;
+    };
+    D.n_phases = H + 3;
+    D.o_params = takeb(sizeof(hb::QueryParams));
+    D.o_pre = takeb((size_t)D.n_phases * 2 * sizeof(int));
+    D.o_words = takeb(kWordsBytes);
+    D.o_in = takeb(9 * (size_t)k);
+    D.o_plan = takeb(n * sizeof(int));
+    const size_t ldm = std::max<size_t>(8, ((size_t)k + 7) / 8 * 8);
+    O.M_bytes = (long long)(ldm * ldm * sizeof(uint32_t));
+    D.o_M = takeb((size_t)O.M_bytes);
+    O.flags_bytes = (long long)flags;
+    D.o_flags = takeb(flags);
+    int maxExt = 0, maxNP = 64;
+    for (int l = 0; l <= H; ++l) maxExt = std::max(maxExt, h->L[l].nExt);
+    for (int l = 1; l <= H; ++l) maxNP = std::max(maxNP, h->L[l].NP);
+    for (auto& x : D.X) x = takeb((size_t)maxExt * O.cap_ldv * sizeof(uint16_t));
+    for (auto& y : D.Y) y = takeb((size_t)maxNP * O.cap_ldv * sizeof(uint16_t));
+    D.o_out = out_in_arena ? takeb((size_t)k * k * sizeof(uint16_t)) : 0;
+    D.total = off;
+    O.words_bytes = (int)kWordsBytes;
+    // preset blocks: about 64 KB each, no more than fit beside the planner
+    const size_t smem = hb::plan_smem_bytes(O.kpow);
+    const long most = smem > 113 * 1024 ? 147 : 295;
+    D.fill_blocks = (int)std::clamp<long>((long)((O.M_bytes + O.flags_bytes) >> 16), 1, most);
+    return D;
+}
+
+// Tile of a device-planned call whose viewpoints are on the host: the same
+// inputs the host planner gives choose_query_cfg (passable viewpoints and the
+// largest root child group).
+int devplan_cfg_host(const htrip_index* h, const int32_t* vps, const uint8_t* pf, int k) {
+    const int H = h->H, g = h->g;
+    std::vector<int> cnt((size_t)g * g, 0);
+    int ns = 0;
+    for (int i = 0; i < k; ++i) {
+        if (!pf[i]) continue;
+        ++ns;
+        if (H >= 1) {
+            const int side = h->L[H - 1].side;
+            const int cx = vps[2 * i + 1] / side, cy = vps[2 * i] / side;
+            ++cnt[(size_t)(cy % g) * g + cx % g];
+        }
+    }
+    const int group = H >= 1 ? *std::max_element(cnt.begin(), cnt.end()) : ns;
+    return choose_query_cfg(h, ns, group);
+}
+
+// Tile of a call whose viewpoints are on the device: the last planned call's
+// record when it had the same k and has completed, else an even spread over
+// the root's children.
+int devplan_cfg_hint(htrip_index* h, int k) {
+    QueryArena& A = h->q;
+    if (A.info && A.plan_seq > 0) {
+        // seq << 32 | status << 26 | viewpoints << 13 | largest root child group
+        const uint64_t rec = *reinterpret_cast<const volatile uint64_t*>(A.info);
+        const unsigned lo = (unsigned)rec;
+        if ((int)(rec >> 32) == A.plan_seq && (lo >> 26) == 0) {
+            A.hint_k = A.info_k_last;
+            A.hint_ns = (int)((lo >> 13) & 0x1fff);
+            A.hint_group = (int)(lo & 0x1fff);
+        }
+    }
+    if (A.hint_k == k) return choose_query_cfg(h, A.hint_ns, A.hint_group);
+    const int g2 = h->g * h->g;
+    return choose_query_cfg(h, k, h->H >= 1 ? (k + g2 - 1) / g2 : k);
+}
+
+// One device-planned request on the index's stream.  Viewpoints and flags
+// come from the host (staged and copied in) or from device memory.  The
+// result goes to out_dev (stream-ordered, returns 0), or, with out_dev null,
+// to host_out after a synchronisation; then the return value is the status
+// word (0 ok, 1 grid barrier timeout, 2 plan capacity exceeded).
+int run_devplan(htrip_index* h, int k, int cfg, const int32_t* vps_host, const uint8_t* pf_host,
+                const int32_t* vps_dev, const uint8_t* pf_dev, uint16_t* out_dev, uint16_t* host_out) {
+    check_query_shape(h);
+    QueryArena& A = h->q;
+    cudaStream_t st = h->stream;
+    const bool to_host = out_dev == nullptr;
+    DevPlanLayout D = devplan_layout(h, k, cfg, to_host);
+    if (D.total > A.dev.n) {
+        if (A.ev_valid) ck(cudaEventSynchronize(A.ev[1]), "previous launch");
+        A.dev.reserve(D.total);
+    }
+    if (!A.ev[0]) {
+        ck(cudaEventCreate(&A.ev[0]), "event");
+        ck(cudaEventCreate(&A.ev[1]), "event");
+    }
+    if (!A.ticket.p) {
+        A.ticket.reserve(64);
+        ck(cudaMemsetAsync(A.ticket.p, 0, sizeof(unsigned), st), "ticket");
+        A.ticket_next = 0;
+    }
+    if (!A.info) {
+        ck(cudaHostAlloc(reinterpret_cast<void**>(&A.info), 2 * sizeof(int), cudaHostAllocMapped), "cudaHostAlloc");
+        std::memset(A.info, 0, 2 * sizeof(int));
+        ck(cudaHostGetDevicePointer(reinterpret_cast<void**>(&A.info_dev), A.info, 0), "mapped record");
+    }
+    unsigned char* base = A.dev.p;
+    if (vps_host) {
+        // the staging buffer may still feed an earlier stream-ordered copy
+        if (A.ev_valid) ck(cudaEventSynchronize(A.ev[1]), "previous launch");
+        const size_t nb = 9 * (size_t)k;
+        A.stage.reserve(nb);
+        std::memcpy(A.stage.p, vps_host, 8 * (size_t)k);
+        std::memcpy(A.stage.p + 8 * (size_t)k, pf_host, k);
+        ck(cudaMemcpyAsync(base + D.o_in, A.stage.p, nb, cudaMemcpyHostToDevice, st), "viewpoints");
+        vps_dev = reinterpret_cast<const int32_t*>(base + D.o_in);
+        pf_dev = base + D.o_in + 8 * (size_t)k;
+    }
+    uint16_t* out = to_host ? reinterpret_cast<uint16_t*>(base + D.o_out) : out_dev;
+    // parameter block template: everything the plan does not decide
+    hb::QueryParams T{};
+    T.H = h->H;
+    T.k = k;
+    T.nExt0 = h->L[0].nExt;
+    T.cfg = cfg;
+    T.ext0 = h->L[0].d_ext.p;
+    T.leaves = h->L[0].ms();
+    for (int j = 0; j < 3; ++j) T.X[j] = reinterpret_cast<uint16_t*>(base + D.X[j]);
+    for (int j = 0; j < 2; ++j) T.Y[j] = reinterpret_cast<uint16_t*>(base + D.Y[j]);
+    T.M = reinterpret_cast<uint32_t*>(base + D.o_M);
+    T.out = out;
+    for (int l = 1; l <= h->H; ++l) {
+        const Level& Lv = h->L[l];
+        T.lv[l].D = Lv.mat.p;
+        T.lv[l].NP = Lv.NP;
+        T.lv[l].nP = Lv.nP;
+        T.lv[l].ext_inv = Lv.d_ext_inv.p;
+        T.lv[l].store_y = 1;
+    }
+    hb::PlanLayout& O = D.O;
+    O.plan = reinterpret_cast<int*>(base + D.o_plan);
+    O.params = reinterpret_cast<hb::QueryParams*>(base + D.o_params);
+    O.unit_pre = reinterpret_cast<int*>(base + D.o_pre);
+    O.words = reinterpret_cast<int*>(base + D.o_words);
+    O.M = T.M;
+    O.flags = base + D.o_flags;
+    O.info = A.info_dev;
+    O.seq = ++A.plan_seq;
+    O.ticket = A.ticket.p;
+    O.ticket_base = A.ticket_next;
+    A.info_k_last = k;
+    ck(hb::launch_plan_query(vps_dev, pf_dev, D.G, O, T, D.fill_blocks, st), "query planner");
+    A.ticket_next += (unsigned)std::max(h->H, 1);
+    if (A.grid == 0) A.grid = hb::query_grid_blocks(h->device);
+    hb::QueryLaunch QL;
+    QL.n_req = 1;
+    QL.n_phases = D.n_phases;
+    QL.req = O.params;
+    QL.unit_pre = O.unit_pre;
+    QL.status = O.words;
+    QL.bar = reinterpret_cast<unsigned*>(base + D.o_words) + 1;
+    QL.trace = reinterpret_cast<unsigned long long*>(base + D.o_words + kTraceOffset);
+    ck(cudaEventRecord(A.ev[0], st), "event");
+    ck(hb::launch_query(QL, cfg, A.grid, st), "query kernel");
+    ck(cudaEventRecord(A.ev[1], st), "event");
+    A.ev_valid = true;
+    A.last_words = D.o_words;
+    A.last_phases = D.n_phases;
+    A.last_h2d = vps_host ? 9 * (uint64_t)k : 0;
+    A.last_d2h = 0;
+    if (!to_host) return 0;
+    const size_t ob = (size_t)k * k * sizeof(uint16_t);
+    A.outstage.reserve(align256(ob) + 256);
+    int* status_host = reinterpret_cast<int*>(A.outstage.p + align256(ob));
+    ck(cudaMemcpyAsync(A.outstage.p, out, ob, cudaMemcpyDeviceToHost, st), "result");
+    ck(cudaMemcpyAsync(status_host, O.words, sizeof(int), cudaMemcpyDeviceToHost, st), "status");
+    A.last_d2h = ob + sizeof(int);
+    ck(cudaStreamSynchronize(st), "query sync");
+    if (*status_host == 0) std::memcpy(host_out, A.outstage.p, ob);
+    return *status_host;
+}
+
+// ---------------------------------------------------------------------------
 // Allocation-free query scratch (htrip_query_all_pairs_noalloc).
 //
 // Some callers cannot allocate device memory once they are running: a
@@ -1574,6 +1887,13 @@ htrip_status htrip_query_all_pairs(htrip_index* h, const int32_t* vps, int32_t k
     HTRIP_GUARD_BEGIN
     ck(cudaSetDevice(h->device), "cudaSetDevice");
     const std::vector<uint8_t> pf = viewpoint_flags(h, vps, k, observed, rows, cols);
+    if (devplan_supported(h, k, true)) {
+        const int status =
+            run_devplan(h, k, devplan_cfg_host(h, vps, pf.data(), k), vps, pf.data(), nullptr, nullptr, nullptr, out);
+        if (status == 1) return fail(HTRIP_ERR_CUDA, "query kernel: grid barrier timed out");
+        if (status == 0) return HTRIP_OK;
+        // status 2: the plan outgrew its worst-case capacity; plan on the host
+    }
     QueryPlan P;
     make_plan(h, vps, pf.data(), k, P);
     const std::vector<QueryReq> R{{h, &P, nullptr}};
@@ -1659,7 +1979,11 @@ htrip_status htrip_query_all_pairs_dev(htrip_index* h, const int32_t* vps_dev, c
     if (k == 0) return HTRIP_OK;
     HTRIP_GUARD_BEGIN
     ck(cudaSetDevice(h->device), "cudaSetDevice");
-    // The viewpoint plan (Morton grouping per level) is built on the host.
+    if (devplan_supported(h, k, false)) {  // planned on the device: no host round trip
+        run_devplan(h, k, devplan_cfg_hint(h, k), nullptr, nullptr, vps_dev, passable_dev, out_dev, nullptr);
+        return HTRIP_OK;
+    }
+    // Larger requests: the viewpoint plan is built on the host.
     std::vector<int32_t> vps(2 * (size_t)k);
     std::vector<uint8_t> pf(k);
     ck(cudaMemcpyAsync(vps.data(), vps_dev, vps.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream), "vps");

@@ -161,6 +161,57 @@ struct QueryLaunch {
 };
 constexpr int kMaxQueryPhases = kMaxQueryLevels + 3;
 
+// Device-side planning of one request (plan.cu): the index's shape and the
+// tile of the launch ...
+struct PlanGeom {
+    int H, g, b, S, leaves_x, RW, NC, nExt0;
+    int g_shift, b_shift;              // log2 of g / b when a power of two, else -1
+    int side[kMaxQueryLevels + 1];     // node side in cells per level
+    int nodes_x[kMaxQueryLevels + 1];  // nodes per row per level
+    int nP[kMaxQueryLevels + 1], NP[kMaxQueryLevels + 1];
+};
+// ... and where the plan goes: int offsets into `plan` with their capacities
+// (worst cases for k viewpoints), each level's flag offset, the request's
+// parameter block and unit prefix, the launch words to clear, the presets,
+// the ticket counter (ticket_base = its value before this launch; it gains
+// max(H, 1) per launch) and an optional host-mapped 8-byte record
+// seq << 32 | status << 26 | viewpoints << 13 | largest root child group.
+struct PlanLayout {
+    int k, kpow;            // kpow = plan_kpow(k): the sort size
+    size_t sort_bytes;      // plan_sort_bytes(kpow)
+    int* plan;
+    int o_vp0, o_inv, o_l0, o_rec;
+    long long flags_off[kMaxQueryLevels + 1];
+    unsigned* ticket;
+    unsigned ticket_base;
+    int o_groups[kMaxQueryLevels + 1], o_items[kMaxQueryLevels + 1], o_meet[kMaxQueryLevels + 1];
+    int o_s2v[kMaxQueryLevels + 1], o_lift[kMaxQueryLevels + 1];
+    int cap_groups[kMaxQueryLevels + 1], cap_slots[kMaxQueryLevels + 1];
+    int cap_items[kMaxQueryLevels + 1], cap_meet[kMaxQueryLevels + 1];
+    int cap_ldv;
+    QueryParams* params;
+    int* unit_pre;          // [H + 3][2]
+    int* words;             // launch words (status, grid barrier, trace), cleared
+    int words_bytes;
+    uint32_t* M;            // pair matrix, preset to 0xFF bytes
+    long long M_bytes;      // multiple of 16
+    uint8_t* flags;         // finite-port flags, cleared
+    long long flags_bytes;
+    int* info;
+    int seq;
+};
+int plan_max_k();                  // largest k the device planner takes
+int plan_kpow(int k);              // power of two >= max(k, 128)
+int plan_threads(int kpow);        // threads of a planning block
+size_t plan_sort_bytes(int kpow);  // shared bytes of the sort buffers
+size_t plan_smem_bytes(int kpow);  // dynamic shared bytes of the planner
+int plan_record_ints();            // ints of the per-level records (o_rec)
+constexpr int kPlanTargetItems = 296;
+// One launch: max(H, 1) planning blocks, then fill_blocks that preset M and
+// the flags.
+cudaError_t launch_plan_query(const int32_t* vps, const uint8_t* pf, const PlanGeom& G, const PlanLayout& O,
+                              const QueryParams& tmpl, int fill_blocks, cudaStream_t st);
+
 // Cooperative launch of the persistent query kernel on `grid` blocks.
 int query_grid_blocks(int device);
 int query_max_ports();  // largest per-child port count the query kernel handles
