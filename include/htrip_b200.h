@@ -142,7 +142,10 @@ htrip_status htrip_query_all_pairs_incremental(htrip_index* h, htrip_incremental
 /* Same query with the per-viewpoint passability already decided by the
  * caller (passable[i] != 0 iff viewpoint i is Free).  vps/passable/out are
  * DEVICE pointers; the call is stream-ordered on the index's stream and
- * returns without synchronising (htrip_sync waits).                       */
+ * returns without synchronising (htrip_sync waits).  For k <= 4096 the plan
+ * is built on the device (no copy back to the host, no host wait); larger
+ * requests are planned on the host.  HTRIP_QUERY_PLANNER=host|device in the
+ * environment overrides where queries are planned.                         */
 htrip_status htrip_query_all_pairs_dev(htrip_index* h, const int32_t* vps_dev,
                                        const uint8_t* passable_dev, int32_t k,
                                        uint16_t* out_dev);
