@@ -223,8 +223,18 @@ struct htrip_index {
     // host staging for its parameter block / plans and for the result
     QueryArena q;
     htrip_batch_stats stats{0, 0, 0};
+    // Per-cell traversal weights (GridMap::weights, grid_map.hpp:56) as the
+    // caller last gave them (wrows x wcols; empty: every weight is 1), and
+    // their device mirror over S x S (null while unweighted).  Kept across
+    // builds and offloads.
+    std::vector<uint16_t> wgrid;
+    int wrows = 0, wcols = 0;
+    DevBuf<uint16_t> wts;
 
-    ~htrip_index() { release(); }
+    ~htrip_index() {
+        release();
+        wts.release();
+    }
     void release() {
         for (auto& l : L) {
             l.d_ext.release(); l.d_seams.release(); l.d_ext_inv.release(); l.mat.release(); l.kflag.release();
@@ -341,6 +351,84 @@ uint64_t reference_bytes(const htrip_index* h) {
         ref += (uint64_t)Lv.nnodes * ((uint64_t)Lv.n * Lv.n + (uint64_t)Lv.nExt * Lv.nExt + (uint64_t)Lv.n * Lv.nExt) * 2;
     }
     return ref;
+}
+
+// GridMap::getCellWeight (grid_map.hpp:273-278): INF outside the grid and on
+// obstacles, else the caller's weight (1 without weights).
+uint16_t host_cell_weight(const htrip_index* h, int r, int c, const uint8_t* obs, int rows, int cols) {
+    if (r < 0 || c < 0 || r >= rows || c >= cols || obs[(size_t)r * cols + c] == 2) return hb::INF;
+    if (h->wgrid.empty() || r >= h->wrows || c >= h->wcols) return 1;
+    return h->wgrid[(size_t)r * h->wcols + c];
+}
+
+// The weights' device mirror over the index's S x S (1 outside the grid,
+// where no cell is passable).
+void upload_weights(htrip_index* h) {
+    if (h->wgrid.empty()) {
+        h->wts.release();
+        return;
+    }
+    const int S = h->S;
+    std::vector<uint16_t> w((size_t)S * S, 1);
+    for (int r = 0; r < std::min(h->wrows, S); ++r)
+        std::memcpy(w.data() + (size_t)r * S, h->wgrid.data() + (size_t)r * h->wcols,
+                    std::min(h->wcols, S) * sizeof(uint16_t));
+    h->wts.reserve(w.size());
+    ck(cudaMemcpyAsync(h->wts.p, w.data(), w.size() * sizeof(uint16_t), cudaMemcpyHostToDevice, h->stream),
+       "weights");
+}
+
+// Listed leaves holding a passable cell of weight != 1: the reference builds
+// those with Dijkstra (leaf_tile.cpp:81-96, 154-192), the others with BFS.
+std::vector<int> weighted_leaves(const htrip_index* h, const std::vector<int>& leaves, const uint8_t* obs, int rows,
+                                 int cols) {
+    std::vector<int> out;
+    if (h->wgrid.empty()) return out;
+    const int b = h->b;
+    for (int leaf : leaves) {
+        const int R0 = (leaf / h->leaves_x) * b, C0 = (leaf % h->leaves_x) * b;
+        bool w = false;
+        for (int r = R0; r < R0 + b && r < rows && !w; ++r)
+            for (int c = C0; c < C0 + b && c < cols && !w; ++c)
+                w = obs[(size_t)r * cols + c] == 1 && host_cell_weight(h, r, c, obs, rows, cols) != 1;
+        if (w) out.push_back(leaf);
+    }
+    return out;
+}
+
+void close_matrices(htrip_index* h, Level& Lv, const std::vector<int>& act);
+
+// Leaf matrices of the listed leaves (all when `leaves` is null) from the
+// passability mirror: bit-parallel BFS, then, for leaves with non-unit
+// weights, the weighted adjacency closed over its passable cells.
+void build_leaves(htrip_index* h, const std::vector<int>* leaves, const uint8_t* obs, int rows, int cols) {
+    cudaStream_t st = h->stream;
+    Level& L0 = h->L[0];
+    DevBuf<int> list;
+    std::vector<int> all;
+    if (!leaves) {
+        all.resize(L0.nnodes);
+        std::iota(all.begin(), all.end(), 0);
+        hb::launch_leaf_bfs(h->pass.p, h->S, h->b, h->leaves_x, L0.nnodes, L0.ms(), st);
+    } else if (!leaves->empty()) {
+        list.reserve(leaves->size());
+        ck(cudaMemcpyAsync(list.p, leaves->data(), leaves->size() * sizeof(int), cudaMemcpyHostToDevice, st), "list");
+        hb::launch_leaf_bfs(h->pass.p, h->S, h->b, h->leaves_x, (int)leaves->size(), L0.ms(), st, list.p);
+    }
+    ck(cudaGetLastError(), "leaf bfs");
+    const std::vector<int> wl = weighted_leaves(h, leaves ? *leaves : all, obs, rows, cols);
+    if (!wl.empty()) {
+        DevBuf<int> wlist;
+        wlist.reserve(wl.size());
+        ck(cudaMemcpyAsync(wlist.p, wl.data(), wl.size() * sizeof(int), cudaMemcpyHostToDevice, st), "list");
+        hb::launch_leaf_weight_init(h->pass.p, h->wts.p, h->S, h->b, h->leaves_x, (int)wl.size(), L0.ms(),
+                                    L0.kflag.p, wlist.p, st);
+        ck(cudaGetLastError(), "weighted leaf init");
+        close_matrices(h, L0, wl);  // synchronises before returning
+        wlist.release();
+    }
+    ck(cudaStreamSynchronize(st), "leaf sync");
+    list.release();
 }
 
 void alloc_levels(htrip_index* h) {
@@ -462,16 +550,15 @@ void do_build(htrip_index* h, const uint8_t* observed, int rows, int cols) {
         for (int c = 0; c < cols; ++c) pass[(size_t)r * S + c] = observed[(size_t)r * cols + c] == 1;
     h->pass.reserve(pass.size());
     ck(cudaMemcpyAsync(h->pass.p, pass.data(), pass.size(), cudaMemcpyHostToDevice, st), "pass");
-    Level& L0 = h->L[0];
-    hb::launch_leaf_bfs(h->pass.p, S, b, h->leaves_x, L0.nnodes, L0.ms(), st);
-    ck(cudaGetLastError(), "leaf bfs");
+    upload_weights(h);
+    build_leaves(h, nullptr, observed, rows, cols);
     for (int l = 1; l <= H; ++l) {
         Level& Lv = h->L[l];
         Level& Lc = h->L[l - 1];
         hb::launch_node_init(Lv.ms(), Lc.ms(), Lc.d_ext.p, Lv.nP, g, Lv.nodes_x, Lc.nodes_x, Lv.nnodes, st);
         ck(cudaGetLastError(), "node init");
         hb::launch_seams_build(Lv.ms(), Lv.d_seams.p, Lv.nseams, h->pass.p, S, Lv.side, Lv.nodes_x, Lv.nnodes,
-                               Lv.kflag.p, st);
+                               Lv.kflag.p, st, nullptr, h->wts.p);
         ck(cudaGetLastError(), "seams build");
         std::vector<int> act(Lv.nnodes);
         std::iota(act.begin(), act.end(), 0);
@@ -536,6 +623,7 @@ void do_lift_root(htrip_index* h, const uint8_t* observed, int rows, int cols) {
         for (int c = 0; c < std::min(cols, S); ++c) pass[(size_t)r * S + c] = observed[(size_t)r * cols + c] == 1;
     h->pass.reserve(pass.size());
     ck(cudaMemcpyAsync(h->pass.p, pass.data(), pass.size(), cudaMemcpyHostToDevice, st), "pass");
+    upload_weights(h);
     // the new area of every level below the new root
     auto fresh = [&](int nodes_x, int old_nodes_x) {
         std::vector<int> v;
@@ -546,13 +634,8 @@ void do_lift_root(htrip_index* h, const uint8_t* observed, int rows, int cols) {
     };
     DevBuf<int> list;
     {
-        Level& L0 = h->L[0];
-        const std::vector<int> nl = fresh(L0.nodes_x, old_S / b);
-        list.reserve(nl.size());
-        ck(cudaMemcpyAsync(list.p, nl.data(), nl.size() * sizeof(int), cudaMemcpyHostToDevice, st), "list");
-        hb::launch_leaf_bfs(h->pass.p, S, b, h->leaves_x, (int)nl.size(), L0.ms(), st, list.p);
-        ck(cudaGetLastError(), "leaf bfs");
-        ck(cudaStreamSynchronize(st), "sync");
+        const std::vector<int> nl = fresh(h->L[0].nodes_x, old_S / b);
+        build_leaves(h, &nl, observed, rows, cols);
     }
     for (int l = 1; l <= h->H; ++l) {
         Level& Lv = h->L[l];
@@ -564,7 +647,7 @@ void do_lift_root(htrip_index* h, const uint8_t* observed, int rows, int cols) {
                              list.p);
         ck(cudaGetLastError(), "node init");
         hb::launch_seams_build(Lv.ms(), Lv.d_seams.p, Lv.nseams, h->pass.p, S, Lv.side, Lv.nodes_x, (int)nn.size(),
-                               Lv.kflag.p, st, list.p);
+                               Lv.kflag.p, st, list.p, h->wts.p);
         ck(cudaGetLastError(), "seams build");
         close_matrices(h, Lv, nn);
         ck(cudaStreamSynchronize(st), "sync");
@@ -606,11 +689,7 @@ void do_rebuild_leaves(htrip_index* h, const std::vector<int>& leaves_in, const 
     DevBuf<int> list;
     DevBuf<hb::Slot> slots;
     DevBuf<uint8_t> changed;
-    list.reserve(cur.size());
-    ck(cudaMemcpyAsync(list.p, cur.data(), cur.size() * sizeof(int), cudaMemcpyHostToDevice, st), "list");
-    hb::launch_leaf_bfs(h->pass.p, S, h->b, h->leaves_x, (int)cur.size(), h->L[0].ms(), st, list.p);
-    ck(cudaGetLastError(), "leaf bfs");
-    ck(cudaStreamSynchronize(st), "sync");
+    build_leaves(h, &cur, observed, rows, cols);
     for (int l = 1; l <= h->H && !cur.empty(); ++l) {
         Level& Lv = h->L[l];
         Level& Lc = h->L[l - 1];
@@ -637,7 +716,7 @@ void do_rebuild_leaves(htrip_index* h, const std::vector<int>& leaves_in, const 
         hb::launch_node_init(Lv.ms(), Lc.ms(), Lc.d_ext.p, Lv.nP, g, Lv.nodes_x, Lc.nodes_x, n, st, list.p);
         ck(cudaGetLastError(), "node init");
         hb::launch_seams_build(Lv.ms(), Lv.d_seams.p, Lv.nseams, h->pass.p, S, Lv.side, Lv.nodes_x, n, Lv.kflag.p,
-                               st, list.p);
+                               st, list.p, h->wts.p);
         ck(cudaGetLastError(), "seams build");
         close_matrices(h, Lv, parents);
         if (track) {
@@ -702,8 +781,8 @@ struct OpenTask {
     htrip_index* h = nullptr;
     bool record_stats = true;
     std::vector<int> leaves;                             // touched leaves, first-touch order
-    std::vector<std::vector<int>> edges;                 // per touched leaf: (u, v) pairs
-    std::vector<std::vector<std::vector<int>>> seams;    // [lvl][slot]: (u, v) V_U pairs
+    std::vector<std::vector<int>> edges;                 // per touched leaf: (u, v, w) triples
+    std::vector<std::vector<std::vector<int>>> seams;    // [lvl][slot]: (u, v, w) V_U triples
     std::vector<std::vector<int>> seam_nodes, seam_slot;
     // progress
     std::vector<int> act, cand;    // active matrices of this level / of the level below
@@ -744,10 +823,15 @@ void open_prepare(OpenTask& T, htrip_index* h, const int32_t* rc, int n, const u
         for (int d = 0; d < 4; ++d) {
             const int nr = r + dr[d], nc = c + dc[d];
             if (!passable(nr, nc)) continue;
+            // GridMap::edgeWeight (leaf_tile.cpp:318-319, minplus_oracle.cpp:579-580)
+            const int w = hb::edge_weight(host_cell_weight(h, r, c, obs, rows, cols),
+                                          host_cell_weight(h, nr, nc, obs, rows, cols));
+            if (w >= hb::INF) continue;
             if (nc / b == tx && nr / b == ty) {
                 auto& e = T.edges[leaf_slot[leaf]];
                 e.push_back((r - ty * b) * b + (c - tx * b));
                 e.push_back((nr - ty * b) * b + (nc - tx * b));
+                e.push_back(w);
             } else {
                 const int lca = find_lca_level(h, r, c, nr, nc);
                 if (lca < 1 || lca > H) continue;
@@ -763,6 +847,7 @@ void open_prepare(OpenTask& T, htrip_index* h, const int32_t* rc, int n, const u
                 if (u >= 0 && v >= 0) {
                     T.seams[lca][slot].push_back(u);
                     T.seams[lca][slot].push_back(v);
+                    T.seams[lca][slot].push_back(w);
                 }
             }
         }
@@ -860,7 +945,7 @@ void run_open_tasks(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t 
         std::memset(A.stage.p + o_cnt, 0, total - o_cnt);
         auto* hs = reinterpret_cast<hb::Slot*>(A.stage.p);
         int* hl = reinterpret_cast<int*>(A.stage.p + o_list);
-        int li = 0;  // in (u, v) pairs
+        int li = 0;  // in (u, v, w) triples
         for (OpenTask* T : live) {
             Level& Lv = T->h->L[l];
             Level* child = l >= 1 ? &T->h->L[l - 1] : nullptr;
@@ -872,8 +957,8 @@ void run_open_tasks(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t 
                 if (l == 0) lst = &T->edges[i];
                 else if (T->seam_slot[l][m] >= 0) lst = &T->seams[l][T->seam_slot[l][m]];
                 if (lst) {
-                    std::memcpy(hl + 2 * li, lst->data(), lst->size() * sizeof(int));
-                    li += (int)lst->size() / 2;
+                    std::memcpy(hl + 3 * li, lst->data(), lst->size() * sizeof(int));
+                    li += (int)lst->size() / 3;
                 }
                 sl.list_end = li;
                 hs[T->slot0 + i] = sl;
@@ -1842,6 +1927,81 @@ htrip_status htrip_leaves_changed(htrip_index* h, const int32_t* leaves, int32_t
     HTRIP_GUARD_END
 }
 
+htrip_status htrip_set_cell_weights(htrip_index* h, const uint16_t* weights, int32_t rows, int32_t cols) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    if (weights && (rows <= 0 || cols <= 0)) return fail(HTRIP_ERR_INVALID, "bad weights grid");
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    if (weights) {
+        h->wgrid.assign(weights, weights + (size_t)rows * cols);
+        h->wrows = rows;
+        h->wcols = cols;
+    } else {
+        h->wgrid.clear();
+        h->wrows = h->wcols = 0;
+    }
+    if (h->built) {
+        upload_weights(h);
+        ck(cudaStreamSynchronize(h->stream), "weights sync");
+    }
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+// GridMap::setCellWeight (grid_map.hpp:297-303): the first weight set gives
+// every cell of the grid weight 1.
+static void set_host_weight(htrip_index* h, int r, int c, uint16_t w, int rows, int cols) {
+    if (h->wgrid.empty() || h->wrows != rows || h->wcols != cols) {
+        std::vector<uint16_t> g((size_t)rows * cols, 1);
+        for (int y = 0; y < std::min(rows, h->wrows); ++y)
+            for (int x = 0; x < std::min(cols, h->wcols); ++x) g[(size_t)y * cols + x] = h->wgrid[(size_t)y * h->wcols + x];
+        h->wgrid = std::move(g);
+        h->wrows = rows;
+        h->wcols = cols;
+    }
+    h->wgrid[(size_t)r * cols + c] = w;
+}
+
+htrip_status htrip_cell_weight_changed(htrip_index* h, int32_t r, int32_t c, uint16_t new_weight,
+                                       const uint8_t* observed, int32_t rows, int32_t cols) {
+    if (!h || !observed || rows <= 0 || cols <= 0) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    if (const htrip_status rs = ready(h)) return rs;
+    // minplus_oracle.cpp:304-307: outside the grid, or the same weight: nothing
+    if (r < 0 || c < 0 || r >= rows || c >= cols) return HTRIP_OK;
+    if (host_cell_weight(h, r, c, observed, rows, cols) == new_weight) return HTRIP_OK;
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    set_host_weight(h, r, c, new_weight, rows, cols);
+    upload_weights(h);
+    if (r >= h->S || c >= h->S) return HTRIP_OK;  // :312 (no leaf holds the cell)
+    // :314-357: the leaf rebuilt from the grid, then every ancestor
+    do_rebuild_leaves(h, {(r / h->b) * h->leaves_x + c / h->b}, observed, rows, cols, true);
+    h->epoch++;  // :359
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
+htrip_status htrip_tile_weights_changed(htrip_index* h, int32_t tx, int32_t ty, const int32_t* rc,
+                                        const uint16_t* weights, int32_t n, const uint8_t* observed, int32_t rows,
+                                        int32_t cols) {
+    if (!h || !observed || rows <= 0 || cols <= 0 || n < 0 || (n > 0 && (!rc || !weights)))
+        return fail(HTRIP_ERR_INVALID, "bad arguments");
+    if (const htrip_status rs = ready(h)) return rs;
+    if (tx < 0 || ty < 0 || tx >= h->leaves_x || ty >= h->leaves_x) return HTRIP_OK;  // minplus_oracle.cpp:366
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    for (int i = 0; i < n; ++i) {  // :368-373: every in-grid cell of the list, whichever tile holds it
+        const int r = rc[2 * i], c = rc[2 * i + 1];
+        if (r >= 0 && c >= 0 && r < rows && c < cols) set_host_weight(h, r, c, weights[i], rows, cols);
+    }
+    upload_weights(h);
+    // :375-421: the leaf (tx, ty) rebuilt once, then every ancestor
+    do_rebuild_leaves(h, {ty * h->leaves_x + tx}, observed, rows, cols, true);
+    h->epoch++;  // :423
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
 htrip_status htrip_lift_root(htrip_index* h, const uint8_t* observed, int32_t rows, int32_t cols) {
     if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
     if (const htrip_status rs = ready(h)) return rs;
@@ -2195,6 +2355,9 @@ htrip_status htrip_clone(const htrip_index* src, htrip_index** out) {
     h->device = src->device;
     h->b = src->b;
     h->g = src->g;
+    h->wgrid = src->wgrid;
+    h->wrows = src->wrows;
+    h->wcols = src->wcols;
     try {
         ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
         if (src->built) {
@@ -2206,6 +2369,11 @@ htrip_status htrip_clone(const htrip_index* src, htrip_index** out) {
                                    cudaMemcpyDeviceToDevice, h->stream), "clone copy");
             h->pass.reserve(src->pass.n);
             ck(cudaMemcpyAsync(h->pass.p, src->pass.p, src->pass.n, cudaMemcpyDeviceToDevice, h->stream), "clone pass");
+            if (src->wts.p) {
+                h->wts.reserve(src->wts.n);
+                ck(cudaMemcpyAsync(h->wts.p, src->wts.p, src->wts.n * sizeof(uint16_t), cudaMemcpyDeviceToDevice,
+                                   h->stream), "clone weights");
+            }
             ck(cudaStreamSynchronize(h->stream), "clone sync");
             h->built = true;
             h->stats = src->stats;
@@ -2574,7 +2742,8 @@ htrip_status htrip_memory_bytes(const htrip_index* h, uint64_t* reference_bytes,
         for (const auto& Lv : h->L)
             dev += (Lv.mat.n + Lv.klist.n * 2 + Lv.kcnt.n * 2) * sizeof(uint16_t) + Lv.kflag.n + Lv.dec.n +
                    (Lv.d_ext.n + Lv.d_seams.n) * sizeof(int);
-        dev += h->pass.n + h->u.dev.n + h->u.snap.n * 2 + h->u.panel.n * 2 + h->u.pflags.n + h->q.dev.n;
+        dev += h->pass.n + h->u.dev.n + h->u.snap.n * 2 + h->u.panel.n * 2 + h->u.pflags.n + h->q.dev.n +
+               h->wts.n * sizeof(uint16_t);
     }
     if (reference_bytes) *reference_bytes = ref;
     if (device_bytes) *device_bytes = dev;

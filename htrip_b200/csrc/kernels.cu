@@ -123,20 +123,67 @@ __global__ void node_init_kernel(MatSet N, MatSet Cm, const int* __restrict__ ce
 
 // Build-time seams: both cells Free -> unit edge, both endpoints are pivots.
 __global__ void seams_build_kernel(MatSet N, const int* __restrict__ seams, int n_seams,
-                                   const uint8_t* __restrict__ pass, int S, int side, int nodes_x,
-                                   uint8_t* kflag, const int* __restrict__ list, int y0) {
+                                   const uint8_t* __restrict__ pass, const uint16_t* __restrict__ wts, int S,
+                                   int side, int nodes_x, uint8_t* kflag, const int* __restrict__ list, int y0) {
     const int node = list ? list[y0 + blockIdx.y] : y0 + blockIdx.y;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_seams) return;
     const int* e = seams + 6 * s;
     const int R0 = (node / nodes_x) * side, C0 = (node % nodes_x) * side;
-    if (!pass[(size_t)(R0 + e[2]) * S + C0 + e[3]] || !pass[(size_t)(R0 + e[4]) * S + C0 + e[5]]) return;
+    const size_t a = (size_t)(R0 + e[2]) * S + C0 + e[3], c = (size_t)(R0 + e[4]) * S + C0 + e[5];
+    if (!pass[a] || !pass[c]) return;
+    const uint16_t w = wts ? edge_weight(wts[a], wts[c]) : (uint16_t)1;  // internal_node.cpp:160-161
+    if (w >= INF) return;
     uint16_t* D = mat_ptr(N, node);
     const int NP = N.NP;
-    D[(size_t)e[0] * NP + e[1]] = 1;
-    D[(size_t)e[1] * NP + e[0]] = 1;
+    D[(size_t)e[0] * NP + e[1]] = min(D[(size_t)e[0] * NP + e[1]], w);
+    D[(size_t)e[1] * NP + e[0]] = min(D[(size_t)e[1] * NP + e[0]], w);
     kflag[(size_t)node * NP + e[0]] = 1;
     kflag[(size_t)node * NP + e[1]] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// Weighted leaf (LeafTile::recomputeFromGrid's Dijkstra branch,
+// leaf_tile.cpp:154-192): D starts as the tile's weighted adjacency - 0 on
+// the diagonal, w(u, v) between 4-adjacent passable cells, INF elsewhere and
+// in the padding - and every passable cell becomes a pivot; the closure over
+// those pivots is the all-pairs shortest-path matrix, equal to the
+// saturated Dijkstra result.  One warp per matrix row.
+// ---------------------------------------------------------------------------
+__global__ void leaf_weight_init_kernel(const uint8_t* __restrict__ pass, const uint16_t* __restrict__ wts, int S,
+                                        int b, int leaves_x, MatSet L, uint8_t* kflag, const int* __restrict__ list,
+                                        int y0) {
+    const int leaf = list ? list[y0 + blockIdx.y] : y0 + blockIdx.y;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int src = blockIdx.x * (blockDim.x >> 5) + warp;
+    const int NP = L.NP, n = b * b;
+    if (src >= NP) return;
+    uint16_t* row = mat_ptr(L, leaf) + (size_t)src * NP;
+    const uint4 inf4 = make_uint4(INF2, INF2, INF2, INF2);
+    for (int j = lane; j < NP / 8; j += 32) reinterpret_cast<uint4*>(row)[j] = inf4;
+    __syncwarp();
+    if (lane != 0) return;
+    uint8_t* f = kflag + (size_t)leaf * NP + src;
+    if (src >= n) {
+        *f = 0;
+        return;
+    }
+    row[src] = 0;
+    const int R0 = (leaf / leaves_x) * b, C0 = (leaf % leaves_x) * b;
+    const int sr = src / b, sc = src % b;
+    const size_t cu = (size_t)(R0 + sr) * S + C0 + sc;
+    const bool pu = pass[cu] != 0;
+    *f = pu ? 1 : 0;
+    if (!pu) return;
+    const int dr[4] = {-1, 1, 0, 0}, dc[4] = {0, 0, -1, 1};
+    for (int d = 0; d < 4; ++d) {
+        const int vr = sr + dr[d], vc = sc + dc[d];
+        if (vr < 0 || vr >= b || vc < 0 || vc >= b) continue;
+        const size_t cv = (size_t)(R0 + vr) * S + C0 + vc;
+        if (!pass[cv]) continue;
+        const uint16_t w = edge_weight(wts[cu], wts[cv]);
+        if (w < INF) row[vr * b + vc] = w;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -372,10 +419,11 @@ __global__ void leaf_edges_kernel(const Slot* __restrict__ S, const int* __restr
     uint8_t* f = sl.kflag;
     int np = 0;
     for (int e = sl.list_begin; e < sl.list_end; ++e) {
-        const int u = edges[2 * e], v = edges[2 * e + 1];
-        if (1 < D[(size_t)u * NP + v]) {
-            D[(size_t)u * NP + v] = 1;
-            D[(size_t)v * NP + u] = 1;
+        const int u = edges[3 * e], v = edges[3 * e + 1];
+        const uint16_t w = (uint16_t)edges[3 * e + 2];
+        if (w < D[(size_t)u * NP + v]) {
+            D[(size_t)u * NP + v] = w;
+            D[(size_t)v * NP + u] = w;
             if (!f[u]) { f[u] = 1; ++np; }
             if (!f[v]) { f[v] = 1; ++np; }
         }
@@ -414,10 +462,11 @@ __global__ void node_seams_kernel(const Slot* __restrict__ S, const int* __restr
     const Slot& sl = S[blockIdx.x];
     uint16_t* D = sl.mat;
     for (int s = sl.list_begin; s < sl.list_end; ++s) {
-        const int u = seams[2 * s], v = seams[2 * s + 1];
-        if (1 < D[(size_t)u * NP + v]) {
-            D[(size_t)u * NP + v] = 1;
-            D[(size_t)v * NP + u] = 1;
+        const int u = seams[3 * s], v = seams[3 * s + 1];
+        const uint16_t w = (uint16_t)seams[3 * s + 2];
+        if (w < D[(size_t)u * NP + v]) {
+            D[(size_t)u * NP + v] = w;
+            D[(size_t)v * NP + u] = w;
             sl.kflag[u] = 1;
             sl.kflag[v] = 1;
         }
@@ -575,11 +624,21 @@ void launch_node_init(MatSet node, MatSet child, const int* child_ext, int nP, i
 }
 
 void launch_seams_build(MatSet node, const int* seams, int n_seams, const uint8_t* pass, int S, int side,
-                        int nodes_x, int n_nodes, uint8_t* kflag, cudaStream_t st, const int* list) {
+                        int nodes_x, int n_nodes, uint8_t* kflag, cudaStream_t st, const int* list,
+                        const uint16_t* wts) {
     if (n_seams == 0) return;
     for (int y0 = 0; y0 < n_nodes; y0 += kMaxGridY) {
         dim3 grid(blocks_for(n_seams, 128), std::min(kMaxGridY, n_nodes - y0));
-        seams_build_kernel<<<grid, 128, 0, st>>>(node, seams, n_seams, pass, S, side, nodes_x, kflag, list, y0);
+        seams_build_kernel<<<grid, 128, 0, st>>>(node, seams, n_seams, pass, wts, S, side, nodes_x, kflag, list, y0);
+    }
+}
+
+void launch_leaf_weight_init(const uint8_t* pass, const uint16_t* wts, int S, int b, int leaves_x, int n_leaves,
+                             MatSet leaves, uint8_t* kflag, const int* list, cudaStream_t st) {
+    constexpr int kWarps = 8;
+    for (int y0 = 0; y0 < n_leaves; y0 += kMaxGridY) {
+        dim3 grid(blocks_for(leaves.NP, kWarps), std::min(kMaxGridY, n_leaves - y0));
+        leaf_weight_init_kernel<<<grid, kWarps * 32, 0, st>>>(pass, wts, S, b, leaves_x, leaves, kflag, list, y0);
     }
 }
 

@@ -33,9 +33,17 @@ void launch_node_init(MatSet node, MatSet child, const int* child_ext, int nP, i
 
 // Seam edges of the build (internal_node.cpp:155-173): seams = 6 ints per
 // candidate {u, v, ur, uc, vr, vc} (node-relative coordinates).
+// wts (optional): per-cell traversal weights (S x S); a seam gets the edge
+// weight w(u, v) = max(1, (w_u + w_v) / 2) (GridMap::edgeWeight), else 1.
 void launch_seams_build(MatSet node, const int* seams, int n_seams, const uint8_t* pass, int S,
                         int side, int nodes_x, int n_nodes, uint8_t* kflag, cudaStream_t st,
-                        const int* list = nullptr);
+                        const int* list = nullptr, const uint16_t* wts = nullptr);
+
+// Weighted leaves (the reference's Dijkstra leaf build): D = the tile's
+// weighted adjacency with a zero diagonal, pivot flags = its passable cells;
+// a closure over those pivots then gives the leaf's shortest-path matrix.
+void launch_leaf_weight_init(const uint8_t* pass, const uint16_t* wts, int S, int b, int leaves_x, int n_leaves,
+                             MatSet leaves, uint8_t* kflag, const int* list, cudaStream_t st);
 
 // One matrix of an update launch (any index, any map size: the launch's
 // matrices share b, g and level, hence order, padding and port tables).
@@ -66,9 +74,9 @@ void launch_closure_round(const Slot* S, int n, int NP, int round, uint16_t* pan
                           cudaStream_t st);
 
 // --- incremental updates -----------------------------------------------------
-// Insert opened in-leaf edges (leaf_tile.cpp:311-330): slot s's (u, v)
-// pairs are edges[list_begin .. list_end); marks pivot flags and adds the
-// new pivots to task_pivots[task].
+// Insert opened in-leaf edges (leaf_tile.cpp:311-330): slot s's (u, v, w)
+// triples are edges[3*list_begin .. 3*list_end); marks pivot flags and adds
+// the new pivots to task_pivots[task].
 void launch_leaf_edges(const Slot* S, int n, const int* edges, int NP, int* task_pivots, cudaStream_t st);
 
 // Child-summary decreases into parent D_U (internal_node.cpp:343-353): for
@@ -77,8 +85,8 @@ void launch_leaf_edges(const Slot* S, int n, const int* edges, int NP, int* task
 void launch_node_child_insert(const Slot* S, int n, const int* child_ext, int nP, int g, int NP, int childNP,
                               cudaStream_t st);
 
-// Seam edges of an update (internal_node.cpp:356-365): slot s's (u, v) V_U
-// pairs are seams[list_begin .. list_end).
+// Seam edges of an update (internal_node.cpp:356-365): slot s's (u, v, w)
+// V_U triples are seams[3*list_begin .. 3*list_end).
 void launch_node_seams(const Slot* S, int n, const int* seams, int NP, cudaStream_t st);
 
 // Snapshot / compare of the non-root slots' exterior block (summary S or

@@ -30,6 +30,15 @@ constexpr u16 INF = 60000;
 constexpr u32 INF2 = 0xEA60EA60u;          // INF in both halves
 constexpr u32 INF_HEADROOM = 65535u - INF; // 5535
 
+// Traversal weight of the edge between two adjacent cells of weights wu, wv
+// (GridMap::edgeWeight, grid_map.hpp:327-334): INF if either is INF or more,
+// else max(1, (wu + wv) / 2).
+__host__ __device__ __forceinline__ u16 edge_weight(u16 wu, u16 wv) {
+    if (wu >= INF || wv >= INF) return INF;
+    const u16 avg = (u16)(((u32)wu + (u32)wv) / 2);
+    return avg == 0 ? (u16)1 : avg;
+}
+
 __device__ __forceinline__ u32 add2(u32 a, u32 b) {
     u32 r;
     asm("add.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));

@@ -92,9 +92,16 @@ void MinPlusOracle::refreshShape() {
     num_leaf_tiles_y = lx;
 }
 
+// The grid's weights to the index (before build / liftRoot).
+static void send_weights(htrip_index* h, const GridMap& grid) {
+    const bool w = grid.hasWeights() && grid.weights.size() >= size_t(grid.rows) * size_t(grid.cols);
+    check(htrip_set_cell_weights(h, w ? grid.weights.data() : nullptr, grid.rows, grid.cols), "set weights");
+}
+
 bool MinPlusOracle::build(const GridMap& grid) {
     if (!config.isValid()) return false;
     if (std::max(grid.rows, grid.cols) <= 0) return false;
+    send_weights(h_, grid);
     const htrip_status st = htrip_build(h_, grid.observedBytes(), grid.rows, grid.cols);
     if (st == HTRIP_ERR_INVALID) return false;
     check(st, "build");
@@ -154,6 +161,38 @@ void MinPlusOracle::onCellBlocked(Point p, const GridMap& grid) {
     ++update_counter;
     check(htrip_cell_blocked(h_, p.r, p.c, grid.observedBytes(), grid.rows, grid.cols), "onCellBlocked");
     ++epoch;  // reference minplus_oracle.cpp:300-301
+}
+
+// minplus_oracle.cpp:304-360
+void MinPlusOracle::onCellWeightChanged(Point p, dist_t new_weight, GridMap& grid) {
+    if (!grid.inBounds(p)) return;
+    if (grid.getCellWeight(p) == new_weight) return;
+    grid.setCellWeight(p, new_weight);
+    if (!built_) return;
+    ++update_counter;
+    check(htrip_cell_weight_changed(h_, p.r, p.c, new_weight, grid.observedBytes(), grid.rows, grid.cols),
+          "onCellWeightChanged");
+    ++epoch;
+}
+
+// minplus_oracle.cpp:362-424
+void MinPlusOracle::onTileWeightsChanged(int tx, int ty, const std::vector<std::pair<Point, dist_t>>& cell_weights,
+                                         GridMap& grid) {
+    if (tx < 0 || ty < 0 || tx >= num_leaf_tiles_x || ty >= num_leaf_tiles_y) return;
+    std::vector<int32_t> rc;
+    std::vector<uint16_t> w;
+    for (const auto& [p, wt] : cell_weights) {
+        if (grid.inBounds(p)) grid.setCellWeight(p, wt);
+        rc.push_back(p.r);
+        rc.push_back(p.c);
+        w.push_back(wt);
+    }
+    if (!built_) return;
+    ++update_counter;
+    check(htrip_tile_weights_changed(h_, tx, ty, rc.data(), w.data(), int32_t(w.size()), grid.observedBytes(),
+                                     grid.rows, grid.cols),
+          "onTileWeightsChanged");
+    ++epoch;
 }
 
 void MinPlusOracle::onBatchLeavesChanged(const std::vector<int>& leaf_indices, const GridMap& grid) {
@@ -227,6 +266,7 @@ dist_t MinPlusOracle::queryDistance(Point s, Point t, const GridMap& grid) const
 
 void MinPlusOracle::liftRoot(const GridMap& grid) {
     if (!built_) return;
+    send_weights(h_, grid);
     check(htrip_lift_root(h_, grid.rows > 0 && grid.cols > 0 ? grid.observedBytes() : nullptr, grid.rows, grid.cols),
           "liftRoot");
     refreshShape();

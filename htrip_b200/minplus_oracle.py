@@ -27,6 +27,7 @@ INF = 60000
 
 _U8P = C.POINTER(C.c_uint8)
 _U16P = C.POINTER(C.c_uint16)
+_OBSTACLE = 2  # CellState::Obstacle (types.hpp)
 _I32P = C.POINTER(C.c_int32)
 _U64P = C.POINTER(C.c_uint64)
 
@@ -87,7 +88,8 @@ EXPORTS = (
     "htrip_autotune_query", "htrip_autotune_export", "htrip_autotune_import", "htrip_autotune_clear",
     "htrip_lift_root", "htrip_query_distance", "htrip_incremental_create", "htrip_incremental_destroy",
     "htrip_query_all_pairs_incremental", "htrip_batch_create_priority", "htrip_cell_blocked",
-    "htrip_leaves_changed", "htrip_selftest_barrier_timeout",
+    "htrip_leaves_changed", "htrip_selftest_barrier_timeout", "htrip_set_cell_weights",
+    "htrip_cell_weight_changed", "htrip_tile_weights_changed",
 )
 
 
@@ -145,6 +147,9 @@ def load_library(path: str | None = None):
     lib.htrip_cell_blocked.argtypes = [P, I, I, _U8P, I, I]
     lib.htrip_selftest_barrier_timeout.argtypes = [C.c_int, _I32P, _I32P, C.POINTER(C.c_float)]
     lib.htrip_leaves_changed.argtypes = [P, _I32P, I, _U8P, I, I]
+    lib.htrip_set_cell_weights.argtypes = [P, _U16P, I, I]
+    lib.htrip_cell_weight_changed.argtypes = [P, I, I, C.c_uint16, _U8P, I, I]
+    lib.htrip_tile_weights_changed.argtypes = [P, I, I, _I32P, _U16P, I, _U8P, I, I]
     lib.htrip_query_distance.argtypes = [P, I, I, I, I, _U8P, I, I, _U16P]
     lib.htrip_incremental_create.argtypes = [C.POINTER(P)]
     lib.htrip_incremental_destroy.argtypes = [P]
@@ -196,10 +201,16 @@ class HierarchyConfig:
 
 
 class GridMap:
-    """Occupancy grid: ``observed`` is a (rows, cols) uint8 CellState array."""
+    """Occupancy grid: ``observed`` is a (rows, cols) uint8 CellState array;
+    ``weights`` the optional (rows, cols) uint16 traversal weights (None:
+    every weight 1), as the reference's GridMap::weights."""
 
-    def __init__(self, observed: np.ndarray):
+    def __init__(self, observed: np.ndarray, weights: np.ndarray | None = None):
         self.observed = np.ascontiguousarray(observed, dtype=np.uint8)
+        self.weights = None if weights is None else np.ascontiguousarray(weights, dtype=np.uint16)
+
+    def hasWeights(self) -> bool:
+        return self.weights is not None
 
     @property
     def rows(self):
@@ -227,6 +238,24 @@ class LastBatchStats:
 def _grid_args(grid):
     obs = grid.observed if isinstance(grid, GridMap) else np.ascontiguousarray(grid, dtype=np.uint8)
     return obs, obs.ctypes.data_as(_U8P), obs.shape[0], obs.shape[1]
+
+
+def _own_weights(grid, weights, rows, cols):
+    """The caller's weights array a weight change writes into: the explicit
+    one, else a GridMap's (created with every weight 1 on first use, as
+    GridMap::setCellWeight does)."""
+    if weights is None and isinstance(grid, GridMap):
+        if grid.weights is None:
+            grid.weights = np.ones((rows, cols), dtype=np.uint16)
+        return grid.weights
+    return weights
+
+
+def _grid_weights(grid, weights):
+    """The weights of a call: the explicit ones, else a GridMap's own."""
+    if weights is None and isinstance(grid, GridMap):
+        return grid.weights
+    return weights
 
 
 def _rc(pts) -> np.ndarray:
@@ -263,9 +292,23 @@ class MinPlusOracle:
         return o
 
     # -- build ------------------------------------------------------------
-    def build(self, grid) -> bool:
+    def setCellWeights(self, weights=None):
+        """Per-cell traversal weights (uint16, the grid's shape; None: every
+        weight 1), the reference's GridMap::weights; build and liftRoot set
+        them from their `weights` argument."""
+        if weights is None:
+            _check(self.lib.htrip_set_cell_weights(self.h, None, 0, 0))
+            return
+        w = np.ascontiguousarray(weights, dtype=np.uint16)
+        self._weights_keep = w
+        _check(self.lib.htrip_set_cell_weights(self.h, w.ctypes.data_as(_U16P), w.shape[0], w.shape[1]))
+
+    def build(self, grid, weights=None) -> bool:
+        """Reference build(grid); `weights` plays the grid's weights (None:
+        an unweighted grid)."""
         if not self.config.isValid():
             return False
+        self.setCellWeights(_grid_weights(grid, weights))
         obs, ptr, rows, cols = _grid_args(grid)
         st = self.lib.htrip_build(self.h, ptr, rows, cols)
         if st == 1:  # HTRIP_ERR_INVALID: the reference returns false
@@ -322,14 +365,42 @@ class MinPlusOracle:
         obs, ptr, rows, cols = _grid_args(grid)
         _check(self.lib.htrip_leaves_changed(self.h, li.ctypes.data_as(_I32P), len(li), ptr, rows, cols))
 
-    def liftRoot(self, grid=None):
+    def liftRoot(self, grid=None, weights=None):
         """Grow the index to S*g, H+1 (reference liftRoot); grid None = the
-        reference's default empty GridMap."""
+        reference's default empty GridMap; `weights` as in build."""
+        self.setCellWeights(_grid_weights(grid, weights))
         if grid is None:
             _check(self.lib.htrip_lift_root(self.h, None, 0, 0))
             return
         obs, ptr, rows, cols = _grid_args(grid)
         _check(self.lib.htrip_lift_root(self.h, ptr, rows, cols))
+
+    def onCellWeightChanged(self, p, new_weight, grid, weights=None):
+        """Reference onCellWeightChanged: cell p's weight becomes new_weight
+        (also written into `weights`, the caller's array, when given) and its
+        leaf and ancestors are rebuilt."""
+        obs, ptr, rows, cols = _grid_args(grid)
+        r, c = int(p[0]), int(p[1])
+        weights = _own_weights(grid, weights, rows, cols)
+        if weights is not None and 0 <= r < rows and 0 <= c < cols:
+            cur = 60000 if obs.reshape(rows, cols)[r, c] == _OBSTACLE else int(weights[r, c])  # getCellWeight
+            if cur != int(new_weight):
+                weights[r, c] = new_weight
+        _check(self.lib.htrip_cell_weight_changed(self.h, r, c, int(new_weight), ptr, rows, cols))
+
+    def onTileWeightsChanged(self, tx, ty, cell_weights, grid, weights=None):
+        """Reference onTileWeightsChanged: cell_weights = [((r, c), w), ...];
+        leaf (tx, ty) and its ancestors are rebuilt once."""
+        rc = _rc([p for p, _ in cell_weights]) if cell_weights else np.zeros((0, 2), np.int32)
+        ws = np.ascontiguousarray([int(w) for _, w in cell_weights], dtype=np.uint16)
+        obs, ptr, rows, cols = _grid_args(grid)
+        weights = _own_weights(grid, weights, rows, cols)
+        if weights is not None:
+            for (r, c), w in cell_weights:
+                if 0 <= r < rows and 0 <= c < cols:
+                    weights[r, c] = w
+        _check(self.lib.htrip_tile_weights_changed(self.h, int(tx), int(ty), rc.ctypes.data_as(_I32P),
+                                                   ws.ctypes.data_as(_U16P), len(ws), ptr, rows, cols))
 
     # -- queries ----------------------------------------------------------
     def queryAllPairs(self, viewpoints, grid, out: np.ndarray | None = None, scratch=None) -> np.ndarray:

@@ -3,8 +3,8 @@
 // Mirrors the members of the reference's GridMap that MinPlusOracle and its
 // callers use (include/htrip/grid_map.hpp:31-160, 221-290): rows / cols,
 // the ground_truth / observed CellState arrays (row-major, one byte per
-// cell), bounds and index helpers, isPassable (observed == Free) and the
-// observed accessors.  The map generators and file loaders of the reference
+// cell), the optional traversal weights (:51-56, 258-334), bounds and index
+// helpers, isPassable (observed == Free) and the observed accessors.  The map generators and file loaders of the reference
 // are test fixtures there and are not part of this library.
 //
 // The oracle reads `observed` as a plain byte array (CellState is a uint8
@@ -23,7 +23,7 @@ public:
     int cols = 0;
     std::vector<CellState> ground_truth;
     std::vector<CellState> observed;
-    std::vector<dist_t> weights;  // empty: unit weights (weighted grids are not supported by this library)
+    std::vector<dist_t> weights;  // per-cell traversal costs, row-major; empty: every weight 1
 
     GridMap() = default;
     GridMap(int r, int c, CellState initial_state = CellState::Unknown)
@@ -52,6 +52,31 @@ public:
     void setObserved(Point p, CellState s) noexcept { setObserved(p.r, p.c, s); }
 
     [[nodiscard]] bool hasWeights() const noexcept { return !weights.empty(); }
+
+    // INF outside the grid and on obstacles, else the cell's weight (1
+    // without weights).
+    [[nodiscard]] dist_t getCellWeight(int r, int c) const noexcept {
+        if (!inBounds(r, c)) return INF;
+        if (observed[size_t(index(r, c))] == CellState::Obstacle) return INF;
+        if (weights.empty()) return 1;
+        return weights[size_t(index(r, c))];
+    }
+    [[nodiscard]] dist_t getCellWeight(Point p) const noexcept { return getCellWeight(p.r, p.c); }
+    // The first weight set gives every cell weight 1.
+    void setCellWeight(int r, int c, dist_t w) noexcept {
+        if (!inBounds(r, c)) return;
+        if (weights.size() < size_t(rows) * size_t(cols)) weights.assign(size_t(rows) * size_t(cols), 1);
+        weights[size_t(index(r, c))] = w;
+    }
+    void setCellWeight(Point p, dist_t w) noexcept { setCellWeight(p.r, p.c, w); }
+    // Cost of the edge between adjacent cells u, v: INF if either weight is
+    // INF or more, else max(1, (w_u + w_v) / 2).
+    [[nodiscard]] dist_t edgeWeight(Point u, Point v) const noexcept {
+        const dist_t wu = getCellWeight(u), wv = getCellWeight(v);
+        if (wu >= INF || wv >= INF) return INF;
+        const dist_t avg = dist_t((uint32_t(wu) + uint32_t(wv)) / 2);
+        return avg == 0 ? dist_t(1) : avg;
+    }
 
     // Copy one cell's ground truth into `observed` (reference
     // GridMap::revealCell, src/grid_map.cpp:231-235); false out of bounds.

@@ -15,6 +15,9 @@
 //   void onCellBlocked(Point, const GridMap&)            :123
 //   void onBatchLeavesChanged(const std::vector<int>&,
 //                             const GridMap&)            :157
+//   void onCellWeightChanged(Point, dist_t, GridMap&)    :132
+//   void onTileWeightsChanged(int, int, cell_weights,
+//                             GridMap&)                  :144
 //   struct HTripQueryScratch (caller-owned, reused)      :189-238
 //   struct LastBatchStats / last_batch_stats             :251-256
 //   void queryAllPairs(vps, grid, out, scratch) const    :337-341
@@ -38,6 +41,7 @@
 #pragma once
 
 #include <cstddef>
+#include <utility>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -128,6 +132,13 @@ public:
     // grid.observed; the leaf (leaves) and every ancestor are rebuilt.
     void onCellBlocked(Point p, const GridMap& grid);
     void onBatchLeavesChanged(const std::vector<int>& leaf_indices, const GridMap& grid);
+    // Weighted grids: build / liftRoot read grid.weights (empty: every weight
+    // 1); a weight change sets it in `grid` and rebuilds the cell's leaf (the
+    // given leaf) and every ancestor.  Change weights through these calls:
+    // the index keeps its own copy of the weights.
+    void onCellWeightChanged(Point p, dist_t new_weight, GridMap& grid);
+    void onTileWeightsChanged(int tx, int ty, const std::vector<std::pair<Point, dist_t>>& cell_weights,
+                              GridMap& grid);
 
     // k x k row-major matrix of exact 4-connected distances (INF when
     // unreachable), resized and filled by the call.

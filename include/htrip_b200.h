@@ -102,6 +102,34 @@ htrip_status htrip_cell_blocked(htrip_index* h, int32_t r, int32_t c, const uint
 htrip_status htrip_leaves_changed(htrip_index* h, const int32_t* leaves, int32_t n, const uint8_t* observed,
                                   int32_t rows, int32_t cols);
 
+/* GridMap::weights                             grid_map.hpp:51-56, 297-303
+ * The per-cell traversal weights (rows x cols, uint16; NULL: every weight
+ * is 1) that build, liftRoot, openings and rebuilds use from now on: an
+ * edge between adjacent passable cells costs max(1, (w_u + w_v) / 2), INF
+ * when either weight is INF or more (GridMap::edgeWeight, :327-334), and a
+ * leaf holding a passable cell of weight != 1 is built as the reference's
+ * Dijkstra leaf build does.  Set them before htrip_build; on a built index
+ * this refreshes the device copy only (the matrices are not recomputed).  */
+htrip_status htrip_set_cell_weights(htrip_index* h, const uint16_t* weights, int32_t rows, int32_t cols);
+
+/* void onCellWeightChanged(Point p, dist_t new_weight, GridMap&)
+ *                                              minplus_oracle.hpp:132
+ * Sets cell (r, c)'s weight (the library's copy; the caller's grid keeps its
+ * own) and rebuilds its leaf and every ancestor; nothing when the cell is
+ * outside the grid or its weight is already new_weight (an obstacle's
+ * weight is INF).                                                          */
+htrip_status htrip_cell_weight_changed(htrip_index* h, int32_t r, int32_t c, uint16_t new_weight,
+                                       const uint8_t* observed, int32_t rows, int32_t cols);
+
+/* void onTileWeightsChanged(int tx, int ty, cell_weights, GridMap&)
+ *                                              minplus_oracle.hpp:144
+ * Sets the weights of the n cells rc[2i], rc[2i+1] to weights[i] (cells
+ * outside the grid skipped), then rebuilds leaf (tx, ty) once and every
+ * ancestor; nothing when (tx, ty) is not a leaf.                           */
+htrip_status htrip_tile_weights_changed(htrip_index* h, int32_t tx, int32_t ty, const int32_t* rc,
+                                        const uint16_t* weights, int32_t n, const uint8_t* observed, int32_t rows,
+                                        int32_t cols);
+
 /* void liftRoot(const GridMap& grid)          minplus_oracle.hpp:380
  * Grows the index: S -> S*g, H -> H+1.  Existing leaves and nodes keep
  * their matrices; leaves and nodes of the new area, and the new root, are

@@ -60,6 +60,10 @@ def _load_ref():
         lib.ref_lift_root.argtypes = [_P]
         lib.ref_cell_blocked.argtypes = [_P, _I, _I]
         lib.ref_leaves_changed.argtypes = [_P, _I32P, _I]
+        lib.ref_set_weights.argtypes = [_P, _U16P]
+        lib.ref_cell_weight_changed.argtypes = [_P, _I, _I, _I]
+        lib.ref_tile_weights_changed.argtypes = [_P, _I, _I, _I32P, _U16P, _I]
+        lib.ref_dijkstra_all_pairs.argtypes = [_P, _I32P, _I, _U16P]
         lib.ref_query_distance.restype = _I
         lib.ref_query_distance.argtypes = [_P, _I, _I, _I, _I]
         lib.ref_query_incremental.argtypes = [_P, _I32P, _I, _U16P]
@@ -139,6 +143,30 @@ class RefOracle:
 
     def cell_blocked(self, r: int, c: int):
         self.lib.ref_cell_blocked(self.h, int(r), int(c))
+
+    def set_weights(self, weights):
+        """The grid's traversal weights (rows x cols uint16) or None."""
+        if weights is None:
+            self.lib.ref_set_weights(self.h, None)
+            return
+        w = np.ascontiguousarray(weights, dtype=np.uint16)
+        assert w.shape == (self.rows, self.cols)
+        self.lib.ref_set_weights(self.h, _p(w, _U16P))
+
+    def cell_weight_changed(self, r: int, c: int, w: int):
+        self.lib.ref_cell_weight_changed(self.h, int(r), int(c), int(w))
+
+    def tile_weights_changed(self, tx: int, ty: int, cells, weights):
+        rc = _rc(cells)
+        w = np.ascontiguousarray(weights, dtype=np.uint16)
+        self.lib.ref_tile_weights_changed(self.h, int(tx), int(ty), _p(rc, _I32P), _p(w, _U16P), len(w))
+
+    def dijkstra(self, vps) -> np.ndarray:
+        """DijkstraOracle::queryAllPairs on the handle's grid."""
+        rc = _rc(vps)
+        out = np.empty((len(rc), len(rc)), dtype=np.uint16)
+        self.lib.ref_dijkstra_all_pairs(self.h, _p(rc, _I32P), len(rc), _p(out, _U16P))
+        return out
 
     def leaves_changed(self, leaves):
         li = np.ascontiguousarray(np.asarray(leaves, dtype=np.int32).ravel())

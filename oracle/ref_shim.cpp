@@ -12,9 +12,13 @@
 //   htrip::MinPlusOracle::{build, onCellOpened, onBatchCellsOpened,
 //   queryAllPairs(vps, grid, out, scratch)}   (include/htrip/minplus_oracle.hpp:78,109,171,337)
 //   htrip::BfsOracle::queryAllPairs           (src/bfs_oracle.cpp:187)
+//   htrip::DijkstraOracle::queryAllPairs      (weighted grids)
+//   GridMap::weights, MinPlusOracle::{onCellWeightChanged, onTileWeightsChanged}
+//                                             (grid_map.hpp:56, minplus_oracle.hpp:132,144)
 // and reads back the public members leaves[i].D/.S and levels[l][n].D_U /
 // .S_U / .child_to_ext for bitwise state comparison.
 #include "htrip/bfs_oracle.hpp"
+#include "htrip/dijkstra_oracle.hpp"
 #include "htrip/grid_map.hpp"
 #include "htrip/minplus_oracle.hpp"
 
@@ -118,6 +122,37 @@ void ref_leaves_changed(void* p, const int32_t* leaves, int n) {
 void ref_lift_root(void* p) {
     auto* h = static_cast<RefHandle*>(p);
     h->oracle.liftRoot(h->grid);
+}
+
+// The grid's traversal weights (rows x cols of the current grid; null
+// clears them: every weight 1).
+void ref_set_weights(void* p, const uint16_t* w) {
+    auto* h = static_cast<RefHandle*>(p);
+    if (!w) {
+        h->grid.weights.clear();
+        return;
+    }
+    h->grid.weights.assign(w, w + static_cast<size_t>(h->grid.rows) * h->grid.cols);
+}
+
+// MinPlusOracle::onCellWeightChanged / onTileWeightsChanged with the
+// handle's grid (they set the grid's weights themselves).
+void ref_cell_weight_changed(void* p, int r, int c, int w) {
+    auto* h = static_cast<RefHandle*>(p);
+    h->oracle.onCellWeightChanged(Point{r, c}, static_cast<dist_t>(w), h->grid);
+}
+void ref_tile_weights_changed(void* p, int tx, int ty, const int32_t* rc, const uint16_t* w, int n) {
+    auto* h = static_cast<RefHandle*>(p);
+    std::vector<std::pair<Point, dist_t>> cw;
+    for (int i = 0; i < n; ++i) cw.emplace_back(Point{rc[2 * i], rc[2 * i + 1]}, w[i]);
+    h->oracle.onTileWeightsChanged(tx, ty, cw, h->grid);
+}
+
+// DijkstraOracle::queryAllPairs on the handle's grid (weighted all pairs).
+void ref_dijkstra_all_pairs(void* p, const int32_t* rc, int k, uint16_t* out) {
+    auto* h = static_cast<RefHandle*>(p);
+    const auto mat = DijkstraOracle::queryAllPairs(h->grid, toPoints(rc, k));
+    std::memcpy(out, mat.data(), mat.size() * sizeof(dist_t));
 }
 
 void ref_open_cell(void* p, int r, int c) {

@@ -10,6 +10,8 @@
 //   test_dropin              full suite on CUDA device 0
 //   test_dropin --no-device  host-only checks: value types, and that the
 //                            oracle refuses to run without a device
+#include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -305,6 +307,72 @@ void next_members() {
     expect_matrix(inc, bfs_matrix(big, vps2), "incremental after liftRoot (epoch changed)");
 }
 
+// Exact weighted all-pairs by a plain Dijkstra over GridMap::edgeWeight
+// (the test's own checker).
+std::vector<dist_t> dijkstra_matrix(const GridMap& g, const std::vector<Point>& vps) {
+    const size_t k = vps.size(), n = size_t(g.rows) * g.cols;
+    std::vector<dist_t> m(k * k, INF);
+    std::vector<uint32_t> d(n);
+    for (size_t a = 0; a < k; ++a) {
+        if (!g.isPassable(vps[a])) continue;
+        std::fill(d.begin(), d.end(), UINT32_MAX);
+        std::vector<std::pair<uint32_t, int>> pq{{0u, g.index(vps[a])}};
+        d[size_t(g.index(vps[a]))] = 0;
+        while (!pq.empty()) {
+            std::pop_heap(pq.begin(), pq.end(), std::greater<>());
+            const auto [du, u] = pq.back();
+            pq.pop_back();
+            if (du > d[size_t(u)]) continue;
+            const Point pu = g.point(u);
+            const int dr[4] = {-1, 1, 0, 0}, dc[4] = {0, 0, -1, 1};
+            for (int t = 0; t < 4; ++t) {
+                const Point pv(pu.r + dr[t], pu.c + dc[t]);
+                if (!g.isPassable(pv)) continue;
+                const dist_t w = g.edgeWeight(pu, pv);
+                if (w >= INF) continue;
+                const uint32_t alt = du + w;
+                if (alt < d[size_t(g.index(pv))]) {
+                    d[size_t(g.index(pv))] = alt;
+                    pq.push_back({alt, g.index(pv)});
+                    std::push_heap(pq.begin(), pq.end(), std::greater<>());
+                }
+            }
+        }
+        for (size_t b = 0; b < k; ++b)
+            if (g.isPassable(vps[b])) m[a * k + b] = dist_t(std::min<uint32_t>(d[size_t(g.index(vps[b]))], INF));
+    }
+    return m;
+}
+
+// Weighted grids: build, opening, onCellWeightChanged, onTileWeightsChanged.
+void weighted_grid() {
+    GridMap truth = rooms_grid(32, 32, 8, 93);
+    uint64_t x = 93;
+    for (int r = 0; r < 32; ++r)
+        for (int c = 0; c < 32; ++c) {
+            x = x * 6364136223846793005ull + 1442695040888963407ull;
+            truth.setCellWeight(r, c, dist_t(1 + (x >> 60) % 7));
+        }
+    GridMap obs = truth;
+    std::vector<Point> cells;
+    for (int c = 1; c < 31; c += 3) cells.push_back(Point(12, c));
+    for (auto& p : cells) obs.setObserved(p, CellState::Unknown);
+    MinPlusOracle o(HierarchyConfig{8, 2, 2, 0});
+    EXPECT(o.build(obs), "weighted build");
+    const auto vps = sample_points(truth, 14, 11, 1);
+    expect_matrix(o.queryAllPairs(vps, obs), dijkstra_matrix(obs, vps), "weighted build vs Dijkstra");
+    for (auto& p : cells) obs.setObserved(p, CellState::Free);
+    o.onBatchCellsOpened(cells, obs);
+    expect_matrix(o.queryAllPairs(vps, obs), dijkstra_matrix(obs, vps), "weighted opening vs Dijkstra");
+    const uint64_t epoch = o.epoch;
+    o.onCellWeightChanged(vps[0], 25, obs);
+    EXPECT(obs.getCellWeight(vps[0]) == 25 && o.epoch == epoch + 1, "onCellWeightChanged sets the grid");
+    expect_matrix(o.queryAllPairs(vps, obs), dijkstra_matrix(obs, vps), "after onCellWeightChanged");
+    o.onTileWeightsChanged(vps[1].c / 8, vps[1].r / 8, {{vps[1], dist_t(3)}, {Point(vps[1].r, vps[1].c / 8 * 8), dist_t(9)}},
+                           obs);
+    expect_matrix(o.queryAllPairs(vps, obs), dijkstra_matrix(obs, vps), "after onTileWeightsChanged");
+}
+
 int host_only() {
     static_assert(add_dist(INF, 0) == INF && add_dist(59999, 1) == INF && add_dist(59998, 1) == 59999);
     static_assert(add_dist(1, 2, 3) == 6 && add_dist(30000, 30000, 1) == INF);
@@ -344,6 +412,7 @@ int main(int argc, char** argv) {
     copy_semantics();
     non_square();
     next_members();
+    weighted_grid();
     std::printf("%s (%d failures)\n", g_fail ? "drop-in suite FAILED" : "drop-in suite passed", g_fail);
     return g_fail ? 1 : 0;
 }
