@@ -279,6 +279,70 @@ def bench_opening(device, steps=400):
     return out
 
 
+def bench_weighted(device, side=256, n_changes=6, seed=5):
+    """Weighted grids (the reference's GridMap::weights, 1..9 per cell) on a
+    fully revealed 256x256 street map with 3072 free cells withheld, b=8:
+    build, the withheld cells opened in 12 batches of 256, and
+    onCellWeightChanged calls (leaf + branch rebuild), each timed on the host
+    per call (submit to host-visible completion) beside the reference's own
+    CPU path on the same inputs, with a state comparison at the end."""
+    from htrip_b200 import workloads as W
+    from htrip_b200.minplus_oracle import HierarchyConfig, MinPlusOracle
+    from oracle.ref import RefOracle, ref_available
+    truth = W.street_grid(side, seed)
+    rng = np.random.default_rng(seed)
+    w = rng.integers(1, 10, size=truth.shape).astype(np.uint16)
+    obs0, cells = W.withheld_open(truth, 12 * 256, seed)
+    batches = np.array_split(cells, 12)
+    free = np.argwhere(truth == W.FREE)
+    changes = [(tuple(int(x) for x in free[i]), int(rng.integers(1, 30)))
+               for i in rng.choice(len(free), n_changes, replace=False)]
+    dev = MinPlusOracle(HierarchyConfig(8, 2, 2), device=device)
+    obs = obs0.copy()
+    dev.build(obs, weights=w)  # warm-up (kernels loaded, arenas sized)
+    t = time.perf_counter()
+    assert dev.build(obs, weights=w)
+    build_s = time.perf_counter() - t
+    open_s, chg_s = [], []
+    for c in batches:
+        obs[c[:, 0], c[:, 1]] = W.FREE
+        t = time.perf_counter()
+        dev.onBatchCellsOpened(c, obs)
+        open_s.append(time.perf_counter() - t)
+    wd = w.copy()
+    for p, nw in changes:
+        t = time.perf_counter()
+        dev.onCellWeightChanged(p, nw, obs, wd)
+        chg_s.append(time.perf_counter() - t)
+    n_cells = sum(len(c) for c in batches)
+    out = {"workload": f"{side}x{side} street, weights 1-9, b=8: build, {len(batches)} x 256 withheld cells "
+                       f"opened, {n_changes} onCellWeightChanged",
+           "build_s": build_s, "cells_per_s": n_cells / sum(open_s),
+           "weight_change_ms_p50": 1e3 * float(np.median(chg_s))}
+    if ref_available():
+        ref = RefOracle(8)
+        ref.set_grid(obs0)
+        ref.set_weights(w)
+        t = time.perf_counter()
+        assert ref.build()
+        rb = time.perf_counter() - t
+        ro, rc = [], []
+        for c in batches:
+            ref.set_cells(c, W.FREE)
+            t = time.perf_counter()
+            ref.open_batch(c)
+            ro.append(time.perf_counter() - t)
+        for p, nw in changes:
+            t = time.perf_counter()
+            ref.cell_weight_changed(p[0], p[1], nw)
+            rc.append(time.perf_counter() - t)
+        out.update({"reference_build_s": rb, "reference_cells_per_s": n_cells / sum(ro),
+                    "reference_weight_change_ms_p50": 1e3 * float(np.median(rc)), "reference_cores": 1,
+                    "reference_kind": "reference",
+                    "parity": "bit-exact" if ref.digest() == dev.stateDigest() else "MISMATCH"})
+    return out
+
+
 _GRID_CACHE = {}
 
 
@@ -569,6 +633,7 @@ def run_ours(args, rank, world, local_rank):
     }
     if world == 1 and not args.headline_only:
         for name, fn in (("cells_opened", lambda: bench_opening(local_rank)),
+                         ("weighted", lambda: bench_weighted(local_rank)),
                          ("batched", lambda: bench_batched(local_rank)),
                          ("served", lambda: bench_served(local_rank))):
             if args.section and args.section != name:
@@ -593,7 +658,7 @@ def main():
                     help="only the queryAllPairs headline (skip the opening / batched / served workloads)")
     ap.add_argument("--tile-config", type=int, choices=[0, 1, 2, 3],
                     help="query tile shape to use for the headline instead of the autotuner's choice")
-    ap.add_argument("--section", choices=["cells_opened", "batched", "served"],
+    ap.add_argument("--section", choices=["cells_opened", "weighted", "batched", "served"],
                     help="run only this one of the further workloads after the headline")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
