@@ -25,6 +25,14 @@
 //    offloaded to host memory, least recently used first
 //    (htrip_offload / htrip_restore); when even that cannot make room the
 //    new session is refused with HTRIP_ERR_OOM.
+//  * Double-buffered sessions (htrip_server_config::double_buffer), the
+//    reference simulator's protocol for every session: the session holds a
+//    front index that queries read and a back index that openings update;
+//    queries never wait behind the session's openings.  The open worker
+//    applies to the back the batch it still lacks (the last one published)
+//    merged with the new openings, then swaps the two; a back index is never
+//    updated while a query launch may still read it.  Each query reports
+//    the number of the session's openings its result includes.
 //  * Latency of a request = time from its submission to its result being
 //    in host memory and marked done.
 #include "../../include/htrip_b200.h"
@@ -57,6 +65,7 @@ struct SReq {
     std::vector<int32_t> rc;  // viewpoints or cells
     uint16_t* out = nullptr;  // query result (k*k), caller memory
     Clock::time_point t0, t1;
+    uint64_t version = 0;     // query: openings its result includes; opening: its number
     bool done = false;
     htrip_status status = HTRIP_OK;
     std::string error;
@@ -64,15 +73,28 @@ struct SReq {
 
 struct Session {
     int64_t id = 0;
-    htrip_index* h = nullptr;
-    std::vector<uint8_t> grid;  // the session's observed grid (CellState)
+    htrip_index* h = nullptr;   // the index (double-buffered: the front one, queried)
+    std::vector<uint8_t> grid;  // the session's observed grid (CellState) as h has it
     int rows = 0, cols = 0;
-    std::deque<SReq*> q;
+    std::deque<SReq*> q;        // requests (double-buffered: the queries)
     bool busy = false;
     bool resident = true;
     uint64_t bytes = 0;
     uint64_t last_use = 0;
+    uint64_t opens_submitted = 0;
+    // double-buffered sessions
+    bool dbuf = false;
+    htrip_index* hb = nullptr;    // the back index (updated by openings)
+    std::vector<uint8_t> grid_b;  // the grid as hb has it
+    std::deque<SReq*> oq;         // queued openings
+    bool qbusy = false, obusy = false;
+    int reads = 0, reads_b = 0;   // query launches in flight on h / on hb
+    uint64_t version = 0;         // openings published into h
+    std::vector<int32_t> pending; // cells of the last published batch (hb lacks them)
 };
+
+bool idle(const Session& s) { return s.dbuf ? !s.qbusy && !s.obusy && s.reads == 0 && s.reads_b == 0 : !s.busy; }
+bool drained(const Session& s) { return s.q.empty() && s.oq.empty() && idle(s); }
 
 }  // namespace
 
@@ -90,6 +112,7 @@ struct htrip_server {
     uint64_t resident_bytes = 0;
     bool stop = false;
     uint64_t completions = 0;  // launches finished (wakes workers waiting for memory)
+    bool dbuf = false;         // new sessions are double-buffered
     htrip_server_stats st{};
     htrip_batch* batch[2] = {nullptr, nullptr};
     std::thread worker[2];
@@ -111,17 +134,18 @@ bool make_room(htrip_server* S, uint64_t need, int64_t keep) {
         Session* victim = nullptr;
         for (auto& kv : S->sessions) {
             Session& s = kv.second;
-            if (!s.resident || s.busy || s.id == keep || !s.q.empty()) continue;
+            if (!s.resident || !idle(s) || s.id == keep || !s.q.empty() || !s.oq.empty()) continue;
             if (!victim || s.last_use < victim->last_use) victim = &s;
         }
         if (!victim)  // sessions with queued work only if nothing else is left
             for (auto& kv : S->sessions) {
                 Session& s = kv.second;
-                if (!s.resident || s.busy || s.id == keep) continue;
+                if (!s.resident || !idle(s) || s.id == keep) continue;
                 if (!victim || s.last_use < victim->last_use) victim = &s;
             }
         if (!victim) return false;
         if (htrip_offload(victim->h) != HTRIP_OK) return false;
+        if (victim->hb && htrip_offload(victim->hb) != HTRIP_OK) return false;
         victim->resident = false;
         S->resident_bytes -= victim->bytes;
         S->st.evictions++;
@@ -134,7 +158,8 @@ bool make_room(htrip_server* S, uint64_t need, int64_t keep) {
 htrip_status ensure_resident(htrip_server* S, Session& s) {
     if (s.resident) return HTRIP_OK;
     if (!make_room(S, s.bytes, s.id)) return sfail(HTRIP_ERR_OOM, "no room to restore the session within the budget");
-    const htrip_status r = htrip_restore(s.h);
+    htrip_status r = htrip_restore(s.h);
+    if (r == HTRIP_OK && s.hb) r = htrip_restore(s.hb);
     if (r != HTRIP_OK) return sfail(r, htrip_last_error());
     s.resident = true;
     S->resident_bytes += s.bytes;
@@ -143,11 +168,16 @@ htrip_status ensure_resident(htrip_server* S, Session& s) {
     return HTRIP_OK;
 }
 
+// Whether worker `kind` can take session s now.
+bool takes(const Session& s, int kind) {
+    if (!s.dbuf) return !s.busy && !s.q.empty() && s.q.front()->kind == kind;
+    if (kind == kQuery) return !s.qbusy && !s.q.empty();
+    return !s.obusy && !s.oq.empty() && s.reads_b == 0;
+}
+
 bool has_work(htrip_server* S, int kind) {
-    for (auto& kv : S->sessions) {
-        const Session& s = kv.second;
-        if (!s.busy && !s.q.empty() && s.q.front()->kind == kind) return true;
-    }
+    for (auto& kv : S->sessions)
+        if (takes(kv.second, kind)) return true;
     return false;
 }
 
@@ -161,25 +191,27 @@ void worker_loop(htrip_server* S, int kind) {
         struct Item {
             Session* s;
             std::vector<SReq*> r;
+            htrip_index* h = nullptr;         // the index the launch reads or updates
+            const uint8_t* grid = nullptr;
         };
         std::vector<Item> items;
         int taken = 0;
         std::vector<Session*> cand;
-        for (auto& kv : S->sessions) {
-            Session& s = kv.second;
-            if (!s.busy && !s.q.empty() && s.q.front()->kind == kind) cand.push_back(&s);
-        }
-        std::sort(cand.begin(), cand.end(),
-                  [](const Session* a, const Session* b) { return a->q.front()->t0 < b->q.front()->t0; });
+        for (auto& kv : S->sessions)
+            if (takes(kv.second, kind)) cand.push_back(&kv.second);
+        auto head = [kind](const Session* s) { return (s->dbuf && kind == kOpen ? s->oq : s->q).front()->t0; };
+        std::sort(cand.begin(), cand.end(), [&](const Session* a, const Session* b) { return head(a) < head(b); });
         for (Session* s : cand) {
             if (taken >= S->max_per_launch) break;
             Item it{s, {}};
-            for (SReq* r : s->q) {
+            for (SReq* r : (s->dbuf && kind == kOpen ? s->oq : s->q)) {
                 if (r->kind != kind || taken >= S->max_per_launch) break;
                 it.r.push_back(r);
                 ++taken;
             }
-            s->busy = true;
+            if (!s->dbuf) s->busy = true;
+            else if (kind == kQuery) s->qbusy = true;
+            else s->obusy = true;
             s->last_use = ++S->tick;
             items.push_back(std::move(it));
         }
@@ -190,9 +222,24 @@ void worker_loop(htrip_server* S, int kind) {
         // waits for some launch to finish before it tries again.
         std::vector<Item> ready;
         for (auto& it : items) {
-            if (ensure_resident(S, *it.s) != HTRIP_OK) {
-                it.s->busy = false;
+            Session& s = *it.s;
+            if (ensure_resident(S, s) != HTRIP_OK) {
+                if (!s.dbuf) s.busy = false;
+                else if (kind == kQuery) s.qbusy = false;
+                else s.obusy = false;
                 continue;
+            }
+            if (s.dbuf && kind == kQuery) {  // the published state, read until the launch ends
+                it.h = s.h;
+                it.grid = s.grid.data();
+                ++s.reads;
+                for (SReq* r : it.r) r->version = s.version;
+            } else if (s.dbuf) {
+                it.h = s.hb;
+                it.grid = s.grid_b.data();
+            } else {
+                it.h = s.h;
+                it.grid = s.grid.data();
             }
             ready.push_back(std::move(it));
         }
@@ -210,23 +257,29 @@ void worker_loop(htrip_server* S, int kind) {
                 std::vector<htrip_query_request> qr;
                 for (auto& it : ready)
                     for (SReq* r : it.r)
-                        qr.push_back({it.s->h, r->rc.data(), (int32_t)(r->rc.size() / 2), it.s->grid.data(),
-                                      it.s->rows, it.s->cols, r->out});
+                        qr.push_back({it.h, r->rc.data(), (int32_t)(r->rc.size() / 2), it.grid, it.s->rows,
+                                      it.s->cols, r->out});
                 rs = htrip_query_batch(S->batch[kind], qr.data(), (int32_t)qr.size());
             } else {
                 std::vector<std::vector<int32_t>> merged(ready.size());
                 std::vector<htrip_open_request> orq;
                 for (size_t i = 0; i < ready.size(); ++i) {
                     Session& s = *ready[i].s;
-                    for (SReq* r : ready[i].r) {
-                        // the caller's protocol: cells become Free before the call
-                        for (size_t c = 0; c + 1 < r->rc.size(); c += 2) {
-                            const int32_t rr = r->rc[c], cc = r->rc[c + 1];
-                            if (rr >= 0 && cc >= 0 && rr < s.rows && cc < s.cols) s.grid[(size_t)rr * s.cols + cc] = 1;
+                    // double-buffered: the back first catches up with the last published batch
+                    if (s.dbuf) merged[i] = s.pending;
+                    std::vector<uint8_t>& g = s.dbuf ? s.grid_b : s.grid;
+                    auto mark = [&](const std::vector<int32_t>& rc) {  // the caller's protocol: Free before the call
+                        for (size_t c = 0; c + 1 < rc.size(); c += 2) {
+                            const int32_t rr = rc[c], cc = rc[c + 1];
+                            if (rr >= 0 && cc >= 0 && rr < s.rows && cc < s.cols) g[(size_t)rr * s.cols + cc] = 1;
                         }
+                    };
+                    mark(merged[i]);
+                    for (SReq* r : ready[i].r) {
+                        mark(r->rc);
                         merged[i].insert(merged[i].end(), r->rc.begin(), r->rc.end());
                     }
-                    orq.push_back({s.h, merged[i].data(), (int32_t)(merged[i].size() / 2), s.grid.data(), s.rows,
+                    orq.push_back({ready[i].h, merged[i].data(), (int32_t)(merged[i].size() / 2), g.data(), s.rows,
                                    s.cols});
                 }
                 rs = htrip_open_batch(S->batch[kind], orq.data(), (int32_t)orq.size());
@@ -236,15 +289,33 @@ void worker_loop(htrip_server* S, int kind) {
         const auto t1 = Clock::now();
         lk.lock();
         for (auto& it : ready) {
+            Session& s = *it.s;
+            std::vector<int32_t> batch;
             for (SReq* r : it.r) {
                 r->status = rs;
                 r->error = err;
                 r->t1 = t1;
                 r->done = true;
-                it.s->q.pop_front();
+                (s.dbuf && kind == kOpen ? s.oq : s.q).pop_front();
+                if (s.dbuf && kind == kOpen) batch.insert(batch.end(), r->rc.begin(), r->rc.end());
             }
-            it.s->busy = false;
-            it.s->last_use = ++S->tick;
+            if (!s.dbuf) {
+                s.busy = false;
+            } else if (kind == kQuery) {
+                if (it.h == s.h) --s.reads;  // the index may have been swapped meanwhile
+                else --s.reads_b;
+                s.qbusy = false;
+            } else {
+                s.obusy = false;
+                if (rs == HTRIP_OK) {  // publish: the back becomes the front
+                    std::swap(s.h, s.hb);
+                    std::swap(s.grid, s.grid_b);
+                    std::swap(s.reads, s.reads_b);
+                    s.version += it.r.size();
+                    s.pending = std::move(batch);
+                }
+            }
+            s.last_use = ++S->tick;
         }
         const double busy = std::chrono::duration<double>(t1 - tb).count();
         if (kind == kQuery) {
@@ -328,7 +399,10 @@ htrip_status submit(htrip_server* S, int64_t sid, int kind, const int32_t* rc, i
     r->t0 = Clock::now();
     SReq* p = r.get();
     S->reqs[p->ticket] = std::move(r);
-    it->second.q.push_back(p);
+    Session& s = it->second;
+    if (kind == kOpen) p->version = ++s.opens_submitted;
+    else p->version = s.opens_submitted;  // single-buffered: every earlier opening
+    (s.dbuf && kind == kOpen ? s.oq : s.q).push_back(p);
     if (kind == kQuery) S->st.requests_query++;
     else S->st.requests_open++;
     *ticket = p->ticket;
@@ -355,6 +429,7 @@ htrip_status htrip_server_create(const htrip_server_config* cfg, htrip_server** 
     S->device = cfg->device;
     S->max_per_launch = cfg->max_requests_per_launch > 0 ? cfg->max_requests_per_launch : 128;
     S->budget = cfg->hbm_budget_bytes;
+    S->dbuf = cfg->double_buffer != 0 && !cfg->plain_per_call;
     if (S->budget == 0) {
         size_t fr = 0, tot = 0;
         cudaSetDevice(S->device);
@@ -389,7 +464,7 @@ htrip_status htrip_server_destroy(htrip_server* S) {
         // finish the queued work first
         S->cv_done.wait(lk, [&] {
             for (auto& kv : S->sessions)
-                if (!kv.second.q.empty() || kv.second.busy) return false;
+                if (!drained(kv.second)) return false;
             return true;
         });
         S->stop = true;
@@ -397,7 +472,10 @@ htrip_status htrip_server_destroy(htrip_server* S) {
     }
     for (auto& w : S->worker)
         if (w.joinable()) w.join();
-    for (auto& kv : S->sessions) htrip_destroy(kv.second.h);
+    for (auto& kv : S->sessions) {
+        htrip_destroy(kv.second.h);
+        htrip_destroy(kv.second.hb);
+    }
     for (auto* b : S->batch) htrip_batch_destroy(b);
     delete S;
     return HTRIP_OK;
@@ -409,6 +487,7 @@ htrip_status htrip_server_add_session(htrip_server* S, htrip_config cfg, const u
     uint64_t est = 0;
     htrip_status r = htrip_estimate_bytes(cfg, rows, cols, &est);
     if (r != HTRIP_OK) return sfail(r, htrip_last_error());
+    if (S->dbuf) est *= 2;  // front and back index
     std::lock_guard<std::mutex> lk(S->mu);
     if (est > S->budget) return sfail(HTRIP_ERR_OOM, "session needs " + std::to_string(est) + " bytes; budget is " +
                                                          std::to_string(S->budget));
@@ -416,16 +495,22 @@ htrip_status htrip_server_add_session(htrip_server* S, htrip_config cfg, const u
         return sfail(HTRIP_ERR_OOM, "session of " + std::to_string(est) + " bytes refused: budget " +
                                         std::to_string(S->budget) + " bytes held by busy sessions");
     htrip_index* h = nullptr;
+    htrip_index* hb = nullptr;
     r = htrip_create(cfg, S->device, &h);
     if (r == HTRIP_OK) r = htrip_build(h, observed, rows, cols);
+    if (r == HTRIP_OK && S->dbuf) r = htrip_clone(h, &hb);
     if (r != HTRIP_OK) {
         const std::string e = htrip_last_error();
         htrip_destroy(h);
+        htrip_destroy(hb);
         return sfail(r, e);
     }
     Session s;
     s.id = S->next_sid++;
     s.h = h;
+    s.hb = hb;
+    s.dbuf = S->dbuf;
+    if (s.dbuf) s.grid_b.assign(observed, observed + (size_t)rows * cols);
     s.grid.assign(observed, observed + (size_t)rows * cols);
     s.rows = rows;
     s.cols = cols;
@@ -444,13 +529,14 @@ htrip_status htrip_server_remove_session(htrip_server* S, int64_t sid) {
     std::unique_lock<std::mutex> lk(S->mu);
     auto it = S->sessions.find(sid);
     if (it == S->sessions.end()) return sfail(HTRIP_ERR_INVALID, "unknown session " + std::to_string(sid));
-    S->cv_done.wait(lk, [&] { return it->second.q.empty() && !it->second.busy; });
+    S->cv_done.wait(lk, [&] { return drained(it->second); });
     if (it->second.resident) {
         S->resident_bytes -= it->second.bytes;
         S->st.resident_sessions--;
     }
     S->st.sessions--;
     htrip_destroy(it->second.h);
+    htrip_destroy(it->second.hb);
     S->sessions.erase(it);
     return HTRIP_OK;
 }
@@ -467,6 +553,10 @@ htrip_status htrip_server_submit_open(htrip_server* S, int64_t sid, const int32_
 }
 
 htrip_status htrip_server_wait(htrip_server* S, uint64_t ticket, double* latency_ms) {
+    return htrip_server_wait_version(S, ticket, latency_ms, nullptr);
+}
+
+htrip_status htrip_server_wait_version(htrip_server* S, uint64_t ticket, double* latency_ms, uint64_t* version) {
     if (!S) return sfail(HTRIP_ERR_INVALID, "null server");
     std::unique_lock<std::mutex> lk(S->mu);
     auto it = S->reqs.find(ticket);
@@ -474,6 +564,7 @@ htrip_status htrip_server_wait(htrip_server* S, uint64_t ticket, double* latency
     SReq* r = it->second.get();
     S->cv_done.wait(lk, [&] { return r->done; });
     if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t1 - r->t0).count();
+    if (version) *version = r->version;
     const htrip_status st = r->status;
     const std::string e = r->error;
     S->reqs.erase(it);

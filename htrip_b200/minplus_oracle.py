@@ -54,7 +54,7 @@ class _OpenRequest(C.Structure):
 
 class _ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64), ("max_requests_per_launch", C.c_int32),
-                ("plain_per_call", C.c_int32)]
+                ("plain_per_call", C.c_int32), ("double_buffer", C.c_int32)]
 
 
 class _ServerStats(C.Structure):
@@ -89,7 +89,7 @@ EXPORTS = (
     "htrip_lift_root", "htrip_query_distance", "htrip_incremental_create", "htrip_incremental_destroy",
     "htrip_query_all_pairs_incremental", "htrip_batch_create_priority", "htrip_cell_blocked",
     "htrip_leaves_changed", "htrip_selftest_barrier_timeout", "htrip_set_cell_weights",
-    "htrip_cell_weight_changed", "htrip_tile_weights_changed",
+    "htrip_cell_weight_changed", "htrip_tile_weights_changed", "htrip_server_wait_version",
 )
 
 
@@ -167,6 +167,7 @@ def load_library(path: str | None = None):
     lib.htrip_server_submit_query.argtypes = [P, C.c_int64, _I32P, I, _U16P, _U64P]
     lib.htrip_server_submit_open.argtypes = [P, C.c_int64, _I32P, I, _U64P]
     lib.htrip_server_wait.argtypes = [P, C.c_uint64, C.POINTER(C.c_double)]
+    lib.htrip_server_wait_version.argtypes = [P, C.c_uint64, C.POINTER(C.c_double), _U64P]
     lib.htrip_server_get_stats.argtypes = [P, C.POINTER(_ServerStats)]
     lib.htrip_server_run_trace.argtypes = [P, C.POINTER(_ServerRequest), C.POINTER(C.c_double), I,
                                            C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -701,10 +702,11 @@ class Server:
 
     QUERY, OPEN = 0, 1
 
-    def __init__(self, device: int = 0, budget_bytes: int = 0, max_per_launch: int = 0, plain: bool = False):
+    def __init__(self, device: int = 0, budget_bytes: int = 0, max_per_launch: int = 0, plain: bool = False,
+                 double_buffer: bool = False):
         self.lib = load_library()
         h = C.c_void_p()
-        cfg = _ServerConfig(device, budget_bytes, max_per_launch, 1 if plain else 0)
+        cfg = _ServerConfig(device, budget_bytes, max_per_launch, 1 if plain else 0, 1 if double_buffer else 0)
         _check_server(self.lib.htrip_server_create(C.byref(cfg), C.byref(h)))
         self.h = h
         self._pending = {}
@@ -750,6 +752,16 @@ class Server:
         finally:
             self._pending.pop(ticket, None)
         return lat.value
+
+    def wait_version(self, ticket: int):
+        """(latency ms, version): for a query the number of the session's
+        openings its result includes, for an opening its own number."""
+        lat, ver = C.c_double(), C.c_uint64()
+        try:
+            _check_server(self.lib.htrip_server_wait_version(self.h, ticket, C.byref(lat), C.byref(ver)))
+        finally:
+            self._pending.pop(ticket, None)
+        return lat.value, ver.value
 
     def stats(self) -> dict:
         st = _ServerStats()

@@ -278,6 +278,16 @@ typedef struct {
                                          through the single-index calls (the
                                          baseline the batched server is
                                          measured against)                     */
+    int32_t double_buffer;            /* 1: every session keeps two indexes, as
+                                         the reference simulator's update thread
+                                         does (robot_simulator.cpp:987-1037):
+                                         queries read the published one and
+                                         never wait behind the session's
+                                         openings, which update the other one
+                                         and then publish it (twice the memory;
+                                         a query may not include openings still
+                                         being applied - htrip_server_wait_version
+                                         says which it includes)               */
 } htrip_server_config;
 
 typedef struct {
@@ -312,6 +322,10 @@ htrip_status htrip_server_submit_open(htrip_server* s, int64_t session, const in
                                       uint64_t* ticket);
 /* Blocks until the request is done; returns its status and latency.      */
 htrip_status htrip_server_wait(htrip_server* s, uint64_t ticket, double* latency_ms);
+/* Same, and *version: for a query, the number of the session's openings
+ * (in submission order) its result includes - all earlier ones, unless the
+ * server is double-buffered; for an opening, its own number.              */
+htrip_status htrip_server_wait_version(htrip_server* s, uint64_t ticket, double* latency_ms, uint64_t* version);
 htrip_status htrip_server_get_stats(htrip_server* s, htrip_server_stats* out);
 /* Open-loop load: request i is submitted arrival_s[i] seconds after the
  * call starts, by the calling thread; then every request is waited for.

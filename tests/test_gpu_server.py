@@ -117,3 +117,71 @@ def test_plain_per_call_mode_gives_same_results(gpu):
     srv.close()
     assert st["launches_query"] + st["launches_open"] == 150
     _replay(sessions, reqs, outs)
+
+
+@pytest.mark.parametrize("tight_budget", [False, True])
+def test_double_buffered_queries_equal_their_published_state(gpu, tight_budget):
+    """Double-buffered sessions (the reference simulator's front / back
+    oracle protocol): every query's result equals a replay of exactly the
+    openings its reported version includes, versions only move forward, and
+    a query submitted after every opening has finished sees them all; with a
+    budget for about two sessions the two indexes of a session are offloaded
+    and restored together."""
+    from htrip_b200.minplus_oracle import MinPlusOracle, Server, estimate_bytes
+    sessions = _sessions()[:4]
+    budget = 0
+    if tight_budget:
+        sizes = sorted(2 * estimate_bytes(_cfg(b), o.shape[0], o.shape[1]) for _, o, _, b in sessions)
+        budget = sizes[-1] + sizes[-2]
+    srv = Server(budget_bytes=budget, double_buffer=True)
+    sids = [srv.add_session(_cfg(b), obs) for _, obs, _, b in sessions]
+    rng = np.random.default_rng(61)
+    batches = [np.array_split(w, 6) for _, _, w, _ in sessions]
+    plan = []  # (session index, kind, payload)
+    for step in range(6):
+        for i in range(len(sessions)):
+            plan.append((i, "open", batches[i][step]))
+            for _ in range(2):
+                plan.append((i, "query", W.sample_free(sessions[i][0], int(rng.integers(4, 40)), int(rng.integers(1 << 30)))))
+    tickets = []
+    for i, kind, payload in plan:
+        if kind == "open":
+            tickets.append((i, kind, payload, srv.submit_open(sids[i], payload), None))
+        else:
+            t, out = srv.submit_query(sids[i], payload)
+            tickets.append((i, kind, payload, t, out))
+    seen = [[] for _ in sessions]
+    for i, kind, payload, t, out in tickets:
+        _, version = srv.wait_version(t)
+        if kind == "query":
+            seen[i].append((version, payload, out))
+    for i, (truth, obs0, withheld, b) in enumerate(sessions):
+        versions = [v for v, _, _ in seen[i]]
+        assert versions == sorted(versions) and 0 <= versions[0] and versions[-1] <= 6
+        # replay: the state after v openings, for every version a query saw
+        dev = MinPlusOracle(_cfg(b))
+        grid = obs0.copy()
+        assert dev.build(grid)
+        applied = 0
+        for v, vps, out in seen[i]:
+            while applied < v:
+                part = batches[i][applied]
+                grid[part[:, 0], part[:, 1]] = W.FREE
+                dev.onBatchCellsOpened(part, grid)
+                applied += 1
+            np.testing.assert_array_equal(out, dev.queryAllPairs(vps, grid), err_msg=f"session {i} version {v}")
+        # after every opening has finished, a new query includes them all
+        vps = W.sample_free(truth, 24, 100 + i)
+        t, out = srv.submit_query(sids[i], vps)
+        _, v = srv.wait_version(t)
+        assert v == 6
+        while applied < 6:
+            part = batches[i][applied]
+            grid[part[:, 0], part[:, 1]] = W.FREE
+            dev.onBatchCellsOpened(part, grid)
+            applied += 1
+        np.testing.assert_array_equal(out, dev.queryAllPairs(vps, grid))
+    st = srv.stats()
+    if tight_budget:
+        assert st["resident_bytes"] <= st["budget_bytes"]
+    srv.close()
