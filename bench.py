@@ -466,14 +466,15 @@ def bench_served(device, rates=(5000.0, 20000.0, 50000.0), max_requests=10000, p
         obs, cells = streams[key]
         pools.append((truth, obs, cells, sp["b"]))
 
-    def run(rate, n_req, plain, trace=None):
-        srv = Server(device=device, plain=plain)
-        sids = [srv.add_session(HierarchyConfig(b, 2, 2), obs) for _, obs, _, b in pools]
+    def run(rate, n_req, plain, trace=None, double=False, pl=None):
+        pl = pools if pl is None else pl
+        srv = Server(device=device, plain=plain, double_buffer=double)
+        sids = [srv.add_session(HierarchyConfig(b, 2, 2), obs) for _, obs, _, b in pl]
         reqs, arrival = trace if trace is not None else \
-            W.served_trace([(t, c) for t, _, c, _ in pools], n_req, rate, int(rate) + 1)
+            W.served_trace([(t, c) for t, _, c, _ in pl], n_req, rate, int(rate) + 1)
         # warm-up: queries only (the sessions' maps stay as the trace expects),
         # so the server's scratch arenas reach their working size untimed
-        wq = [(s, 0, rc) for s, k, rc in W.served_trace([(t, c[:0]) for t, _, c, _ in pools], 400, 2000.0, 99)[0]]
+        wq = [(s, 0, rc) for s, k, rc in W.served_trace([(t, c[:0]) for t, _, c, _ in pl], 400, 2000.0, 99)[0]]
         srv.run_trace([(sids[s], k, rc) for s, k, rc in wq], np.zeros(len(wq)))
         outs, lat, wall = srv.run_trace([(sids[s], k, rc) for s, k, rc in reqs], arrival)
         st = srv.stats()
@@ -482,7 +483,7 @@ def bench_served(device, rates=(5000.0, 20000.0, 50000.0), max_requests=10000, p
         o = [l for (s, k, rc), l in zip(reqs, lat) if k == 1]
         entries = sum(len(rc) ** 2 for s, k, rc in reqs if k == 0)
         cells = sum(len(rc) for s, k, rc in reqs if k == 1)
-        return {"rate_req_s": rate, "requests": n_req, "wall_s": wall,
+        return {"rate_req_s": rate, "requests": len(reqs), "wall_s": wall,
                 "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99),
                 "query_p50_ms": _pct(q, 50), "query_p99_ms": _pct(q, 99),
                 "open_p50_ms": _pct(o, 50), "open_p99_ms": _pct(o, 99),
@@ -505,10 +506,25 @@ def bench_served(device, rates=(5000.0, 20000.0, 50000.0), max_requests=10000, p
     n = min(plain_requests, len(reqs0))
     plain, preqs, pouts = run(rates[0], n, True, trace=(reqs0[:n], arrival0[:n]))
     same = all(a is None or np.array_equal(a, b) for a, b in zip(first[1][:n], pouts[:n]))
+    # double-buffered sessions (queries read the published index, openings
+    # update the other one) against single-buffered ones, on the first half
+    # of the sessions (twice the memory per session), same traces
+    half = pools[: len(pools) // 2]
+    dbuf = []
+    for r in (rates[0], rates[1]) if len(rates) > 1 else rates:
+        tr = W.served_trace([(t, c) for t, _, c, _ in half], min(max_requests, int(r)), r, int(r) + 7)
+        single, _, _ = run(r, 0, False, trace=tr, pl=half)
+        double, _, _ = run(r, 0, False, trace=tr, double=True, pl=half)
+        dbuf.append({"rate_req_s": r, "single_buffered": single, "double_buffered": double})
+    half_gib = sum(sp["est"] for sp in specs[: len(specs) // 2]) / 2**30
     return {"workload": f"{len(specs)} sessions (sides 128-1024, b 8/16/32, {total / 2**30:.0f} GiB of indexes), "
                         "Poisson arrivals, 70% queryAllPairs (k log-uniform 4-512), 30% openings (1-512 cells)",
             "served": served, "plain_per_call": plain,
-            "parity_served_vs_plain": "bit-exact" if same else "MISMATCH"}
+            "parity_served_vs_plain": "bit-exact" if same else "MISMATCH",
+            "double_buffered": {"workload": f"the first {len(half)} sessions ({half_gib:.0f} GiB single-buffered); "
+                                            "queries may not include openings still being applied "
+                                            "(parity: tests/test_gpu_server.py replays each query's version)",
+                                "runs": dbuf}}
 
 
 def max_over_ranks(values, world, device):
