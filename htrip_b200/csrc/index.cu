@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <map>
 #include <tuple>
 #include <cstdint>
@@ -1232,8 +1233,8 @@ void make_plan(const htrip_index* h, const int32_t* vps, const uint8_t* pass_fla
 //   [QueryParams x n][unit prefix, n_phases x (n+1) ints][4 words][plans]
 //       <- one host->device copy of the staged head (words start at zero)
 //   [M of every request]      <- one memset to 0xFF (no pair found yet)
-//   [flags of every request]  <- one memset to 0
-//   [X0 X1 X2 Y0 Y1 of every request][results k*k u16 of every request]
+//   [flags + completion counters of every request]  <- one memset to 0
+//   [X_0..X_{H-1} Y_1..Y_H of every request][results k*k u16 of every request]
 // ---------------------------------------------------------------------------
 
 struct QueryReq {
@@ -1251,8 +1252,27 @@ struct LaunchLayout {
     int n = 0, n_phases = 0;
     size_t o_params = 0, o_pre = 0, o_words = 0, head = 0;
     size_t o_M = 0, M_bytes = 0, o_flags = 0, flags_bytes = 0, o_out = 0, out_bytes = 0, total = 0;
-    std::vector<size_t> plan, M, flags, X[3], Y[2], out;
+    std::vector<size_t> plan, M, flags, ctr, out;
+    std::vector<std::array<size_t, hb::kMaxQueryLevels + 1>> X, Y;
 };
+
+// Rows of the per-level buffers of a query on h: X_l (l < H) holds the
+// exterior ports of level l, which are the child ports of level l+1; Yt_l
+// (l >= 1) the columns of the level-l matrices.
+size_t query_x_rows(const htrip_index* h, int l) {
+    return (size_t)std::max(h->L[l].nExt, l + 1 <= h->H ? h->L[l + 1].nP : 0);
+}
+size_t query_y_rows(const htrip_index* h, int l) { return (size_t)std::max(h->L[l].NP, 64); }
+
+// The persistent kernel's schedule: dataflow (default) or grid barriers
+// (HTRIP_QUERY_DATAFLOW=0).
+int query_dataflow_mode() {
+    static const int mode = [] {
+        const char* e = std::getenv("HTRIP_QUERY_DATAFLOW");
+        return e && std::strcmp(e, "0") == 0 ? 0 : 1;
+    }();
+    return mode;
+}
 
 void check_query_shape(const htrip_index* h) {
     if (h->H > hb::kMaxQueryLevels) throw CudaError{cudaErrorInvalidValue, "hierarchy deeper than the query supports"};
@@ -1280,14 +1300,17 @@ LaunchLayout layout_launch(const std::vector<QueryReq>& R) {
     for (const auto& r : R) L.M.push_back(take((size_t)r.P->ldm * r.P->ldm * sizeof(uint32_t)));
     L.M_bytes = off - L.o_M;
     L.o_flags = off;
-    for (const auto& r : R) L.flags.push_back(take(r.P->flags_total));
+    for (const auto& r : R) {
+        L.flags.push_back(take(r.P->flags_total));
+        L.ctr.push_back(take(hb::query_counter_words(r.h->H, r.P->k) * sizeof(unsigned)));
+    }
     L.flags_bytes = off - L.o_flags;
     for (const auto& r : R) {
-        int maxExt = 0, maxNP = 64;
-        for (int l = 0; l <= r.h->H; ++l) maxExt = std::max(maxExt, r.h->L[l].nExt);
-        for (int l = 1; l <= r.h->H; ++l) maxNP = std::max(maxNP, r.h->L[l].NP);
-        for (int i = 0; i < 3; ++i) L.X[i].push_back(take((size_t)maxExt * r.P->ldv * sizeof(uint16_t)));
-        for (int i = 0; i < 2; ++i) L.Y[i].push_back(take((size_t)maxNP * r.P->ldv * sizeof(uint16_t)));
+        std::array<size_t, hb::kMaxQueryLevels + 1> x{}, y{};
+        for (int l = 0; l < r.h->H; ++l) x[l] = take(query_x_rows(r.h, l) * r.P->ldv * sizeof(uint16_t));
+        for (int l = 1; l <= r.h->H; ++l) y[l] = take(query_y_rows(r.h, l) * r.P->ldv * sizeof(uint16_t));
+        L.X.push_back(x);
+        L.Y.push_back(y);
     }
     L.o_out = off;
     for (const auto& r : R) L.out.push_back(r.out_dev ? 0 : take((size_t)r.P->k * r.P->k * sizeof(uint16_t)));
@@ -1328,9 +1351,10 @@ hb::QueryParams make_params(const htrip_index* h, const QueryPlan& P, unsigned c
     Q.l0 = plan + P.o_l0;
     Q.ext0 = h->L[0].d_ext.p;
     Q.leaves = h->L[0].ms();
-    for (int j = 0; j < 3; ++j) Q.X[j] = reinterpret_cast<uint16_t*>(base + L.X[j][i]);
-    for (int j = 0; j < 2; ++j) Q.Y[j] = reinterpret_cast<uint16_t*>(base + L.Y[j][i]);
+    for (int l = 0; l < H; ++l) Q.X[l] = reinterpret_cast<uint16_t*>(base + L.X[i][l]);
+    for (int l = 1; l <= H; ++l) Q.Y[l] = reinterpret_cast<uint16_t*>(base + L.Y[i][l]);
     Q.M = reinterpret_cast<uint32_t*>(base + L.M[i]);
+    Q.ctr = reinterpret_cast<unsigned*>(base + L.ctr[i]);
     Q.out = out_dev;
     for (int l = 1; l <= H; ++l) {
         const Level& Lv = h->L[l];
@@ -1388,6 +1412,7 @@ void issue_query_launch(cudaStream_t st, int device, int& grid, int cfg, const s
     QL.status = reinterpret_cast<int*>(base + L.o_words);
     QL.bar = reinterpret_cast<unsigned*>(base + L.o_words) + 1;
     QL.trace = reinterpret_cast<unsigned long long*>(base + L.o_words + kTraceOffset);
+    QL.dataflow = query_dataflow_mode();
     if (ev) ck(cudaEventRecord(ev[0], st), "event");
     ck(hb::launch_query(QL, cfg, grid, st), "query kernel");
     if (ev) ck(cudaEventRecord(ev[1], st), "event");
@@ -1504,7 +1529,8 @@ int choose_query_cfg(const htrip_index* h, int ns, int root_group) {
 // is two launches (planner, query kernel) and no copy.  Arena layout, every
 // piece 256-byte aligned:
 //   [QueryParams][unit prefix][launch words][viewpoints 8k + flags k]
-//   [plan ints][M][flags][X0 X1 X2 Y0 Y1][result k*k u16, host-bound calls]
+//   [plan ints][M][flags + completion counters][X_0..X_{H-1} Y_1..Y_H]
+//   [result k*k u16, host-bound calls]
 // The plan capacities are worst cases for k viewpoints, so the planner's
 // overflow status (2) is a guard, not a path: a synchronous call that sees
 // it replans on the host.
@@ -1513,7 +1539,7 @@ struct DevPlanLayout {
     hb::PlanGeom G{};
     hb::PlanLayout O{};
     size_t o_params = 0, o_pre = 0, o_words = 0, o_in = 0, o_plan = 0, o_M = 0, o_flags = 0, o_out = 0;
-    size_t X[3] = {}, Y[2] = {}, total = 0;
+    size_t X[hb::kMaxQueryLevels + 1] = {}, Y[hb::kMaxQueryLevels + 1] = {}, o_ctr = 0, total = 0;
     int n_phases = 0, fill_blocks = 1;
 };
 
@@ -1628,13 +1654,13 @@ DevPlanLayout devplan_layout(const htrip_index* h, int k, int cfg, bool out_in_a
     const size_t ldm = std::max<size_t>(8, ((size_t)k + 7) / 8 * 8);
     O.M_bytes = (long long)(ldm * ldm * sizeof(uint32_t));
     D.o_M = takeb((size_t)O.M_bytes);
-    O.flags_bytes = (long long)flags;
-    D.o_flags = takeb(flags);
-    int maxExt = 0, maxNP = 64;
-    for (int l = 0; l <= H; ++l) maxExt = std::max(maxExt, h->L[l].nExt);
-    for (int l = 1; l <= H; ++l) maxNP = std::max(maxNP, h->L[l].NP);
-    for (auto& x : D.X) x = takeb((size_t)maxExt * O.cap_ldv * sizeof(uint16_t));
-    for (auto& y : D.Y) y = takeb((size_t)maxNP * O.cap_ldv * sizeof(uint16_t));
+    // the planner's preset blocks clear the flags and the counters after them
+    const size_t ctr_at = (flags + 15) / 16 * 16;
+    O.flags_bytes = (long long)(ctr_at + hb::query_counter_words(H, k) * sizeof(unsigned));
+    D.o_flags = takeb((size_t)O.flags_bytes);
+    D.o_ctr = D.o_flags + ctr_at;
+    for (int l = 0; l < H; ++l) D.X[l] = takeb(query_x_rows(h, l) * O.cap_ldv * sizeof(uint16_t));
+    for (int l = 1; l <= H; ++l) D.Y[l] = takeb(query_y_rows(h, l) * O.cap_ldv * sizeof(uint16_t));
     D.o_out = out_in_arena ? takeb((size_t)k * k * sizeof(uint16_t)) : 0;
     D.total = off;
     O.words_bytes = (int)kWordsBytes;
@@ -1736,9 +1762,10 @@ int run_devplan(htrip_index* h, int k, int cfg, const int32_t* vps_host, const u
     T.cfg = cfg;
     T.ext0 = h->L[0].d_ext.p;
     T.leaves = h->L[0].ms();
-    for (int j = 0; j < 3; ++j) T.X[j] = reinterpret_cast<uint16_t*>(base + D.X[j]);
-    for (int j = 0; j < 2; ++j) T.Y[j] = reinterpret_cast<uint16_t*>(base + D.Y[j]);
+    for (int l = 0; l < h->H; ++l) T.X[l] = reinterpret_cast<uint16_t*>(base + D.X[l]);
+    for (int l = 1; l <= h->H; ++l) T.Y[l] = reinterpret_cast<uint16_t*>(base + D.Y[l]);
     T.M = reinterpret_cast<uint32_t*>(base + D.o_M);
+    T.ctr = reinterpret_cast<unsigned*>(base + D.o_ctr);
     T.out = out;
     for (int l = 1; l <= h->H; ++l) {
         const Level& Lv = h->L[l];
@@ -1771,6 +1798,7 @@ int run_devplan(htrip_index* h, int k, int cfg, const int32_t* vps_host, const u
     QL.status = O.words;
     QL.bar = reinterpret_cast<unsigned*>(base + D.o_words) + 1;
     QL.trace = reinterpret_cast<unsigned long long*>(base + D.o_words + kTraceOffset);
+    QL.dataflow = query_dataflow_mode();
     ck(cudaEventRecord(A.ev[0], st), "event");
     ck(hb::launch_query(QL, cfg, A.grid, st), "query kernel");
     ck(cudaEventRecord(A.ev[1], st), "event");
@@ -2507,7 +2535,7 @@ static htrip_status arena_phases(const QueryArena& A, cudaStream_t st, uint64_t*
     ck(cudaStreamSynchronize(st), "trace sync");
     const int P = A.last_phases;
     *n = std::min<int32_t>(max_n, P);
-    for (int i = 0; i < *n; ++i) ns[i] = t[i + 1] - t[i];
+    for (int i = 0; i < *n; ++i) ns[i] = t[i + 1] > t[i] ? t[i + 1] - t[i] : 0;
     if (max_n >= 2 * P) {
         for (int i = 0; i < P; ++i) {
             const unsigned long long e = t[hb::kMaxQueryPhases + 1 + i];

@@ -134,12 +134,20 @@ struct QueryParams {
     const int* l0;          // per level-1 slot {sorted index or -1, level-1 group}
     const int* ext0;        // leaf port -> cell
     MatSet leaves;
-    uint16_t* X[3];         // port vectors X_l in P.X[l % 3] ([port][ldv])
-    uint16_t* Y[2];         // projections Yt_l in P.Y[l & 1] ([column][ldv])
+    uint16_t* X[kMaxQueryLevels + 1];  // port vectors X_l, l < H ([exterior port of level l][ldv])
+    uint16_t* Y[kMaxQueryLevels + 1];  // projections Yt_l, l >= 1 ([column of level l][ldv])
     uint32_t* M;            // sorted-order pair matrix (ldm), preset to 0xFFFFFFFF
     uint16_t* out;          // k x k result
+    unsigned* ctr;          // completion counters of the dataflow launch, cleared before it
+                            // (query_counter_words): [0] level-0 gather units, [1] project,
+                            // meet and same-leaf pair units, [2] root project items,
+                            // [4 + l*k + g] rows x column tiles of level-(l-1) project items
+                            // done for level-l group g (its target: cnt x column tiles)
     QueryLevel lv[kMaxQueryLevels + 1];
 };
+
+// Words of a request's completion counters.
+inline size_t query_counter_words(int H, int k) { return 4 + (size_t)(H + 1) * (size_t)(k > 0 ? k : 1); }
 
 // CTA work units of a request in phase t of the launch (host and device
 // agree on these numbers):
@@ -163,9 +171,14 @@ struct QueryLaunch {
     const int* unit_pre;       // [n_phases][n_req + 1]: exclusive prefix of units
     int* status;               // 0 ok, 1 grid barrier timeout
     unsigned* bar;             // grid barrier {count, generation}
-    unsigned long long* trace; // [0, n_phases]: phase starts as CTA 0 sees them; then from
-                               // [kMaxQueryPhases + 1 + t]: the latest end of work of phase t
-                               // over all CTAs; or null
+    unsigned long long* trace; // [0, n_phases]: phase starts as CTA 0 sees them (dataflow: [0]
+                               // the start, [t + 1] the latest end of a unit of phase t); then
+                               // from [kMaxQueryPhases + 1 + t]: the latest end of work of
+                               // phase t over all CTAs; or null
+    int dataflow;              // 1: no grid barrier - the CTAs stride over the units of all
+                               // phases in order and each unit first waits (bounded) for the
+                               // units whose results it reads (QueryParams::ctr); 0: phases
+                               // separated by grid barriers
 };
 constexpr int kMaxQueryPhases = kMaxQueryLevels + 3;
 

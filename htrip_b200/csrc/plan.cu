@@ -251,9 +251,12 @@ plan_query_kernel(const int32_t* __restrict__ vps, const uint8_t* __restrict__ p
                 Pq->cfg = tmpl.cfg;
                 Pq->ext0 = tmpl.ext0;
                 Pq->leaves = tmpl.leaves;
-                for (int j = 0; j < 3; ++j) Pq->X[j] = tmpl.X[j];
-                for (int j = 0; j < 2; ++j) Pq->Y[j] = tmpl.Y[j];
+                for (int j = 0; j <= kMaxQueryLevels; ++j) {
+                    Pq->X[j] = tmpl.X[j];
+                    Pq->Y[j] = tmpl.Y[j];
+                }
                 Pq->M = tmpl.M;
+                Pq->ctr = tmpl.ctr;
                 Pq->out = tmpl.out;
             }
         }

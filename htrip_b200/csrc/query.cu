@@ -33,9 +33,12 @@
 //            combine with atomicMin on a 32-bit k x k matrix.
 //
 // Phases: [level 0] | [project 1] | [project 2 + meet 1] | ... |
-// [project H + meet H-1] | [meet H] | [finalize], separated by grid
-// barriers (H + 2 in total); meets of level l-1 overlap projects of level l
-// because Yt and X are double / triple buffered.
+// [project H + meet H-1] | [meet H] | [finalize]; every level has its own
+// X and Yt buffers.  The default (dataflow) launch runs the units of all
+// phases without a grid barrier: each unit waits for the units it reads on
+// per-request completion counters, so a node's next level starts as soon as
+// its own children are done instead of when the slowest CTA of the level is.
+// The barrier launch (H + 2 grid barriers) stays selectable.
 //
 // Every sum is the exact clamped tropical product of minplus.cuh, so the
 // matrix equals the reference's bit for bit.
@@ -98,11 +101,16 @@ __device__ __forceinline__ void cp_wait() {
 // kPipeRows) of the compacted row list kl[0..n):
 //   acc[r][c] = min over its rows p of A[p*lda + r] (+) B[p*ldb + lane pair c].
 // A rows are RW consecutive u16 (16-byte aligned); B is already offset to the
-// lane's CP pairs (4*CP-byte aligned).  `pipe` is the warp's staging ring.
+// lane's CP pairs.  `pipe` is the warp's staging ring.  B0 is the warp's
+// first column (16-byte aligned); each B row is copied as 16-byte chunks,
+// chunks from column `bcols` on are taken from column 0 instead (their lanes'
+// results are not used).  All operand copies bypass L1 (cp.async.cg): the
+// X / Y rows may have been written by other CTAs of the same launch.
 template <int RW, int CP>
 __device__ __forceinline__ void warp_minplus_list(uint32_t (&acc)[RW][CP], const int* kl, int n, int warp,
                                                   const uint16_t* __restrict__ A, int lda,
-                                                  const uint16_t* __restrict__ B, int ldb, uint32_t* pipe) {
+                                                  const uint16_t* __restrict__ B0, int ldb, int bcols,
+                                                  uint32_t* pipe) {
     constexpr int U = kPipeRows, NS = kPipeStages, SW = pipe_slot_words<RW, CP>();
     const int lane = threadIdx.x & 31;
     const int stride = kWarps * U;
@@ -118,7 +126,10 @@ __device__ __forceinline__ void warp_minplus_list(uint32_t (&acc)[RW][CP], const
                 if (t < n) {
                     const int row = kl[t];
                     const uint32_t slot = sbase + (uint32_t)((st * U + u) * SW) * 4u;
-                    cp_async<CP * 4>(slot + lane * CP * 4, B + (size_t)row * ldb);
+                    if (lane < 8 * CP) {
+                        const int c8 = lane * 8 < bcols ? lane * 8 : 0;
+                        cp_async<16>(slot + lane * 16, B0 + (size_t)row * ldb + c8);
+                    }
                     if (lane < RW / 8) cp_async<16>(slot + CP * 128 + lane * 16, A + (size_t)row * lda + lane * 8);
                 }
             }
@@ -188,7 +199,7 @@ __device__ __forceinline__ int compact_flags(const uint8_t* __restrict__ flags, 
     const int per = (n + kThreads - 1) / kThreads;
     const int p0 = kb + tid * per, p1 = min(ke, p0 + per);
     int cntl = 0;
-    for (int p = p0; p < p1; ++p) cntl += flags[p] != 0;
+    for (int p = p0; p < p1; ++p) cntl += __ldcg(flags + p) != 0;
     int incl = cntl;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -205,7 +216,7 @@ __device__ __forceinline__ int compact_flags(const uint8_t* __restrict__ flags, 
     }
     int pos = base + incl - cntl;
     for (int p = p0; p < p1; ++p)
-        if (flags[p]) kl[pos++] = p;
+        if (__ldcg(flags + p)) kl[pos++] = p;
     __syncthreads();
     return total;
 }
@@ -334,16 +345,16 @@ __device__ void do_project(const QueryParams& P, const QueryLevel& L, const Quer
     const uint16_t* D = L.D + (size_t)node * L.NP * L.NP + (size_t)q * L.nP * L.NP;
     const int col = n0 + lane * 2 * CP;
     const bool live_col = col < L.NP;
-    const uint16_t* Xp = P.X[(l - 1) % 3] + slot0 + m0;
+    const uint16_t* Xp = P.X[l - 1] + slot0 + m0;
     uint32_t acc[RW][CP];
 #pragma unroll
     for (int r = 0; r < RW; ++r)
 #pragma unroll
         for (int c = 0; c < CP; ++c) acc[r][c] = INF2;
-    warp_minplus_list<RW, CP>(acc, kl, nA, warp, Xp, P.ldv, D + (live_col ? col : n0), L.NP,
+    warp_minplus_list<RW, CP>(acc, kl, nA, warp, Xp, P.ldv, D + n0, L.NP, L.NP - n0,
                               red + warp * pipe_warp_words<RW, CP>());
     cta_reduce<RW, CP>(acc, red);
-    uint16_t* Y = P.Y[l & 1];
+    uint16_t* Y = P.Y[l];
 #pragma unroll
     for (int cc = 0; cc < 2 * CP; ++cc) {
         const bool do_y = L.store_y && (cc % kWarps) == warp;
@@ -368,7 +379,7 @@ __device__ void do_project(const QueryParams& P, const QueryLevel& L, const Quer
         if (do_lift) {  // exterior column e of this node -> X_l[e][level-(l+1) slot]
             const int e = im.col[lane * 2 * CP + cc];
             if (e >= 0) {
-                uint16_t* Xn = P.X[l % 3] + (size_t)e * P.ldv;
+                uint16_t* Xn = P.X[l] + (size_t)e * P.ldv;
 #pragma unroll
                 for (int r = 0; r < RW; ++r) {
                     const int slot = im.row[0][r];
@@ -397,14 +408,15 @@ __device__ void do_meet(const QueryParams& P, const QueryLevel& L, int item, int
         else im.row[0][t - 64 * CP] = t - 64 * CP < nj ? L.s2v[j0 + t - 64 * CP] : -1;
     }
     const int nA = compact_flags(L.flags + (size_t)g2 * L.nP, kb, ke, kl, wsum);
-    const uint16_t* Xp = P.X[(l - 1) % 3] + j0;
-    const uint16_t* Y = P.Y[l & 1] + (size_t)coloff * P.ldv + i0 + lane * 2 * CP;
+    const uint16_t* Xp = P.X[l - 1] + j0;
+    const uint16_t* Y = P.Y[l] + (size_t)coloff * P.ldv + i0;
     uint32_t acc[RW][CP];
 #pragma unroll
     for (int r = 0; r < RW; ++r)
 #pragma unroll
         for (int c = 0; c < CP; ++c) acc[r][c] = INF2;
-    warp_minplus_list<RW, CP>(acc, kl, nA, warp, Xp, P.ldv, Y, P.ldv, red + warp * pipe_warp_words<RW, CP>());
+    warp_minplus_list<RW, CP>(acc, kl, nA, warp, Xp, P.ldv, Y, P.ldv, P.ldv - i0,
+                              red + warp * pipe_warp_words<RW, CP>());
     cta_reduce<RW, CP>(acc, red);
 #pragma unroll
     for (int r = 0; r < RW; ++r) {
@@ -446,7 +458,9 @@ __device__ void run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum,
             if (j < P.ns) {
                 const int* v = P.vp0 + 4 * j;
                 const uint16_t* row = P.leaves.base + ((size_t)v[0] * P.leaves.NP + v[1]) * P.leaves.NP;
-                for (int jj = j + 1; jj < v[3]; ++jj) P.M[(size_t)j * P.ldm + jj] = row[P.vp0[4 * jj + 1]];
+                // atomicMin: the level-1 meets (intra-child shortcuts) may
+                // already have lowered the entry in a dataflow launch
+                for (int jj = j + 1; jj < v[3]; ++jj) atomicMin(&P.M[(size_t)j * P.ldm + jj], (uint32_t)row[P.vp0[4 * jj + 1]]);
             }
         }
         return;
@@ -466,14 +480,138 @@ __device__ void run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum,
         uint32_t v = INF;
         if (ia >= 0 && ic >= 0) {
             if (ia == ic) v = 0;
-            else v = min(ia < ic ? P.M[(size_t)ia * P.ldm + ic] : P.M[(size_t)ic * P.ldm + ia], (uint32_t)INF);
+            else v = min(__ldcg(ia < ic ? P.M + (size_t)ia * P.ldm + ic : P.M + (size_t)ic * P.ldm + ia), (uint32_t)INF);
         }
         P.out[e] = (uint16_t)v;
     }
 }
 
-// The persistent kernel: phases separated by grid barriers; in each phase
-// the CTAs stride over the units of every request of the launch.
+// ---------------------------------------------------------------------------
+// Dataflow order.  Instead of a grid barrier after every phase, each unit
+// waits for the units it reads and counts itself done on the request's
+// completion counters (QueryParams::ctr):
+//   project, level 1          all level-0 gather units (ctr[0])
+//   project, level l >= 2     the level-(l-1) project items of its group's
+//     (group g)               node: ctr[4 + l*k + g] reaches cnt_g x column
+//                             tiles of level l-1 (every row of such an item
+//                             lifts into group g; each item adds its rows)
+//   meet, level l < H         the level-l project items of its node, i.e.
+//                             the counter of the level-(l+1) group it lifts to
+//   meet, level H             every root project item (ctr[2])
+//   output                    every project, meet and pair unit (ctr[1])
+// A dependency is always a unit of an earlier phase, and the CTAs take the
+// units of all phases in one ascending stride, so the lowest unfinished unit
+// always has its inputs (all CTAs are resident: cooperative launch).  Data
+// produced inside the launch is read through L2 only (cp.async.cg,
+// ld.global.cg): the L1 of an SM may hold a line of it from before it was
+// written.
+// ---------------------------------------------------------------------------
+constexpr unsigned kWaitPolls = 1u << 24;
+
+// Bounded wait of the whole CTA until *c >= target: thread 0 polls, the CTA
+// follows.  False after a timeout (recorded in *status) or when another CTA
+// has recorded one.
+__device__ __forceinline__ bool wait_count(const unsigned* c, unsigned target, int* status) {
+    int ok = 1;
+    if (threadIdx.x == 0) {
+        const volatile unsigned* vc = c;
+        const volatile int* vs = status;
+        unsigned it = 0;
+        while (*vc < target) {
+            if (*vs != 0) {
+                ok = 0;
+                break;
+            }
+            if (++it > kWaitPolls) {
+                atomicExch(status, 1);
+                ok = 0;
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+    }
+    return __syncthreads_and(ok) != 0;
+}
+
+__device__ __forceinline__ unsigned col_tiles(int NP, int NC) { return (unsigned)((NP + NC - 1) / NC); }
+
+// Waits for the inputs of unit u of phase t of request P (see above).
+template <int RW, int CP>
+__device__ __forceinline__ bool dep_wait(const QueryParams& P, int t, int u, int* status) {
+    constexpr int NC = 64 * CP;
+    if (t == 0) return true;
+    const unsigned* c = nullptr;
+    unsigned target = 0;
+    if (threadIdx.x == 0) {
+        const int H = P.H;
+        if (t == H + 2) {
+            target = (unsigned)((P.ns + kThreads - 1) / kThreads);
+            for (int l = 1; l <= H; ++l) target += (unsigned)(P.lv[l].n_items + P.lv[l].n_meet);
+            c = P.ctr + 1;
+        } else {
+            const int np = t <= H ? P.lv[t].n_items : 0;
+            if (u < np) {  // project item of level t
+                if (t == 1) {
+                    const long total = (long)P.n_l0_slots * P.nExt0;
+                    target = (unsigned)((total + kQueryL0Chunk - 1) / kQueryL0Chunk);
+                    c = P.ctr;
+                } else {
+                    const int gi = P.lv[t].items[3 * u];
+                    target = (unsigned)P.lv[t].groups[5 * gi + 3] * col_tiles(P.lv[t - 1].NP, NC);
+                    c = P.ctr + 4 + (size_t)t * P.k + gi;
+                }
+            } else {  // meet item of level t - 1
+                const int l = t - 1;
+                if (l == H) {
+                    target = (unsigned)P.lv[H].n_items;
+                    c = P.ctr + 2;
+                } else {
+                    const int j0 = P.lv[l].meet[7 * (u - np) + 1];
+                    const int pg = P.lv[l].lift[2 * j0 + 1];
+                    target = (unsigned)P.lv[l + 1].groups[5 * pg + 3] * col_tiles(P.lv[l].NP, NC);
+                    c = P.ctr + 4 + (size_t)(l + 1) * P.k + pg;
+                }
+            }
+        }
+    }
+    // thread 0 alone waits (the others pass a null counter and target 0)
+    return wait_count(c ? c : P.ctr, target, status);
+}
+
+// Counts unit u of phase t of request P as done, after every thread of the
+// CTA has issued its stores (the fence orders them before the counts).
+template <int RW, int CP>
+__device__ __forceinline__ void dep_signal(const QueryParams& P, int t, int u) {
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    const int H = P.H;
+    if (t == H + 2) return;
+    __threadfence();
+    if (t == 0) {
+        const long total = (long)P.n_l0_slots * P.nExt0;
+        const int n_fill = (int)((total + kQueryL0Chunk - 1) / kQueryL0Chunk);
+        atomicAdd(P.ctr + (u < n_fill ? 0 : 1), 1u);
+        return;
+    }
+    const int np = t <= H ? P.lv[t].n_items : 0;
+    if (u < np) {
+        if (t == H) {
+            atomicAdd(P.ctr + 2, 1u);
+        } else {
+            const int* it = P.lv[t].items + 3 * u;
+            const int* G = P.lv[t].groups + 5 * it[0];
+            const int rows = min(RW, G[3] - it[1]);
+            const int pg = P.lv[t].lift[2 * G[2] + 1];
+            atomicAdd(P.ctr + 4 + (size_t)(t + 1) * P.k + pg, (unsigned)rows);
+        }
+    }
+    atomicAdd(P.ctr + 1, 1u);
+}
+
+// The persistent kernel.  Barrier mode: phases separated by grid barriers;
+// in each phase the CTAs stride over the units of every request of the
+// launch.  Dataflow mode: one stride over the units of all phases.
 template <int RW, int CP>
 __global__ void __launch_bounds__(kThreads, 512 / kThreads) q_persistent_kernel(const QueryLaunch B) {
     extern __shared__ __align__(16) int qsm[];
@@ -483,6 +621,37 @@ __global__ void __launch_bounds__(kThreads, 512 / kThreads) q_persistent_kernel(
     __shared__ ItemMeta im;
     const bool stamp = B.trace && blockIdx.x == 0 && threadIdx.x == 0;
     if (stamp) B.trace[0] = global_timer();
+    if (B.dataflow) {
+        int total = 0;
+        for (int t = 0; t < B.n_phases; ++t) total += B.unit_pre[(size_t)t * (B.n_req + 1) + B.n_req];
+        for (int w = blockIdx.x; w < total; w += gridDim.x) {
+            int t = 0, wl = w;
+            for (;;) {
+                const int nt = B.unit_pre[(size_t)t * (B.n_req + 1) + B.n_req];
+                if (wl < nt) break;
+                wl -= nt;
+                ++t;
+            }
+            const int* pre = B.unit_pre + (size_t)t * (B.n_req + 1);
+            int lo = 0, hi = B.n_req;  // pre[lo] <= wl < pre[hi]
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (pre[mid] <= wl) lo = mid;
+                else hi = mid;
+            }
+            const QueryParams& P = B.req[lo];
+            const int u = wl - pre[lo];
+            if (!dep_wait<RW, CP>(P, t, u, B.status)) return;
+            run_unit<RW, CP>(P, t, u, kl, wsum, red, im);
+            dep_signal<RW, CP>(P, t, u);
+            if (B.trace && threadIdx.x == 0) {
+                const unsigned long long now = global_timer();
+                atomicMax(B.trace + t + 1, now);
+                atomicMax(B.trace + kMaxQueryPhases + 1 + t, now);
+            }
+        }
+        return;
+    }
     for (int t = 0; t < B.n_phases; ++t) {
         const int* pre = B.unit_pre + (size_t)t * (B.n_req + 1);
         const int total = pre[B.n_req];
