@@ -2485,18 +2485,27 @@ htrip_status htrip_state_digest(const htrip_index* h, uint64_t* out, int32_t n_o
     HTRIP_GUARD_END
 }
 
-htrip_status htrip_selftest_barrier_timeout(int device, int32_t* status, int32_t* ctas_returned, float* ms) {
+static htrip_status timeout_selftest(int kind, int device, int32_t* status, int32_t* ctas_returned, float* ms) {
     if (!status || !ctas_returned || !ms) return fail(HTRIP_ERR_INVALID, "null argument");
     HTRIP_GUARD_BEGIN
     ck(cudaSetDevice(device), "cudaSetDevice");
     int st = 0, ret = 0;
     float t = 0.f;
-    ck(hb::barrier_timeout_selftest(&st, &ret, &t), "barrier self-test");
+    ck(kind == 0 ? hb::barrier_timeout_selftest(&st, &ret, &t) : hb::wait_timeout_selftest(&st, &ret, &t),
+       "timeout self-test");
     *status = st;
     *ctas_returned = ret;
     *ms = t;
     return HTRIP_OK;
     HTRIP_GUARD_END
+}
+
+htrip_status htrip_selftest_barrier_timeout(int device, int32_t* status, int32_t* ctas_returned, float* ms) {
+    return timeout_selftest(0, device, status, ctas_returned, ms);
+}
+
+htrip_status htrip_selftest_wait_timeout(int device, int32_t* status, int32_t* ctas_returned, float* ms) {
+    return timeout_selftest(1, device, status, ctas_returned, ms);
 }
 
 htrip_status htrip_measure_minplus_rate(int device, int variant, double* entries_per_s) {

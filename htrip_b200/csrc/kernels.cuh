@@ -240,6 +240,7 @@ int query_max_ports();  // largest per-child port count the query kernel handles
 // fifth CTA) with a short poll limit: *status is the status word the
 // timeout sets (1), *returned the number of CTAs that returned (4).
 cudaError_t barrier_timeout_selftest(int* status, int* returned, float* ms);
+cudaError_t wait_timeout_selftest(int* status, int* returned, float* ms);
 cudaError_t launch_query(const QueryLaunch& L, int cfg, int grid, cudaStream_t st);
 
 // *out += canonical checksum of the first `count` matrices of M (logical

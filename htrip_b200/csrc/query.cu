@@ -499,9 +499,10 @@ __device__ void run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum,
 //                             the counter of the level-(l+1) group it lifts to
 //   meet, level H             every root project item (ctr[2])
 //   output                    every project, meet and pair unit (ctr[1])
-// A dependency is always a unit of an earlier phase, and the CTAs take the
-// units of all phases in one ascending stride, so the lowest unfinished unit
-// always has its inputs (all CTAs are resident: cooperative launch).  Data
+// A dependency is always a unit of an earlier phase, and the units of all
+// phases are handed out in ascending order (one ticket counter), so the
+// lowest unfinished unit has been handed out and has its inputs: every
+// wait ends (all CTAs are resident: cooperative launch).  Data
 // produced inside the launch is read through L2 only (cp.async.cg,
 // ld.global.cg): the L1 of an SM may hold a line of it from before it was
 // written.
@@ -511,7 +512,8 @@ constexpr unsigned kWaitPolls = 1u << 24;
 // Bounded wait of the whole CTA until *c >= target: thread 0 polls, the CTA
 // follows.  False after a timeout (recorded in *status) or when another CTA
 // has recorded one.
-__device__ __forceinline__ bool wait_count(const unsigned* c, unsigned target, int* status) {
+__device__ __forceinline__ bool wait_count(const unsigned* c, unsigned target, int* status,
+                                           unsigned limit = kWaitPolls) {
     int ok = 1;
     if (threadIdx.x == 0) {
         const volatile unsigned* vc = c;
@@ -522,7 +524,7 @@ __device__ __forceinline__ bool wait_count(const unsigned* c, unsigned target, i
                 ok = 0;
                 break;
             }
-            if (++it > kWaitPolls) {
+            if (++it > limit) {
                 atomicExch(status, 1);
                 ok = 0;
                 break;
@@ -534,13 +536,24 @@ __device__ __forceinline__ bool wait_count(const unsigned* c, unsigned target, i
     return __syncthreads_and(ok) != 0;
 }
 
+// Self-test of the bounded counter wait: every CTA waits for a count that
+// nothing adds, gives up after `limit` polls (or once another CTA recorded
+// the timeout) and returns.
+__global__ void wait_timeout_probe_kernel(const unsigned* ctr, int* status, unsigned limit, int* returned) {
+    wait_count(ctr, 1u, status, limit);
+    if (threadIdx.x == 0) atomicAdd(returned, 1);
+}
+
 __device__ __forceinline__ unsigned col_tiles(int NP, int NC) { return (unsigned)((NP + NC - 1) / NC); }
 
 // Waits for the inputs of unit u of phase t of request P (see above).
 template <int RW, int CP>
 __device__ __forceinline__ bool dep_wait(const QueryParams& P, int t, int u, int* status) {
     constexpr int NC = 64 * CP;
-    if (t == 0) return true;
+    if (t == 0) {  // level-0 units read nothing of the launch; the barrier
+        __syncthreads();  // still orders this unit's reads of next_w before its update
+        return true;
+    }
     const unsigned* c = nullptr;
     unsigned target = 0;
     if (threadIdx.x == 0) {
@@ -622,9 +635,17 @@ __global__ void __launch_bounds__(kThreads, 512 / kThreads) q_persistent_kernel(
     const bool stamp = B.trace && blockIdx.x == 0 && threadIdx.x == 0;
     if (stamp) B.trace[0] = global_timer();
     if (B.dataflow) {
+        // Units are handed out in ascending order by a ticket (the barrier's
+        // count word, unused here); a CTA takes its next ticket when it starts
+        // a unit, so the fetch overlaps the work.
+        __shared__ int next_w;
         int total = 0;
         for (int t = 0; t < B.n_phases; ++t) total += B.unit_pre[(size_t)t * (B.n_req + 1) + B.n_req];
-        for (int w = blockIdx.x; w < total; w += gridDim.x) {
+        if (threadIdx.x == 0) next_w = (int)atomicAdd(B.bar, 1u);
+        __syncthreads();
+        for (;;) {
+            const int w = next_w;
+            if (w >= total) break;
             int t = 0, wl = w;
             for (;;) {
                 const int nt = B.unit_pre[(size_t)t * (B.n_req + 1) + B.n_req];
@@ -642,8 +663,11 @@ __global__ void __launch_bounds__(kThreads, 512 / kThreads) q_persistent_kernel(
             const QueryParams& P = B.req[lo];
             const int u = wl - pre[lo];
             if (!dep_wait<RW, CP>(P, t, u, B.status)) return;
+            // every thread has read next_w (the wait is a CTA barrier)
+            const int nxt = threadIdx.x == 0 ? (int)atomicAdd(B.bar, 1u) : 0;
             run_unit<RW, CP>(P, t, u, kl, wsum, red, im);
-            dep_signal<RW, CP>(P, t, u);
+            if (threadIdx.x == 0) next_w = nxt;
+            dep_signal<RW, CP>(P, t, u);  // begins with a CTA barrier: next_w is visible after it
             if (B.trace && threadIdx.x == 0) {
                 const unsigned long long now = global_timer();
                 atomicMax(B.trace + t + 1, now);
@@ -703,8 +727,11 @@ void configure_query_kernels() {
 
 int query_max_ports() { return kMaxList - 64; }
 
-cudaError_t barrier_timeout_selftest(int* status, int* returned, float* ms) {
-    // words: {status, barrier count, barrier generation, CTAs returned}
+// Runs one 4-CTA probe launch whose waits can never be satisfied (kind 0:
+// the grid barrier, expecting a fifth CTA; kind 1: a completion counter that
+// nothing adds to) with a short poll limit.
+static cudaError_t timeout_selftest(int kind, int* status, int* returned, float* ms) {
+    // words: {status, barrier count / counter, barrier generation, CTAs returned}
     unsigned* w = nullptr;
     cudaError_t e = cudaMalloc(&w, 4 * sizeof(unsigned));
     if (e != cudaSuccess) return e;
@@ -713,7 +740,11 @@ cudaError_t barrier_timeout_selftest(int* status, int* returned, float* ms) {
     cudaEventCreate(&e1);
     cudaMemset(w, 0, 4 * sizeof(unsigned));
     cudaEventRecord(e0);
-    barrier_timeout_probe_kernel<<<4, 64>>>(w + 1, reinterpret_cast<int*>(w), 1u << 14, reinterpret_cast<int*>(w + 3));
+    if (kind == 0)
+        barrier_timeout_probe_kernel<<<4, 64>>>(w + 1, reinterpret_cast<int*>(w), 1u << 14,
+                                                reinterpret_cast<int*>(w + 3));
+    else
+        wait_timeout_probe_kernel<<<4, 64>>>(w + 1, reinterpret_cast<int*>(w), 1u << 14, reinterpret_cast<int*>(w + 3));
     cudaEventRecord(e1);
     e = cudaEventSynchronize(e1);
     unsigned h[4] = {0, 0, 0, 0};
@@ -725,6 +756,14 @@ cudaError_t barrier_timeout_selftest(int* status, int* returned, float* ms) {
     cudaEventDestroy(e1);
     cudaFree(w);
     return e;
+}
+
+cudaError_t barrier_timeout_selftest(int* status, int* returned, float* ms) {
+    return timeout_selftest(0, status, returned, ms);
+}
+
+cudaError_t wait_timeout_selftest(int* status, int* returned, float* ms) {
+    return timeout_selftest(1, status, returned, ms);
 }
 
 int query_grid_blocks(int device) {

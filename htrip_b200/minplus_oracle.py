@@ -88,7 +88,7 @@ EXPORTS = (
     "htrip_autotune_query", "htrip_autotune_export", "htrip_autotune_import", "htrip_autotune_clear",
     "htrip_lift_root", "htrip_query_distance", "htrip_incremental_create", "htrip_incremental_destroy",
     "htrip_query_all_pairs_incremental", "htrip_batch_create_priority", "htrip_cell_blocked",
-    "htrip_leaves_changed", "htrip_selftest_barrier_timeout", "htrip_set_cell_weights",
+    "htrip_leaves_changed", "htrip_selftest_barrier_timeout", "htrip_selftest_wait_timeout", "htrip_set_cell_weights",
     "htrip_cell_weight_changed", "htrip_tile_weights_changed", "htrip_server_wait_version",
 )
 
@@ -146,6 +146,7 @@ def load_library(path: str | None = None):
     lib.htrip_lift_root.argtypes = [P, _U8P, I, I]
     lib.htrip_cell_blocked.argtypes = [P, I, I, _U8P, I, I]
     lib.htrip_selftest_barrier_timeout.argtypes = [C.c_int, _I32P, _I32P, C.POINTER(C.c_float)]
+    lib.htrip_selftest_wait_timeout.argtypes = [C.c_int, _I32P, _I32P, C.POINTER(C.c_float)]
     lib.htrip_leaves_changed.argtypes = [P, _I32P, I, _U8P, I, I]
     lib.htrip_set_cell_weights.argtypes = [P, _U16P, I, I]
     lib.htrip_cell_weight_changed.argtypes = [P, I, I, C.c_uint16, _U8P, I, I]
@@ -678,6 +679,14 @@ def selftest_barrier_timeout(device: int = 0):
     lib = load_library()
     st, ret, ms = C.c_int32(), C.c_int32(), C.c_float()
     _check(lib.htrip_selftest_barrier_timeout(device, C.byref(st), C.byref(ret), C.byref(ms)))
+    return st.value, ret.value, ms.value
+
+
+def selftest_wait_timeout(device: int = 0):
+    """(status, CTAs returned, ms) of completion-counter waits that cannot be satisfied."""
+    lib = load_library()
+    st, ret, ms = C.c_int32(), C.c_int32(), C.c_float()
+    _check(lib.htrip_selftest_wait_timeout(device, C.byref(st), C.byref(ret), C.byref(ms)))
     return st.value, ret.value, ms.value
 
 

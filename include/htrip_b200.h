@@ -379,10 +379,13 @@ htrip_status htrip_last_open_work(const htrip_index* h, uint64_t* alg_bytes, uin
 /* Phase trace of the last query launch of an index / a batch: ns[i] =
  * global-timer nanoseconds of phase i of the persistent query kernel
  * (0: level-0 gathers; 1..H+1: projections of level i with the meets of
- * level i-1; H+2: output), as seen by its first CTA.  With max_n >= 2 *
- * phases, ns[phases + i] is the part of phase i until its last CTA finished
- * its work (the rest of the phase is the grid-barrier wait).  *n = entries
- * written.                                                                */
+ * level i-1; H+2: output).  Barrier schedule (HTRIP_QUERY_DATAFLOW=0): the
+ * phase as its first CTA sees it; with max_n >= 2 * phases, ns[phases + i]
+ * is the part of phase i until its last CTA finished its work (the rest is
+ * the grid-barrier wait).  Dataflow schedule (default; phases overlap): the
+ * time from the end of the last unit of phase i-1 (the launch start for
+ * i = 0) to the end of the last unit of phase i, in both halves.  *n =
+ * entries written.                                                        */
 htrip_status htrip_last_query_phases(const htrip_index* h, uint64_t* ns, int32_t max_n, int32_t* n);
 htrip_status htrip_batch_last_phases(const htrip_batch* b, uint64_t* ns, int32_t max_n, int32_t* n);
 
@@ -394,6 +397,12 @@ htrip_status htrip_batch_last_phases(const htrip_batch* b, uint64_t* ns, int32_t
  * fifth CTA) with a short limit: *status = 1 (timeout recorded),
  * *ctas_returned = 4, *ms = the launch's duration.                        */
 htrip_status htrip_selftest_barrier_timeout(int device, int32_t* status, int32_t* ctas_returned, float* ms);
+
+/* The same for the completion-counter waits of the query kernel's default
+ * (dataflow) schedule: a 4-CTA launch in which every CTA waits for a count
+ * that nothing adds, with a short poll limit: *status = 1, *ctas_returned =
+ * 4, *ms = the launch's duration.                                          */
+htrip_status htrip_selftest_wait_timeout(int device, int32_t* status, int32_t* ctas_returned, float* ms);
 
 /* Wait for all work queued on the index's stream.                         */
 htrip_status htrip_sync(htrip_index* h);

@@ -1,7 +1,8 @@
-"""Failure detection without a GPU fault: the query kernel's grid-barrier
-waits are bounded.  A launch whose barrier can never complete gives up after
-its poll limit, records the timeout in its status word, every CTA returns,
-and the context stays usable (a query on it is still exact)."""
+"""Failure detection without a GPU fault: the query kernel's waits are
+bounded, both the grid barrier (barrier schedule) and the completion-counter
+waits (dataflow schedule).  A launch whose wait can never be satisfied gives
+up after its poll limit, records the timeout in its status word, every CTA
+returns, and the context stays usable (a query on it is still exact)."""
 import numpy as np
 import pytest
 
@@ -21,4 +22,18 @@ def test_barrier_wait_runs_out_and_context_survives(gpu):
     dev = MinPlusOracle(HierarchyConfig(8, 2, 2))
     assert dev.build(grid)
     vps = viewpoints(grid, 12, 3)
+    np.testing.assert_array_equal(dev.queryAllPairs(vps, grid), port_bfs(grid, vps))
+
+
+def test_counter_wait_runs_out_and_context_survives(gpu):
+    from htrip_b200.minplus_oracle import HierarchyConfig, MinPlusOracle, selftest_wait_timeout
+    from oracle.ref import port_bfs
+    status, returned, ms = selftest_wait_timeout(0)
+    assert status == 1
+    assert returned == 4
+    assert ms < 2000.0
+    grid = make_grid("street", 32, 32, 4)
+    dev = MinPlusOracle(HierarchyConfig(8, 2, 2))
+    assert dev.build(grid)
+    vps = viewpoints(grid, 12, 4)
     np.testing.assert_array_equal(dev.queryAllPairs(vps, grid), port_bfs(grid, vps))
