@@ -1050,7 +1050,7 @@ struct QueryPlan {
     int o_vp0 = 0, o_inv = 0, o_l0 = 0, n_l0 = 0;
     struct Lvl {
         int o_groups = 0, n_groups = 0, max_group = 0, slots = 0;
-        int o_items = 0, n_items = 0;
+        int o_items = 0, n_items = 0, split = 1;
         int o_meet = 0, n_meet = 0;
         int o_s2v = 0, o_lift = 0;
         size_t flags_off = 0;
@@ -1062,6 +1062,23 @@ struct QueryPlan {
 // Tile configuration of a query (hb::query_config_tile); the autotuner may
 // override the default choice per (index shape, viewpoint count) bucket.
 int choose_query_cfg(const htrip_index* h, int ns, int root_group);
+
+// Parts per project item of level l (QueryLevel::split).  Root items are the
+// longest (the root's child port list: ~1000 ports for a 256-cell child,
+// against a few dozen at level 1).  Cutting them costs a unit's fixed
+// overhead (a few microseconds) per extra part, which only pays when the
+// root has fewer items than the grid has CTAs; on a 512 x 512 map with 256
+// viewpoints (344 root items) 1 / 2 / 3 / 4 parts measured 136 / 143 / 153
+// / 164 us per query kernel.  HTRIP_QUERY_ROOT_SPLIT=n (1..8) sets the
+// root's split.
+int query_item_split(const htrip_index* h, int l) {
+    if (l < 1 || l != h->H) return 1;
+    static const int forced = [] {
+        const char* e = std::getenv("HTRIP_QUERY_ROOT_SPLIT");
+        return e ? std::clamp(std::atoi(e), 1, 8) : 0;
+    }();
+    return forced ? forced : 1;
+}
 
 // Plans a query; force_cfg >= 0 imposes the tile configuration (requests
 // that share a launch share one).
@@ -1179,6 +1196,7 @@ void make_plan(const htrip_index* h, const int32_t* vps, const uint8_t* pass_fla
                 for (int n0 = n_begin; n0 < Lv.NP; n0 += NC) P.buf.insert(P.buf.end(), {gi, m0, n0});
         }
         Q.n_items = ((int)P.buf.size() - Q.o_items) / 3;
+        Q.split = query_item_split(h, l);
         Q.o_s2v = (int)P.buf.size();
         P.buf.resize(P.buf.size() + Q.slots + NC, -1);
         for (const CG& c : G)
@@ -1252,7 +1270,7 @@ struct LaunchLayout {
     int n = 0, n_phases = 0;
     size_t o_params = 0, o_pre = 0, o_words = 0, head = 0;
     size_t o_M = 0, M_bytes = 0, o_flags = 0, flags_bytes = 0, o_out = 0, out_bytes = 0, total = 0;
-    std::vector<size_t> plan, M, flags, ctr, out;
+    std::vector<size_t> plan, M, flags, ctr, ticket, part, out;
     std::vector<std::array<size_t, hb::kMaxQueryLevels + 1>> X, Y;
 };
 
@@ -1303,8 +1321,15 @@ LaunchLayout layout_launch(const std::vector<QueryReq>& R) {
     for (const auto& r : R) {
         L.flags.push_back(take(r.P->flags_total));
         L.ctr.push_back(take(hb::query_counter_words(r.h->H, r.P->k) * sizeof(unsigned)));
+        const QueryPlan::Lvl& root = r.P->lv[r.h->H];
+        L.ticket.push_back(root.split > 1 ? take((size_t)root.n_items * sizeof(unsigned)) : 0);
     }
     L.flags_bytes = off - L.o_flags;
+    for (const auto& r : R) {
+        const QueryPlan::Lvl& root = r.P->lv[r.h->H];
+        const hb::QueryTile tile = hb::query_config_tile(r.P->cfg);
+        L.part.push_back(root.split > 1 ? take((size_t)root.n_items * root.split * tile.RW * tile.NCOL * 2) : 0);
+    }
     for (const auto& r : R) {
         std::array<size_t, hb::kMaxQueryLevels + 1> x{}, y{};
         for (int l = 0; l < r.h->H; ++l) x[l] = take(query_x_rows(r.h, l) * r.P->ldv * sizeof(uint16_t));
@@ -1328,7 +1353,7 @@ void query_units(const htrip_index* h, const QueryPlan& P, int n_phases, int* un
     units[0] = (int)((fill + hb::kQueryL0Chunk - 1) / hb::kQueryL0Chunk) +
                (P.n_sorted + hb::kQueryThreads - 1) / hb::kQueryThreads;
     for (int t = 1; t <= H + 1; ++t)
-        units[t] = (t <= H ? P.lv[t].n_items : 0) + (t - 1 >= 1 ? P.lv[t - 1].n_meet : 0);
+        units[t] = (t <= H ? P.lv[t].n_items * P.lv[t].split : 0) + (t - 1 >= 1 ? P.lv[t - 1].n_meet : 0);
     units[H + 2] = (int)(((long)P.k * P.k + hb::kQueryFinChunk - 1) / hb::kQueryFinChunk);
 }
 
@@ -1373,6 +1398,11 @@ hb::QueryParams make_params(const htrip_index* h, const QueryPlan& P, unsigned c
         q.s2v = plan + PL.o_s2v;
         q.lift = l < H ? plan + PL.o_lift : nullptr;
         q.store_y = 1;
+        q.split = PL.split;
+        if (PL.split > 1) {
+            q.part = reinterpret_cast<uint32_t*>(base + L.part[i]);
+            q.ticket = reinterpret_cast<unsigned*>(base + L.ticket[i]);
+        }
     }
     return Q;
 }
@@ -1539,7 +1569,9 @@ struct DevPlanLayout {
     hb::PlanGeom G{};
     hb::PlanLayout O{};
     size_t o_params = 0, o_pre = 0, o_words = 0, o_in = 0, o_plan = 0, o_M = 0, o_flags = 0, o_out = 0;
-    size_t X[hb::kMaxQueryLevels + 1] = {}, Y[hb::kMaxQueryLevels + 1] = {}, o_ctr = 0, total = 0;
+    size_t X[hb::kMaxQueryLevels + 1] = {}, Y[hb::kMaxQueryLevels + 1] = {}, o_ctr = 0, o_ticket = 0, o_part = 0;
+    size_t total = 0;
+    int root_split = 1;
     int n_phases = 0, fill_blocks = 1;
 };
 
@@ -1654,11 +1686,17 @@ DevPlanLayout devplan_layout(const htrip_index* h, int k, int cfg, bool out_in_a
     const size_t ldm = std::max<size_t>(8, ((size_t)k + 7) / 8 * 8);
     O.M_bytes = (long long)(ldm * ldm * sizeof(uint32_t));
     D.o_M = takeb((size_t)O.M_bytes);
-    // the planner's preset blocks clear the flags and the counters after them
+    // the planner's preset blocks clear the flags, the counters and the split
+    // items' tickets after them
+    D.root_split = H >= 1 ? query_item_split(h, H) : 1;
     const size_t ctr_at = (flags + 15) / 16 * 16;
-    O.flags_bytes = (long long)(ctr_at + hb::query_counter_words(H, k) * sizeof(unsigned));
+    const size_t ticket_at = ctr_at + hb::query_counter_words(H, k) * sizeof(unsigned);
+    const size_t root_items = H >= 1 ? (size_t)O.cap_items[H] : 0;
+    O.flags_bytes = (long long)(ticket_at + (D.root_split > 1 ? root_items * sizeof(unsigned) : 0));
     D.o_flags = takeb((size_t)O.flags_bytes);
     D.o_ctr = D.o_flags + ctr_at;
+    D.o_ticket = D.o_flags + ticket_at;
+    D.o_part = D.root_split > 1 ? takeb(root_items * D.root_split * RW * NC * 2) : 0;
     for (int l = 0; l < H; ++l) D.X[l] = takeb(query_x_rows(h, l) * O.cap_ldv * sizeof(uint16_t));
     for (int l = 1; l <= H; ++l) D.Y[l] = takeb(query_y_rows(h, l) * O.cap_ldv * sizeof(uint16_t));
     D.o_out = out_in_arena ? takeb((size_t)k * k * sizeof(uint16_t)) : 0;
@@ -1774,6 +1812,11 @@ int run_devplan(htrip_index* h, int k, int cfg, const int32_t* vps_host, const u
         T.lv[l].nP = Lv.nP;
         T.lv[l].ext_inv = Lv.d_ext_inv.p;
         T.lv[l].store_y = 1;
+        T.lv[l].split = l == h->H ? D.root_split : 1;
+        if (T.lv[l].split > 1) {
+            T.lv[l].part = reinterpret_cast<uint32_t*>(base + D.o_part);
+            T.lv[l].ticket = reinterpret_cast<unsigned*>(base + D.o_ticket);
+        }
     }
     hb::PlanLayout& O = D.O;
     O.plan = reinterpret_cast<int*>(base + D.o_plan);

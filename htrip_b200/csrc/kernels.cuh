@@ -124,6 +124,10 @@ struct QueryLevel {
     const int* s2v;         // level-l slot -> sorted viewpoint or -1
     const int* lift;        // level-l slot -> {level-(l+1) slot, level-(l+1) group}
     int store_y;
+    int split;              // >= 1: every project item runs as `split` units, each over one
+                            // part of its compacted port list
+    uint32_t* part;         // split > 1: partial tiles [item][part][RW * NC / 2 words]
+    unsigned* ticket;       // split > 1: parts of each item done, cleared before the launch
 };
 
 // One queryAllPairs request of a launch.
@@ -153,8 +157,9 @@ inline size_t query_counter_words(int H, int k) { return 4 + (size_t)(H + 1) * (
 // agree on these numbers):
 //   t = 0          level-0 port gathers in chunks of kQueryL0Chunk, then
 //                  same-leaf pair rows in chunks of kQueryThreads
-//   1 <= t <= H+1  project items of level t (t <= H), then meet items of
-//                  level t-1 (t >= 2)
+//   1 <= t <= H+1  project items of level t (t <= H; `split` units per
+//                  item, its parts in order), then meet items of level t-1
+//                  (t >= 2)
 //   t = H+2        output chunks of kQueryFinChunk entries
 #ifndef HB_QUERY_THREADS
 #define HB_QUERY_THREADS 256

@@ -243,6 +243,9 @@ plan_query_kernel(const int32_t* __restrict__ vps, const uint8_t* __restrict__ p
             lv.nP = tmpl.lv[l].nP;
             lv.ext_inv = tmpl.lv[l].ext_inv;
             lv.store_y = tmpl.lv[l].store_y;
+            lv.split = tmpl.lv[l].split;
+            lv.part = tmpl.lv[l].part;
+            lv.ticket = tmpl.lv[l].ticket;
         }
         if (blockIdx.x == 0) {
             for (int i = lane; i < O.words_bytes / 4; i += 32) O.words[i] = 0;
@@ -514,7 +517,8 @@ plan_query_kernel(const int32_t* __restrict__ vps, const uint8_t* __restrict__ p
     const int n_l0 = H >= 1 ? __shfl_sync(0xffffffffu, own ? vr[3] : 0, 0) : 0;
     const int root = H >= 1 ? __shfl_sync(0xffffffffu, r_root, H - 1) : ns;
     // phase t: project items of level t (lane t-1), meet items of level t-1 (lane t-2)
-    const int items_t = __shfl_sync(0xffffffffu, r_items, max(lane - 1, 0));
+    const int items_t = __shfl_sync(0xffffffffu, r_items, max(lane - 1, 0)) *
+                        (lane >= 1 && lane <= H ? tmpl.lv[lane].split : 1);
     const int meet_t = __shfl_sync(0xffffffffu, r_meet, max(lane - 2, 0));
     const int n_phases = H + 3;
     if (lane < n_phases) {

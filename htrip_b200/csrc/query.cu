@@ -318,12 +318,48 @@ struct ItemMeta {
     int row[2][16];
 };
 
-// project item {group, m0, n0}: tile of RW slots x 64*CP node columns; the
-// CTA's warps split the group's finite ports.  After the reduction the
-// epilogue (Y stores and lift scatters) is spread over the warps.
+// Split item: every part stores its reduced tile (warp 0); the part that
+// completes the item's ticket folds the others into its own and returns
+// true (it runs the epilogue), the others return false.
 template <int RW, int CP>
-__device__ void do_project(const QueryParams& P, const QueryLevel& L, const QueryLevel* Ln, int item, int l,
-                           int* kl, int* wsum, uint32_t* red, ItemMeta& im) {
+__device__ bool combine_parts(const QueryLevel& L, int item, int part, uint32_t (&acc)[RW][CP]) {
+    constexpr int E = RW * CP * 32;
+    __shared__ int last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp == 0) {
+        uint32_t* mine = L.part + ((size_t)item * L.split + part) * E;
+#pragma unroll
+        for (int r = 0; r < RW; ++r)
+#pragma unroll
+            for (int c = 0; c < CP; ++c) mine[(r * CP + c) * 32 + lane] = acc[r][c];
+        __threadfence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned old = atomicAdd(L.ticket + item, 1u);
+        last = old == (unsigned)(L.split - 1);
+        __threadfence();
+    }
+    __syncthreads();
+    if (!last) return false;
+    for (int p = 0; p < L.split; ++p) {
+        if (p == part) continue;
+        const uint32_t* o = L.part + ((size_t)item * L.split + p) * E;
+#pragma unroll
+        for (int r = 0; r < RW; ++r)
+#pragma unroll
+            for (int c = 0; c < CP; ++c) acc[r][c] = min2(acc[r][c], __ldcg(o + (r * CP + c) * 32 + lane));
+    }
+    return true;
+}
+
+// project item {group, m0, n0}: tile of RW slots x 64*CP node columns; the
+// CTA's warps split the group's finite ports (part `part` of L.split of
+// them).  After the reduction the epilogue (Y stores and lift scatters) is
+// spread over the warps.  Returns whether the item is complete.
+template <int RW, int CP>
+__device__ bool do_project(const QueryParams& P, const QueryLevel& L, const QueryLevel* Ln, int item, int part,
+                           int l, int* kl, int* wsum, uint32_t* red, ItemMeta& im) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, tid = threadIdx.x;
     const int* it = L.items + 3 * item;
     const int gi = it[0], m0 = it[1], n0 = it[2];
@@ -342,6 +378,7 @@ __device__ void do_project(const QueryParams& P, const QueryLevel& L, const Quer
         }
     }
     const int nA = compact_flags(L.flags + (size_t)gi * L.nP, 0, L.nP, kl, wsum);
+    const int kb = (int)((long)nA * part / L.split), ke = (int)((long)nA * (part + 1) / L.split);
     const uint16_t* D = L.D + (size_t)node * L.NP * L.NP + (size_t)q * L.nP * L.NP;
     const int col = n0 + lane * 2 * CP;
     const bool live_col = col < L.NP;
@@ -351,9 +388,13 @@ __device__ void do_project(const QueryParams& P, const QueryLevel& L, const Quer
     for (int r = 0; r < RW; ++r)
 #pragma unroll
         for (int c = 0; c < CP; ++c) acc[r][c] = INF2;
-    warp_minplus_list<RW, CP>(acc, kl, nA, warp, Xp, P.ldv, D + n0, L.NP, L.NP - n0,
+    warp_minplus_list<RW, CP>(acc, kl + kb, ke - kb, warp, Xp, P.ldv, D + n0, L.NP, L.NP - n0,
                               red + warp * pipe_warp_words<RW, CP>());
     cta_reduce<RW, CP>(acc, red);
+    if (L.split > 1 && !combine_parts<RW, CP>(L, item, part, acc)) {
+        __syncthreads();  // kl / red / im are reused by the next item
+        return false;
+    }
     uint16_t* Y = P.Y[l];
 #pragma unroll
     for (int cc = 0; cc < 2 * CP; ++cc) {
@@ -392,6 +433,7 @@ __device__ void do_project(const QueryParams& P, const QueryLevel& L, const Quer
         }
     }
     __syncthreads();  // kl / red / im are reused by the next item
+    return true;
 }
 
 // meet item {i0, j0, nj, g2, coloff, kb, ke}: rows = RW viewpoints j of
@@ -433,9 +475,10 @@ __device__ void do_meet(const QueryParams& P, const QueryLevel& L, int item, int
     __syncthreads();
 }
 
-// One CTA work unit of request P in phase t (see QueryLaunch).
+// One CTA work unit of request P in phase t (see QueryLaunch).  Returns
+// false for a part of a split project item that did not complete it.
 template <int RW, int CP>
-__device__ void run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum, uint32_t* red, ItemMeta& im) {
+__device__ bool run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum, uint32_t* red, ItemMeta& im) {
     const int tid = threadIdx.x;
     if (t == 0) {
         // level 0: X0 in level-1 slot order (+ level-1 flags), same-leaf pairs
@@ -463,13 +506,16 @@ __device__ void run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum,
                 for (int jj = j + 1; jj < v[3]; ++jj) atomicMin(&P.M[(size_t)j * P.ldm + jj], (uint32_t)row[P.vp0[4 * jj + 1]]);
             }
         }
-        return;
+        return true;
     }
     if (t <= P.H + 1) {
-        const int np = t <= P.H ? P.lv[t].n_items : 0;
-        if (u < np) do_project<RW, CP>(P, P.lv[t], t < P.H ? &P.lv[t + 1] : nullptr, u, t, kl, wsum, red, im);
-        else do_meet<RW, CP>(P, P.lv[t - 1], u - np, t - 1, kl, wsum, red, im);
-        return;
+        const int S = t <= P.H ? P.lv[t].split : 1;
+        const int np = t <= P.H ? P.lv[t].n_items * S : 0;
+        if (u < np)
+            return do_project<RW, CP>(P, P.lv[t], t < P.H ? &P.lv[t + 1] : nullptr, u / S, u % S, t, kl, wsum, red,
+                                      im);
+        do_meet<RW, CP>(P, P.lv[t - 1], u - np, t - 1, kl, wsum, red, im);
+        return true;
     }
     // t == H + 2: out[a][c] for one chunk of the k x k output
     const int kk = P.k * P.k;
@@ -484,6 +530,7 @@ __device__ void run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum,
         }
         P.out[e] = (uint16_t)v;
     }
+    return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -560,17 +607,17 @@ __device__ __forceinline__ bool dep_wait(const QueryParams& P, int t, int u, int
         const int H = P.H;
         if (t == H + 2) {
             target = (unsigned)((P.ns + kThreads - 1) / kThreads);
-            for (int l = 1; l <= H; ++l) target += (unsigned)(P.lv[l].n_items + P.lv[l].n_meet);
+            for (int l = 1; l <= H; ++l) target += (unsigned)(P.lv[l].n_items * P.lv[l].split + P.lv[l].n_meet);
             c = P.ctr + 1;
         } else {
-            const int np = t <= H ? P.lv[t].n_items : 0;
-            if (u < np) {  // project item of level t
+            const int np = t <= H ? P.lv[t].n_items * P.lv[t].split : 0;
+            if (u < np) {  // project item (part) of level t
                 if (t == 1) {
                     const long total = (long)P.n_l0_slots * P.nExt0;
                     target = (unsigned)((total + kQueryL0Chunk - 1) / kQueryL0Chunk);
                     c = P.ctr;
                 } else {
-                    const int gi = P.lv[t].items[3 * u];
+                    const int gi = P.lv[t].items[3 * (u / P.lv[t].split)];
                     target = (unsigned)P.lv[t].groups[5 * gi + 3] * col_tiles(P.lv[t - 1].NP, NC);
                     c = P.ctr + 4 + (size_t)t * P.k + gi;
                 }
@@ -593,9 +640,10 @@ __device__ __forceinline__ bool dep_wait(const QueryParams& P, int t, int u, int
 }
 
 // Counts unit u of phase t of request P as done, after every thread of the
-// CTA has issued its stores (the fence orders them before the counts).
+// CTA has issued its stores (the fence orders them before the counts); a
+// project item counts toward its consumers once complete (all its parts).
 template <int RW, int CP>
-__device__ __forceinline__ void dep_signal(const QueryParams& P, int t, int u) {
+__device__ __forceinline__ void dep_signal(const QueryParams& P, int t, int u, bool complete) {
     __syncthreads();
     if (threadIdx.x != 0) return;
     const int H = P.H;
@@ -607,12 +655,13 @@ __device__ __forceinline__ void dep_signal(const QueryParams& P, int t, int u) {
         atomicAdd(P.ctr + (u < n_fill ? 0 : 1), 1u);
         return;
     }
-    const int np = t <= H ? P.lv[t].n_items : 0;
-    if (u < np) {
+    const int S = t <= H ? P.lv[t].split : 1;
+    const int np = t <= H ? P.lv[t].n_items * S : 0;
+    if (u < np && complete) {
         if (t == H) {
             atomicAdd(P.ctr + 2, 1u);
         } else {
-            const int* it = P.lv[t].items + 3 * u;
+            const int* it = P.lv[t].items + 3 * (u / S);
             const int* G = P.lv[t].groups + 5 * it[0];
             const int rows = min(RW, G[3] - it[1]);
             const int pg = P.lv[t].lift[2 * G[2] + 1];
@@ -665,9 +714,9 @@ __global__ void __launch_bounds__(kThreads, 512 / kThreads) q_persistent_kernel(
             if (!dep_wait<RW, CP>(P, t, u, B.status)) return;
             // every thread has read next_w (the wait is a CTA barrier)
             const int nxt = threadIdx.x == 0 ? (int)atomicAdd(B.bar, 1u) : 0;
-            run_unit<RW, CP>(P, t, u, kl, wsum, red, im);
+            const bool complete = run_unit<RW, CP>(P, t, u, kl, wsum, red, im);
             if (threadIdx.x == 0) next_w = nxt;
-            dep_signal<RW, CP>(P, t, u);  // begins with a CTA barrier: next_w is visible after it
+            dep_signal<RW, CP>(P, t, u, complete);  // begins with a CTA barrier: next_w is visible after it
             if (B.trace && threadIdx.x == 0) {
                 const unsigned long long now = global_timer();
                 atomicMax(B.trace + t + 1, now);

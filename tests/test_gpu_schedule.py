@@ -1,9 +1,12 @@
-"""The query kernel's two schedules give the same results.  The default
+"""The query kernel's schedules give the same results.  The default
 (dataflow) schedule runs every unit as soon as the units it reads are done;
-HTRIP_QUERY_DATAFLOW=0 separates the phases by grid barriers.  The whole
-query, batch and device-planner parity suites run again in a child process
-with the barrier schedule (tolerance 0: integer distances), and one query
-is compared between the schedules directly."""
+HTRIP_QUERY_DATAFLOW=0 separates the phases by grid barriers.  Root project
+items run in parts (split-K) when the root's child port list is long;
+HTRIP_QUERY_ROOT_SPLIT=n forces n parts on every root level, so that the
+small parity grids run the split path too.  The query, batch and
+device-planner parity suites run again in child processes under these
+settings (tolerance 0: integer distances), and one query is compared
+between the schedules directly."""
 import os
 import subprocess
 import sys
@@ -43,10 +46,17 @@ def test_schedules_agree_on_one_query(gpu, tmp_path):
     np.testing.assert_array_equal(outs[0], outs[1])
 
 
-def test_barrier_schedule_passes_the_query_suites(gpu):
-    env = dict(os.environ, HTRIP_QUERY_DATAFLOW="0")
-    files = [os.path.join(ROOT, "tests", f) for f in
-             ("test_gpu_parity.py", "test_gpu_batch.py", "test_gpu_devplan.py", "test_gpu_configs.py")]
+SUITES = ("test_gpu_parity.py", "test_gpu_batch.py", "test_gpu_devplan.py", "test_gpu_configs.py")
+
+
+@pytest.mark.parametrize("settings", [
+    {"HTRIP_QUERY_DATAFLOW": "0"},                                   # grid barriers
+    {"HTRIP_QUERY_ROOT_SPLIT": "3"},                                 # root items in 3 uneven parts
+    {"HTRIP_QUERY_DATAFLOW": "0", "HTRIP_QUERY_ROOT_SPLIT": "2"},    # parts under grid barriers
+], ids=["barrier", "split3", "barrier-split2"])
+def test_query_suites_under_schedule(gpu, settings):
+    env = dict(os.environ, **settings)
+    files = [os.path.join(ROOT, "tests", f) for f in SUITES]
     r = subprocess.run([sys.executable, "-m", "pytest", *files, "-q", "-x", "-p", "no:cacheprovider",
                         "-k", "not planned_on_the_device"], cwd=ROOT, env=env, capture_output=True, text=True,
                        timeout=900)
