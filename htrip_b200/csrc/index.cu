@@ -1065,19 +1065,39 @@ int choose_query_cfg(const htrip_index* h, int ns, int root_group);
 
 // Parts per project item of level l (QueryLevel::split).  Root items are the
 // longest (the root's child port list: ~1000 ports for a 256-cell child,
-// against a few dozen at level 1).  Cutting them costs a unit's fixed
-// overhead (a few microseconds) per extra part, which only pays when the
-// root has fewer items than the grid has CTAs; on a 512 x 512 map with 256
-// viewpoints (344 root items) 1 / 2 / 3 / 4 parts measured 136 / 143 / 153
-// / 164 us per query kernel.  HTRIP_QUERY_ROOT_SPLIT=n (1..8) sets the
-// root's split.
-int query_item_split(const htrip_index* h, int l) {
-    if (l < 1 || l != h->H) return 1;
+// against a few dozen at level 1).  Cutting one costs a unit's fixed
+// overhead (a few microseconds) per extra part, which pays only while the
+// root has no more items than the grid has CTAs.  On a 512 x 512 maze
+// (root child ports 1020) the query kernel measured, for 1 / 2 / 4 parts:
+// k = 16: 89 / 81 / 75 us, k = 64 (86 root items): 93 / 87 / 99 us,
+// k = 128 (172 items): 134 / 122 / 134 us, k = 256 (344 items): 136 / 143
+// / 164 us.  So: 2 parts for long root port lists (>= 256) when the items
+// fit the grid.  HTRIP_QUERY_ROOT_SPLIT=n (1..8) imposes n parts on every
+// root level regardless of size.
+int query_split_forced() {
     static const int forced = [] {
         const char* e = std::getenv("HTRIP_QUERY_ROOT_SPLIT");
         return e ? std::clamp(std::atoi(e), 1, 8) : 0;
     }();
-    return forced ? forced : 1;
+    return forced;
+}
+
+// The split a level may use (1: never) ...
+int query_item_split(const htrip_index* h, int l) {
+    if (l < 1 || l != h->H) return 1;
+    if (query_split_forced()) return query_split_forced();
+    return h->L[l].nP >= 256 ? 2 : 1;
+}
+
+// ... and the number of items up to which it does (the query grid's CTAs).
+int query_split_items(const htrip_index* h) {
+    if (query_split_forced()) return INT32_MAX;
+    static std::mutex mu;
+    static std::map<int, int> grid;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = grid.find(h->device);
+    if (it == grid.end()) it = grid.emplace(h->device, hb::query_grid_blocks(h->device)).first;
+    return it->second;
 }
 
 // Plans a query; force_cfg >= 0 imposes the tile configuration (requests
@@ -1196,7 +1216,7 @@ void make_plan(const htrip_index* h, const int32_t* vps, const uint8_t* pass_fla
                 for (int n0 = n_begin; n0 < Lv.NP; n0 += NC) P.buf.insert(P.buf.end(), {gi, m0, n0});
         }
         Q.n_items = ((int)P.buf.size() - Q.o_items) / 3;
-        Q.split = query_item_split(h, l);
+        Q.split = Q.n_items <= query_split_items(h) ? query_item_split(h, l) : 1;
         Q.o_s2v = (int)P.buf.size();
         P.buf.resize(P.buf.size() + Q.slots + NC, -1);
         for (const CG& c : G)
@@ -1689,9 +1709,10 @@ DevPlanLayout devplan_layout(const htrip_index* h, int k, int cfg, bool out_in_a
     // the planner's preset blocks clear the flags, the counters and the split
     // items' tickets after them
     D.root_split = H >= 1 ? query_item_split(h, H) : 1;
+    G.split_items = query_split_items(h);
     const size_t ctr_at = (flags + 15) / 16 * 16;
     const size_t ticket_at = ctr_at + hb::query_counter_words(H, k) * sizeof(unsigned);
-    const size_t root_items = H >= 1 ? (size_t)O.cap_items[H] : 0;
+    const size_t root_items = H >= 1 ? std::min<size_t>(O.cap_items[H], (size_t)G.split_items) : 0;
     O.flags_bytes = (long long)(ticket_at + (D.root_split > 1 ? root_items * sizeof(unsigned) : 0));
     D.o_flags = takeb((size_t)O.flags_bytes);
     D.o_ctr = D.o_flags + ctr_at;

@@ -195,6 +195,8 @@ struct PlanGeom {
     int side[kMaxQueryLevels + 1];     // node side in cells per level
     int nodes_x[kMaxQueryLevels + 1];  // nodes per row per level
     int nP[kMaxQueryLevels + 1], NP[kMaxQueryLevels + 1];
+    int split_items;                   // a level whose template split is > 1 runs split only
+                                       // with at most this many project items
 };
 // ... and where the plan goes: int offsets into `plan` with their capacities
 // (worst cases for k viewpoints), each level's flag offset, the request's

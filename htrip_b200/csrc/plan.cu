@@ -139,6 +139,13 @@ __device__ void plan_fill(const PlanLayout& O, int first) {
     for (long i = f16 * 16 + b * blockDim.x + threadIdx.x; i < O.flags_bytes; i += stride) O.flags[i] = 0;
 }
 
+// Parts per project item of level l: the template's split while the level
+// has at most G.split_items items (the host sized the part scratch so).
+__device__ __forceinline__ int level_split(const QueryParams& tmpl, const PlanGeom& G, int l, int n_items) {
+    const int s = tmpl.lv[l].split;
+    return s > 1 && n_items <= G.split_items ? s : 1;
+}
+
 __device__ __forceinline__ bool vp_inside(const int32_t* vps, const uint8_t* pf, int i, int S) {
     const int r = vps[2 * i], c = vps[2 * i + 1];  // loaded together with the flag
     return pf[i] && r >= 0 && c >= 0 && r < S && c < S;
@@ -243,7 +250,6 @@ plan_query_kernel(const int32_t* __restrict__ vps, const uint8_t* __restrict__ p
             lv.nP = tmpl.lv[l].nP;
             lv.ext_inv = tmpl.lv[l].ext_inv;
             lv.store_y = tmpl.lv[l].store_y;
-            lv.split = tmpl.lv[l].split;
             lv.part = tmpl.lv[l].part;
             lv.ticket = tmpl.lv[l].ticket;
         }
@@ -468,6 +474,7 @@ plan_query_kernel(const int32_t* __restrict__ vps, const uint8_t* __restrict__ p
                 lv.flags = O.flags + O.flags_off[l];
                 lv.items = items;
                 lv.n_items = n_items;
+                lv.split = level_split(tmpl, G, l, n_items);
                 lv.meet = meet;
                 lv.n_meet = n_meet;
                 lv.s2v = s2v;
@@ -517,8 +524,8 @@ plan_query_kernel(const int32_t* __restrict__ vps, const uint8_t* __restrict__ p
     const int n_l0 = H >= 1 ? __shfl_sync(0xffffffffu, own ? vr[3] : 0, 0) : 0;
     const int root = H >= 1 ? __shfl_sync(0xffffffffu, r_root, H - 1) : ns;
     // phase t: project items of level t (lane t-1), meet items of level t-1 (lane t-2)
-    const int items_t = __shfl_sync(0xffffffffu, r_items, max(lane - 1, 0)) *
-                        (lane >= 1 && lane <= H ? tmpl.lv[lane].split : 1);
+    const int items_l = __shfl_sync(0xffffffffu, r_items, max(lane - 1, 0));
+    const int items_t = items_l * (lane >= 1 && lane <= H ? level_split(tmpl, G, lane, items_l) : 1);
     const int meet_t = __shfl_sync(0xffffffffu, r_meet, max(lane - 2, 0));
     const int n_phases = H + 3;
     if (lane < n_phases) {

@@ -360,23 +360,11 @@ __device__ bool combine_parts(const QueryLevel& L, int item, int part, uint32_t 
 template <int RW, int CP>
 __device__ bool do_project(const QueryParams& P, const QueryLevel& L, const QueryLevel* Ln, int item, int part,
                            int l, int* kl, int* wsum, uint32_t* red, ItemMeta& im) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, tid = threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int* it = L.items + 3 * item;
     const int gi = it[0], m0 = it[1], n0 = it[2];
     const int* G = L.groups + 5 * gi;
-    const int node = G[0], q = G[1], slot0 = G[2], cnt = G[3];
-    if (Ln) {
-        for (int t = tid; t < 64 * CP + RW; t += kThreads) {
-            if (t < 64 * CP) {
-                im.col[t] = n0 + t < L.NP ? L.ext_inv[n0 + t] : -1;
-            } else {
-                const int r = t - 64 * CP;
-                const bool ok = m0 + r < cnt;
-                im.row[0][r] = ok ? L.lift[2 * (slot0 + m0 + r)] : -1;
-                im.row[1][r] = ok ? L.lift[2 * (slot0 + m0 + r) + 1] : -1;
-            }
-        }
-    }
+    const int node = G[0], q = G[1], slot0 = G[2];
     const int nA = compact_flags(L.flags + (size_t)gi * L.nP, 0, L.nP, kl, wsum);
     const int kb = (int)((long)nA * part / L.split), ke = (int)((long)nA * (part + 1) / L.split);
     const uint16_t* D = L.D + (size_t)node * L.NP * L.NP + (size_t)q * L.nP * L.NP;
@@ -442,13 +430,9 @@ __device__ bool do_project(const QueryParams& P, const QueryLevel& L, const Quer
 template <int RW, int CP>
 __device__ void do_meet(const QueryParams& P, const QueryLevel& L, int item, int l, int* kl, int* wsum,
                         uint32_t* red, ItemMeta& im) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, tid = threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int* it = L.meet + 7 * item;
-    const int i0 = it[0], j0 = it[1], nj = it[2], g2 = it[3], coloff = it[4], kb = it[5], ke = it[6];
-    for (int t = tid; t < 64 * CP + RW; t += kThreads) {
-        if (t < 64 * CP) im.col[t] = L.s2v[i0 + t];
-        else im.row[0][t - 64 * CP] = t - 64 * CP < nj ? L.s2v[j0 + t - 64 * CP] : -1;
-    }
+    const int i0 = it[0], j0 = it[1], g2 = it[3], coloff = it[4], kb = it[5], ke = it[6];
     const int nA = compact_flags(L.flags + (size_t)g2 * L.nP, kb, ke, kl, wsum);
     const uint16_t* Xp = P.X[l - 1] + j0;
     const uint16_t* Y = P.Y[l] + (size_t)coloff * P.ldv + i0;
@@ -475,7 +459,47 @@ __device__ void do_meet(const QueryParams& P, const QueryLevel& L, int item, int
     __syncthreads();
 }
 
-// One CTA work unit of request P in phase t (see QueryLaunch).  Returns
+// Metadata of unit u of phase t staged in shared memory before the unit
+// waits for its inputs (none of it is produced by the launch): per tile
+// column the exterior index (project, lifting levels) or viewpoint (meet),
+// per tile row the lift slot and group (project) or viewpoint (meet).  The
+// caller's next CTA barrier publishes it.
+template <int RW, int CP>
+__device__ void unit_prologue(const QueryParams& P, int t, int u, ItemMeta& im) {
+    if (t < 1 || t > P.H + 1) return;
+    const int tid = threadIdx.x;
+    const int S = t <= P.H ? P.lv[t].split : 1;
+    const int np = t <= P.H ? P.lv[t].n_items * S : 0;
+    if (u < np) {
+        if (t == P.H) return;  // root items lift nothing
+        const QueryLevel& L = P.lv[t];
+        const int* it = L.items + 3 * (u / S);
+        const int gi = it[0], m0 = it[1], n0 = it[2];
+        const int* G = L.groups + 5 * gi;
+        const int slot0 = G[2], cnt = G[3];
+        for (int e = tid; e < 64 * CP + RW; e += kThreads) {
+            if (e < 64 * CP) {
+                im.col[e] = n0 + e < L.NP ? L.ext_inv[n0 + e] : -1;
+            } else {
+                const int r = e - 64 * CP;
+                const bool ok = m0 + r < cnt;
+                im.row[0][r] = ok ? L.lift[2 * (slot0 + m0 + r)] : -1;
+                im.row[1][r] = ok ? L.lift[2 * (slot0 + m0 + r) + 1] : -1;
+            }
+        }
+    } else {
+        const QueryLevel& L = P.lv[t - 1];
+        const int* it = L.meet + 7 * (u - np);
+        const int i0 = it[0], j0 = it[1], nj = it[2];
+        for (int e = tid; e < 64 * CP + RW; e += kThreads) {
+            if (e < 64 * CP) im.col[e] = L.s2v[i0 + e];
+            else im.row[0][e - 64 * CP] = e - 64 * CP < nj ? L.s2v[j0 + e - 64 * CP] : -1;
+        }
+    }
+}
+
+// One CTA work unit of request P in phase t (see QueryLaunch); its
+// metadata is staged (unit_prologue).  Returns
 // false for a part of a split project item that did not complete it.
 template <int RW, int CP>
 __device__ bool run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum, uint32_t* red, ItemMeta& im) {
@@ -711,6 +735,7 @@ __global__ void __launch_bounds__(kThreads, 512 / kThreads) q_persistent_kernel(
             }
             const QueryParams& P = B.req[lo];
             const int u = wl - pre[lo];
+            unit_prologue<RW, CP>(P, t, u, im);  // overlaps the wait; the wait's barrier publishes it
             if (!dep_wait<RW, CP>(P, t, u, B.status)) return;
             // every thread has read next_w (the wait is a CTA barrier)
             const int nxt = threadIdx.x == 0 ? (int)atomicAdd(B.bar, 1u) : 0;
@@ -735,6 +760,8 @@ __global__ void __launch_bounds__(kThreads, 512 / kThreads) q_persistent_kernel(
                 if (pre[mid] <= w) lo = mid;
                 else hi = mid;
             }
+            unit_prologue<RW, CP>(B.req[lo], t, w - pre[lo], im);
+            __syncthreads();
             run_unit<RW, CP>(B.req[lo], t, w - pre[lo], kl, wsum, red, im);
         }
         if (B.trace && threadIdx.x == 0)  // the phase's last CTA to finish its units
