@@ -580,13 +580,17 @@ __device__ bool run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum,
 // ---------------------------------------------------------------------------
 constexpr unsigned kWaitPolls = 1u << 24;
 
-// Bounded wait of the whole CTA until *c >= target: thread 0 polls, the CTA
-// follows.  False after a timeout (recorded in *status) or when another CTA
-// has recorded one.
+// The thread that looks up and polls a unit's dependency: lane 0 of warp 1,
+// so that it runs beside thread 0's fence and counts for the previous unit.
+constexpr int kWaiter = 32;
+
+// Bounded wait of the whole CTA until *c >= target: thread kWaiter polls,
+// the CTA follows.  False after a timeout (recorded in *status) or when
+// another CTA has recorded one.
 __device__ __forceinline__ bool wait_count(const unsigned* c, unsigned target, int* status,
                                            unsigned limit = kWaitPolls) {
     int ok = 1;
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == kWaiter) {
         const volatile unsigned* vc = c;
         const volatile int* vs = status;
         unsigned it = 0;
@@ -627,7 +631,7 @@ __device__ __forceinline__ bool dep_wait(const QueryParams& P, int t, int u, int
     }
     const unsigned* c = nullptr;
     unsigned target = 0;
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == kWaiter) {
         const int H = P.H;
         if (t == H + 2) {
             target = (unsigned)((P.ns + kThreads - 1) / kThreads);
@@ -659,7 +663,7 @@ __device__ __forceinline__ bool dep_wait(const QueryParams& P, int t, int u, int
             }
         }
     }
-    // thread 0 alone waits (the others pass a null counter and target 0)
+    // thread kWaiter alone waits (the others pass a null counter and target 0)
     return wait_count(c ? c : P.ctr, target, status);
 }
 
