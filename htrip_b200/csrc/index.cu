@@ -191,6 +191,7 @@ struct UpdateArena {
     DevBuf<uint16_t> panel;
     DevBuf<uint8_t> pflags;
     HostBuf stage, rb;
+    cudaEvent_t ev_cnt = nullptr;  // an opening level's pivot counts reached the host
     void release() {
         dev.release();
         snap.release();
@@ -198,6 +199,8 @@ struct UpdateArena {
         pflags.release();
         stage.release();
         rb.release();
+        if (ev_cnt) cudaEventDestroy(ev_cnt);
+        ev_cnt = nullptr;
     }
 };
 
@@ -481,18 +484,31 @@ hb::Slot level_slot(Level& Lv, Level* child, int m, int task, int root) {
 // Closure rounds of `n` slots (already uploaded at d_slots, pivots already
 // compacted, counts cnt[] on the host) of order NP, in chunks that bound the
 // panel scratch.  Issued on `st`, not waited for.
-void close_slots(UpdateArena& A, const hb::Slot* d_slots, const int* cnt, int n, int NP, cudaStream_t st) {
+// Slots per closure launch: the panel scratch of a launch stays under 128 MB.
+size_t closure_chunk(int NP) {
     const size_t per = (size_t)hb::kPivotChunk * NP;
-    const size_t cap = std::max<size_t>(1, (size_t)(128u << 20) / (per * sizeof(uint16_t)));
+    return std::max<size_t>(1, (size_t)(128u << 20) / (per * sizeof(uint16_t)));
+}
+
+// Closure of n slots over their pivot lists, rounds from r0 on: up to the
+// largest count of a chunk (cnt, host copy of the slots' counts), or, with
+// cnt null, round r0 alone for every chunk (the kernels return at once for
+// a slot whose pivots end before the round).
+void close_slots(UpdateArena& A, const hb::Slot* d_slots, const int* cnt, int n, int NP, cudaStream_t st,
+                 int r0 = 0) {
+    const size_t cap = closure_chunk(NP);
     for (size_t c0 = 0; c0 < (size_t)n; c0 += cap) {
         const int nc = (int)std::min(cap, (size_t)n - c0);
-        int maxk = 0;
-        for (int i = 0; i < nc; ++i) maxk = std::max(maxk, cnt[c0 + i]);
-        if (maxk == 0) continue;
+        int rounds = r0 + 1;
+        if (cnt) {
+            int maxk = 0;
+            for (int i = 0; i < nc; ++i) maxk = std::max(maxk, cnt[c0 + i]);
+            rounds = (maxk + hb::kPivotChunk - 1) / hb::kPivotChunk;
+        }
+        if (rounds <= r0) continue;
         A.panel.reserve(hb::closure_scratch_elems(NP, nc));
         A.pflags.reserve((size_t)nc * (NP / hb::kFlagTile));
-        const int rounds = (maxk + hb::kPivotChunk - 1) / hb::kPivotChunk;
-        for (int r = 0; r < rounds; ++r) {
+        for (int r = r0; r < rounds; ++r) {
             hb::launch_closure_round(d_slots + c0, nc, NP, r, A.panel.p, A.pflags.p, st);
             ck(cudaGetLastError(), "closure round");
         }
@@ -994,13 +1010,31 @@ void run_open_tasks(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t 
         ck(cudaMemcpyAsync(A.rb.p, A.dev.p + o_cnt, o_dec - o_cnt, cudaMemcpyDeviceToHost, st), "counts");
         if (l == 0)
             ck(cudaMemcpyAsync(hpiv, dpiv, n_tasks * sizeof(int), cudaMemcpyDeviceToHost, st), "pivots");
-        ck(cudaStreamSynchronize(st), "open insert stage");
-        // ---- close stage
+        if (!A.ev_cnt) ck(cudaEventCreateWithFlags(&A.ev_cnt, cudaEventDisableTiming), "event");
+        ck(cudaEventRecord(A.ev_cnt, st), "counts event");
+        // ---- close stage.  Round 0 of every slot goes out before the counts
+        // reach the host (slots without pivots return at once), so the GPU
+        // works while the host waits; the scratch of every group is reserved
+        // first (a reserve that grows would free a buffer queued kernels use).
+        {
+            size_t elems = 0, fl = 0;
+            for (const Group& G : groups) {
+                const int NP = live[G.t0]->h->L[l].NP;
+                const size_t nc = std::min(closure_chunk(NP), (size_t)(G.s1 - G.s0));
+                elems = std::max(elems, hb::closure_scratch_elems(NP, (int)nc));
+                fl = std::max(fl, nc * (NP / hb::kFlagTile));
+            }
+            A.panel.reserve(elems);
+            A.pflags.reserve(fl);
+        }
+        for (const Group& G : groups)
+            close_slots(A, ds + G.s0, nullptr, G.s1 - G.s0, live[G.t0]->h->L[l].NP, st, 0);
+        ck(cudaEventSynchronize(A.ev_cnt), "open insert stage");
         for (const Group& G : groups) {
             const htrip_index* h0 = live[G.t0]->h;
             const Level& Lv = h0->L[l];
             const int n = G.s1 - G.s0;
-            close_slots(A, ds + G.s0, hcnt + G.s0, n, Lv.NP, st);
+            close_slots(A, ds + G.s0, hcnt + G.s0, n, Lv.NP, st, 1);
             hb::launch_ext_compare(ds + G.s0, n, Lv.d_ext.p, Lv.nExt, Lv.NP, A.snap.p + G.snap_off, ddec + G.s0,
                                    h0->g, st);
             ck(cudaGetLastError(), "open close");
