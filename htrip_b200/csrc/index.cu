@@ -1504,7 +1504,7 @@ void issue_query_launch(cudaStream_t st, int device, int& grid, int cfg, const s
 
 // Runs the planned requests through the arena `A` on stream `st`.  Results
 // whose out_dev is null are copied into host_out[i] (k*k each).  Returns
-// the kernel's status word (0 ok, 1 grid barrier timeout); synchronous.
+// the kernel's status word (0 ok, 1 a bounded wait timed out); synchronous.
 int run_queries(QueryArena& A, int device, cudaStream_t st, const std::vector<QueryReq>& R,
                 const std::vector<uint16_t*>& host_out, bool sync) {
     int cfg = 0;
@@ -1808,7 +1808,7 @@ int devplan_cfg_hint(htrip_index* h, int k) {
 // come from the host (staged and copied in) or from device memory.  The
 // result goes to out_dev (stream-ordered, returns 0), or, with out_dev null,
 // to host_out after a synchronisation; then the return value is the status
-// word (0 ok, 1 grid barrier timeout, 2 plan capacity exceeded).
+// word (0 ok, 1 a bounded wait timed out, 2 plan capacity exceeded).
 int run_devplan(htrip_index* h, int k, int cfg, const int32_t* vps_host, const uint8_t* pf_host,
                 const int32_t* vps_dev, const uint8_t* pf_dev, uint16_t* out_dev, uint16_t* host_out) {
     check_query_shape(h);
@@ -2176,7 +2176,7 @@ htrip_status htrip_query_all_pairs(htrip_index* h, const int32_t* vps, int32_t k
     if (devplan_supported(h, k, true)) {
         const int status =
             run_devplan(h, k, devplan_cfg_host(h, vps, pf.data(), k), vps, pf.data(), nullptr, nullptr, nullptr, out);
-        if (status == 1) return fail(HTRIP_ERR_CUDA, "query kernel: grid barrier timed out");
+        if (status == 1) return fail(HTRIP_ERR_CUDA, "query kernel: a bounded wait timed out");
         if (status == 0) return HTRIP_OK;
         // status 2: the plan outgrew its worst-case capacity; plan on the host
     }
@@ -2184,7 +2184,7 @@ htrip_status htrip_query_all_pairs(htrip_index* h, const int32_t* vps, int32_t k
     make_plan(h, vps, pf.data(), k, P);
     const std::vector<QueryReq> R{{h, &P, nullptr}};
     if (run_queries(h->q, h->device, h->stream, R, {out}, true) != 0)
-        return fail(HTRIP_ERR_CUDA, "query kernel: grid barrier timed out");
+        return fail(HTRIP_ERR_CUDA, "query kernel: a bounded wait timed out");
     return HTRIP_OK;
     HTRIP_GUARD_END
 }
@@ -2332,7 +2332,7 @@ htrip_status htrip_query_all_pairs_noalloc(htrip_index* h, const int32_t* vps, i
     ck(cudaMemcpyAsync(out, outs[0], (size_t)k * k * sizeof(uint16_t), cudaMemcpyDeviceToHost, st), "out");
     ck(cudaMemcpyAsync(&status, base + L.o_words, sizeof(int), cudaMemcpyDeviceToHost, st), "status");
     ck(cudaStreamSynchronize(st), "query sync");
-    if (status != 0) return fail(HTRIP_ERR_CUDA, "query kernel: grid barrier timed out");
+    if (status != 0) return fail(HTRIP_ERR_CUDA, "query kernel: a bounded wait timed out");
     return HTRIP_OK;
     HTRIP_GUARD_END
 }
@@ -2411,7 +2411,7 @@ htrip_status htrip_query_batch(htrip_batch* b, const htrip_query_request* reqs, 
     std::vector<QueryReq> R;
     for (size_t i = 0; i < plans.size(); ++i) R.push_back({hs[i], &plans[i], nullptr});
     if (run_queries(b->q, b->device, b->stream, R, outs, true) != 0)
-        return fail(HTRIP_ERR_CUDA, "query kernel: grid barrier timed out");
+        return fail(HTRIP_ERR_CUDA, "query kernel: a bounded wait timed out");
     return HTRIP_OK;
     HTRIP_GUARD_END
 }
@@ -2684,7 +2684,7 @@ htrip_status htrip_autotune_query(htrip_index* h, const int32_t* vps, int32_t k,
         float t = 0.f;
         for (int r = 0; r <= reps; ++r) {  // the first launch warms up and is not counted
             if (run_queries(h->q, h->device, h->stream, R, {nullptr}, true) != 0)
-                return fail(HTRIP_ERR_CUDA, "query kernel: grid barrier timed out");
+                return fail(HTRIP_ERR_CUDA, "query kernel: a bounded wait timed out");
             float ms = 0.f;
             ck(cudaEventElapsedTime(&ms, h->q.ev[0], h->q.ev[1]), "event time");
             if (r > 0) t = (r == 1) ? ms : std::min(t, ms);

@@ -174,7 +174,7 @@ struct QueryLaunch {
     int n_phases;              // max over requests of H + 3
     const QueryParams* req;    // device array of n_req requests
     const int* unit_pre;       // [n_phases][n_req + 1]: exclusive prefix of units
-    int* status;               // 0 ok, 1 grid barrier timeout
+    int* status;               // 0 ok, 1 a bounded wait (counter or grid barrier) timed out
     unsigned* bar;             // grid barrier {count, generation}
     unsigned long long* trace; // [0, n_phases]: phase starts as CTA 0 sees them (dataflow: [0]
                                // the start, [t + 1] the latest end of a unit of phase t); then

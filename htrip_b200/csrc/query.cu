@@ -570,6 +570,8 @@ __device__ bool run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum,
 //                             the counter of the level-(l+1) group it lifts to
 //   meet, level H             every root project item (ctr[2])
 //   output                    every project, meet and pair unit (ctr[1])
+// A project item cut into parts (QueryLevel::split) counts toward its
+// consumers once, when the part that completes it has run the epilogue.
 // A dependency is always a unit of an earlier phase, and the units of all
 // phases are handed out in ascending order (one ticket counter), so the
 // lowest unfinished unit has been handed out and has its inputs: every
