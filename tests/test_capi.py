@@ -28,3 +28,19 @@ def test_last_error_callable_without_device():
     lib = ctypes.CDLL(B.build())
     lib.htrip_last_error.restype = ctypes.c_char_p
     assert isinstance(lib.htrip_last_error(), bytes)
+
+
+def test_no_cpu_fallback_without_a_device():
+    """Without a GPU an index cannot be made and smoke() fails: there is no CPU path."""
+    import pytest
+
+    import __graft_entry__
+    from htrip_b200.minplus_oracle import HierarchyConfig, HtripError, MinPlusOracle
+    try:
+        MinPlusOracle(HierarchyConfig(8, 2, 2))
+    except HtripError as e:
+        assert "no CUDA device" in str(e)
+    else:
+        pytest.skip("a GPU is present")
+    with pytest.raises(HtripError, match="no CUDA device"):
+        __graft_entry__.smoke()
