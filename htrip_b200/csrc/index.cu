@@ -2631,7 +2631,8 @@ htrip_status htrip_last_query_kernel_ms(const htrip_index* h, float* ms) {
 
 // ns[i] = duration of phase i; with max_n >= 2 * phases, ns[phases + i] =
 // the part of it until the last CTA finished its work (the rest is the wait
-// in the grid barrier).
+// in the grid barrier).  Dataflow launches: both halves hold the time from
+// the end of phase i-1's last unit to the end of phase i's last unit.
 static htrip_status arena_phases(const QueryArena& A, cudaStream_t st, uint64_t* ns, int32_t max_n, int32_t* n) {
     if (!ns || !n || max_n < 0) return fail(HTRIP_ERR_INVALID, "bad arguments");
     if (!A.ev_valid) return fail(HTRIP_ERR_INVALID, "no query has run");

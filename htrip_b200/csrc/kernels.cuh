@@ -175,15 +175,16 @@ struct QueryLaunch {
     const QueryParams* req;    // device array of n_req requests
     const int* unit_pre;       // [n_phases][n_req + 1]: exclusive prefix of units
     int* status;               // 0 ok, 1 a bounded wait (counter or grid barrier) timed out
-    unsigned* bar;             // grid barrier {count, generation}
+    unsigned* bar;             // grid barrier {count, generation}; dataflow: bar[0] is the
+                               // ticket that hands out the units
     unsigned long long* trace; // [0, n_phases]: phase starts as CTA 0 sees them (dataflow: [0]
                                // the start, [t + 1] the latest end of a unit of phase t); then
                                // from [kMaxQueryPhases + 1 + t]: the latest end of work of
                                // phase t over all CTAs; or null
-    int dataflow;              // 1: no grid barrier - the CTAs stride over the units of all
-                               // phases in order and each unit first waits (bounded) for the
-                               // units whose results it reads (QueryParams::ctr); 0: phases
-                               // separated by grid barriers
+    int dataflow;              // 1: no grid barrier - the CTAs take the units of all phases
+                               // in ascending order (ticket bar[0]) and each unit first waits
+                               // (bounded) for the units whose results it reads
+                               // (QueryParams::ctr); 0: phases separated by grid barriers
 };
 constexpr int kMaxQueryPhases = kMaxQueryLevels + 3;
 

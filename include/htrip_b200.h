@@ -390,7 +390,8 @@ htrip_status htrip_last_query_phases(const htrip_index* h, uint64_t* ns, int32_t
 htrip_status htrip_batch_last_phases(const htrip_batch* b, uint64_t* ns, int32_t max_n, int32_t* n);
 
 /* Failure-detection self-test (no reference counterpart).  Every wait in
- * the query kernel's grid barrier is bounded: after a poll limit the CTA
+ * the query kernel's grid barrier (barrier schedule, HTRIP_QUERY_DATAFLOW=0)
+ * is bounded: after a poll limit the CTA
  * records a timeout in the launch's status word and returns, and the host
  * call fails with HTRIP_ERR_CUDA while the context stays usable.  This runs
  * a 4-CTA launch of the same barrier that can never complete (it expects a
