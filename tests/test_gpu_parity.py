@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 from helpers import make_grid, reveal_plan, viewpoints
+from htrip_b200 import workloads as W
 from oracle.ref import RefOracle, ref_available
 
 pytestmark = [pytest.mark.gpu,
@@ -190,3 +191,48 @@ def test_clone_is_deep(gpu):
     # the clone still answers for the old grid
     vps = viewpoints(obs, 10, 5)
     np.testing.assert_array_equal(snap.queryAllPairs(vps, obs), ref.query(vps))
+
+
+def _open_both(ref, dev, obs, part):
+    obs[part[:, 0], part[:, 1]] = W.FREE
+    ref.set_cells(part, W.FREE)
+    ref.open_batch(part)
+    dev.onBatchCellsOpened(part, obs)
+    st = dev.last_batch_stats
+    assert (st.n_touched_leaves, st.n_dirty_ancestors, st.n_pivots) == ref.stats()
+    assert dev.stateDigest() == ref.digest()
+
+
+def test_batched_opening_shapes(gpu):
+    """test_exactness.cpp:1029-1210: an 8-cell batch across tiles, a 28-cell
+    batch, a whole 64-cell column in one batch, an H = 0 batch, and liftRoot
+    after a batch; state, stats and queries against the reference."""
+    truth = make_grid("noise", 64, 64, 61)
+    truth[:, 37] = W.FREE                              # the column that opens at once
+    rng = np.random.default_rng(61)
+    free = np.argwhere(truth == W.FREE)
+    free = free[free[:, 1] != 37]
+    pick = free[rng.choice(len(free), 36, replace=False)]
+    col = np.stack([np.arange(64), np.full(64, 37)], 1)
+    obs = truth.copy()
+    for part in (pick, col):
+        obs[part[:, 0], part[:, 1]] = W.OBSTACLE
+    ref, dev = _build_both(obs, 8, 2)
+    for part in (pick[:8], pick[8:], col):         # 8 cells, 28 cells, the column
+        _open_both(ref, dev, obs, part)
+        _check_query(ref, dev, obs, 20, len(part))
+    big = make_grid("noise", 128, 128, 62)            # liftRoot after the batches
+    big[:64, :64] = obs
+    ref.set_grid(big)
+    ref.lift_root()
+    dev.liftRoot(big)
+    assert (dev.S, dev.H) == (ref.S, ref.H)
+    assert dev.stateDigest() == ref.digest()
+    _check_query(ref, dev, big, 24, 63)
+    small = make_grid("open", 16, 16, 64)             # H = 0: one leaf
+    cells = np.array([[3, 4], [3, 5], [9, 9], [15, 0]])
+    small[cells[:, 0], cells[:, 1]] = W.OBSTACLE
+    ref0, dev0 = _build_both(small, 16, 2)
+    assert dev0.H == 0
+    _open_both(ref0, dev0, small, cells)
+    _check_query(ref0, dev0, small, 12, 65)
