@@ -51,13 +51,10 @@ def make_inputs(rank: int):
     return grid, vps
 
 
-def config_dict(extra=None):
-    d = {"workload": "queryAllPairs, 512x512 maze (corridor 1, wall 1), b=16, g=2, k=256",
-         "grid": WORKLOAD["side"], "b": WORKLOAD["b"], "g": WORKLOAD["g"], "k": WORKLOAD["k"],
-         "l2": "256 MB L2 flush before every timed query"}
-    if extra:
-        d.update(extra)
-    return d
+def config_dict():
+    """The workload, identical in both arms (per-arm details are top-level keys)."""
+    return {"workload": "queryAllPairs, 512x512 maze (corridor 1, wall 1), b=16, g=2, k=256",
+            "grid": WORKLOAD["side"], "b": WORKLOAD["b"], "g": WORKLOAD["g"], "k": WORKLOAD["k"]}
 
 
 class ClockSampler:
@@ -182,7 +179,8 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "entries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16",
-            "data": "synthetic", "config": config_dict({"threads": nthreads}),
+            "data": "synthetic", "config": config_dict(), "parallelism": f"{nthreads} host threads",
+            "timing": "host clock around each step (all threads' queries)",
             "cpu_baseline": {"value": value, "unit": "entries/s", "cores": nthreads, "kind": kind,
                              "sample": f"each step: {nthreads} concurrent queryAllPairs calls (k={k}), one per thread"},
             "e2e": {"value": value, "unit": "entries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -276,6 +274,115 @@ def bench_opening(device, steps=400):
                       "reference_kind": "reference", "parity": "bit-exact" if ref.digest() == dev.stateDigest()
                       else "MISMATCH"})
     out["small_stream_vs_reference"] = small
+    return out
+
+
+# Query workloads of the other configurations: (name, grid maker, b, k).
+QUERY_CONFIGS = (
+    ("street256_k16", "256x256 street (30% rectangles, largest component), b=16, k=16",
+     lambda W: W.street_grid(256, 1), 16, 16),
+    ("maze512w1_k64", "512x512 maze, corridor 1, wall 1, b=16, k=64", lambda W: W.maze_grid(512, 1, 2), 16, 64),
+    ("maze512w1_k256", "512x512 maze, corridor 1, wall 1, b=16, k=256", lambda W: W.maze_grid(512, 1, 2), 16, 256),
+    ("maze512w16_k64", "512x512 maze, corridor 16, wall 1, b=16, k=64", lambda W: W.maze_grid(512, 16, 2), 16, 64),
+    ("maze512w16_k256", "512x512 maze, corridor 16, wall 1, b=16, k=256", lambda W: W.maze_grid(512, 16, 2), 16,
+     256),
+)
+
+
+def bench_configs(device, repeat=50, cpu_seconds=2.0):
+    """queryAllPairs on each query configuration: the GPU path (device-resident
+    viewpoints and output, CUDA events per query, 256 MB L2 flush before every
+    query outside the timed interval; `e2e` through the host-buffer C ABI),
+    the query kernel's issue roofline (dense and executed work), and on the
+    same grid and viewpoints the reference's CPU queryAllPairs on one core
+    and on every host core (one query per thread) and the reference's
+    BfsOracle::queryAllPairs (k BFS runs) on one core; every matrix is
+    compared with the reference's and BFS's."""
+    import torch
+
+    from htrip_b200 import workloads as W
+    from htrip_b200.minplus_oracle import HierarchyConfig, MinPlusOracle, minplus_rate
+    from oracle.ref import RefOracle, ref_available
+    rate_clamped = max(minplus_rate(device, 0) for _ in range(2))
+    rate_fast = max(minplus_rate(device, 2) for _ in range(2))
+    nthreads = os.cpu_count() or 1
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")
+    out = {}
+    for name, desc, make, b, k in QUERY_CONFIGS:
+        grid = make(W)
+        vps = W.sample_free(grid, k, 7)
+        idx = MinPlusOracle(HierarchyConfig(b, 2, 2), device=device)
+        assert idx.build(grid)
+        idx.autotuneQuery(vps, grid, reps=3)
+        host = idx.queryAllPairs(vps, grid)
+        stream = torch.cuda.ExternalStream(idx.stream(), device=device)
+        vd = torch.from_numpy(vps).to(f"cuda:{device}")
+        pf = torch.ones(k, dtype=torch.uint8, device=f"cuda:{device}")
+        od = torch.empty((k, k), dtype=torch.int16, device=f"cuda:{device}")
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(repeat)]
+        ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(repeat)]
+        kern = []
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                idx.queryAllPairsDevice(vd.data_ptr(), pf.data_ptr(), k, od.data_ptr())
+            for e in ev:
+                flush.zero_()
+                e[0].record(stream)
+                idx.queryAllPairsDevice(vd.data_ptr(), pf.data_ptr(), k, od.data_ptr())
+                e[1].record(stream)
+                kern.append(idx.lastQueryKernelMs())
+            for e in ev2:
+                flush.zero_()
+                e[0].record(stream)
+                idx.queryAllPairs(vps, grid, host)
+                e[1].record(stream)
+            torch.cuda.synchronize()
+            idx.setQueryWorkCounting(True)
+            idx.queryAllPairsDevice(vd.data_ptr(), pf.data_ptr(), k, od.data_ptr())
+            exec_entries = idx.lastQueryExecuted()[0]
+            idx.setQueryWorkCounting(False)
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(c) for a, c in ev) / repeat
+        e2e_ms = sum(a.elapsed_time(c) for a, c in ev2) / repeat
+        kern_s = float(np.mean(kern)) * 1e-3
+        alg_bytes, alg_ops = idx.queryWork(vps, grid)
+        dev_out = od.cpu().numpy().view(np.uint16)
+        row = {"workload": desc, "gpu_entries_per_s": k * k / (ms * 1e-3), "gpu_ms_per_query": ms,
+               "e2e_entries_per_s": k * k / (e2e_ms * 1e-3), "e2e_ms_per_query": e2e_ms,
+               "kernel_ms": kern_s * 1e3,
+               "roofline": {"bound": "issue", "unit": "T min-plus entries/s",
+                            "achieved": alg_ops / kern_s / 1e12, "peak": rate_clamped / 1e12,
+                            "frac": alg_ops / kern_s / rate_clamped,
+                            "frac_unclamped": alg_ops / kern_s / rate_fast,
+                            "executed_frac": exec_entries / kern_s / rate_clamped,
+                            "alg_minplus_ops": alg_ops, "executed_minplus_ops": exec_entries,
+                            "alg_bytes": alg_bytes}}
+        if ref_available():
+            ref = RefOracle(b, 2)
+            ref.set_grid(grid)
+            assert ref.build()
+            sec, ref_out = ref.time_query(vps, 1, 1)
+            reps = max(1, min(200, int(cpu_seconds / max(sec, 1e-4))))
+            sec, ref_out = ref.time_query(vps, 1, reps)
+            ref.time_query(vps, nthreads, 1)  # warm-up of the threads
+            nsec, _ = ref.time_query(vps, nthreads, 1)
+            t = time.perf_counter()
+            bfs_out = ref.bfs(vps)
+            bfs_s = time.perf_counter() - t
+            ok = np.array_equal(dev_out, ref_out) and np.array_equal(dev_out, bfs_out) and \
+                np.array_equal(host, ref_out)
+            row.update({"reference_1core_entries_per_s": reps * k * k / sec,
+                        "reference_ncore_entries_per_s": nthreads * k * k / nsec, "host_cores": nthreads,
+                        "bfs_1core_entries_per_s": k * k / bfs_s, "bfs_1core_ms_per_query": 1e3 * bfs_s,
+                        "reference_kind": "reference (oracle/_ref, the unmodified reference compiled here)",
+                        "cpu_sample": f"{reps} reference queries on 1 core; {nthreads} concurrent on "
+                                      f"{nthreads} threads; 1 BfsOracle::queryAllPairs",
+                        "speedup_vs_reference_1core": (k * k / (ms * 1e-3)) / (reps * k * k / sec),
+                        "speedup_vs_reference_ncore": (k * k / (ms * 1e-3)) / (nthreads * k * k / nsec),
+                        "parity": "bit-exact" if ok else "MISMATCH"})
+            del ref
+        out[name] = row
+        del idx
     return out
 
 
@@ -580,21 +687,25 @@ def run_ours(args, rank, world, local_rank):
     pf = torch.ones(k, dtype=torch.uint8, device=f"cuda:{local_rank}")
     od = torch.empty((k, k), dtype=torch.int16, device=f"cuda:{local_rank}")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    R = args.repeat  # queries per step
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps * R)]
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps * R)]
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
+    # Each step is R queries; the L2 is flushed (256 MB written) before every
+    # query, outside its event pair, and the step's time is the sum of its
+    # queries' event intervals on the index's stream.
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             idx.queryAllPairsDevice(vd.data_ptr(), pf.data_ptr(), k, od.data_ptr())
         barrier()
         kern_ms = []
         with ClockSampler(local_rank) as clk:
-            for i in range(args.steps):
+            for i in range(args.steps * R):
                 flush.zero_()
                 ev[i][0].record(stream)
                 idx.queryAllPairsDevice(vd.data_ptr(), pf.data_ptr(), k, od.data_ptr())
@@ -606,13 +717,19 @@ def run_ours(args, rank, world, local_rank):
         for _ in range(args.warmup):
             idx.queryAllPairs(vps, grid, out_host)
         barrier()
-        for i in range(args.steps):
+        for i in range(args.steps * R):
             flush.zero_()
             ev2[i][0].record(stream)
             idx.queryAllPairs(vps, grid, out_host)
             ev2[i][1].record(stream)
         barrier()
         e2e_ms = sum(a.elapsed_time(b) for a, b in ev2) / args.steps
+        # executed work of one (untimed) launch: operand rows streamed / skipped
+        idx.setQueryWorkCounting(True)
+        flush.zero_()
+        idx.queryAllPairsDevice(vd.data_ptr(), pf.data_ptr(), k, od.data_ptr())
+        exec_entries, exec_rows, skip_rows = idx.lastQueryExecuted()
+        idx.setQueryWorkCounting(False)
     if not np.array_equal(od.cpu().numpy().view(np.uint16), out_host):
         parity = "MISMATCH (device path)"
 
@@ -623,32 +740,56 @@ def run_ours(args, rank, world, local_rank):
     alg_bytes, alg_ops = idx.queryWork(vps, grid)
     peak, peak_kind = measured_peaks()
     from htrip_b200.minplus_oracle import minplus_rate
-    issue_peak = max(minplus_rate(local_rank, 0) for _ in range(3))  # clamped packed-u16 update, register-only
-    achieved = alg_bytes / (kern_ms_avg * 1e-3) / 1e9
+    # register-only packed-u16 update rates of this GPU: clamped (any value)
+    # and unclamped (values <= 5535) forms
+    rate_clamped = max(minplus_rate(local_rank, 0) for _ in range(3))
+    rate_fast = max(minplus_rate(local_rank, 2) for _ in range(3))
+    kern_s = kern_ms_avg * 1e-3
+    traffic = profile_traffic()
     h2d, d2h = idx.lastQueryIO()
+    roofline = {
+        # The query kernel does no tensor-core work and moves little DRAM
+        # traffic; its roof is integer-SIMD issue (packed u16 add / min), and
+        # what keeps it below that roof is per-unit latency at levels 1-4.
+        "bound": "issue", "unit": "T min-plus entries/s",
+        "achieved": alg_ops / kern_s / 1e12, "peak": rate_clamped / 1e12,
+        "frac": alg_ops / kern_s / rate_clamped,
+        "peak_source": "measured on this GPU (htrip_measure_minplus_rate: clamped packed-u16 update)",
+        "peak_unclamped": rate_fast / 1e12, "frac_unclamped": alg_ops / kern_s / rate_fast,
+        "limiter": "latency (dependent global round trips per work unit at levels 1-4)",
+        "kernel": "q_persistent_kernel", "kernel_ms": kern_ms_avg,
+        "alg_minplus_ops_per_launch": alg_ops, "executed_minplus_ops_per_launch": exec_entries,
+        "executed_frac": exec_entries / kern_s / rate_clamped,
+        "executed_frac_unclamped": exec_entries / kern_s / rate_fast,
+        "executed_operand_rows": exec_rows, "skipped_operand_rows": skip_rows,
+        "alg_bytes_per_launch": alg_bytes, "traffic": traffic,
+        "traffic_ratio": (traffic / alg_bytes) if traffic else None,
+        "hbm": {"achieved": alg_bytes / kern_s / 1e9, "peak": peak, "unit": "GB/s",
+                "frac": alg_bytes / kern_s / 1e9 / peak, "peak_source": peak_kind,
+                "dram_achieved": (traffic / kern_s / 1e9) if traffic else None,
+                "dram_frac": (traffic / kern_s / 1e9 / peak) if traffic else None},
+    }
     line = {
-        "metric": METRIC, "value": aggregate_entries_per_s(world, k, dev_ms), "unit": "entries/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
-        "config": config_dict({"parallelism": f"replicas x{world}", "build_s": round(build_s, 4),
-                               "query_tile_config": tile_cfg}),
-        "e2e": {"value": aggregate_entries_per_s(world, k, e2e_ms), "unit": "entries/s", "ms_per_step": e2e_ms,
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": profile_traffic(), "peak_source": peak_kind,
-                     "kernel": "q_persistent_kernel", "kernel_ms": kern_ms_avg,
-                     "alg_bytes_per_launch": alg_bytes, "alg_minplus_ops_per_launch": alg_ops,
-                     "minplus_gops": alg_ops / (kern_ms_avg * 1e-3) / 1e9,
-                     "issue": {"achieved": alg_ops / (kern_ms_avg * 1e-3) / 1e12, "peak": issue_peak / 1e12,
-                               "unit": "T min-plus entries/s", "frac": alg_ops / (kern_ms_avg * 1e-3) / issue_peak,
-                               "peak_source": "measured (htrip_measure_minplus_rate, clamped packed-u16 update)"}},
+        "metric": METRIC, "value": aggregate_entries_per_s(world, R * k * k, dev_ms), "unit": "entries/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": config_dict(), "parallelism": f"replicas x{world}", "queries_per_step": R,
+        "timing": "CUDA events around each query on the index's stream; 256 MB L2 flush before every query, "
+                  "outside the timed intervals",
+        "build_s": round(build_s, 4), "query_tile_config": tile_cfg,
+        "ms_per_query": dev_ms / R,
+        "e2e": {"value": aggregate_entries_per_s(world, R * k * k, e2e_ms), "unit": "entries/s",
+                "ms_per_step": e2e_ms, "ms_per_query": e2e_ms / R,
+                "h2d_bytes_per_step": R * h2d, "d2h_bytes_per_step": R * d2h},
+        "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
-        "gpu_launches": 2 * args.steps,  # per step: the planner (with the presets) and the query kernel
+        "gpu_launches": 2 * R * args.steps,  # per query: the planner (with the presets) and the query kernel
         "parity": parity,
     }
     if world == 1 and not args.headline_only:
-        for name, fn in (("cells_opened", lambda: bench_opening(local_rank)),
+        for name, fn in (("configs", lambda: bench_configs(local_rank)),
+                         ("cells_opened", lambda: bench_opening(local_rank)),
                          ("weighted", lambda: bench_weighted(local_rank)),
                          ("batched", lambda: bench_batched(local_rank)),
                          ("served", lambda: bench_served(local_rank))):
@@ -670,11 +811,12 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--repeat", type=int, default=100, help="queryAllPairs calls per step")
     ap.add_argument("--headline-only", action="store_true",
                     help="only the queryAllPairs headline (skip the opening / batched / served workloads)")
     ap.add_argument("--tile-config", type=int, choices=[0, 1, 2, 3],
                     help="query tile shape to use for the headline instead of the autotuner's choice")
-    ap.add_argument("--section", choices=["cells_opened", "weighted", "batched", "served"],
+    ap.add_argument("--section", choices=["configs", "cells_opened", "weighted", "batched", "served"],
                     help="run only this one of the further workloads after the headline")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

@@ -116,7 +116,17 @@ struct Level {
     DevBuf<uint8_t> kflag;
     DevBuf<int> klist, kcnt;
     DevBuf<uint8_t> dec;
+    // device-driven openings: per matrix index, 1 = an exterior port (leaf
+    // perimeter cell / node exterior port); per node, the stamp of the last
+    // opening call whose update decreased its exterior block (dstamp) and of
+    // the last call that put it on the level's work list (mstamp)
+    DevBuf<uint8_t> d_isext;
+    DevBuf<uint32_t> dstamp, mstamp;
     MatSet ms() const { return MatSet{mat.p, n, NP}; }
+    void release() {
+        d_ext.release(); d_seams.release(); d_ext_inv.release(); mat.release(); kflag.release();
+        klist.release(); kcnt.release(); dec.release(); d_isext.release(); dstamp.release(); mstamp.release();
+    }
 };
 
 inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
@@ -192,6 +202,11 @@ struct UpdateArena {
     DevBuf<uint8_t> pflags;
     HostBuf stage, rb;
     cudaEvent_t ev_cnt = nullptr;  // an opening level's pivot counts reached the host
+    int open_grid = 0;             // CTAs of the persistent opening kernel
+    // phase time stamps of the last device-driven opening launch (device,
+    // and where they are in the arena)
+    size_t trace_off = 0;
+    int trace_valid = 0;
     void release() {
         dev.release();
         snap.release();
@@ -201,6 +216,7 @@ struct UpdateArena {
         rb.release();
         if (ev_cnt) cudaEventDestroy(ev_cnt);
         ev_cnt = nullptr;
+        trace_valid = 0;
     }
 };
 
@@ -216,6 +232,15 @@ struct htrip_index {
     size_t parked_pass = 0;
     uint64_t ref_bytes = 0;  // the reference's totalMemoryBytes accounting of this index
     uint64_t open_ops = 0, open_bytes = 0;  // algorithmic work of the last opening call
+    // per level of the last opening call: {active matrices, sum of pivot
+    // counts, largest pivot count, closure rounds}
+    std::vector<std::array<int64_t, 4>> open_levels;
+    // query launches of this index count their executed work (a measurement
+    // mode: a few atomics per work unit)
+    bool count_work = false;
+    // stamp of the last device-driven opening call (per-node stamps in the
+    // level arrays compare against it; never 0)
+    uint32_t open_stamp = 0;
     uint64_t epoch = 0;           // build / root growth count (reference MinPlusOracle::epoch)
     uint64_t update_counter = 0;  // opening calls since creation
     int S = 0, H = 0, rows = 0, cols = 0, leaves_x = 0;
@@ -240,10 +265,7 @@ struct htrip_index {
         wts.release();
     }
     void release() {
-        for (auto& l : L) {
-            l.d_ext.release(); l.d_seams.release(); l.d_ext_inv.release(); l.mat.release(); l.kflag.release();
-            l.klist.release(); l.kcnt.release(); l.dec.release();
-        }
+        for (auto& l : L) l.release();
         L.clear();
         pass.release();
         u.release();
@@ -460,6 +482,14 @@ void alloc_levels(htrip_index* h) {
         // decrease flags are zero outside an opening call (each level's flags
         // are cleared by the level above once it has read them)
         ck(cudaMemsetAsync(Lv.dec.p, 0, Lv.nnodes, h->stream), "dec");
+        std::vector<uint8_t> isext(Lv.NP, 0);
+        for (int e = 0; e < Lv.nExt; ++e) isext[Lv.ext[e]] = 1;
+        Lv.d_isext.reserve(Lv.NP);
+        ck(cudaMemcpyAsync(Lv.d_isext.p, isext.data(), Lv.NP, cudaMemcpyHostToDevice, h->stream), "isext");
+        Lv.dstamp.reserve(Lv.nnodes);
+        Lv.mstamp.reserve(Lv.nnodes);
+        ck(cudaMemsetAsync(Lv.dstamp.p, 0, Lv.nnodes * sizeof(uint32_t), h->stream), "dstamp");
+        ck(cudaMemsetAsync(Lv.mstamp.p, 0, Lv.nnodes * sizeof(uint32_t), h->stream), "mstamp");
     }
 }
 
@@ -620,8 +650,7 @@ void do_lift_root(htrip_index* h, const uint8_t* observed, int rows, int cols) {
                                  cudaMemcpyDeviceToDevice, st), "move matrices");
         }
     } catch (...) {
-        for (auto& l : h->L) { l.d_ext.release(); l.d_seams.release(); l.d_ext_inv.release(); l.mat.release();
-                               l.kflag.release(); l.klist.release(); l.kcnt.release(); l.dec.release(); }
+        for (auto& l : h->L) l.release();
         h->L = std::move(old);  // the old matrices are intact
         h->S = old_S;
         h->H = old_H;
@@ -631,8 +660,7 @@ void do_lift_root(htrip_index* h, const uint8_t* observed, int rows, int cols) {
         h->ref_bytes = old_ref;
         throw;
     }
-    for (auto& l : old) { l.d_ext.release(); l.d_seams.release(); l.d_ext_inv.release(); l.mat.release();
-                          l.kflag.release(); l.klist.release(); l.kcnt.release(); l.dec.release(); }
+    for (auto& l : old) l.release();
     old.clear();
     const int S = h->S;
     std::vector<uint8_t> pass((size_t)S * S, 0);
@@ -871,6 +899,7 @@ void open_prepare(OpenTask& T, htrip_index* h, const int32_t* rc, int n, const u
     }
     if (record_stats) h->stats = {0, 0, 0};
     h->open_ops = h->open_bytes = 0;
+    h->open_levels.assign(H + 1, {0, 0, 0, 0});
 }
 
 bool open_has_work(const OpenTask& T) { return !T.leaves.empty(); }
@@ -1045,12 +1074,17 @@ void run_open_tasks(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t 
         for (OpenTask* T : live) {
             htrip_index* h = T->h;
             const uint64_t n = (uint64_t)h->L[l].n;
+            auto& lv = h->open_levels[l];
+            lv[0] = (int64_t)T->act.size();
             for (size_t i = 0; i < T->act.size(); ++i) {
                 const uint64_t k = (uint64_t)hcnt[T->slot0 + i];
+                lv[1] += (int64_t)k;
+                lv[2] = std::max<int64_t>(lv[2], (int64_t)k);
                 if (!k) continue;
                 h->open_ops += n * n * k;
                 h->open_bytes += 4 * n * n + 4 * k * n;
             }
+            lv[3] = (lv[2] + hb::kPivotChunk - 1) / hb::kPivotChunk;
             if (l == 0 && T->record_stats) {
                 h->stats.n_touched_leaves = (int)T->act.size();
                 h->stats.n_pivots = hpiv[T->task];
@@ -1063,13 +1097,242 @@ void run_open_tasks(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t 
         if (T->record_stats) T->h->stats.n_dirty_ancestors = T->n_dirty;
 }
 
+// Which opening path runs: the device-driven one (HTRIP_OPEN_PATH=device: one
+// persistent launch per call, the level loop and the closure rounds on the
+// device) or the host-driven one (default: per level an insert and a close
+// stage, with the pivot counts and the decrease flags read back to the host).
+bool open_on_device() {
+    static const bool dev = [] {
+        const char* e = std::getenv("HTRIP_OPEN_PATH");
+        return e && std::strcmp(e, "device") == 0;
+    }();
+    return dev;
+}
+
+// Device-driven openings of any number of tasks (distinct indexes of one
+// device): tasks of equal (b, g) share one launch of the persistent opening
+// kernel (open.cu).  Per launch the host uploads, in one copy, the task
+// descriptors, every level's work list (level 0: the touched leaves with
+// their opened edges; levels >= 1: the nodes with new seams, with room for
+// the parents the device appends) and the edge / seam triples; the kernel
+// writes each task's statistics, which come back in one copy.  One host wait
+// for the whole call.
+void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t st, int device) {
+    std::map<int, std::vector<OpenTask*>> groups;
+    for (OpenTask* T : tasks) groups[T->h->b * 1024 + T->h->g].push_back(T);
+    struct GL {
+        std::vector<OpenTask*> ts;
+        int maxH = 0;
+        int cap[hb::kOpenMaxLevels] = {}, n_seam[hb::kOpenMaxLevels] = {};
+        size_t o_tasks = 0, o_out = 0, o_words = 0, o_trace = 0, o_slots[hb::kOpenMaxLevels] = {}, o_trip = 0;
+        size_t begin = 0, end = 0;
+        size_t panel = 0, pflags = 0;
+        int n_trip = 0;
+    };
+    std::vector<GL> gl;
+    size_t off = 0, panel_elems = 1, pflag_bytes = 1;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off += align256(std::max<size_t>(bytes, 1));
+        return o;
+    };
+    for (auto& kv : groups) {
+        GL g;
+        g.ts = kv.second;
+        for (OpenTask* T : g.ts) {
+            if (T->h->H + 1 > hb::kOpenMaxLevels) throw CudaError{cudaErrorInvalidValue, "hierarchy too deep"};
+            g.maxH = std::max(g.maxH, T->h->H);
+        }
+        // capacity of every level's list: the touched leaves, then per level
+        // the seam nodes and every parent of the level below's capacity set
+        for (OpenTask* T : g.ts) {
+            htrip_index* h = T->h;
+            std::vector<int> cur = T->leaves;
+            g.cap[0] += (int)cur.size();
+            for (const auto& e : T->edges) g.n_trip += (int)e.size() / 3;
+            for (int l = 1; l <= h->H; ++l) {
+                const Level& Lv = h->L[l];
+                const Level& Lc = h->L[l - 1];
+                std::vector<char> seen(Lv.nnodes, 0);
+                std::vector<int> next;
+                for (int node : T->seam_nodes[l]) {
+                    seen[node] = 1;
+                    next.push_back(node);
+                }
+                g.n_seam[l] += (int)T->seam_nodes[l].size();
+                for (const auto& sv : T->seams[l]) g.n_trip += (int)sv.size() / 3;
+                for (int c : cur) {
+                    const int p = ((c / Lc.nodes_x) / h->g) * Lv.nodes_x + (c % Lc.nodes_x) / h->g;
+                    if (!seen[p]) { seen[p] = 1; next.push_back(p); }
+                }
+                g.cap[l] += (int)next.size();
+                cur = std::move(next);
+            }
+        }
+        const htrip_index* h0 = g.ts[0]->h;
+        for (int l = 0; l <= g.maxH; ++l) {
+            const int NP = l <= h0->H ? h0->L[l].NP : 0;
+            // levels above the first task's depth share its (b, g) geometry; take it from the deepest task
+            int np = NP;
+            for (OpenTask* T : g.ts)
+                if (T->h->H >= l) np = T->h->L[l].NP;
+            panel_elems = std::max(panel_elems, (size_t)g.cap[l] * hb::kOpenB * np);
+            pflag_bytes = std::max(pflag_bytes, (size_t)g.cap[l] * (np / 64));
+        }
+        g.begin = off;
+        g.o_tasks = take(g.ts.size() * sizeof(hb::OpenTask));
+        g.o_out = take(g.ts.size() * sizeof(hb::OpenTaskOut));
+        g.o_words = take((2 * hb::kOpenMaxLevels + 4) * sizeof(int));
+        g.o_trace = take(hb::kOpenTrace * sizeof(unsigned long long));
+        for (int l = 0; l <= g.maxH; ++l) g.o_slots[l] = take((size_t)std::max(1, g.cap[l]) * sizeof(int4));
+        g.o_trip = take((size_t)g.n_trip * 3 * sizeof(int));
+        g.end = off;
+        gl.push_back(std::move(g));
+    }
+    A.dev.reserve(off);
+    A.stage.reserve(off);
+    A.rb.reserve(off);
+    A.panel.reserve(panel_elems);
+    A.pflags.reserve(pflag_bytes);
+    if (!A.open_grid) A.open_grid = hb::open_grid_blocks(device);
+    unsigned char* base = A.dev.p;
+    for (GL& g : gl) {
+        unsigned char* hs = A.stage.p;
+        std::memset(hs + g.begin, 0, g.end - g.begin);
+        auto* hT = reinterpret_cast<hb::OpenTask*>(hs + g.o_tasks);
+        auto* hO = reinterpret_cast<hb::OpenTaskOut*>(hs + g.o_out);
+        int* words = reinterpret_cast<int*>(hs + g.o_words);  // count[17] maxk[17] status bar[3]
+        int* trip = reinterpret_cast<int*>(hs + g.o_trip);
+        int nt = 0;
+        std::vector<int> fill(g.maxH + 1, 0);
+        for (int l = 1; l <= g.maxH; ++l) fill[l] = 0;
+        for (size_t t = 0; t < g.ts.size(); ++t) {
+            OpenTask* T = g.ts[t];
+            htrip_index* h = T->h;
+            T->task = (int)t;
+            if (++h->open_stamp == 0) h->open_stamp = 1;
+            hb::OpenTask& d = hT[t];
+            d.H = h->H;
+            d.g = h->g;
+            d.stamp = h->open_stamp;
+            d.out = reinterpret_cast<hb::OpenTaskOut*>(base + g.o_out) + t;
+            for (int l = 0; l <= h->H; ++l) {
+                Level& Lv = h->L[l];
+                d.lv[l] = hb::OpenTaskLevel{Lv.mat.p, Lv.kflag.p, Lv.klist.p, Lv.kcnt.p, Lv.dstamp.p, Lv.mstamp.p,
+                                            Lv.nodes_x};
+            }
+            int seam_total = 0;
+            for (int l = 1; l <= h->H; ++l) seam_total += (int)T->seam_nodes[l].size();
+            hO[t].n_dirty = seam_total;
+        }
+        // level 0: the touched leaves of every task, each with its edges
+        {
+            int4* sl = reinterpret_cast<int4*>(hs + g.o_slots[0]);
+            int n0 = 0;
+            for (size_t t = 0; t < g.ts.size(); ++t) {
+                OpenTask* T = g.ts[t];
+                for (size_t i = 0; i < T->leaves.size(); ++i) {
+                    const auto& e = T->edges[i];
+                    std::memcpy(trip + 3 * nt, e.data(), e.size() * sizeof(int));
+                    sl[n0++] = make_int4((int)t, T->leaves[i], nt, nt + (int)e.size() / 3);
+                    nt += (int)e.size() / 3;
+                }
+            }
+            words[0] = n0;
+        }
+        // levels >= 1: the seam nodes first, each with its seams
+        for (int l = 1; l <= g.maxH; ++l) {
+            int4* sl = reinterpret_cast<int4*>(hs + g.o_slots[l]);
+            int n = 0;
+            for (size_t t = 0; t < g.ts.size(); ++t) {
+                OpenTask* T = g.ts[t];
+                if (T->h->H < l) continue;
+                for (size_t i = 0; i < T->seam_nodes[l].size(); ++i) {
+                    const auto& sv = T->seams[l][i];
+                    std::memcpy(trip + 3 * nt, sv.data(), sv.size() * sizeof(int));
+                    sl[n++] = make_int4((int)t, T->seam_nodes[l][i], nt, nt + (int)sv.size() / 3);
+                    nt += (int)sv.size() / 3;
+                }
+            }
+            words[l] = n;
+        }
+        hb::OpenLaunch OL{};
+        OL.n_tasks = (int)g.ts.size();
+        OL.maxH = g.maxH;
+        OL.g = g.ts[0]->h->g;
+        OL.tasks = reinterpret_cast<const hb::OpenTask*>(base + g.o_tasks);
+        for (int l = 0; l <= g.maxH; ++l) {
+            const htrip_index* hl = nullptr;
+            for (OpenTask* T : g.ts)
+                if (T->h->H >= l) { hl = T->h; break; }
+            const Level& Lv = hl->L[l];
+            OL.geo[l].NP = Lv.NP;
+            OL.geo[l].n = Lv.n;
+            OL.geo[l].nExt = Lv.nExt;
+            OL.geo[l].nP = Lv.nP;
+            OL.geo[l].isext = Lv.d_isext.p;
+            OL.geo[l].child_ext = l >= 1 ? hl->L[l - 1].d_ext.p : nullptr;
+            OL.geo[l].childNP = l >= 1 ? hl->L[l - 1].NP : 0;
+            OL.slots[l] = reinterpret_cast<int4*>(base + g.o_slots[l]);
+            OL.cap[l] = g.cap[l];
+            OL.n_seam[l] = l >= 1 ? words[l] : 0;
+        }
+        OL.count = reinterpret_cast<int*>(base + g.o_words);
+        OL.maxk = OL.count + hb::kOpenMaxLevels;
+        OL.status = OL.count + 2 * hb::kOpenMaxLevels;
+        OL.bar = reinterpret_cast<unsigned*>(OL.status + 1);
+        OL.triples = reinterpret_cast<const int*>(base + g.o_trip);
+        OL.panel = A.panel.p;
+        OL.pflags = A.pflags.p;
+        OL.trace = reinterpret_cast<unsigned long long*>(base + g.o_trace);
+        ck(cudaMemcpyAsync(base + g.begin, hs + g.begin, g.end - g.begin, cudaMemcpyHostToDevice, st), "open upload");
+        ck(hb::launch_open(OL, A.open_grid, st), "opening kernel");
+        // statistics and the status word back (the trace stays on the device)
+        ck(cudaMemcpyAsync(A.rb.p + g.o_out, base + g.o_out, g.o_trace - g.o_out, cudaMemcpyDeviceToHost, st),
+           "open results");
+        A.trace_off = g.o_trace;
+        A.trace_valid = 1;
+    }
+    ck(cudaStreamSynchronize(st), "opening");
+    for (GL& g : gl) {
+        const int* words = reinterpret_cast<const int*>(A.rb.p + g.o_words);
+        const int status = words[2 * hb::kOpenMaxLevels];
+        if (status != 0)
+            throw CudaError{cudaErrorLaunchFailure, status == 1 ? "opening kernel: a bounded barrier wait timed out"
+                                                                : "opening kernel: a work list overflowed"};
+        const auto* out = reinterpret_cast<const hb::OpenTaskOut*>(A.rb.p + g.o_out);
+        for (size_t t = 0; t < g.ts.size(); ++t) {
+            OpenTask* T = g.ts[t];
+            htrip_index* h = T->h;
+            const hb::OpenTaskOut& o = out[t];
+            for (int l = 0; l <= h->H; ++l) {
+                auto& lv = h->open_levels[l];
+                lv = {o.level[l][0], o.level[l][1], o.level[l][2],
+                      (o.level[l][2] + hb::kOpenB - 1) / hb::kOpenB};
+            }
+            h->open_ops = o.ops;
+            h->open_bytes = o.bytes;
+            if (T->record_stats) {
+                h->stats.n_touched_leaves = (int)T->leaves.size();
+                h->stats.n_pivots = o.new_pivots;
+                h->stats.n_dirty_ancestors = o.n_dirty;
+            }
+        }
+    }
+}
+
+void run_open(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t st, int device) {
+    if (open_on_device()) run_open_device(tasks, A, st, device);
+    else run_open_tasks(tasks, A, st);
+}
+
 void do_open(htrip_index* h, const int32_t* rc, int n, const uint8_t* obs, int rows, int cols, bool record_stats) {
     h->update_counter++;
     OpenTask T;
     open_prepare(T, h, rc, n, obs, rows, cols, record_stats);
     if (!open_has_work(T)) return;
     std::vector<OpenTask*> tasks{&T};
-    run_open_tasks(tasks, h->u, h->stream);
+    run_open(tasks, h->u, h->stream, h->device);
 }
 
 // ---------------------------------------------------------------------------
@@ -1315,8 +1578,10 @@ struct QueryReq {
     uint16_t* out_dev;  // result on the device; nullptr = in the arena
 };
 
-// Launch words: {status, barrier count, barrier generation, pad}, then the
-// phase time stamps at byte kTraceOffset.
+// Launch words: {status, barrier count, barrier generation, pad}, the
+// executed-work counters (QueryParams::work, 3 x u64) at byte kWorkOffset,
+// then the phase time stamps at byte kTraceOffset.
+constexpr size_t kWorkOffset = 16;
 constexpr size_t kTraceOffset = 64;
 constexpr size_t kWordsBytes = kTraceOffset + (2 * hb::kMaxQueryPhases + 1) * sizeof(unsigned long long);
 
@@ -1435,6 +1700,9 @@ hb::QueryParams make_params(const htrip_index* h, const QueryPlan& P, unsigned c
     Q.M = reinterpret_cast<uint32_t*>(base + L.M[i]);
     Q.ctr = reinterpret_cast<unsigned*>(base + L.ctr[i]);
     Q.out = out_dev;
+    // executed-work counters: single-request launches of an index that counts
+    Q.work = h->count_work && L.n == 1 ? reinterpret_cast<unsigned long long*>(base + L.o_words + kWorkOffset)
+                                        : nullptr;
     for (int l = 1; l <= H; ++l) {
         const Level& Lv = h->L[l];
         const QueryPlan::Lvl& PL = P.lv[l];
@@ -1860,6 +2128,7 @@ int run_devplan(htrip_index* h, int k, int cfg, const int32_t* vps_host, const u
     T.M = reinterpret_cast<uint32_t*>(base + D.o_M);
     T.ctr = reinterpret_cast<unsigned*>(base + D.o_ctr);
     T.out = out;
+    T.work = h->count_work ? reinterpret_cast<unsigned long long*>(base + D.o_words + kWorkOffset) : nullptr;
     for (int l = 1; l <= h->H; ++l) {
         const Level& Lv = h->L[l];
         T.lv[l].D = Lv.mat.p;
@@ -2321,18 +2590,33 @@ htrip_status htrip_query_all_pairs_noalloc(htrip_index* h, const int32_t* vps, i
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     unsigned char* base = noalloc_scratch(h->device);
     cudaStream_t st = h->stream;
+    // Declared after the lock, so it runs before the lock is released on
+    // every exit path (an exception included): once work that uses the
+    // shared array is queued, the lock is not given up before that work has
+    // finished, or the next caller's launch could overlap it.
+    struct DrainOnExit {
+        cudaStream_t st;
+        bool armed = false;
+        ~DrainOnExit() {
+            if (armed) cudaStreamSynchronize(st);  // errors are reported by the call itself
+        }
+    } drain{st};
     // The array keeps the previous call's contents: the launch head (with
     // zeroed status / barrier words), the pair matrix and the flags are
     // rewritten by every call.
     std::vector<uint16_t*> outs;
     int grid = h->q.grid;
+    drain.armed = true;
     issue_query_launch(st, h->device, grid, P.cfg, R, L, base, stage.data(), nullptr, outs);
     h->q.grid = grid;
+    // The status word first: the caller's `out` is written only by a launch
+    // whose every wait completed.
     int status = 0;
-    ck(cudaMemcpyAsync(out, outs[0], (size_t)k * k * sizeof(uint16_t), cudaMemcpyDeviceToHost, st), "out");
     ck(cudaMemcpyAsync(&status, base + L.o_words, sizeof(int), cudaMemcpyDeviceToHost, st), "status");
     ck(cudaStreamSynchronize(st), "query sync");
     if (status != 0) return fail(HTRIP_ERR_CUDA, "query kernel: a bounded wait timed out");
+    ck(cudaMemcpyAsync(out, outs[0], (size_t)k * k * sizeof(uint16_t), cudaMemcpyDeviceToHost, st), "out");
+    ck(cudaStreamSynchronize(st), "result sync");
     return HTRIP_OK;
     HTRIP_GUARD_END
 }
@@ -2454,7 +2738,7 @@ htrip_status htrip_open_batch(htrip_batch* b, const htrip_open_request* reqs, in
         std::vector<OpenTask*> work;
         for (auto& T : tasks)
             if (open_has_work(T)) work.push_back(&T);
-        if (!work.empty()) run_open_tasks(work, b->u, b->stream);
+        if (!work.empty()) run_open(work, b->u, b->stream, b->device);
     }
     return HTRIP_OK;
     HTRIP_GUARD_END
@@ -2655,6 +2939,28 @@ static htrip_status arena_phases(const QueryArena& A, cudaStream_t st, uint64_t*
     HTRIP_GUARD_END
 }
 
+htrip_status htrip_set_query_work_counting(htrip_index* h, int32_t on) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    h->count_work = on != 0;
+    return HTRIP_OK;
+}
+
+htrip_status htrip_last_query_executed(htrip_index* h, uint64_t* entries, uint64_t* rows, uint64_t* skipped) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    if (!h->count_work || !h->q.ev_valid) return fail(HTRIP_ERR_INVALID, "no counted query launch");
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    unsigned long long w[3] = {0, 0, 0};
+    ck(cudaMemcpyAsync(w, h->q.dev.p + h->q.last_words + kWorkOffset, sizeof(w), cudaMemcpyDeviceToHost, h->stream),
+       "work counters");
+    ck(cudaStreamSynchronize(h->stream), "sync");
+    if (entries) *entries = w[0];
+    if (rows) *rows = w[1];
+    if (skipped) *skipped = w[2];
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
 htrip_status htrip_last_query_phases(const htrip_index* h, uint64_t* ns, int32_t max_n, int32_t* n) {
     if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
     return arena_phases(h->q, h->stream, ns, max_n, n);
@@ -2746,6 +3052,15 @@ htrip_status htrip_autotune_import(const char* text) {
 htrip_status htrip_autotune_clear(void) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune.clear();
+    return HTRIP_OK;
+}
+
+htrip_status htrip_last_open_levels(const htrip_index* h, int64_t* out, int32_t max_levels, int32_t* n_levels) {
+    if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
+    const int n = std::min<int>((int)h->open_levels.size(), std::max(0, max_levels));
+    for (int l = 0; l < n; ++l)
+        for (int j = 0; j < 4; ++j) out[4 * l + j] = h->open_levels[l][j];
+    if (n_levels) *n_levels = (int32_t)h->open_levels.size();
     return HTRIP_OK;
 }
 

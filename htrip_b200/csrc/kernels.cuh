@@ -99,6 +99,76 @@ void launch_ext_snapshot(const Slot* S, int n, const int* ext, int nExt, int NP,
 void launch_ext_compare(const Slot* S, int n, const int* ext, int nExt, int NP, const uint16_t* snap,
                         uint8_t* slot_dec, int g, cudaStream_t st, int any_change = 0);
 
+// --- device-driven openings (open.cu) -----------------------------------------
+// One onBatchCellsOpened call (or several, on indexes of equal b and g) as ONE
+// cooperative persistent kernel: the level loop, the work list of every level
+// and the closure rounds run on the device, phases separated by bounded grid
+// barriers; the host uploads the call's cell-derived lists once and reads the
+// statistics back once.
+constexpr int kOpenMaxLevels = 17;  // H <= 16
+constexpr int kOpenB = 64;          // pivots closed per round
+
+// Geometry of one level, shared by every index of a launch (equal b and g).
+struct OpenLevelGeom {
+    int NP, n, nExt, nP;       // padded / logical order, exterior ports, ports per child
+    const uint8_t* isext;      // [NP] 1 = exterior port (leaf perimeter cell / node exterior port)
+    const int* child_ext;      // levels >= 1: the child level's port -> matrix index (nP entries)
+    int childNP;               // levels >= 1: the child level's padded order
+};
+
+// One index ("task") of a launch, per level.
+struct OpenTaskLevel {
+    uint16_t* mat;             // matrices (NP x NP each)
+    uint8_t* kflag;            // pivot flags [node][NP] (zero outside a call)
+    int* klist;                // pivot lists [node][NP]
+    int* kcnt;                 // pivot counts [node]
+    uint32_t* dstamp;          // [node] stamp of the call that decreased the node's exterior block
+    uint32_t* mstamp;          // [node] stamp of the call that listed the node
+    int nodes_x;
+};
+
+// Results of one task, written by the kernel (the host zeroes them first,
+// except n_dirty, which starts at the task's number of seam-only nodes).
+struct OpenTaskOut {
+    int new_pivots;            // leaf pivots set by the call (LastBatchStats::n_pivots)
+    int n_dirty;               // listed nodes of levels >= 1 (LastBatchStats::n_dirty_ancestors)
+    int level[kOpenMaxLevels][3];  // per level: matrices, sum of pivot counts, largest pivot count
+    unsigned long long ops, bytes; // algorithmic work: n^2 k ops, 4 n^2 + 4 k n bytes per matrix
+};
+
+struct OpenTask {
+    int H;
+    int g;
+    uint32_t stamp;            // this call's stamp (never 0)
+    OpenTaskOut* out;
+    OpenTaskLevel lv[kOpenMaxLevels];
+};
+
+// Work list entry: {task, node, list_begin, list_end}; the list is the slot's
+// range of (u, v, w) triples (level 0: opened in-leaf edges; above: seams).
+struct OpenLaunch {
+    int n_tasks, maxH, g;
+    const OpenTask* tasks;
+    OpenLevelGeom geo[kOpenMaxLevels];
+    int4* slots[kOpenMaxLevels];   // per level; levels >= 1 start with the seam nodes
+    int* count;                    // [kOpenMaxLevels] listed slots per level (grows during the call)
+    int cap[kOpenMaxLevels];       // capacity of each level's list
+    int n_seam[kOpenMaxLevels];    // seam nodes at the head of each level's list (stamped first)
+    int* maxk;                     // [kOpenMaxLevels] largest pivot count per level
+    const int* triples;            // (u, v, w)
+    uint16_t* panel;               // per slot kOpenB x NP (the round's closed pivot rows)
+    uint8_t* pflags;               // per slot NP / 64: 64-column blocks of the panel holding a finite value
+    int* status;                   // 0 ok, 1 a bounded barrier wait timed out, 2 a list overflowed
+    unsigned* bar;                 // {arrived, generation, unit ticket}
+    unsigned long long* trace;     // or null: [0] start, then one stamp per phase (max kOpenTrace)
+};
+constexpr int kOpenTrace = 1024;
+
+// Shared memory and grid of the launch on `device`; the launch itself.
+size_t open_smem_bytes();
+int open_grid_blocks(int device);
+cudaError_t launch_open(const OpenLaunch& L, int grid, cudaStream_t st);
+
 // --- query (query.cu) -------------------------------------------------------
 constexpr int kMaxQueryLevels = 16;
 constexpr int kNumQueryConfigs = 4;
@@ -148,6 +218,9 @@ struct QueryParams {
                             // [4 + l*k + g] rows x column tiles of level-(l-1) project items
                             // done for level-l group g (its target: cnt x column tiles)
     QueryLevel lv[kMaxQueryLevels + 1];
+    unsigned long long* work;  // or null: [0] tile entries updated (operand rows streamed x
+                               // tile rows x tile columns), [1] operand rows streamed,
+                               // [2] operand rows skipped (no finite value in the tile)
 };
 
 // Words of a request's completion counters.

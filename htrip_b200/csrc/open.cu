@@ -1,0 +1,651 @@
+// onBatchCellsOpened on the device (reference MinPlusOracle::onBatchCellsOpened,
+// src/minplus_oracle.cpp:530-729, with LeafTile::onBatchCellsOpened,
+// src/leaf_tile.cpp:297-374, and InternalNode::applyConwayPerturbations,
+// src/internal_node.cpp:332-413) as ONE cooperative persistent kernel.
+//
+// The host buckets the opened cells (touched leaves with their new in-leaf
+// edges, seam edges per lowest common ancestor) and uploads them once.  The
+// kernel then walks the levels l = 0..H itself:
+//
+//   list(l)    leaves: the touched leaves.  Nodes: the nodes holding new
+//              seams (placed first by the host) and the parents of every
+//              level-(l-1) matrix whose exterior block decreased, appended
+//              by the CTA that saw the decrease (a per-node stamp makes each
+//              node appear once) - the reference's active parents.
+//   insert(l)  leaves: the opened edges (w < D[u][v]: set both entries, mark
+//              u and v as pivots).  Nodes: every entry of a decreased child's
+//              summary that is smaller than the node's entry (the
+//              reference's ChildDecrease list) and the seams.
+//   compact(l) pivot flags -> sorted pivot list per matrix.
+//   rounds     blocked pivot-set Kleene closure, kOpenB pivots per round:
+//              panel: every CTA of a column tile closes the round's pivot
+//                block T = D[K, K] itself (Floyd-Warshall in shared memory)
+//                and computes P[:, tile] = T* (x) D[K, tile];
+//              update: D = min(D, P^T (x) P) over upper-triangle tiles, each
+//                also written transposed (D is symmetric), and only where an
+//                entry changed.
+//   A matrix whose exterior block decreased (refreshBoundarySummary,
+//   leaf_tile.cpp:253-273, internal_node.cpp:415-433) is seen where the
+//   decrease happens: an insert or an update tile lowers an entry whose row
+//   and column are both exterior ports.  No snapshot, no host round trip.
+//
+// Phases are separated by grid barriers whose waits are bounded: after the
+// poll limit a CTA records a timeout in the status word and every CTA
+// returns.  Work units inside a phase are handed out by a ticket that the
+// barrier resets.  Every sum is the exact clamped tropical product of
+// minplus.cuh, and the closure of a matrix over its pivot set is unique, so
+// the result equals the reference's bit for bit.
+#include "kernels.cuh"
+#include "minplus.cuh"
+
+#include <algorithm>
+
+namespace hb {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int B = kOpenB;
+constexpr unsigned kBarrierPolls = 1u << 24;
+constexpr int kInsertChunk = 4096;  // child-summary entries per insert unit
+
+__device__ __forceinline__ unsigned long long global_timer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid barrier over every CTA of the launch; the last CTA to arrive resets
+// the unit ticket for the next phase.  Bounded: a CTA that polls too long
+// records status 1; a CTA that sees a non-zero status stops waiting.  Returns
+// false when the launch must end.
+__device__ bool open_barrier(const OpenLaunch& L) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = L.bar + 1;
+        const unsigned gen = *vgen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(L.bar, 1u);
+        int ok = 1;
+        if (arrived == gridDim.x - 1) {
+            atomicExch(L.bar, 0u);
+            atomicExch(L.bar + 2, 0u);
+            __threadfence();
+            atomicAdd(L.bar + 1, 1u);
+        } else {
+            unsigned it = 0;
+            while (*vgen == gen) {
+                if (*(volatile int*)L.status != 0) {
+                    ok = 0;
+                    break;
+                }
+                if (++it > kBarrierPolls) {
+                    atomicCAS(L.status, 0, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        s_ok = ok && *(volatile int*)L.status == 0;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Next work unit of the phase for this CTA (all threads get it).
+__device__ __forceinline__ int next_unit(const OpenLaunch& L, int* s_unit) {
+    __syncthreads();
+    if (threadIdx.x == 0) *s_unit = (int)atomicAdd(L.bar + 2, 1u);
+    __syncthreads();
+    return *s_unit;
+}
+
+__device__ __forceinline__ uint16_t* node_mat(const OpenTaskLevel& T, int node, int NP) {
+    return T.mat + (size_t)node * NP * NP;
+}
+
+// The exterior block of matrix `node` of level l decreased in this call:
+// record it once and list its parent for level l + 1 (once per call).
+__device__ void mark_dec(const OpenLaunch& L, int l, int task, int node) {
+    const OpenTask& T = L.tasks[task];
+    if (l >= T.H) return;  // the root has no summary above it
+    if (atomicExch(T.lv[l].dstamp + node, T.stamp) == T.stamp) return;
+    const int nx = T.lv[l].nodes_x, g = T.g;
+    const int p = ((node / nx) / g) * T.lv[l + 1].nodes_x + (node % nx) / g;
+    if (atomicExch(T.lv[l + 1].mstamp + p, T.stamp) == T.stamp) return;
+    const int idx = atomicAdd(L.count + l + 1, 1);
+    if (idx >= L.cap[l + 1]) {
+        atomicCAS(L.status, 0, 2);
+        return;
+    }
+    L.slots[l + 1][idx] = make_int4(task, p, 0, 0);
+    atomicAdd(&T.out->n_dirty, 1);
+}
+
+// ---------------------------------------------------------------------------
+// Phase 0: the seam nodes at the head of every level's list are stamped as
+// listed, so that a parent appended later is never listed twice.
+// ---------------------------------------------------------------------------
+__device__ void stamp_phase(const OpenLaunch& L) {
+    const int gt = blockIdx.x * kThreads + threadIdx.x, gs = gridDim.x * kThreads;
+    for (int l = 1; l <= L.maxH; ++l)
+        for (int s = gt; s < L.n_seam[l]; s += gs) {
+            const int4 e = L.slots[l][s];
+            const OpenTask& T = L.tasks[e.x];
+            T.lv[l].mstamp[e.y] = T.stamp;
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Insert phase.
+// ---------------------------------------------------------------------------
+// Serial edge / seam list of one slot (leaf_tile.cpp:311-330,
+// internal_node.cpp:356-365): an entry counts, and its endpoints become
+// pivots, only if it shortens D[u][v].  Run by one thread.
+__device__ void insert_list(const OpenLaunch& L, int l, int4 e, int* new_pivots, bool* dec) {
+    const OpenTask& T = L.tasks[e.x];
+    const OpenLevelGeom& G = L.geo[l];
+    const int NP = G.NP;
+    uint16_t* D = node_mat(T.lv[l], e.y, NP);
+    uint8_t* f = T.lv[l].kflag + (size_t)e.y * NP;
+    int np = 0;
+    bool d = false;
+    for (int t = e.z; t < e.w; ++t) {
+        const int u = L.triples[3 * t], v = L.triples[3 * t + 1];
+        const uint16_t w = (uint16_t)L.triples[3 * t + 2];
+        if (w < D[(size_t)u * NP + v]) {
+            D[(size_t)u * NP + v] = w;
+            D[(size_t)v * NP + u] = w;
+            if (!f[u]) { f[u] = 1; ++np; }
+            if (!f[v]) { f[v] = 1; ++np; }
+            d |= G.isext[u] && G.isext[v];
+        }
+    }
+    *new_pivots = np;
+    *dec = d;
+}
+
+__device__ void insert_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
+    const OpenLevelGeom& G = L.geo[l];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ int s_dec;
+    const int list_units = (N + kWarps - 1) / kWarps;  // one slot per warp (lane 0)
+    const int g2 = L.g * L.g;
+    const int chunks = l >= 1 ? (G.nP * G.nP + kInsertChunk - 1) / kInsertChunk : 0;
+    const int child_units = l >= 1 ? N * g2 * chunks : 0;
+    const int units = list_units + child_units;
+    for (int u = next_unit(L, s_unit); u < units; u = next_unit(L, s_unit)) {
+        if (u < list_units) {
+            const int s = u * kWarps + warp;
+            if (s < N && lane == 0) {
+                const int4 e = L.slots[l][s];
+                if (e.w > e.z) {
+                    int np = 0;
+                    bool dec = false;
+                    insert_list(L, l, e, &np, &dec);
+                    const OpenTask& T = L.tasks[e.x];
+                    if (l == 0 && np) atomicAdd(&T.out->new_pivots, np);
+                    if (dec) mark_dec(L, l, e.x, e.y);
+                }
+            }
+            continue;
+        }
+        // child-summary decreases (internal_node.cpp:343-353): inserting every
+        // child summary entry smaller than the node's is the same as inserting
+        // the reference's decrease list (an entry that did not decrease is
+        // never smaller than the node's, which is <= the old summary)
+        const int cu = u - list_units;
+        const int s = cu / (g2 * chunks);
+        const int q = (cu / chunks) % g2;
+        const int c = cu % chunks;
+        const int4 e = L.slots[l][s];
+        const OpenTask& T = L.tasks[e.x];
+        const int nx = T.lv[l].nodes_x, g = L.g;
+        const int child = ((e.y / nx) * g + q / g) * T.lv[l - 1].nodes_x + ((e.y % nx) * g + q % g);
+        if (T.lv[l - 1].dstamp[child] != T.stamp) continue;  // uniform over the CTA
+        if (threadIdx.x == 0) s_dec = 0;
+        __syncthreads();
+        const int NP = G.NP, nP = G.nP, cNP = G.childNP;
+        const uint16_t* cm = node_mat(T.lv[l - 1], child, cNP);
+        uint16_t* D = node_mat(T.lv[l], e.y, NP);
+        uint8_t* f = T.lv[l].kflag + (size_t)e.y * NP;
+        const int i1 = min(nP * nP, (c + 1) * kInsertChunk);
+        bool dec = false;
+        for (int idx = c * kInsertChunk + threadIdx.x; idx < i1; idx += kThreads) {
+            const int p = idx / nP, pp = idx - p * nP;
+            const uint16_t w = cm[(size_t)G.child_ext[p] * cNP + G.child_ext[pp]];
+            const int a = q * nP + p, b = q * nP + pp;
+            if (w < D[(size_t)a * NP + b]) {
+                D[(size_t)a * NP + b] = w;  // (b, a) is written by its own thread
+                f[a] = 1;
+                f[b] = 1;
+                dec |= G.isext[a] && G.isext[b];
+            }
+        }
+        if (__any_sync(FULL, dec) && lane == 0) s_dec = 1;
+        __syncthreads();
+        if (threadIdx.x == 0 && s_dec) mark_dec(L, l, e.x, e.y);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Compact phase: one CTA per slot turns the pivot flags into the ascending
+// pivot list (and clears the flags); per-level statistics and the largest
+// pivot count of the level (which sets the number of rounds).
+// ---------------------------------------------------------------------------
+__device__ void compact_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
+    const OpenLevelGeom& G = L.geo[l];
+    __shared__ int warp_tot[kWarps];
+    __shared__ int base;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int s = next_unit(L, s_unit); s < N; s = next_unit(L, s_unit)) {
+        const int4 e = L.slots[l][s];
+        const OpenTask& T = L.tasks[e.x];
+        uint8_t* f = T.lv[l].kflag + (size_t)e.y * G.NP;
+        int* out = T.lv[l].klist + (size_t)e.y * G.NP;
+        if (threadIdx.x == 0) base = 0;
+        __syncthreads();
+        for (int j0 = 0; j0 < G.NP; j0 += kThreads) {
+            const int j = j0 + threadIdx.x;
+            const bool on = j < G.NP && f[j];
+            const unsigned bal = __ballot_sync(FULL, on);
+            if (lane == 0) warp_tot[warp] = __popc(bal);
+            __syncthreads();
+            int off = base;
+            for (int w = 0; w < warp; ++w) off += warp_tot[w];
+            if (on) {
+                out[off + __popc(bal & ((1u << lane) - 1u))] = j;
+                f[j] = 0;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0)
+                for (int w = 0; w < kWarps; ++w) base += warp_tot[w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            const int k = base;
+            T.lv[l].kcnt[e.y] = k;
+            atomicAdd(&T.out->level[l][0], 1);
+            atomicAdd(&T.out->level[l][1], k);
+            atomicMax(&T.out->level[l][2], k);
+            atomicMax(L.maxk + l, k);
+            if (k) {
+                const unsigned long long n = (unsigned long long)G.n;
+                atomicAdd(&T.out->ops, n * n * (unsigned long long)k);
+                atomicAdd(&T.out->bytes, 4ull * n * n + 4ull * (unsigned long long)k * n);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Panel phase of round r: unit = (slot, column tile of 64*CP columns).
+//   T* = closure of T = D[Kc, Kc] (Floyd-Warshall over the round's pivots, in
+//        shared memory; the reference's sequential relaxation restricted to
+//        the pivots),
+//   P[a][j] = min_c T*[a][c] (+) D[Kc[c]][j]   for the tile's columns j,
+// stored in the slot's panel, with the 64-column blocks holding a finite
+// value flagged for the update.
+// ---------------------------------------------------------------------------
+constexpr int kTLD = B + 8;  // padded row of T (144 bytes): column reads hit distinct banks
+
+template <int CP>
+__device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, unsigned char* smem) {
+    constexpr int NT = 64 * CP;
+    const OpenLevelGeom& G = L.geo[l];
+    const int NP = G.NP;
+    const int4 e = L.slots[l][s];
+    const OpenTask& T = L.tasks[e.x];
+    const int mk = min(B, T.lv[l].kcnt[e.y] - r * B);
+    if (mk <= 0) return;  // uniform
+    uint16_t (*Ts)[kTLD] = reinterpret_cast<uint16_t (*)[kTLD]>(smem);
+    uint16_t* Bs = reinterpret_cast<uint16_t*>(smem + B * kTLD * sizeof(uint16_t));  // [B][NT]
+    int* kc = reinterpret_cast<int*>(smem + B * kTLD * sizeof(uint16_t) + B * NT * sizeof(uint16_t));
+    __shared__ int tile_any[4];
+    const uint16_t* D = node_mat(T.lv[l], e.y, NP);
+    const int tid = threadIdx.x;
+    if (tid < mk) kc[tid] = T.lv[l].klist[(size_t)e.y * NP + r * B + tid];
+    if (tid < 4) tile_any[tid] = 0;
+    __syncthreads();
+    for (int idx = tid; idx < B * B; idx += kThreads) {
+        const int a = idx / B, c = idx % B;
+        Ts[a][c] = (a < mk && c < mk) ? D[(size_t)kc[a] * NP + kc[c]] : (a == c ? 0 : INF);
+    }
+    for (int idx = tid; idx < mk * (NT / 8); idx += kThreads) {
+        const int a = idx / (NT / 8), c8 = idx % (NT / 8);
+        reinterpret_cast<uint4*>(Bs + a * NT)[c8] = reinterpret_cast<const uint4*>(D + (size_t)kc[a] * NP + j0)[c8];
+    }
+    __syncthreads();
+    {   // Floyd-Warshall over the pivot block: thread t owns row t / 4, 16 columns
+        const int a = tid >> 2, c0 = (tid & 3) * 16;
+        uint32_t v[8];
+        const uint4 x0 = *reinterpret_cast<const uint4*>(&Ts[a][c0]);
+        const uint4 y0 = *reinterpret_cast<const uint4*>(&Ts[a][c0 + 8]);
+        v[0] = x0.x; v[1] = x0.y; v[2] = x0.z; v[3] = x0.w; v[4] = y0.x; v[5] = y0.y; v[6] = y0.z; v[7] = y0.w;
+        // step kk reads row kk and column kk, which it leaves unchanged
+        // (T[kk][kk] = 0): one barrier per step orders it before step kk + 1
+        for (int kk = 0; kk < mk; ++kk) {
+            const uint32_t t = Ts[a][kk];
+            const uint4 x = *reinterpret_cast<const uint4*>(&Ts[kk][c0]);
+            const uint4 y = *reinterpret_cast<const uint4*>(&Ts[kk][c0 + 8]);
+            if (t < INF) {
+                const uint32_t rw[8] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
+                const uint32_t aa = splat(t), tt = splat(INF - t);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) v[i] = acc_clamp(v[i], rw[i], aa, tt);
+                *reinterpret_cast<uint4*>(&Ts[a][c0]) = make_uint4(v[0], v[1], v[2], v[3]);
+                *reinterpret_cast<uint4*>(&Ts[a][c0 + 8]) = make_uint4(v[4], v[5], v[6], v[7]);
+            }
+            __syncthreads();
+        }
+    }
+    // P = T* (x) D[Kc, tile]: warp w owns pivot rows 8w..8w+7, lane the CP
+    // column pairs from 2*CP*lane (T* symmetric: T*[c][a] = T*[a][c])
+    const int warp = tid >> 5, lane = tid & 31;
+    uint32_t acc[8][CP];
+#pragma unroll
+    for (int rr = 0; rr < 8; ++rr)
+#pragma unroll
+        for (int cc = 0; cc < CP; ++cc) acc[rr][cc] = INF2;
+    for (int k = 0; k < mk; ++k) {
+        uint32_t bv[CP];
+#pragma unroll
+        for (int cc = 0; cc < CP; ++cc) bv[cc] = reinterpret_cast<const uint32_t*>(Bs + k * NT + lane * 2 * CP)[cc];
+        const uint4 av = *reinterpret_cast<const uint4*>(&Ts[k][warp * 8]);
+        const uint32_t aw[4] = {av.x, av.y, av.z, av.w};
+#pragma unroll
+        for (int r2 = 0; r2 < 4; ++r2) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint32_t a = h ? (aw[r2] >> 16) : (aw[r2] & 0xffffu);
+                if (a <= INF_HEADROOM) {
+                    const uint32_t aa = splat(a);
+#pragma unroll
+                    for (int cc = 0; cc < CP; ++cc) acc[2 * r2 + h][cc] = acc_fast(acc[2 * r2 + h][cc], bv[cc], aa);
+                } else if (a < INF) {
+                    const uint32_t aa = splat(a), tt = splat(INF - a);
+#pragma unroll
+                    for (int cc = 0; cc < CP; ++cc)
+                        acc[2 * r2 + h][cc] = acc_clamp(acc[2 * r2 + h][cc], bv[cc], aa, tt);
+                }
+            }
+        }
+    }
+    uint16_t* P = L.panel + (size_t)s * B * NP;
+    bool any = false;
+    const int col = j0 + lane * 2 * CP;
+#pragma unroll
+    for (int rr = 0; rr < 8; ++rr) {
+        const int a = warp * 8 + rr;
+        if (a >= mk) continue;
+        uint32_t* dst = reinterpret_cast<uint32_t*>(P + (size_t)a * NP + col);
+#pragma unroll
+        for (int cc = 0; cc < CP; ++cc) {
+            dst[cc] = acc[rr][cc];
+            any |= acc[rr][cc] != INF2;
+        }
+    }
+    if (any) tile_any[(lane * 2 * CP) / 64] = 1;
+    __syncthreads();
+    if (tid < NT / 64) L.pflags[(size_t)s * (NP / 64) + j0 / 64 + tid] = tile_any[tid] ? 1 : 0;
+}
+
+__device__ void panel_phase(const OpenLaunch& L, int l, int N, int r, int* s_unit, unsigned char* smem) {
+    const int NP = L.geo[l].NP;
+    const int NT = NP >= 256 ? 256 : NP;
+    const int tiles = NP / NT;
+    const int units = N * tiles;
+    for (int u = next_unit(L, s_unit); u < units; u = next_unit(L, s_unit)) {
+        const int s = u / tiles, j0 = (u % tiles) * NT;
+        if (NT == 256) panel_unit<4>(L, l, s, j0, r, smem);
+        else if (NT == 128) panel_unit<2>(L, l, s, j0, r, smem);
+        else panel_unit<1>(L, l, s, j0, r, smem);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Update phase of round r: unit = (slot, tile pair I <= J) of TT x TT tiles.
+//   D[i][j] = min(D[i][j], min_a P[a][i] (+) P[a][j])   (a < mk)
+// computed once for the upper-triangle tile and written to (I, J) and,
+// transposed, to (J, I); tiles whose rows or columns hold no finite panel
+// value are skipped, unchanged rows are not written.  An exterior x exterior
+// entry that decreased marks the matrix's summary as decreased.
+// Warp w owns rows RW*w .. RW*w + RW - 1 of the tile, each lane CP column
+// pairs.  Per pivot k the warp's RW panel values share one class, staged
+// with the panel: 0 all INF (skip), 1 all <= INF_HEADROOM (2-op form, no
+// wrap), 2 otherwise (3-op clamped form).
+// ---------------------------------------------------------------------------
+template <int RW, int CP>
+__device__ void update_unit(const OpenLaunch& L, int l, int s, int I, int J, int r, unsigned char* smem) {
+    constexpr int TT = 8 * RW;  // == 64 * CP
+    static_assert(TT == 64 * CP, "square tiles");
+    const OpenLevelGeom& G = L.geo[l];
+    const int NP = G.NP;
+    const int4 e = L.slots[l][s];
+    const OpenTask& T = L.tasks[e.x];
+    const int mk = min(B, T.lv[l].kcnt[e.y] - r * B);
+    if (mk <= 0) return;
+    const uint8_t* pf = L.pflags + (size_t)s * (NP / 64);
+    bool live_i = false, live_j = false;
+#pragma unroll
+    for (int t = 0; t < TT / 64; ++t) {
+        live_i |= pf[I * (TT / 64) + t] != 0;
+        live_j |= pf[J * (TT / 64) + t] != 0;
+    }
+    if (!live_i || !live_j) return;  // uniform
+    uint32_t* As = reinterpret_cast<uint32_t*>(smem);                                  // [B][TT] splatted
+    uint16_t* Bs = reinterpret_cast<uint16_t*>(smem + (size_t)B * TT * sizeof(uint32_t));  // [B][TT]
+    uint8_t* cls = smem + (size_t)B * TT * (sizeof(uint32_t) + sizeof(uint16_t));          // [B][kWarps]
+    __shared__ int s_any, s_dec;
+    const uint16_t* P = L.panel + (size_t)s * B * NP;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int i0 = I * TT, jb = J * TT;
+    if (tid == 0) { s_any = 0; s_dec = 0; }
+    for (int idx = tid; idx < mk * (TT / 8); idx += kThreads) {
+        const int a = idx / (TT / 8), c8 = idx % (TT / 8);
+        const uint4 va = reinterpret_cast<const uint4*>(P + (size_t)a * NP + i0)[c8];
+        const uint4 vb = reinterpret_cast<const uint4*>(P + (size_t)a * NP + jb)[c8];
+        reinterpret_cast<uint4*>(Bs + a * TT)[c8] = vb;
+        const uint32_t w[4] = {va.x, va.y, va.z, va.w};
+        uint4* dst = reinterpret_cast<uint4*>(As + a * TT + c8 * 8);
+        dst[0] = make_uint4(splat(w[0]), splat(w[0] >> 16), splat(w[1]), splat(w[1] >> 16));
+        dst[1] = make_uint4(splat(w[2]), splat(w[2] >> 16), splat(w[3]), splat(w[3] >> 16));
+    }
+    __syncthreads();
+    for (int idx = tid; idx < mk * kWarps; idx += kThreads) {
+        const int a = idx / kWarps, w = idx % kWarps;
+        const uint32_t* ar = As + a * TT + w * RW;
+        uint32_t mn = 0xffffu, mx = 0;
+#pragma unroll
+        for (int rr = 0; rr < RW; ++rr) {
+            const uint32_t v = ar[rr] & 0xffffu;
+            mn = min(mn, v);
+            mx = max(mx, v);
+        }
+        cls[idx] = mn >= INF ? 0 : (mx <= INF_HEADROOM ? 1 : 2);
+    }
+    __syncthreads();
+    uint32_t acc[RW][CP];
+#pragma unroll
+    for (int rr = 0; rr < RW; ++rr)
+#pragma unroll
+        for (int cc = 0; cc < CP; ++cc) acc[rr][cc] = INF2;
+    for (int k = 0; k < mk; ++k) {
+        const int c = cls[k * kWarps + warp];
+        if (c == 0) continue;  // uniform over the warp
+        uint32_t bv[CP];
+#pragma unroll
+        for (int cc = 0; cc < CP; ++cc) bv[cc] = reinterpret_cast<const uint32_t*>(Bs + k * TT + lane * 2 * CP)[cc];
+        const uint32_t* ar = As + k * TT + warp * RW;
+        uint32_t av[RW];
+#pragma unroll
+        for (int q = 0; q < RW / 4; ++q) {
+            const uint4 x = reinterpret_cast<const uint4*>(ar)[q];
+            av[4 * q] = x.x; av[4 * q + 1] = x.y; av[4 * q + 2] = x.z; av[4 * q + 3] = x.w;
+        }
+        if (c == 1) {
+#pragma unroll
+            for (int rr = 0; rr < RW; ++rr)
+#pragma unroll
+                for (int cc = 0; cc < CP; ++cc) acc[rr][cc] = acc_fast(acc[rr][cc], bv[cc], av[rr]);
+        } else {
+#pragma unroll
+            for (int rr = 0; rr < RW; ++rr) {
+                const uint32_t tt = INF2 - av[rr];
+#pragma unroll
+                for (int cc = 0; cc < CP; ++cc) acc[rr][cc] = acc_clamp(acc[rr][cc], bv[cc], av[rr], tt);
+            }
+        }
+    }
+    // epilogue: new = min(acc, old); changed entries are written
+    uint16_t* D = node_mat(T.lv[l], e.y, NP);
+    const int col = jb + lane * 2 * CP;
+    uint32_t cext[CP];
+#pragma unroll
+    for (int cc = 0; cc < CP; ++cc)
+        cext[cc] = (G.isext[col + 2 * cc] ? 0xffffu : 0u) | (G.isext[col + 2 * cc + 1] ? 0xffff0000u : 0u);
+    bool any = false, dec = false;
+#pragma unroll
+    for (int rr = 0; rr < RW; ++rr) {
+        const int row = i0 + warp * RW + rr;
+        uint32_t* dp = reinterpret_cast<uint32_t*>(D + (size_t)row * NP + col);
+        const bool rext = G.isext[row] != 0;
+        uint32_t old[CP];
+#pragma unroll
+        for (int cc = 0; cc < CP; ++cc) old[cc] = dp[cc];
+        uint32_t ch = 0;
+#pragma unroll
+        for (int cc = 0; cc < CP; ++cc) {
+            acc[rr][cc] = min2(acc[rr][cc], old[cc]);
+            const uint32_t diff = acc[rr][cc] ^ old[cc];
+            ch |= diff;
+            if (rext) dec |= (diff & cext[cc]) != 0;
+        }
+        if (ch) {
+            any = true;
+#pragma unroll
+            for (int cc = 0; cc < CP; ++cc) dp[cc] = acc[rr][cc];
+        }
+    }
+    if (__any_sync(FULL, any) && lane == 0) s_any = 1;
+    if (__any_sync(FULL, dec) && lane == 0) s_dec = 1;
+    __syncthreads();  // the staging buffers are free from here on
+    if (I != J && s_any) {
+        // the transposed tile, through shared memory: Tt[j][i], rows padded by 8
+        constexpr int LD = TT + 8;
+        uint16_t* Tt = reinterpret_cast<uint16_t*>(smem);
+#pragma unroll
+        for (int rr = 0; rr < RW; ++rr) {
+            const int i = warp * RW + rr;
+#pragma unroll
+            for (int cc = 0; cc < CP; ++cc) {
+                const int j = lane * 2 * CP + 2 * cc;
+                Tt[j * LD + i] = (uint16_t)(acc[rr][cc] & 0xffffu);
+                Tt[(j + 1) * LD + i] = (uint16_t)(acc[rr][cc] >> 16);
+            }
+        }
+        __syncthreads();
+        for (int idx = tid; idx < TT * (TT / 8); idx += kThreads) {
+            const int j = idx / (TT / 8), c8 = idx % (TT / 8);
+            const uint16_t* src = Tt + j * LD + c8 * 8;
+            uint4 v;
+            v.x = src[0] | ((uint32_t)src[1] << 16);
+            v.y = src[2] | ((uint32_t)src[3] << 16);
+            v.z = src[4] | ((uint32_t)src[5] << 16);
+            v.w = src[6] | ((uint32_t)src[7] << 16);
+            reinterpret_cast<uint4*>(D + (size_t)(jb + j) * NP + i0)[c8] = v;
+        }
+    }
+    if (tid == 0 && s_dec) mark_dec(L, l, e.x, e.y);
+}
+
+// Upper-triangle tile pair t of an nt x nt tile grid: I <= J.
+__device__ __forceinline__ void tri_pair(int t, int nt, int& I, int& J) {
+    int i = 0;
+    while (t >= nt - i) {
+        t -= nt - i;
+        ++i;
+    }
+    I = i;
+    J = i + t;
+}
+
+__device__ void update_phase(const OpenLaunch& L, int l, int N, int r, int* s_unit, unsigned char* smem) {
+    const int NP = L.geo[l].NP;
+    const int TT = NP >= 128 ? 128 : 64;
+    const int nt = NP / TT;
+    const int per = nt * (nt + 1) / 2;
+    const int units = N * per;
+    for (int u = next_unit(L, s_unit); u < units; u = next_unit(L, s_unit)) {
+        const int s = u / per;
+        int I, J;
+        tri_pair(u % per, nt, I, J);
+        if (TT == 128) update_unit<16, 2>(L, l, s, I, J, r, smem);
+        else update_unit<8, 1>(L, l, s, I, J, r, smem);
+    }
+}
+
+constexpr size_t kPanelSmem = (size_t)B * kTLD * sizeof(uint16_t) + (size_t)B * 256 * sizeof(uint16_t) + B * sizeof(int);
+constexpr size_t kUpdateSmem = (size_t)B * 128 * (sizeof(uint32_t) + sizeof(uint16_t)) + (size_t)B * kWarps;
+constexpr size_t kTransposeSmem = (size_t)128 * (128 + 8) * sizeof(uint16_t);
+constexpr size_t kOpenSmem = std::max(kPanelSmem, std::max(kUpdateSmem, kTransposeSmem));
+
+__global__ void __launch_bounds__(kThreads, 2) open_persistent_kernel(const OpenLaunch L) {
+    extern __shared__ __align__(16) unsigned char osm[];
+    __shared__ int s_unit;
+    int phase = 0;
+    const bool stamp = L.trace && blockIdx.x == 0 && threadIdx.x == 0;
+    if (stamp) L.trace[0] = global_timer();
+    auto end_phase = [&]() -> bool {
+        const bool ok = open_barrier(L);
+        if (stamp && phase < kOpenTrace - 1) L.trace[1 + phase] = global_timer();
+        ++phase;
+        return ok;
+    };
+    stamp_phase(L);
+    if (!end_phase()) return;
+    for (int l = 0; l <= L.maxH; ++l) {
+        const int N = min(*(volatile int*)(L.count + l), L.cap[l]);
+        if (N == 0) continue;
+        insert_phase(L, l, N, &s_unit);
+        if (!end_phase()) return;
+        compact_phase(L, l, N, &s_unit);
+        if (!end_phase()) return;
+        const int rounds = (*(volatile int*)(L.maxk + l) + B - 1) / B;
+        for (int r = 0; r < rounds; ++r) {
+            panel_phase(L, l, N, r, &s_unit, osm);
+            if (!end_phase()) return;
+            update_phase(L, l, N, r, &s_unit, osm);
+            if (!end_phase()) return;
+        }
+    }
+}
+
+}  // namespace
+
+size_t open_smem_bytes() { return kOpenSmem; }
+
+int open_grid_blocks(int device) {
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(open_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kOpenSmem);
+        configured = true;
+    }
+    int sms = 0, per = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, open_persistent_kernel, kThreads, kOpenSmem);
+    return sms * std::max(1, std::min(per, 2));
+}
+
+cudaError_t launch_open(const OpenLaunch& L, int grid, cudaStream_t st) {
+    void* args[] = {const_cast<OpenLaunch*>(&L)};
+    return cudaLaunchCooperativeKernel((const void*)open_persistent_kernel, dim3(grid), dim3(kThreads), args,
+                                       kOpenSmem, st);
+}
+
+}  // namespace hb

@@ -267,6 +267,7 @@ plan_query_kernel(const int32_t* __restrict__ vps, const uint8_t* __restrict__ p
                 Pq->M = tmpl.M;
                 Pq->ctr = tmpl.ctr;
                 Pq->out = tmpl.out;
+                Pq->work = tmpl.work;
             }
         }
     }

@@ -106,8 +106,9 @@ __device__ __forceinline__ void cp_wait() {
 // chunks from column `bcols` on are taken from column 0 instead (their lanes'
 // results are not used).  All operand copies bypass L1 (cp.async.cg): the
 // X / Y rows may have been written by other CTAs of the same launch.
+// Returns the number of rows the warp skipped (no finite value in the tile).
 template <int RW, int CP>
-__device__ __forceinline__ void warp_minplus_list(uint32_t (&acc)[RW][CP], const int* kl, int n, int warp,
+__device__ __forceinline__ int warp_minplus_list(uint32_t (&acc)[RW][CP], const int* kl, int n, int warp,
                                                   const uint16_t* __restrict__ A, int lda,
                                                   const uint16_t* __restrict__ B0, int ldb, int bcols,
                                                   uint32_t* pipe) {
@@ -117,6 +118,7 @@ __device__ __forceinline__ void warp_minplus_list(uint32_t (&acc)[RW][CP], const
     const int first = warp * U;
     const int n_it = first < n ? (n - first + stride - 1) / stride : 0;
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(pipe);
+    int skipped = 0;
     auto issue = [&](int it) {
         if (it < n_it) {
             const int st = it % NS;
@@ -166,7 +168,10 @@ __device__ __forceinline__ void warp_minplus_list(uint32_t (&acc)[RW][CP], const
                 }
                 mn = min2(mn, mn >> 16) & 0xffffu;
                 mx = max2(mx, mx >> 16) & 0xffffu;
-                if (mn >= INF) continue;
+                if (mn >= INF) {
+                    ++skipped;
+                    continue;
+                }
                 if (mx <= INF_HEADROOM) {
 #pragma unroll
                     for (int r2 = 0; r2 < RW / 2; ++r2) {
@@ -189,6 +194,21 @@ __device__ __forceinline__ void warp_minplus_list(uint32_t (&acc)[RW][CP], const
         __syncwarp();
     }
     cp_wait<0>();
+    return skipped;
+}
+
+// Executed-work counters of a request (QueryParams::work): each warp adds
+// the rows of its share of the unit's operand list it streamed and skipped.
+template <int RW, int CP>
+__device__ __forceinline__ void count_work(unsigned long long* work, int n, int warp, int skipped) {
+    if (!work || (threadIdx.x & 31) != 0) return;
+    const int stride = kWarps * kPipeRows, first = warp * kPipeRows;
+    int mine = 0;  // rows of the list this warp streamed (see warp_minplus_list)
+    for (int t = first; t < n; t += stride) mine += min(kPipeRows, n - t);
+    if (mine == 0) return;
+    atomicAdd(work, (unsigned long long)(mine - skipped) * RW * 64 * CP);
+    atomicAdd(work + 1, (unsigned long long)(mine - skipped));
+    atomicAdd(work + 2, (unsigned long long)skipped);
 }
 
 // Compacts the set flags of rows [kb, ke) into kl (ascending); returns the
@@ -376,8 +396,9 @@ __device__ bool do_project(const QueryParams& P, const QueryLevel& L, const Quer
     for (int r = 0; r < RW; ++r)
 #pragma unroll
         for (int c = 0; c < CP; ++c) acc[r][c] = INF2;
-    warp_minplus_list<RW, CP>(acc, kl + kb, ke - kb, warp, Xp, P.ldv, D + n0, L.NP, L.NP - n0,
-                              red + warp * pipe_warp_words<RW, CP>());
+    const int skipped = warp_minplus_list<RW, CP>(acc, kl + kb, ke - kb, warp, Xp, P.ldv, D + n0, L.NP, L.NP - n0,
+                                                  red + warp * pipe_warp_words<RW, CP>());
+    count_work<RW, CP>(P.work, ke - kb, warp, skipped);
     cta_reduce<RW, CP>(acc, red);
     if (L.split > 1 && !combine_parts<RW, CP>(L, item, part, acc)) {
         __syncthreads();  // kl / red / im are reused by the next item
@@ -441,8 +462,9 @@ __device__ void do_meet(const QueryParams& P, const QueryLevel& L, int item, int
     for (int r = 0; r < RW; ++r)
 #pragma unroll
         for (int c = 0; c < CP; ++c) acc[r][c] = INF2;
-    warp_minplus_list<RW, CP>(acc, kl, nA, warp, Xp, P.ldv, Y, P.ldv, P.ldv - i0,
-                              red + warp * pipe_warp_words<RW, CP>());
+    const int skipped = warp_minplus_list<RW, CP>(acc, kl, nA, warp, Xp, P.ldv, Y, P.ldv, P.ldv - i0,
+                                                  red + warp * pipe_warp_words<RW, CP>());
+    count_work<RW, CP>(P.work, nA, warp, skipped);
     cta_reduce<RW, CP>(acc, red);
 #pragma unroll
     for (int r = 0; r < RW; ++r) {

@@ -90,6 +90,7 @@ EXPORTS = (
     "htrip_query_all_pairs_incremental", "htrip_batch_create_priority", "htrip_cell_blocked",
     "htrip_leaves_changed", "htrip_selftest_barrier_timeout", "htrip_selftest_wait_timeout", "htrip_set_cell_weights",
     "htrip_cell_weight_changed", "htrip_tile_weights_changed", "htrip_server_wait_version",
+    "htrip_last_open_levels", "htrip_set_query_work_counting", "htrip_last_query_executed",
 )
 
 
@@ -139,6 +140,9 @@ def load_library(path: str | None = None):
     lib.htrip_measure_minplus_rate.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
     lib.htrip_last_query_phases.argtypes = [P, _U64P, I, _I32P]
     lib.htrip_last_open_work.argtypes = [P, _U64P, _U64P]
+    lib.htrip_last_open_levels.argtypes = [P, C.POINTER(C.c_int64), I, _I32P]
+    lib.htrip_set_query_work_counting.argtypes = [P, I]
+    lib.htrip_last_query_executed.argtypes = [P, _U64P, _U64P, _U64P]
     lib.htrip_autotune_query.argtypes = [P, _I32P, I, _U8P, I, I, I, _I32P, C.POINTER(C.c_float)]
     lib.htrip_autotune_export.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
     lib.htrip_autotune_import.argtypes = [C.c_char_p]
@@ -489,6 +493,26 @@ class MinPlusOracle:
         b, o = C.c_uint64(), C.c_uint64()
         _check(self.lib.htrip_last_open_work(self.h, C.byref(b), C.byref(o)))
         return b.value, o.value
+
+    def setQueryWorkCounting(self, on: bool):
+        """Count the executed work of this index's query launches (a few atomics
+        per work unit; off by default)."""
+        _check(self.lib.htrip_set_query_work_counting(self.h, 1 if on else 0))
+
+    def lastQueryExecuted(self):
+        """(tile entries updated, operand rows streamed, rows skipped) of the
+        last counted query launch (htrip_last_query_executed)."""
+        e, r, s = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        _check(self.lib.htrip_last_query_executed(self.h, C.byref(e), C.byref(r), C.byref(s)))
+        return e.value, r.value, s.value
+
+    def lastOpenLevels(self):
+        """Per level of the last opening call: (matrices, sum of pivots, largest
+        pivot count, closure rounds) (htrip_last_open_levels)."""
+        buf = (C.c_int64 * (4 * 32))()
+        n = C.c_int32()
+        _check(self.lib.htrip_last_open_levels(self.h, buf, 32, C.byref(n)))
+        return [tuple(int(buf[4 * l + j]) for j in range(4)) for l in range(min(n.value, 32))]
 
     def lastQueryPhases(self):
         """Per-phase nanoseconds of the last query launch (htrip_last_query_phases)."""

@@ -346,6 +346,16 @@ htrip_status htrip_server_run_trace(htrip_server* s, const htrip_server_request*
 htrip_status htrip_query_work(const htrip_index* h, const int32_t* vps, int32_t k, const uint8_t* observed,
                               int32_t rows, int32_t cols, uint64_t* alg_bytes, uint64_t* alg_ops);
 htrip_status htrip_last_query_kernel_ms(const htrip_index* h, float* ms);
+
+/* Executed work of the query kernel (no reference counterpart; a
+ * measurement mode, off by default).  While counting is on, every query
+ * launch of the index that serves it alone counts, per operand row the
+ * kernel streamed, the tile entries it updated (rows x tile rows x tile
+ * columns), and the rows it skipped because the tile held no finite value:
+ * the work actually done, beside htrip_query_work's dense count.
+ * htrip_last_query_executed reads the counters of the last launch.       */
+htrip_status htrip_set_query_work_counting(htrip_index* h, int32_t on);
+htrip_status htrip_last_query_executed(htrip_index* h, uint64_t* entries, uint64_t* rows, uint64_t* skipped);
 htrip_status htrip_last_query_io(const htrip_index* h, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
 
 /* Register-only rate (entries/s) of the packed-u16 clamped min-plus update
@@ -375,6 +385,12 @@ htrip_status htrip_autotune_clear(void);
  * order n (b^2 or nV) closed over the pivot set K, n^2 |K| min-plus
  * operations and 2 n^2 2 + |K| n 2 2 bytes, summed over leaves and nodes.  */
 htrip_status htrip_last_open_work(const htrip_index* h, uint64_t* alg_bytes, uint64_t* alg_ops);
+
+/* Per level l = 0..H of the index's last opening call (no reference
+ * counterpart): out[4l] matrices updated, out[4l+1] the sum of their pivot
+ * counts, out[4l+2] the largest pivot count, out[4l+3] closure rounds of
+ * 64 pivots.  Writes min(max_levels, H + 1) levels; *n_levels = H + 1.     */
+htrip_status htrip_last_open_levels(const htrip_index* h, int64_t* out, int32_t max_levels, int32_t* n_levels);
 
 /* Phase trace of the last query launch of an index / a batch: ns[i] =
  * global-timer nanoseconds of phase i of the persistent query kernel
