@@ -2939,6 +2939,23 @@ static htrip_status arena_phases(const QueryArena& A, cudaStream_t st, uint64_t*
     HTRIP_GUARD_END
 }
 
+htrip_status htrip_last_open_trace(htrip_index* h, uint64_t* ns, int32_t max_n, int32_t* n) {
+    if (!h || (max_n > 0 && !ns)) return fail(HTRIP_ERR_INVALID, "bad arguments");
+    if (!h->u.trace_valid) return fail(HTRIP_ERR_INVALID, "no device-driven opening has run on this index");
+    HTRIP_GUARD_BEGIN
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    std::vector<unsigned long long> t(hb::kOpenTrace, 0);
+    ck(cudaMemcpyAsync(t.data(), h->u.dev.p + h->u.trace_off, t.size() * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, h->stream), "trace");
+    ck(cudaStreamSynchronize(h->stream), "sync");
+    int m = 0;  // phases stamped: stamps after t[0] that are set and not earlier than it
+    while (m + 1 < (int)t.size() && t[m + 1] >= t[0] && t[m + 1] != 0) ++m;
+    for (int i = 0; i < std::min(m, (int)max_n); ++i) ns[i] = t[i + 1] - t[i];
+    if (n) *n = m;
+    return HTRIP_OK;
+    HTRIP_GUARD_END
+}
+
 htrip_status htrip_set_query_work_counting(htrip_index* h, int32_t on) {
     if (!h) return fail(HTRIP_ERR_INVALID, "null handle");
     h->count_work = on != 0;

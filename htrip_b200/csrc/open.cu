@@ -49,7 +49,7 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int B = kOpenB;
 constexpr unsigned kBarrierPolls = 1u << 24;
-constexpr int kInsertChunk = 4096;  // child-summary entries per insert unit
+constexpr int kInsertChunk = 65536;  // child-summary entries per insert unit
 
 __device__ __forceinline__ unsigned long long global_timer() {
     unsigned long long t;

@@ -91,6 +91,7 @@ EXPORTS = (
     "htrip_leaves_changed", "htrip_selftest_barrier_timeout", "htrip_selftest_wait_timeout", "htrip_set_cell_weights",
     "htrip_cell_weight_changed", "htrip_tile_weights_changed", "htrip_server_wait_version",
     "htrip_last_open_levels", "htrip_set_query_work_counting", "htrip_last_query_executed",
+    "htrip_last_open_trace",
 )
 
 
@@ -142,6 +143,7 @@ def load_library(path: str | None = None):
     lib.htrip_last_open_work.argtypes = [P, _U64P, _U64P]
     lib.htrip_last_open_levels.argtypes = [P, C.POINTER(C.c_int64), I, _I32P]
     lib.htrip_set_query_work_counting.argtypes = [P, I]
+    lib.htrip_last_open_trace.argtypes = [P, _U64P, I, _I32P]
     lib.htrip_last_query_executed.argtypes = [P, _U64P, _U64P, _U64P]
     lib.htrip_autotune_query.argtypes = [P, _I32P, I, _U8P, I, I, I, _I32P, C.POINTER(C.c_float)]
     lib.htrip_autotune_export.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
@@ -505,6 +507,13 @@ class MinPlusOracle:
         e, r, s = C.c_uint64(), C.c_uint64(), C.c_uint64()
         _check(self.lib.htrip_last_query_executed(self.h, C.byref(e), C.byref(r), C.byref(s)))
         return e.value, r.value, s.value
+
+    def lastOpenTrace(self):
+        """Phase durations (ns) of the last device-driven opening launch."""
+        buf = (C.c_uint64 * 1024)()
+        n = C.c_int32()
+        _check(self.lib.htrip_last_open_trace(self.h, buf, 1024, C.byref(n)))
+        return [int(buf[i]) for i in range(min(n.value, 1024))]
 
     def lastOpenLevels(self):
         """Per level of the last opening call: (matrices, sum of pivots, largest

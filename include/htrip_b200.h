@@ -386,6 +386,13 @@ htrip_status htrip_autotune_clear(void);
  * operations and 2 n^2 2 + |K| n 2 2 bytes, summed over leaves and nodes.  */
 htrip_status htrip_last_open_work(const htrip_index* h, uint64_t* alg_bytes, uint64_t* alg_ops);
 
+/* Phase durations of the index's last device-driven opening launch (no
+ * reference counterpart): ns[i] = global-timer nanoseconds of phase i of the
+ * persistent opening kernel, in order: the seam-node stamping, then per level
+ * with work the insert and compact phases and each closure round's panel and
+ * update phases.  *n = phases recorded.                                    */
+htrip_status htrip_last_open_trace(htrip_index* h, uint64_t* ns, int32_t max_n, int32_t* n);
+
 /* Per level l = 0..H of the index's last opening call (no reference
  * counterpart): out[4l] matrices updated, out[4l+1] the sum of their pivot
  * counts, out[4l+2] the largest pivot count, out[4l+3] closure rounds of

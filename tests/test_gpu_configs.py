@@ -8,7 +8,8 @@
   calls of 256 cells in BFS-ring order from 16 radius-40 disks; after every
   call the index equals a fresh device build of the same grid (digest) and
   queryAllPairs over 16 robot poses + 48 frontier cells equals the rebuilt
-  index's answer; every 50th step the matrix is also checked against BFS.
+  index's answer; the reference's own index runs the same stream, and every
+  50th step its whole state, stats and answers (and BFS's) are compared.
 * The same stream on a 256x256 grid checked against the reference's own
   incremental index after every call (digest, stats and query).
 """
@@ -65,15 +66,18 @@ def _step_viewpoints(obs, starts, step):
 
 
 def test_incremental_1024_b8_every_step_equals_rebuild(gpu):
+    """Every step against a device rebuild; the reference's own incremental
+    index runs the same stream beside it, and every 50th step its state,
+    stats and query answers are compared too (with BFS)."""
     truth = W.street_grid(1024, 3)
     obs, starts, batches = W.exploration_stream(truth, 16, 40, 256, 400, 3)
     assert len(batches) == 400
-    dev = _dev(8)
-    assert dev.build(obs)
-    bfs = RefOracle(8)
+    ref, dev = _both(obs, 8)
     for step, cells in enumerate(batches):
         obs[cells[:, 0], cells[:, 1]] = W.FREE
         dev.onBatchCellsOpened(cells, obs)
+        ref.set_cells(cells, W.FREE)
+        ref.open_batch(cells)
         fresh = _dev(8)
         assert fresh.build(obs)
         assert dev.stateDigest() == fresh.stateDigest(), f"index differs from a rebuild after step {step}"
@@ -81,8 +85,11 @@ def test_incremental_1024_b8_every_step_equals_rebuild(gpu):
         got = dev.queryAllPairs(vps, obs)
         np.testing.assert_array_equal(got, fresh.queryAllPairs(vps, obs), err_msg=f"step {step}")
         if step % 50 == 49:
-            bfs.set_grid(obs)
-            np.testing.assert_array_equal(got, bfs.bfs(vps), err_msg=f"BFS step {step}")
+            st = dev.last_batch_stats
+            assert (st.n_touched_leaves, st.n_dirty_ancestors, st.n_pivots) == ref.stats(), f"stats step {step}"
+            assert dev.stateDigest() == ref.digest(), f"index differs from the reference after step {step}"
+            np.testing.assert_array_equal(got, ref.query(vps), err_msg=f"reference step {step}")
+            np.testing.assert_array_equal(got, ref.bfs(vps), err_msg=f"BFS step {step}")
         del fresh
 
 
