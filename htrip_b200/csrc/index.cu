@@ -131,6 +131,31 @@ struct Level {
 
 inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
+// Cooperative launches (the query kernel, the opening kernel) of one device
+// run one after another on the GPU, whatever stream issued them: each waits
+// for an event recorded after the previous one.  Each such grid takes every
+// SM, so running two at once gains nothing, and ordering them keeps two
+// grids that wait on their own CTAs from holding parts of the GPU at once.
+// The host only takes a short lock; nothing waits on the host.
+constexpr int kCoopMaxDevices = 64;
+struct CoopChain {
+    std::mutex mu;
+    cudaEvent_t ev = nullptr;
+    cudaStream_t st = nullptr;
+};
+CoopChain g_coop[kCoopMaxDevices];
+
+template <class F>
+void coop_launch(int device, cudaStream_t st, F&& launch, const char* what) {
+    CoopChain& c = g_coop[std::clamp(device, 0, kCoopMaxDevices - 1)];
+    std::lock_guard<std::mutex> lk(c.mu);
+    if (c.ev && c.st != st) ck(cudaStreamWaitEvent(st, c.ev, 0), "cooperative launch order");
+    if (!c.ev) ck(cudaEventCreateWithFlags(&c.ev, cudaEventDisableTiming), "event");
+    ck(launch(), what);
+    ck(cudaEventRecord(c.ev, st), "cooperative launch order");
+    c.st = st;
+}
+
 // Pinned host buffer (grows, never shrinks).
 struct HostBuf {
     unsigned char* p = nullptr;
@@ -1125,8 +1150,8 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
         int maxH = 0;
         int cap[hb::kOpenMaxLevels] = {}, n_seam[hb::kOpenMaxLevels] = {};
         size_t o_tasks = 0, o_out = 0, o_words = 0, o_trace = 0, o_slots[hb::kOpenMaxLevels] = {}, o_trip = 0;
+        size_t o_dchild[hb::kOpenMaxLevels] = {};
         size_t begin = 0, end = 0;
-        size_t panel = 0, pflags = 0;
         int n_trip = 0;
     };
     std::vector<GL> gl;
@@ -1182,9 +1207,10 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
         g.begin = off;
         g.o_tasks = take(g.ts.size() * sizeof(hb::OpenTask));
         g.o_out = take(g.ts.size() * sizeof(hb::OpenTaskOut));
-        g.o_words = take((2 * hb::kOpenMaxLevels + 4) * sizeof(int));
+        g.o_words = take((3 * hb::kOpenMaxLevels + 4) * sizeof(int));
         g.o_trace = take(hb::kOpenTrace * sizeof(unsigned long long));
         for (int l = 0; l <= g.maxH; ++l) g.o_slots[l] = take((size_t)std::max(1, g.cap[l]) * sizeof(int4));
+        for (int l = 1; l <= g.maxH; ++l) g.o_dchild[l] = take((size_t)std::max(1, g.cap[l - 1]) * sizeof(int4));
         g.o_trip = take((size_t)g.n_trip * 3 * sizeof(int));
         g.end = off;
         gl.push_back(std::move(g));
@@ -1201,11 +1227,9 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
         std::memset(hs + g.begin, 0, g.end - g.begin);
         auto* hT = reinterpret_cast<hb::OpenTask*>(hs + g.o_tasks);
         auto* hO = reinterpret_cast<hb::OpenTaskOut*>(hs + g.o_out);
-        int* words = reinterpret_cast<int*>(hs + g.o_words);  // count[17] maxk[17] status bar[3]
+        int* words = reinterpret_cast<int*>(hs + g.o_words);  // count[17] maxk[17] dcount[17] status bar[3]
         int* trip = reinterpret_cast<int*>(hs + g.o_trip);
         int nt = 0;
-        std::vector<int> fill(g.maxH + 1, 0);
-        for (int l = 1; l <= g.maxH; ++l) fill[l] = 0;
         for (size_t t = 0; t < g.ts.size(); ++t) {
             OpenTask* T = g.ts[t];
             htrip_index* h = T->h;
@@ -1274,19 +1298,21 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
             OL.geo[l].child_ext = l >= 1 ? hl->L[l - 1].d_ext.p : nullptr;
             OL.geo[l].childNP = l >= 1 ? hl->L[l - 1].NP : 0;
             OL.slots[l] = reinterpret_cast<int4*>(base + g.o_slots[l]);
+            OL.dchild[l] = l >= 1 ? reinterpret_cast<int4*>(base + g.o_dchild[l]) : nullptr;
             OL.cap[l] = g.cap[l];
             OL.n_seam[l] = l >= 1 ? words[l] : 0;
         }
         OL.count = reinterpret_cast<int*>(base + g.o_words);
         OL.maxk = OL.count + hb::kOpenMaxLevels;
-        OL.status = OL.count + 2 * hb::kOpenMaxLevels;
+        OL.dcount = OL.count + 2 * hb::kOpenMaxLevels;
+        OL.status = OL.count + 3 * hb::kOpenMaxLevels;
         OL.bar = reinterpret_cast<unsigned*>(OL.status + 1);
         OL.triples = reinterpret_cast<const int*>(base + g.o_trip);
         OL.panel = A.panel.p;
         OL.pflags = A.pflags.p;
         OL.trace = reinterpret_cast<unsigned long long*>(base + g.o_trace);
         ck(cudaMemcpyAsync(base + g.begin, hs + g.begin, g.end - g.begin, cudaMemcpyHostToDevice, st), "open upload");
-        ck(hb::launch_open(OL, A.open_grid, st), "opening kernel");
+        coop_launch(device, st, [&] { return hb::launch_open(OL, A.open_grid, st); }, "opening kernel");
         // statistics and the status word back (the trace stays on the device)
         ck(cudaMemcpyAsync(A.rb.p + g.o_out, base + g.o_out, g.o_trace - g.o_out, cudaMemcpyDeviceToHost, st),
            "open results");
@@ -1296,7 +1322,7 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
     ck(cudaStreamSynchronize(st), "opening");
     for (GL& g : gl) {
         const int* words = reinterpret_cast<const int*>(A.rb.p + g.o_words);
-        const int status = words[2 * hb::kOpenMaxLevels];
+        const int status = words[3 * hb::kOpenMaxLevels];
         if (status != 0)
             throw CudaError{cudaErrorLaunchFailure, status == 1 ? "opening kernel: a bounded barrier wait timed out"
                                                                 : "opening kernel: a work list overflowed"};
@@ -1765,8 +1791,14 @@ void issue_query_launch(cudaStream_t st, int device, int& grid, int cfg, const s
     QL.bar = reinterpret_cast<unsigned*>(base + L.o_words) + 1;
     QL.trace = reinterpret_cast<unsigned long long*>(base + L.o_words + kTraceOffset);
     QL.dataflow = query_dataflow_mode();
-    if (ev) ck(cudaEventRecord(ev[0], st), "event");
-    ck(hb::launch_query(QL, cfg, grid, st), "query kernel");
+    // the start event after any wait for another stream's cooperative kernel
+    coop_launch(device, st, [&] {
+        if (ev) {
+            const cudaError_t e = cudaEventRecord(ev[0], st);
+            if (e != cudaSuccess) return e;
+        }
+        return hb::launch_query(QL, cfg, grid, st);
+    }, "query kernel");
     if (ev) ck(cudaEventRecord(ev[1], st), "event");
 }
 
@@ -2166,8 +2198,10 @@ int run_devplan(htrip_index* h, int k, int cfg, const int32_t* vps_host, const u
     QL.bar = reinterpret_cast<unsigned*>(base + D.o_words) + 1;
     QL.trace = reinterpret_cast<unsigned long long*>(base + D.o_words + kTraceOffset);
     QL.dataflow = query_dataflow_mode();
-    ck(cudaEventRecord(A.ev[0], st), "event");
-    ck(hb::launch_query(QL, cfg, A.grid, st), "query kernel");
+    coop_launch(h->device, st, [&] {
+        const cudaError_t e = cudaEventRecord(A.ev[0], st);
+        return e != cudaSuccess ? e : hb::launch_query(QL, cfg, A.grid, st);
+    }, "query kernel");
     ck(cudaEventRecord(A.ev[1], st), "event");
     A.ev_valid = true;
     A.last_words = D.o_words;

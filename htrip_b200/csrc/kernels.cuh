@@ -152,6 +152,9 @@ struct OpenLaunch {
     OpenLevelGeom geo[kOpenMaxLevels];
     int4* slots[kOpenMaxLevels];   // per level; levels >= 1 start with the seam nodes
     int* count;                    // [kOpenMaxLevels] listed slots per level (grows during the call)
+    int4* dchild[kOpenMaxLevels];  // levels >= 1: {task, child, node, quad} of every child whose
+                                   // summary decreased (capacity: the child level's cap)
+    int* dcount;                   // [kOpenMaxLevels] entries of dchild
     int cap[kOpenMaxLevels];       // capacity of each level's list
     int n_seam[kOpenMaxLevels];    // seam nodes at the head of each level's list (stamped first)
     int* maxk;                     // [kOpenMaxLevels] largest pivot count per level

@@ -49,12 +49,20 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int B = kOpenB;
 constexpr unsigned kBarrierPolls = 1u << 24;
-constexpr int kInsertChunk = 65536;  // child-summary entries per insert unit
+constexpr int kInsertChunk = 16384;  // child-summary entries per insert unit
 
 __device__ __forceinline__ unsigned long long global_timer() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
 // Grid barrier over every CTA of the launch; the last CTA to arrive resets
@@ -117,6 +125,15 @@ __device__ void mark_dec(const OpenLaunch& L, int l, int task, int node) {
     if (atomicExch(T.lv[l].dstamp + node, T.stamp) == T.stamp) return;
     const int nx = T.lv[l].nodes_x, g = T.g;
     const int p = ((node / nx) / g) * T.lv[l + 1].nodes_x + (node % nx) / g;
+    const int q = ((node / nx) % g) * g + (node % nx) % g;
+    {   // the parent's insert phase scans this child's summary
+        const int di = atomicAdd(L.dcount + l + 1, 1);
+        if (di >= L.cap[l]) {
+            atomicCAS(L.status, 0, 2);
+            return;
+        }
+        L.dchild[l + 1][di] = make_int4(task, node, p, q);
+    }
     if (atomicExch(T.lv[l + 1].mstamp + p, T.stamp) == T.stamp) return;
     const int idx = atomicAdd(L.count + l + 1, 1);
     if (idx >= L.cap[l + 1]) {
@@ -144,92 +161,118 @@ __device__ void stamp_phase(const OpenLaunch& L) {
 // ---------------------------------------------------------------------------
 // Insert phase.
 // ---------------------------------------------------------------------------
-// Serial edge / seam list of one slot (leaf_tile.cpp:311-330,
-// internal_node.cpp:356-365): an entry counts, and its endpoints become
-// pivots, only if it shortens D[u][v].  Run by one thread.
+// Edge / seam list of one slot (leaf_tile.cpp:311-330,
+// internal_node.cpp:356-365), one warp: an entry counts, and its endpoints
+// become pivots, only if it shortens D[u][v].  The lanes take the entries in
+// parallel: a pair listed twice (both cells opened) has the same weight, so
+// the set of shortened pairs, and the pivots, are those of the sequential
+// loop; a pivot flag counts once (atomicOr on its 4-byte word).
 __device__ void insert_list(const OpenLaunch& L, int l, int4 e, int* new_pivots, bool* dec) {
     const OpenTask& T = L.tasks[e.x];
     const OpenLevelGeom& G = L.geo[l];
-    const int NP = G.NP;
+    const int NP = G.NP, lane = threadIdx.x & 31;
     uint16_t* D = node_mat(T.lv[l], e.y, NP);
     uint8_t* f = T.lv[l].kflag + (size_t)e.y * NP;
     int np = 0;
     bool d = false;
-    for (int t = e.z; t < e.w; ++t) {
+    for (int t = e.z + lane; t < e.w; t += 32) {
         const int u = L.triples[3 * t], v = L.triples[3 * t + 1];
         const uint16_t w = (uint16_t)L.triples[3 * t + 2];
         if (w < D[(size_t)u * NP + v]) {
             D[(size_t)u * NP + v] = w;
             D[(size_t)v * NP + u] = w;
-            if (!f[u]) { f[u] = 1; ++np; }
-            if (!f[v]) { f[v] = 1; ++np; }
+            const int ends[2] = {u, v};
+#pragma unroll
+            for (int x = 0; x < 2; ++x) {
+                const int a = ends[x];
+                const unsigned sh = (unsigned)(a & 3) * 8u;
+                const unsigned old = atomicOr(reinterpret_cast<unsigned*>(f + (a & ~3)), 1u << sh);
+                np += ((old >> sh) & 0xffu) == 0;
+            }
             d |= G.isext[u] && G.isext[v];
         }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) np += __shfl_xor_sync(FULL, np, o);
     *new_pivots = np;
-    *dec = d;
+    *dec = __any_sync(FULL, d);
 }
 
+// Insert phase of level l.  Units: the slots' edge / seam lists (one warp
+// per slot), then, for levels >= 1, every child whose summary decreased in
+// this call (listed by mark_dec) in chunks of kInsertChunk entries of its
+// nP x nP summary: every summary entry smaller than the node's entry is
+// inserted (internal_node.cpp:343-353) - the same as inserting the
+// reference's decrease list, since an entry that did not decrease is never
+// smaller than the node's, which is <= the old summary.
 __device__ void insert_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
     const OpenLevelGeom& G = L.geo[l];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     __shared__ int s_dec;
-    const int list_units = (N + kWarps - 1) / kWarps;  // one slot per warp (lane 0)
-    const int g2 = L.g * L.g;
+    const int list_units = (N + kWarps - 1) / kWarps;
+    const int nd = l >= 1 ? min(*(volatile int*)(L.dcount + l), L.cap[l - 1]) : 0;
     const int chunks = l >= 1 ? (G.nP * G.nP + kInsertChunk - 1) / kInsertChunk : 0;
-    const int child_units = l >= 1 ? N * g2 * chunks : 0;
-    const int units = list_units + child_units;
+    const int units = list_units + nd * chunks;
     for (int u = next_unit(L, s_unit); u < units; u = next_unit(L, s_unit)) {
         if (u < list_units) {
             const int s = u * kWarps + warp;
-            if (s < N && lane == 0) {
+            if (s < N) {
                 const int4 e = L.slots[l][s];
-                if (e.w > e.z) {
+                if (e.w > e.z) {  // uniform over the warp
                     int np = 0;
                     bool dec = false;
                     insert_list(L, l, e, &np, &dec);
-                    const OpenTask& T = L.tasks[e.x];
-                    if (l == 0 && np) atomicAdd(&T.out->new_pivots, np);
-                    if (dec) mark_dec(L, l, e.x, e.y);
+                    if (lane == 0) {
+                        const OpenTask& T = L.tasks[e.x];
+                        if (l == 0 && np) atomicAdd(&T.out->new_pivots, np);
+                        if (dec) mark_dec(L, l, e.x, e.y);
+                    }
                 }
             }
             continue;
         }
-        // child-summary decreases (internal_node.cpp:343-353): inserting every
-        // child summary entry smaller than the node's is the same as inserting
-        // the reference's decrease list (an entry that did not decrease is
-        // never smaller than the node's, which is <= the old summary)
         const int cu = u - list_units;
-        const int s = cu / (g2 * chunks);
-        const int q = (cu / chunks) % g2;
+        const int4 dc = L.dchild[l][cu / chunks];  // {task, child, node, quad}
         const int c = cu % chunks;
-        const int4 e = L.slots[l][s];
-        const OpenTask& T = L.tasks[e.x];
-        const int nx = T.lv[l].nodes_x, g = L.g;
-        const int child = ((e.y / nx) * g + q / g) * T.lv[l - 1].nodes_x + ((e.y % nx) * g + q % g);
-        if (T.lv[l - 1].dstamp[child] != T.stamp) continue;  // uniform over the CTA
+        const OpenTask& T = L.tasks[dc.x];
         if (threadIdx.x == 0) s_dec = 0;
         __syncthreads();
-        const int NP = G.NP, nP = G.nP, cNP = G.childNP;
-        const uint16_t* cm = node_mat(T.lv[l - 1], child, cNP);
-        uint16_t* D = node_mat(T.lv[l], e.y, NP);
-        uint8_t* f = T.lv[l].kflag + (size_t)e.y * NP;
-        const int i1 = min(nP * nP, (c + 1) * kInsertChunk);
+        const int NP = G.NP, nP = G.nP, cNP = G.childNP, q = dc.w;
+        const uint16_t* cm = node_mat(T.lv[l - 1], dc.y, cNP);
+        uint16_t* D = node_mat(T.lv[l], dc.z, NP);
+        uint8_t* f = T.lv[l].kflag + (size_t)dc.z * NP;
+        const int i0 = c * kInsertChunk, i1 = min(nP * nP, i0 + kInsertChunk);
         bool dec = false;
-        for (int idx = c * kInsertChunk + threadIdx.x; idx < i1; idx += kThreads) {
-            const int p = idx / nP, pp = idx - p * nP;
-            const uint16_t w = cm[(size_t)G.child_ext[p] * cNP + G.child_ext[pp]];
-            const int a = q * nP + p, b = q * nP + pp;
-            if (w < D[(size_t)a * NP + b]) {
-                D[(size_t)a * NP + b] = w;  // (b, a) is written by its own thread
-                f[a] = 1;
-                f[b] = 1;
-                dec |= G.isext[a] && G.isext[b];
+        // batches of 4 entries per thread: all loads first, then the updates
+        constexpr int U = 4;
+        for (int b0 = i0 + threadIdx.x; b0 < i1; b0 += U * kThreads) {
+            uint16_t w[U], d[U];
+            int a[U], bb[U];
+#pragma unroll
+            for (int x = 0; x < U; ++x) {
+                const int idx = b0 + x * kThreads;
+                a[x] = -1;
+                if (idx < i1) {
+                    const int p = idx / nP, pp = idx - p * nP;
+                    a[x] = q * nP + p;
+                    bb[x] = q * nP + pp;
+                    w[x] = cm[(size_t)G.child_ext[p] * cNP + G.child_ext[pp]];
+                    d[x] = D[(size_t)a[x] * NP + bb[x]];
+                }
+            }
+#pragma unroll
+            for (int x = 0; x < U; ++x) {
+                if (a[x] >= 0 && w[x] < d[x]) {
+                    D[(size_t)a[x] * NP + bb[x]] = w[x];  // (b, a) is written by its own thread
+                    f[a[x]] = 1;
+                    f[bb[x]] = 1;
+                    dec |= G.isext[a[x]] && G.isext[bb[x]];
+                }
             }
         }
         if (__any_sync(FULL, dec) && lane == 0) s_dec = 1;
         __syncthreads();
-        if (threadIdx.x == 0 && s_dec) mark_dec(L, l, e.x, e.y);
+        if (threadIdx.x == 0 && s_dec) mark_dec(L, l, dc.x, dc.z);
     }
 }
 
@@ -250,17 +293,28 @@ __device__ void compact_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
         int* out = T.lv[l].klist + (size_t)e.y * G.NP;
         if (threadIdx.x == 0) base = 0;
         __syncthreads();
-        for (int j0 = 0; j0 < G.NP; j0 += kThreads) {
-            const int j = j0 + threadIdx.x;
-            const bool on = j < G.NP && f[j];
-            const unsigned bal = __ballot_sync(FULL, on);
-            if (lane == 0) warp_tot[warp] = __popc(bal);
+        // each thread takes 4 consecutive flags (one 32-bit word) per step
+        for (int j0 = 0; j0 < G.NP; j0 += 4 * kThreads) {
+            const int j = j0 + 4 * threadIdx.x;
+            unsigned wv = 0;
+            if (j < G.NP) wv = *reinterpret_cast<const unsigned*>(f + j);
+            const int cnt = (wv & 0xffu ? 1 : 0) + (wv & 0xff00u ? 1 : 0) + (wv & 0xff0000u ? 1 : 0) +
+                            (wv & 0xff000000u ? 1 : 0);
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += v;
+            }
+            if (lane == 31) warp_tot[warp] = incl;
             __syncthreads();
-            int off = base;
+            int off = base + incl - cnt;
             for (int w = 0; w < warp; ++w) off += warp_tot[w];
-            if (on) {
-                out[off + __popc(bal & ((1u << lane) - 1u))] = j;
-                f[j] = 0;
+            if (wv) {
+#pragma unroll
+                for (int x = 0; x < 4; ++x)
+                    if ((wv >> (8 * x)) & 0xffu) out[off++] = j + x;
+                *reinterpret_cast<unsigned*>(f + j) = 0u;
             }
             __syncthreads();
             if (threadIdx.x == 0)
@@ -312,13 +366,25 @@ __device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, uns
     if (tid < mk) kc[tid] = T.lv[l].klist[(size_t)e.y * NP + r * B + tid];
     if (tid < 4) tile_any[tid] = 0;
     __syncthreads();
-    for (int idx = tid; idx < B * B; idx += kThreads) {
-        const int a = idx / B, c = idx % B;
-        Ts[a][c] = (a < mk && c < mk) ? D[(size_t)kc[a] * NP + kc[c]] : (a == c ? 0 : INF);
-    }
-    for (int idx = tid; idx < mk * (NT / 8); idx += kThreads) {
-        const int a = idx / (NT / 8), c8 = idx % (NT / 8);
-        reinterpret_cast<uint4*>(Bs + a * NT)[c8] = reinterpret_cast<const uint4*>(D + (size_t)kc[a] * NP + j0)[c8];
+    {   // the tile's pivot rows by asynchronous copies, meanwhile the pivot
+        // block (scattered entries) with all of a thread's loads issued first
+        for (int idx = tid; idx < mk * (NT / 8); idx += kThreads) {
+            const int a = idx / (NT / 8), c8 = idx % (NT / 8);
+            cp_async16(Bs + a * NT + c8 * 8, D + (size_t)kc[a] * NP + j0 + c8 * 8);
+        }
+        constexpr int NTB = B * B / kThreads;
+        uint16_t tv[NTB];
+#pragma unroll
+        for (int x = 0; x < NTB; ++x) {
+            const int idx = tid + x * kThreads, a = idx / B, c = idx % B;
+            tv[x] = (a < mk && c < mk) ? D[(size_t)kc[a] * NP + kc[c]] : (a == c ? 0 : INF);
+        }
+#pragma unroll
+        for (int x = 0; x < NTB; ++x) {
+            const int idx = tid + x * kThreads;
+            Ts[idx / B][idx % B] = tv[x];
+        }
+        cp_async_wait_all();
     }
     __syncthreads();
     {   // Floyd-Warshall over the pivot block: thread t owns row t / 4, 16 columns
@@ -441,20 +507,42 @@ __device__ void update_unit(const OpenLaunch& L, int l, int s, int I, int J, int
     uint32_t* As = reinterpret_cast<uint32_t*>(smem);                                  // [B][TT] splatted
     uint16_t* Bs = reinterpret_cast<uint16_t*>(smem + (size_t)B * TT * sizeof(uint32_t));  // [B][TT]
     uint8_t* cls = smem + (size_t)B * TT * (sizeof(uint32_t) + sizeof(uint16_t));          // [B][kWarps]
+    uint16_t* Os = reinterpret_cast<uint16_t*>(cls + B * kWarps);                          // [TT][TT] old tile
     __shared__ int s_any, s_dec;
     const uint16_t* P = L.panel + (size_t)s * B * NP;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int i0 = I * TT, jb = J * TT;
     if (tid == 0) { s_any = 0; s_dec = 0; }
-    for (int idx = tid; idx < mk * (TT / 8); idx += kThreads) {
-        const int a = idx / (TT / 8), c8 = idx % (TT / 8);
-        const uint4 va = reinterpret_cast<const uint4*>(P + (size_t)a * NP + i0)[c8];
-        const uint4 vb = reinterpret_cast<const uint4*>(P + (size_t)a * NP + jb)[c8];
-        reinterpret_cast<uint4*>(Bs + a * TT)[c8] = vb;
-        const uint32_t w[4] = {va.x, va.y, va.z, va.w};
-        uint4* dst = reinterpret_cast<uint4*>(As + a * TT + c8 * 8);
-        dst[0] = make_uint4(splat(w[0]), splat(w[0] >> 16), splat(w[1]), splat(w[1] >> 16));
-        dst[1] = make_uint4(splat(w[2]), splat(w[2] >> 16), splat(w[3]), splat(w[3] >> 16));
+    uint16_t* D = node_mat(T.lv[l], e.y, NP);
+    {   // asynchronous copies of the column panel and of the old tile (read
+        // only in the epilogue); the row panel is splatted through registers
+        for (int idx = tid; idx < mk * (TT / 8); idx += kThreads) {
+            const int a = idx / (TT / 8), c8 = idx % (TT / 8);
+            cp_async16(Bs + a * TT + c8 * 8, P + (size_t)a * NP + jb + c8 * 8);
+        }
+        for (int idx = tid; idx < TT * (TT / 8); idx += kThreads) {
+            const int rr = idx / (TT / 8), c8 = idx % (TT / 8);
+            cp_async16(Os + rr * TT + c8 * 8, D + (size_t)(i0 + rr) * NP + jb + c8 * 8);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        constexpr int NS = B * (TT / 8) / kThreads;
+        uint4 va[NS];
+#pragma unroll
+        for (int x = 0; x < NS; ++x) {
+            const int idx = tid + x * kThreads, a = idx / (TT / 8), c8 = idx % (TT / 8);
+            if (a < mk) va[x] = reinterpret_cast<const uint4*>(P + (size_t)a * NP + i0)[c8];
+        }
+#pragma unroll
+        for (int x = 0; x < NS; ++x) {
+            const int idx = tid + x * kThreads, a = idx / (TT / 8), c8 = idx % (TT / 8);
+            if (a < mk) {
+                const uint32_t w[4] = {va[x].x, va[x].y, va[x].z, va[x].w};
+                uint4* dst = reinterpret_cast<uint4*>(As + a * TT + c8 * 8);
+                dst[0] = make_uint4(splat(w[0]), splat(w[0] >> 16), splat(w[1]), splat(w[1] >> 16));
+                dst[1] = make_uint4(splat(w[2]), splat(w[2] >> 16), splat(w[3]), splat(w[3] >> 16));
+            }
+        }
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     }
     __syncthreads();
     for (int idx = tid; idx < mk * kWarps; idx += kThreads) {
@@ -503,7 +591,6 @@ __device__ void update_unit(const OpenLaunch& L, int l, int s, int I, int J, int
         }
     }
     // epilogue: new = min(acc, old); changed entries are written
-    uint16_t* D = node_mat(T.lv[l], e.y, NP);
     const int col = jb + lane * 2 * CP;
     uint32_t cext[CP];
 #pragma unroll
@@ -515,9 +602,7 @@ __device__ void update_unit(const OpenLaunch& L, int l, int s, int I, int J, int
         const int row = i0 + warp * RW + rr;
         uint32_t* dp = reinterpret_cast<uint32_t*>(D + (size_t)row * NP + col);
         const bool rext = G.isext[row] != 0;
-        uint32_t old[CP];
-#pragma unroll
-        for (int cc = 0; cc < CP; ++cc) old[cc] = dp[cc];
+        const uint32_t* old = reinterpret_cast<const uint32_t*>(Os + (warp * RW + rr) * TT + lane * 2 * CP);
         uint32_t ch = 0;
 #pragma unroll
         for (int cc = 0; cc < CP; ++cc) {
@@ -591,7 +676,8 @@ __device__ void update_phase(const OpenLaunch& L, int l, int N, int r, int* s_un
 }
 
 constexpr size_t kPanelSmem = (size_t)B * kTLD * sizeof(uint16_t) + (size_t)B * 256 * sizeof(uint16_t) + B * sizeof(int);
-constexpr size_t kUpdateSmem = (size_t)B * 128 * (sizeof(uint32_t) + sizeof(uint16_t)) + (size_t)B * kWarps;
+constexpr size_t kUpdateSmem = (size_t)B * 128 * (sizeof(uint32_t) + sizeof(uint16_t)) + (size_t)B * kWarps +
+                               (size_t)128 * 128 * sizeof(uint16_t);
 constexpr size_t kTransposeSmem = (size_t)128 * (128 + 8) * sizeof(uint16_t);
 constexpr size_t kOpenSmem = std::max(kPanelSmem, std::max(kUpdateSmem, kTransposeSmem));
 
