@@ -651,9 +651,17 @@ def bench_served(device, server_rates=(1000.0, 2000.0, 5000.0, 10000.0, 20000.0,
         srv = Server(device=device, plain=plain, double_buffer=double)
         sids = [srv.add_session(HierarchyConfig(b, 2, 2), obs) for _, obs, _, b in pl]
         reqs, arrival = trace
-        # warm-up: queries only (the sessions' maps stay as the trace expects),
-        # so the server's scratch arenas reach their working size untimed
+        # warm-up, untimed, so that every scratch arena (the server's and each
+        # session's own) reaches its working size before the trace: queries,
+        # and per session one opening of 512 cells that are already Free
+        # (spread over its map), which lowers no distance and so leaves every
+        # index as the trace expects
         wq = [(s, 0, rc) for s, k, rc in W.served_trace([(t, c[:0]) for t, _, c, _ in pl], 400, 2000.0, 99)[0]]
+        rng = np.random.default_rng(98)
+        for i, (_, obs, _, _) in enumerate(pl):
+            free = np.argwhere(obs == W.FREE).astype(np.int32)
+            if len(free):
+                wq.append((i, 1, free[rng.choice(len(free), size=min(512, len(free)), replace=False)]))
         srv.run_trace([(sids[s], k, rc) for s, k, rc in wq], np.zeros(len(wq)))
         outs, lat, wall = srv.run_trace([(sids[s], k, rc) for s, k, rc in reqs], arrival)
         st = srv.stats()

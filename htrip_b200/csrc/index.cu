@@ -1122,14 +1122,14 @@ void run_open_tasks(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t 
         if (T->record_stats) T->h->stats.n_dirty_ancestors = T->n_dirty;
 }
 
-// Which opening path runs: the device-driven one (HTRIP_OPEN_PATH=device: one
-// persistent launch per call, the level loop and the closure rounds on the
-// device) or the host-driven one (default: per level an insert and a close
+// Which opening path runs: the device-driven one (default: one persistent
+// launch per call, the level loop and the closure rounds on the device) or
+// the host-driven one (HTRIP_OPEN_PATH=host: per level an insert and a close
 // stage, with the pivot counts and the decrease flags read back to the host).
 bool open_on_device() {
     static const bool dev = [] {
         const char* e = std::getenv("HTRIP_OPEN_PATH");
-        return e && std::strcmp(e, "device") == 0;
+        return !(e && std::strcmp(e, "host") == 0);
     }();
     return dev;
 }
@@ -1150,7 +1150,7 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
         int maxH = 0;
         int cap[hb::kOpenMaxLevels] = {}, n_seam[hb::kOpenMaxLevels] = {};
         size_t o_tasks = 0, o_out = 0, o_words = 0, o_trace = 0, o_slots[hb::kOpenMaxLevels] = {}, o_trip = 0;
-        size_t o_dchild[hb::kOpenMaxLevels] = {};
+        size_t o_dchild[hb::kOpenMaxLevels] = {}, o_rec[hb::kOpenMaxLevels] = {}, o_pdone = 0;
         size_t begin = 0, end = 0;
         int n_trip = 0;
     };
@@ -1194,15 +1194,16 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
                 cur = std::move(next);
             }
         }
-        const htrip_index* h0 = g.ts[0]->h;
+        size_t pdone_words = 1;
         for (int l = 0; l <= g.maxH; ++l) {
-            const int NP = l <= h0->H ? h0->L[l].NP : 0;
-            // levels above the first task's depth share its (b, g) geometry; take it from the deepest task
-            int np = NP;
+            // every task of the group that reaches level l has the same (b, g)
+            // geometry there: take it from any of them
+            int np = 64;
             for (OpenTask* T : g.ts)
                 if (T->h->H >= l) np = T->h->L[l].NP;
             panel_elems = std::max(panel_elems, (size_t)g.cap[l] * hb::kOpenB * np);
             pflag_bytes = std::max(pflag_bytes, (size_t)g.cap[l] * (np / 64));
+            pdone_words = std::max(pdone_words, (size_t)g.cap[l] * (np / 64));
         }
         g.begin = off;
         g.o_tasks = take(g.ts.size() * sizeof(hb::OpenTask));
@@ -1211,6 +1212,8 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
         g.o_trace = take(hb::kOpenTrace * sizeof(unsigned long long));
         for (int l = 0; l <= g.maxH; ++l) g.o_slots[l] = take((size_t)std::max(1, g.cap[l]) * sizeof(int4));
         for (int l = 1; l <= g.maxH; ++l) g.o_dchild[l] = take((size_t)std::max(1, g.cap[l - 1]) * sizeof(int4));
+        for (int l = 0; l <= g.maxH; ++l) g.o_rec[l] = take((size_t)std::max(1, g.cap[l]) * sizeof(hb::OpenSlotRec));
+        g.o_pdone = take(pdone_words * sizeof(unsigned));  // zero at launch (the staging is cleared)
         g.o_trip = take((size_t)g.n_trip * 3 * sizeof(int));
         g.end = off;
         gl.push_back(std::move(g));
@@ -1299,6 +1302,7 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
             OL.geo[l].childNP = l >= 1 ? hl->L[l - 1].NP : 0;
             OL.slots[l] = reinterpret_cast<int4*>(base + g.o_slots[l]);
             OL.dchild[l] = l >= 1 ? reinterpret_cast<int4*>(base + g.o_dchild[l]) : nullptr;
+            OL.rec[l] = reinterpret_cast<hb::OpenSlotRec*>(base + g.o_rec[l]);
             OL.cap[l] = g.cap[l];
             OL.n_seam[l] = l >= 1 ? words[l] : 0;
         }
@@ -1311,6 +1315,7 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
         OL.panel = A.panel.p;
         OL.pflags = A.pflags.p;
         OL.trace = reinterpret_cast<unsigned long long*>(base + g.o_trace);
+        OL.pdone = reinterpret_cast<unsigned*>(base + g.o_pdone);
         ck(cudaMemcpyAsync(base + g.begin, hs + g.begin, g.end - g.begin, cudaMemcpyHostToDevice, st), "open upload");
         coop_launch(device, st, [&] { return hb::launch_open(OL, A.open_grid, st); }, "opening kernel");
         // statistics and the status word back (the trace stays on the device)

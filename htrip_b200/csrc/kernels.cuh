@@ -144,6 +144,14 @@ struct OpenTask {
     OpenTaskLevel lv[kOpenMaxLevels];
 };
 
+// What the closure phases of a slot need, in one record written by the slot's
+// compaction: its matrix, its pivot list and count, its task and node.
+struct OpenSlotRec {
+    uint16_t* mat;
+    const int* klist;
+    int kcnt, task, node, pad;
+};
+
 // Work list entry: {task, node, list_begin, list_end}; the list is the slot's
 // range of (u, v, w) triples (level 0: opened in-leaf edges; above: seams).
 struct OpenLaunch {
@@ -155,6 +163,9 @@ struct OpenLaunch {
     int4* dchild[kOpenMaxLevels];  // levels >= 1: {task, child, node, quad} of every child whose
                                    // summary decreased (capacity: the child level's cap)
     int* dcount;                   // [kOpenMaxLevels] entries of dchild
+    OpenSlotRec* rec[kOpenMaxLevels];  // per level and slot (capacity: the level's cap)
+    unsigned* pdone;               // per slot and 64-column block: id of the last round whose panel
+                                   // tile starting there is written (zero at launch)
     int cap[kOpenMaxLevels];       // capacity of each level's list
     int n_seam[kOpenMaxLevels];    // seam nodes at the head of each level's list (stamped first)
     int* maxk;                     // [kOpenMaxLevels] largest pivot count per level

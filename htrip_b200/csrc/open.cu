@@ -49,7 +49,7 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int B = kOpenB;
 constexpr unsigned kBarrierPolls = 1u << 24;
-constexpr int kInsertChunk = 16384;  // child-summary entries per insert unit
+constexpr int kInsertChunk = 2048;  // child-summary entries per insert unit
 
 __device__ __forceinline__ unsigned long long global_timer() {
     unsigned long long t;
@@ -113,6 +113,22 @@ __device__ __forceinline__ int next_unit(const OpenLaunch& L, int* s_unit) {
     return *s_unit;
 }
 
+// Data that other CTAs of this launch wrote (work lists, slot records,
+// stamps, matrices, panels, flags) is read through L2 only (ld.global.cg /
+// cp.async.cg): the L1 of this SM may still hold a line of it from before the
+// write, and grid barriers do not invalidate L1.
+__device__ __forceinline__ int4 ld_slot(const int4* p) { return __ldcg(p); }
+__device__ __forceinline__ OpenSlotRec ld_rec(const OpenSlotRec* p) {
+    static_assert(sizeof(OpenSlotRec) == 32, "two 16-byte loads");
+    const uint4 a = __ldcg(reinterpret_cast<const uint4*>(p));
+    const uint4 b = __ldcg(reinterpret_cast<const uint4*>(p) + 1);
+    OpenSlotRec r;
+    uint4* d = reinterpret_cast<uint4*>(&r);
+    d[0] = a;
+    d[1] = b;
+    return r;
+}
+
 __device__ __forceinline__ uint16_t* node_mat(const OpenTaskLevel& T, int node, int NP) {
     return T.mat + (size_t)node * NP * NP;
 }
@@ -152,7 +168,7 @@ __device__ void stamp_phase(const OpenLaunch& L) {
     const int gt = blockIdx.x * kThreads + threadIdx.x, gs = gridDim.x * kThreads;
     for (int l = 1; l <= L.maxH; ++l)
         for (int s = gt; s < L.n_seam[l]; s += gs) {
-            const int4 e = L.slots[l][s];
+            const int4 e = ld_slot(L.slots[l] + s);
             const OpenTask& T = L.tasks[e.x];
             T.lv[l].mstamp[e.y] = T.stamp;
         }
@@ -178,7 +194,7 @@ __device__ void insert_list(const OpenLaunch& L, int l, int4 e, int* new_pivots,
     for (int t = e.z + lane; t < e.w; t += 32) {
         const int u = L.triples[3 * t], v = L.triples[3 * t + 1];
         const uint16_t w = (uint16_t)L.triples[3 * t + 2];
-        if (w < D[(size_t)u * NP + v]) {
+        if (w < __ldcg(D + (size_t)u * NP + v)) {
             D[(size_t)u * NP + v] = w;
             D[(size_t)v * NP + u] = w;
             const int ends[2] = {u, v};
@@ -217,7 +233,7 @@ __device__ void insert_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
         if (u < list_units) {
             const int s = u * kWarps + warp;
             if (s < N) {
-                const int4 e = L.slots[l][s];
+                const int4 e = ld_slot(L.slots[l] + s);
                 if (e.w > e.z) {  // uniform over the warp
                     int np = 0;
                     bool dec = false;
@@ -232,7 +248,7 @@ __device__ void insert_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
             continue;
         }
         const int cu = u - list_units;
-        const int4 dc = L.dchild[l][cu / chunks];  // {task, child, node, quad}
+        const int4 dc = ld_slot(L.dchild[l] + cu / chunks);  // {task, child, node, quad}
         const int c = cu % chunks;
         const OpenTask& T = L.tasks[dc.x];
         if (threadIdx.x == 0) s_dec = 0;
@@ -256,8 +272,8 @@ __device__ void insert_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
                     const int p = idx / nP, pp = idx - p * nP;
                     a[x] = q * nP + p;
                     bb[x] = q * nP + pp;
-                    w[x] = cm[(size_t)G.child_ext[p] * cNP + G.child_ext[pp]];
-                    d[x] = D[(size_t)a[x] * NP + bb[x]];
+                    w[x] = __ldcg(cm + (size_t)G.child_ext[p] * cNP + G.child_ext[pp]);
+                    d[x] = __ldcg(D + (size_t)a[x] * NP + bb[x]);
                 }
             }
 #pragma unroll
@@ -287,7 +303,7 @@ __device__ void compact_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
     __shared__ int base;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int s = next_unit(L, s_unit); s < N; s = next_unit(L, s_unit)) {
-        const int4 e = L.slots[l][s];
+        const int4 e = ld_slot(L.slots[l] + s);
         const OpenTask& T = L.tasks[e.x];
         uint8_t* f = T.lv[l].kflag + (size_t)e.y * G.NP;
         int* out = T.lv[l].klist + (size_t)e.y * G.NP;
@@ -297,7 +313,7 @@ __device__ void compact_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
         for (int j0 = 0; j0 < G.NP; j0 += 4 * kThreads) {
             const int j = j0 + 4 * threadIdx.x;
             unsigned wv = 0;
-            if (j < G.NP) wv = *reinterpret_cast<const unsigned*>(f + j);
+            if (j < G.NP) wv = __ldcg(reinterpret_cast<const unsigned*>(f + j));
             const int cnt = (wv & 0xffu ? 1 : 0) + (wv & 0xff00u ? 1 : 0) + (wv & 0xff0000u ? 1 : 0) +
                             (wv & 0xff000000u ? 1 : 0);
             int incl = cnt;
@@ -324,6 +340,7 @@ __device__ void compact_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
         if (threadIdx.x == 0) {
             const int k = base;
             T.lv[l].kcnt[e.y] = k;
+            L.rec[l][s] = OpenSlotRec{node_mat(T.lv[l], e.y, G.NP), out, k, e.x, e.y, 0};
             atomicAdd(&T.out->level[l][0], 1);
             atomicAdd(&T.out->level[l][1], k);
             atomicMax(&T.out->level[l][2], k);
@@ -348,22 +365,103 @@ __device__ void compact_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
 // ---------------------------------------------------------------------------
 constexpr int kTLD = B + 8;  // padded row of T (144 bytes): column reads hit distinct banks
 
+// Floyd-Warshall over the round's pivot block T (mk <= B rows, identity
+// beyond) in shared memory: thread t owns row t / 4 and 16 columns.  Step kk
+// reads row kk and column kk, whose values it rewrites unchanged
+// (T[kk][kk] = 0), so one barrier per step orders it before step kk + 1; a
+// = INF gives no change through the clamped form, so no branch is needed.
+__device__ __forceinline__ void close_pivot_block(uint16_t (*Ts)[kTLD], int mk) {
+    const int tid = threadIdx.x;
+    const int a = tid >> 2, c0 = (tid & 3) * 16;
+    uint32_t v[8];
+    const uint4 x0 = *reinterpret_cast<const uint4*>(&Ts[a][c0]);
+    const uint4 y0 = *reinterpret_cast<const uint4*>(&Ts[a][c0 + 8]);
+    v[0] = x0.x; v[1] = x0.y; v[2] = x0.z; v[3] = x0.w; v[4] = y0.x; v[5] = y0.y; v[6] = y0.z; v[7] = y0.w;
+    for (int kk = 0; kk < mk; ++kk) {
+        const uint32_t t = Ts[a][kk];
+        const uint4 x = *reinterpret_cast<const uint4*>(&Ts[kk][c0]);
+        const uint4 y = *reinterpret_cast<const uint4*>(&Ts[kk][c0 + 8]);
+        const uint32_t rw[8] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
+        const uint32_t aa = splat(t), tt = INF2 - aa;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] = acc_clamp(v[i], rw[i], aa, tt);
+        *reinterpret_cast<uint4*>(&Ts[a][c0]) = make_uint4(v[0], v[1], v[2], v[3]);
+        *reinterpret_cast<uint4*>(&Ts[a][c0 + 8]) = make_uint4(v[4], v[5], v[6], v[7]);
+        __syncthreads();
+    }
+}
+
+// Class of pivot k for warp w's 8 rows of T* (entries T*[k][8w .. 8w+7]):
+// 0 all INF (skip), 1 all <= INF_HEADROOM (2-op form), 2 otherwise.
+__device__ __forceinline__ void panel_classes(uint16_t (*Ts)[kTLD], int mk, uint8_t* cls) {
+    for (int idx = threadIdx.x; idx < mk * kWarps; idx += kThreads) {
+        const int k = idx / kWarps, w = idx % kWarps;
+        uint32_t mn = 0xffffu, mx = 0;
+#pragma unroll
+        for (int rr = 0; rr < 8; ++rr) {
+            const uint32_t v = Ts[k][w * 8 + rr];
+            mn = min(mn, v);
+            mx = max(mx, v);
+        }
+        cls[idx] = mn >= INF ? 0 : (mx <= INF_HEADROOM ? 1 : 2);
+    }
+}
+
+// acc[r][c] = min_k T*[k][8w + r] (+) Bs[k][lane's pair c]  (T* symmetric:
+// T*[k][a] = T*[a][k]); warp w owns pivot rows 8w..8w+7.
 template <int CP>
-__device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, unsigned char* smem) {
+__device__ __forceinline__ void panel_gemm(uint16_t (*Ts)[kTLD], const uint16_t* Bs, int ldb, int mk,
+                                           const uint8_t* cls, uint32_t (&acc)[8][CP]) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int rr = 0; rr < 8; ++rr)
+#pragma unroll
+        for (int cc = 0; cc < CP; ++cc) acc[rr][cc] = INF2;
+    for (int k = 0; k < mk; ++k) {
+        const int c = cls[k * kWarps + warp];
+        if (c == 0) continue;  // uniform over the warp
+        uint32_t bv[CP];
+#pragma unroll
+        for (int cc = 0; cc < CP; ++cc) bv[cc] = reinterpret_cast<const uint32_t*>(Bs + k * ldb + lane * 2 * CP)[cc];
+        const uint4 av = *reinterpret_cast<const uint4*>(&Ts[k][warp * 8]);
+        const uint32_t aw[4] = {av.x, av.y, av.z, av.w};
+        uint32_t aa[8];
+#pragma unroll
+        for (int r2 = 0; r2 < 4; ++r2) {
+            aa[2 * r2] = splat(aw[r2]);
+            aa[2 * r2 + 1] = splat(aw[r2] >> 16);
+        }
+        if (c == 1) {
+#pragma unroll
+            for (int rr = 0; rr < 8; ++rr)
+#pragma unroll
+                for (int cc = 0; cc < CP; ++cc) acc[rr][cc] = acc_fast(acc[rr][cc], bv[cc], aa[rr]);
+        } else {
+#pragma unroll
+            for (int rr = 0; rr < 8; ++rr) {
+                const uint32_t tt = INF2 - aa[rr];
+#pragma unroll
+                for (int cc = 0; cc < CP; ++cc) acc[rr][cc] = acc_clamp(acc[rr][cc], bv[cc], aa[rr], tt);
+            }
+        }
+    }
+}
+
+template <int CP>
+__device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, unsigned rid, unsigned char* smem) {
     constexpr int NT = 64 * CP;
-    const OpenLevelGeom& G = L.geo[l];
-    const int NP = G.NP;
-    const int4 e = L.slots[l][s];
-    const OpenTask& T = L.tasks[e.x];
-    const int mk = min(B, T.lv[l].kcnt[e.y] - r * B);
+    const int NP = L.geo[l].NP;
+    const OpenSlotRec rec = ld_rec(L.rec[l] + s);
+    const int mk = min(B, rec.kcnt - r * B);
     if (mk <= 0) return;  // uniform
     uint16_t (*Ts)[kTLD] = reinterpret_cast<uint16_t (*)[kTLD]>(smem);
     uint16_t* Bs = reinterpret_cast<uint16_t*>(smem + B * kTLD * sizeof(uint16_t));  // [B][NT]
     int* kc = reinterpret_cast<int*>(smem + B * kTLD * sizeof(uint16_t) + B * NT * sizeof(uint16_t));
+    uint8_t* cls = reinterpret_cast<uint8_t*>(kc + B);                                 // [B][kWarps]
     __shared__ int tile_any[4];
-    const uint16_t* D = node_mat(T.lv[l], e.y, NP);
+    const uint16_t* D = rec.mat;
     const int tid = threadIdx.x;
-    if (tid < mk) kc[tid] = T.lv[l].klist[(size_t)e.y * NP + r * B + tid];
+    if (tid < mk) kc[tid] = __ldcg(rec.klist + r * B + tid);
     if (tid < 4) tile_any[tid] = 0;
     __syncthreads();
     {   // the tile's pivot rows by asynchronous copies, meanwhile the pivot
@@ -377,7 +475,7 @@ __device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, uns
 #pragma unroll
         for (int x = 0; x < NTB; ++x) {
             const int idx = tid + x * kThreads, a = idx / B, c = idx % B;
-            tv[x] = (a < mk && c < mk) ? D[(size_t)kc[a] * NP + kc[c]] : (a == c ? 0 : INF);
+            tv[x] = (a < mk && c < mk) ? __ldcg(D + (size_t)kc[a] * NP + kc[c]) : (a == c ? 0 : INF);
         }
 #pragma unroll
         for (int x = 0; x < NTB; ++x) {
@@ -387,61 +485,12 @@ __device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, uns
         cp_async_wait_all();
     }
     __syncthreads();
-    {   // Floyd-Warshall over the pivot block: thread t owns row t / 4, 16 columns
-        const int a = tid >> 2, c0 = (tid & 3) * 16;
-        uint32_t v[8];
-        const uint4 x0 = *reinterpret_cast<const uint4*>(&Ts[a][c0]);
-        const uint4 y0 = *reinterpret_cast<const uint4*>(&Ts[a][c0 + 8]);
-        v[0] = x0.x; v[1] = x0.y; v[2] = x0.z; v[3] = x0.w; v[4] = y0.x; v[5] = y0.y; v[6] = y0.z; v[7] = y0.w;
-        // step kk reads row kk and column kk, which it leaves unchanged
-        // (T[kk][kk] = 0): one barrier per step orders it before step kk + 1
-        for (int kk = 0; kk < mk; ++kk) {
-            const uint32_t t = Ts[a][kk];
-            const uint4 x = *reinterpret_cast<const uint4*>(&Ts[kk][c0]);
-            const uint4 y = *reinterpret_cast<const uint4*>(&Ts[kk][c0 + 8]);
-            if (t < INF) {
-                const uint32_t rw[8] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
-                const uint32_t aa = splat(t), tt = splat(INF - t);
-#pragma unroll
-                for (int i = 0; i < 8; ++i) v[i] = acc_clamp(v[i], rw[i], aa, tt);
-                *reinterpret_cast<uint4*>(&Ts[a][c0]) = make_uint4(v[0], v[1], v[2], v[3]);
-                *reinterpret_cast<uint4*>(&Ts[a][c0 + 8]) = make_uint4(v[4], v[5], v[6], v[7]);
-            }
-            __syncthreads();
-        }
-    }
-    // P = T* (x) D[Kc, tile]: warp w owns pivot rows 8w..8w+7, lane the CP
-    // column pairs from 2*CP*lane (T* symmetric: T*[c][a] = T*[a][c])
+    close_pivot_block(Ts, mk);
+    panel_classes(Ts, mk, cls);
+    __syncthreads();
     const int warp = tid >> 5, lane = tid & 31;
     uint32_t acc[8][CP];
-#pragma unroll
-    for (int rr = 0; rr < 8; ++rr)
-#pragma unroll
-        for (int cc = 0; cc < CP; ++cc) acc[rr][cc] = INF2;
-    for (int k = 0; k < mk; ++k) {
-        uint32_t bv[CP];
-#pragma unroll
-        for (int cc = 0; cc < CP; ++cc) bv[cc] = reinterpret_cast<const uint32_t*>(Bs + k * NT + lane * 2 * CP)[cc];
-        const uint4 av = *reinterpret_cast<const uint4*>(&Ts[k][warp * 8]);
-        const uint32_t aw[4] = {av.x, av.y, av.z, av.w};
-#pragma unroll
-        for (int r2 = 0; r2 < 4; ++r2) {
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const uint32_t a = h ? (aw[r2] >> 16) : (aw[r2] & 0xffffu);
-                if (a <= INF_HEADROOM) {
-                    const uint32_t aa = splat(a);
-#pragma unroll
-                    for (int cc = 0; cc < CP; ++cc) acc[2 * r2 + h][cc] = acc_fast(acc[2 * r2 + h][cc], bv[cc], aa);
-                } else if (a < INF) {
-                    const uint32_t aa = splat(a), tt = splat(INF - a);
-#pragma unroll
-                    for (int cc = 0; cc < CP; ++cc)
-                        acc[2 * r2 + h][cc] = acc_clamp(acc[2 * r2 + h][cc], bv[cc], aa, tt);
-                }
-            }
-        }
-    }
+    panel_gemm<CP>(Ts, Bs, NT, mk, cls, acc);
     uint16_t* P = L.panel + (size_t)s * B * NP;
     bool any = false;
     const int col = j0 + lane * 2 * CP;
@@ -459,18 +508,10 @@ __device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, uns
     if (any) tile_any[(lane * 2 * CP) / 64] = 1;
     __syncthreads();
     if (tid < NT / 64) L.pflags[(size_t)s * (NP / 64) + j0 / 64 + tid] = tile_any[tid] ? 1 : 0;
-}
-
-__device__ void panel_phase(const OpenLaunch& L, int l, int N, int r, int* s_unit, unsigned char* smem) {
-    const int NP = L.geo[l].NP;
-    const int NT = NP >= 256 ? 256 : NP;
-    const int tiles = NP / NT;
-    const int units = N * tiles;
-    for (int u = next_unit(L, s_unit); u < units; u = next_unit(L, s_unit)) {
-        const int s = u / tiles, j0 = (u % tiles) * NT;
-        if (NT == 256) panel_unit<4>(L, l, s, j0, r, smem);
-        else if (NT == 128) panel_unit<2>(L, l, s, j0, r, smem);
-        else panel_unit<1>(L, l, s, j0, r, smem);
+    __syncthreads();
+    if (tid == 0) {  // the tile (and its flags) is written: release it to the update units
+        __threadfence();
+        atomicExch(L.pdone + (size_t)s * (NP / 64) + j0 / 64, rid);
     }
 }
 
@@ -487,21 +528,41 @@ __device__ void panel_phase(const OpenLaunch& L, int l, int N, int r, int* s_uni
 // wrap), 2 otherwise (3-op clamped form).
 // ---------------------------------------------------------------------------
 template <int RW, int CP>
-__device__ void update_unit(const OpenLaunch& L, int l, int s, int I, int J, int r, unsigned char* smem) {
+__device__ void update_unit(const OpenLaunch& L, int l, int s, int I, int J, int r, unsigned rid,
+                            unsigned char* smem) {
     constexpr int TT = 8 * RW;  // == 64 * CP
     static_assert(TT == 64 * CP, "square tiles");
     const OpenLevelGeom& G = L.geo[l];
     const int NP = G.NP;
-    const int4 e = L.slots[l][s];
-    const OpenTask& T = L.tasks[e.x];
-    const int mk = min(B, T.lv[l].kcnt[e.y] - r * B);
-    if (mk <= 0) return;
     const uint8_t* pf = L.pflags + (size_t)s * (NP / 64);
+    const OpenSlotRec rec = ld_rec(L.rec[l] + s);
+    const int mk = min(B, rec.kcnt - r * B);
+    if (mk <= 0) return;  // uniform; no panel was made for this slot either
+    {   // bounded wait for the two panel tiles this tile reads (units of lower
+        // tickets, handed out first: every wait ends)
+        __shared__ int s_ok;
+        if (threadIdx.x == 0) {
+            const int NT = NP >= 256 ? 256 : NP;
+            const unsigned* wi = L.pdone + (size_t)s * (NP / 64) + (I * TT / NT) * NT / 64;
+            const unsigned* wj = L.pdone + (size_t)s * (NP / 64) + (J * TT / NT) * NT / 64;
+            int ok = 1;
+            unsigned it = 0;
+            while (*(volatile const unsigned*)wi != rid || *(volatile const unsigned*)wj != rid) {
+                if (*(volatile int*)L.status != 0) { ok = 0; break; }
+                if (++it > kBarrierPolls) { atomicCAS(L.status, 0, 1); ok = 0; break; }
+                __nanosleep(32);
+            }
+            __threadfence();
+            s_ok = ok;
+        }
+        __syncthreads();
+        if (!s_ok) return;
+    }
     bool live_i = false, live_j = false;
 #pragma unroll
     for (int t = 0; t < TT / 64; ++t) {
-        live_i |= pf[I * (TT / 64) + t] != 0;
-        live_j |= pf[J * (TT / 64) + t] != 0;
+        live_i |= __ldcg(pf + I * (TT / 64) + t) != 0;
+        live_j |= __ldcg(pf + J * (TT / 64) + t) != 0;
     }
     if (!live_i || !live_j) return;  // uniform
     uint32_t* As = reinterpret_cast<uint32_t*>(smem);                                  // [B][TT] splatted
@@ -513,7 +574,7 @@ __device__ void update_unit(const OpenLaunch& L, int l, int s, int I, int J, int
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int i0 = I * TT, jb = J * TT;
     if (tid == 0) { s_any = 0; s_dec = 0; }
-    uint16_t* D = node_mat(T.lv[l], e.y, NP);
+    uint16_t* D = rec.mat;
     {   // asynchronous copies of the column panel and of the old tile (read
         // only in the epilogue); the row panel is splatted through registers
         for (int idx = tid; idx < mk * (TT / 8); idx += kThreads) {
@@ -530,7 +591,7 @@ __device__ void update_unit(const OpenLaunch& L, int l, int s, int I, int J, int
 #pragma unroll
         for (int x = 0; x < NS; ++x) {
             const int idx = tid + x * kThreads, a = idx / (TT / 8), c8 = idx % (TT / 8);
-            if (a < mk) va[x] = reinterpret_cast<const uint4*>(P + (size_t)a * NP + i0)[c8];
+            if (a < mk) va[x] = __ldcg(reinterpret_cast<const uint4*>(P + (size_t)a * NP + i0) + c8);
         }
 #pragma unroll
         for (int x = 0; x < NS; ++x) {
@@ -646,7 +707,7 @@ __device__ void update_unit(const OpenLaunch& L, int l, int s, int I, int J, int
             reinterpret_cast<uint4*>(D + (size_t)(jb + j) * NP + i0)[c8] = v;
         }
     }
-    if (tid == 0 && s_dec) mark_dec(L, l, e.x, e.y);
+    if (tid == 0 && s_dec) mark_dec(L, l, rec.task, rec.node);
 }
 
 // Upper-triangle tile pair t of an nt x nt tile grid: I <= J.
@@ -660,22 +721,259 @@ __device__ __forceinline__ void tri_pair(int t, int nt, int& I, int& J) {
     J = i + t;
 }
 
-__device__ void update_phase(const OpenLaunch& L, int l, int N, int r, int* s_unit, unsigned char* smem) {
+// One closure round of level l as one phase: the panel units (slot x column
+// tile) take the lower tickets, the update units (slot x upper-triangle tile
+// pair) the higher ones; an update unit waits only for the two panel tiles
+// it reads, so no grid barrier separates the panel from the update.
+__device__ void round_phase(const OpenLaunch& L, int l, int N, int r, unsigned rid, int* s_unit,
+                            unsigned char* smem) {
     const int NP = L.geo[l].NP;
+    const int NT = NP >= 256 ? 256 : NP;
+    const int tiles = NP / NT;
     const int TT = NP >= 128 ? 128 : 64;
     const int nt = NP / TT;
     const int per = nt * (nt + 1) / 2;
-    const int units = N * per;
+    const int n_panel = N * tiles;
+    const int units = n_panel + N * per;
     for (int u = next_unit(L, s_unit); u < units; u = next_unit(L, s_unit)) {
-        const int s = u / per;
+        if (u < n_panel) {
+            const int s = u / tiles, j0 = (u % tiles) * NT;
+            if (NT == 256) panel_unit<4>(L, l, s, j0, r, rid, smem);
+            else if (NT == 128) panel_unit<2>(L, l, s, j0, r, rid, smem);
+            else panel_unit<1>(L, l, s, j0, r, rid, smem);
+            continue;
+        }
+        const int v = u - n_panel;
+        const int s = v / per;
         int I, J;
-        tri_pair(u % per, nt, I, J);
-        if (TT == 128) update_unit<16, 2>(L, l, s, I, J, r, smem);
-        else update_unit<8, 1>(L, l, s, I, J, r, smem);
+        tri_pair(v % per, nt, I, J);
+        if (TT == 128) update_unit<16, 2>(L, l, s, I, J, r, rid, smem);
+        else update_unit<8, 1>(L, l, s, I, J, r, rid, smem);
     }
 }
 
-constexpr size_t kPanelSmem = (size_t)B * kTLD * sizeof(uint16_t) + (size_t)B * 256 * sizeof(uint16_t) + B * sizeof(int);
+// ---------------------------------------------------------------------------
+// Levels whose matrices fit in shared memory (NP <= 128: leaves of b <= 11,
+// the lowest node levels): one unit per slot does the whole update of its
+// matrix in shared memory - the child-summary decreases, the edge / seam
+// list, the pivot compaction and every closure round (pivot block,
+// panel, full update) - and writes the matrix back once.  One phase per
+// level instead of 2 + 2 x rounds.
+// ---------------------------------------------------------------------------
+template <int RW, int CP>
+__device__ void small_unit(const OpenLaunch& L, int l, int s, unsigned char* smem) {
+    constexpr int NP = 8 * RW;
+    static_assert(NP == 64 * CP, "square matrix of 8 warps x RW rows and 32 lanes x CP pairs");
+    const OpenLevelGeom& G = L.geo[l];
+    const int4 e = ld_slot(L.slots[l] + s);
+    const OpenTask& T = L.tasks[e.x];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    uint16_t* Dg = node_mat(T.lv[l], e.y, NP);
+    uint16_t* Dm = reinterpret_cast<uint16_t*>(smem);                               // [NP][NP]
+    uint16_t* Pm = Dm + NP * NP;                                                     // [B][NP]
+    uint16_t (*Ts)[kTLD] = reinterpret_cast<uint16_t (*)[kTLD]>(Pm + B * NP);       // [B][kTLD]
+    int* kl = reinterpret_cast<int*>(&Ts[B][0]);                                     // [NP]
+    uint8_t* fl = reinterpret_cast<uint8_t*>(kl + NP);                               // [NP]
+    uint8_t* cls = fl + NP;                                                          // [B][kWarps]
+    __shared__ int s_dec, s_chg, s_np, s_k;
+    __shared__ int wtot[kWarps];
+    for (int idx = tid; idx < NP * NP / 8; idx += kThreads) cp_async16(Dm + idx * 8, Dg + idx * 8);
+    for (int j = tid; j < NP / 4; j += kThreads) reinterpret_cast<unsigned*>(fl)[j] = 0u;
+    if (tid == 0) { s_dec = 0; s_chg = 0; s_np = 0; }
+    cp_async_wait_all();
+    __syncthreads();
+    bool dec = false, chg = false;
+    if (l >= 1) {  // child-summary decreases (internal_node.cpp:343-353), as in insert_phase
+        const int nx = T.lv[l].nodes_x, g = L.g, nP = G.nP, cNP = G.childNP;
+        for (int q = 0; q < g * g; ++q) {
+            const int child = ((e.y / nx) * g + q / g) * T.lv[l - 1].nodes_x + ((e.y % nx) * g + q % g);
+            if (__ldcg(T.lv[l - 1].dstamp + child) != T.stamp) continue;  // uniform
+            const uint16_t* cm = node_mat(T.lv[l - 1], child, cNP);
+            for (int idx = tid; idx < nP * nP; idx += kThreads) {
+                const int p = idx / nP, pp = idx - p * nP;
+                const uint16_t w = __ldcg(cm + (size_t)G.child_ext[p] * cNP + G.child_ext[pp]);
+                const int a = q * nP + p, b = q * nP + pp;
+                if (w < Dm[a * NP + b]) {
+                    Dm[a * NP + b] = w;  // (b, a) is written by its own thread
+                    fl[a] = 1;
+                    fl[b] = 1;
+                    dec |= G.isext[a] && G.isext[b];
+                    chg = true;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (warp == 0 && e.w > e.z) {  // the edge / seam list, lanes in parallel (see insert_list)
+        int np = 0;
+        for (int t = e.z + lane; t < e.w; t += 32) {
+            const int u = L.triples[3 * t], v = L.triples[3 * t + 1];
+            const uint16_t w = (uint16_t)L.triples[3 * t + 2];
+            if (w < Dm[u * NP + v]) {
+                Dm[u * NP + v] = w;
+                Dm[v * NP + u] = w;
+                const int ends[2] = {u, v};
+#pragma unroll
+                for (int x = 0; x < 2; ++x) {
+                    const int a = ends[x];
+                    const unsigned sh = (unsigned)(a & 3) * 8u;
+                    const unsigned old = atomicOr(reinterpret_cast<unsigned*>(fl + (a & ~3)), 1u << sh);
+                    np += ((old >> sh) & 0xffu) == 0;
+                }
+                dec |= G.isext[u] && G.isext[v];
+                chg = true;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) np += __shfl_xor_sync(FULL, np, o);
+        if (lane == 0) s_np = np;
+    }
+    __syncthreads();
+    {   // pivot flags -> ascending list (NP <= 128 <= kThreads: one step)
+        const bool on = tid < NP && fl[tid];
+        const unsigned bal = __ballot_sync(FULL, on);
+        if (lane == 0) wtot[warp] = __popc(bal);
+        __syncthreads();
+        int off = 0, tot = 0;
+        for (int w = 0; w < kWarps; ++w) {
+            if (w < warp) off += wtot[w];
+            tot += wtot[w];
+        }
+        if (on) kl[off + __popc(bal & ((1u << lane) - 1u))] = tid;
+        if (tid == 0) s_k = tot;
+        __syncthreads();
+    }
+    const int k = s_k;
+    if (tid == 0) {
+        atomicAdd(&T.out->level[l][0], 1);
+        atomicAdd(&T.out->level[l][1], k);
+        atomicMax(&T.out->level[l][2], k);
+        if (l == 0 && s_np) atomicAdd(&T.out->new_pivots, s_np);
+        if (k) {
+            const unsigned long long n = (unsigned long long)G.n;
+            atomicAdd(&T.out->ops, n * n * (unsigned long long)k);
+            atomicAdd(&T.out->bytes, 4ull * n * n + 4ull * (unsigned long long)k * n);
+        }
+    }
+    for (int r = 0; r * B < k; ++r) {
+        const int mk = min(B, k - r * B);
+        const int* kc = kl + r * B;
+        for (int idx = tid; idx < B * B; idx += kThreads) {
+            const int a = idx / B, c = idx % B;
+            Ts[a][c] = (a < mk && c < mk) ? Dm[kc[a] * NP + kc[c]] : (a == c ? 0 : INF);
+        }
+        for (int idx = tid; idx < mk * (NP / 8); idx += kThreads) {  // the pivot rows
+            const int a = idx / (NP / 8), c8 = idx % (NP / 8);
+            reinterpret_cast<uint4*>(Pm + a * NP)[c8] = reinterpret_cast<const uint4*>(Dm + kc[a] * NP)[c8];
+        }
+        __syncthreads();
+        close_pivot_block(Ts, mk);
+        panel_classes(Ts, mk, cls);
+        __syncthreads();
+        {   // the panel P = T* (x) D[Kc, :], into Pm
+            uint32_t pacc[8][CP];
+            panel_gemm<CP>(Ts, Pm, NP, mk, cls, pacc);
+            __syncthreads();
+#pragma unroll
+            for (int rr = 0; rr < 8; ++rr) {
+                const int a = warp * 8 + rr;
+                if (a < mk)
+#pragma unroll
+                    for (int cc = 0; cc < CP; ++cc)
+                        reinterpret_cast<uint32_t*>(Pm + a * NP + lane * 2 * CP)[cc] = pacc[rr][cc];
+            }
+        }
+        __syncthreads();
+        for (int idx = tid; idx < mk * kWarps; idx += kThreads) {  // update classes per warp row group
+            const int a = idx / kWarps, w = idx % kWarps;
+            uint32_t mn = 0xffffu, mx = 0;
+#pragma unroll
+            for (int rr = 0; rr < RW; ++rr) {
+                const uint32_t v = Pm[a * NP + w * RW + rr];
+                mn = min(mn, v);
+                mx = max(mx, v);
+            }
+            cls[idx] = mn >= INF ? 0 : (mx <= INF_HEADROOM ? 1 : 2);
+        }
+        __syncthreads();
+        // D = min(D, P^T (x) P): warp w rows RW*w.., lane CP pairs
+        uint32_t acc[RW][CP];
+#pragma unroll
+        for (int rr = 0; rr < RW; ++rr)
+#pragma unroll
+            for (int cc = 0; cc < CP; ++cc) acc[rr][cc] = INF2;
+        for (int kk = 0; kk < mk; ++kk) {
+            const int c = cls[kk * kWarps + warp];
+            if (c == 0) continue;  // uniform over the warp
+            uint32_t bv[CP];
+#pragma unroll
+            for (int cc = 0; cc < CP; ++cc) bv[cc] = reinterpret_cast<const uint32_t*>(Pm + kk * NP + lane * 2 * CP)[cc];
+            uint32_t av[RW];
+#pragma unroll
+            for (int q2 = 0; q2 < RW / 2; ++q2) {
+                const uint32_t w2 = reinterpret_cast<const uint32_t*>(Pm + kk * NP + warp * RW)[q2];
+                av[2 * q2] = splat(w2);
+                av[2 * q2 + 1] = splat(w2 >> 16);
+            }
+            if (c == 1) {
+#pragma unroll
+                for (int rr = 0; rr < RW; ++rr)
+#pragma unroll
+                    for (int cc = 0; cc < CP; ++cc) acc[rr][cc] = acc_fast(acc[rr][cc], bv[cc], av[rr]);
+            } else {
+#pragma unroll
+                for (int rr = 0; rr < RW; ++rr) {
+                    const uint32_t tt = INF2 - av[rr];
+#pragma unroll
+                    for (int cc = 0; cc < CP; ++cc) acc[rr][cc] = acc_clamp(acc[rr][cc], bv[cc], av[rr], tt);
+                }
+            }
+        }
+        const int col = lane * 2 * CP;
+        uint32_t cext[CP];
+#pragma unroll
+        for (int cc = 0; cc < CP; ++cc)
+            cext[cc] = (G.isext[col + 2 * cc] ? 0xffffu : 0u) | (G.isext[col + 2 * cc + 1] ? 0xffff0000u : 0u);
+#pragma unroll
+        for (int rr = 0; rr < RW; ++rr) {
+            const int row = warp * RW + rr;
+            uint32_t* dp = reinterpret_cast<uint32_t*>(Dm + row * NP + col);
+            const bool rext = G.isext[row] != 0;
+#pragma unroll
+            for (int cc = 0; cc < CP; ++cc) {
+                const uint32_t o = dp[cc], nv = min2(acc[rr][cc], o);
+                const uint32_t diff = nv ^ o;
+                if (diff) {
+                    dp[cc] = nv;
+                    chg = true;
+                    if (rext) dec |= (diff & cext[cc]) != 0;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (__any_sync(FULL, chg) && lane == 0) s_chg = 1;
+    if (__any_sync(FULL, dec) && lane == 0) s_dec = 1;
+    __syncthreads();
+    if (s_chg)
+        for (int idx = tid; idx < NP * NP / 8; idx += kThreads)
+            reinterpret_cast<uint4*>(Dg)[idx] = reinterpret_cast<const uint4*>(Dm)[idx];
+    if (tid == 0) {
+        T.lv[l].kcnt[e.y] = k;
+        if (s_dec) mark_dec(L, l, e.x, e.y);
+    }
+}
+
+__device__ void small_phase(const OpenLaunch& L, int l, int N, int* s_unit, unsigned char* smem) {
+    const int NP = L.geo[l].NP;
+    for (int s = next_unit(L, s_unit); s < N; s = next_unit(L, s_unit)) {
+        if (NP == 128) small_unit<16, 2>(L, l, s, smem);
+        else small_unit<8, 1>(L, l, s, smem);
+    }
+}
+
+constexpr size_t kPanelSmem = (size_t)B * kTLD * sizeof(uint16_t) + (size_t)B * 256 * sizeof(uint16_t) +
+                              B * sizeof(int) + (size_t)B * kWarps;
 constexpr size_t kUpdateSmem = (size_t)B * 128 * (sizeof(uint32_t) + sizeof(uint16_t)) + (size_t)B * kWarps +
                                (size_t)128 * 128 * sizeof(uint16_t);
 constexpr size_t kTransposeSmem = (size_t)128 * (128 + 8) * sizeof(uint16_t);
@@ -685,6 +983,7 @@ __global__ void __launch_bounds__(kThreads, 2) open_persistent_kernel(const Open
     extern __shared__ __align__(16) unsigned char osm[];
     __shared__ int s_unit;
     int phase = 0;
+    unsigned rid = 0;  // closure rounds of the launch so far (panel tile release ids)
     const bool stamp = L.trace && blockIdx.x == 0 && threadIdx.x == 0;
     if (stamp) L.trace[0] = global_timer();
     auto end_phase = [&]() -> bool {
@@ -698,15 +997,18 @@ __global__ void __launch_bounds__(kThreads, 2) open_persistent_kernel(const Open
     for (int l = 0; l <= L.maxH; ++l) {
         const int N = min(*(volatile int*)(L.count + l), L.cap[l]);
         if (N == 0) continue;
+        if (L.geo[l].NP <= 128) {  // the whole level in one phase, one matrix per unit
+            small_phase(L, l, N, &s_unit, osm);
+            if (!end_phase()) return;
+            continue;
+        }
         insert_phase(L, l, N, &s_unit);
         if (!end_phase()) return;
         compact_phase(L, l, N, &s_unit);
         if (!end_phase()) return;
         const int rounds = (*(volatile int*)(L.maxk + l) + B - 1) / B;
         for (int r = 0; r < rounds; ++r) {
-            panel_phase(L, l, N, r, &s_unit, osm);
-            if (!end_phase()) return;
-            update_phase(L, l, N, r, &s_unit, osm);
+            round_phase(L, l, N, r, ++rid, &s_unit, osm);
             if (!end_phase()) return;
         }
     }

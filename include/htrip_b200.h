@@ -389,8 +389,9 @@ htrip_status htrip_last_open_work(const htrip_index* h, uint64_t* alg_bytes, uin
 /* Phase durations of the index's last device-driven opening launch (no
  * reference counterpart): ns[i] = global-timer nanoseconds of phase i of the
  * persistent opening kernel, in order: the seam-node stamping, then per level
- * with work the insert and compact phases and each closure round's panel and
- * update phases.  *n = phases recorded.                                    */
+ * with work either one phase (matrices of padded order <= 128, updated
+ * whole in shared memory) or the insert and compact phases and one phase per
+ * closure round (panel and update).  *n = phases recorded.               */
 htrip_status htrip_last_open_trace(htrip_index* h, uint64_t* ns, int32_t max_n, int32_t* n);
 
 /* Per level l = 0..H of the index's last opening call (no reference
