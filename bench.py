@@ -655,13 +655,15 @@ def bench_served(device, server_rates=(1000.0, 2000.0, 5000.0, 10000.0, 20000.0,
         # session's own) reaches its working size before the trace: queries,
         # and per session one opening of 512 cells that are already Free
         # (spread over its map), which lowers no distance and so leaves every
-        # index as the trace expects
+        # index as the trace expects, and one query of 512 viewpoints
         wq = [(s, 0, rc) for s, k, rc in W.served_trace([(t, c[:0]) for t, _, c, _ in pl], 400, 2000.0, 99)[0]]
         rng = np.random.default_rng(98)
-        for i, (_, obs, _, _) in enumerate(pl):
+        for i, (truth, obs, _, _) in enumerate(pl):
             free = np.argwhere(obs == W.FREE).astype(np.int32)
             if len(free):
                 wq.append((i, 1, free[rng.choice(len(free), size=min(512, len(free)), replace=False)]))
+            tfree = np.argwhere(truth == W.FREE).astype(np.int32)  # a query of the largest k of the trace
+            wq.append((i, 0, tfree[rng.choice(len(tfree), size=min(512, len(tfree)), replace=False)]))
         srv.run_trace([(sids[s], k, rc) for s, k, rc in wq], np.zeros(len(wq)))
         outs, lat, wall = srv.run_trace([(sids[s], k, rc) for s, k, rc in reqs], arrival)
         st = srv.stats()

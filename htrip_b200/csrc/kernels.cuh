@@ -235,6 +235,11 @@ struct QueryParams {
     unsigned long long* work;  // or null: [0] tile entries updated (operand rows streamed x
                                // tile rows x tile columns), [1] operand rows streamed,
                                // [2] operand rows skipped (no finite value in the tile)
+    const uint8_t* dirty;      // or null (every viewpoint): per sorted viewpoint, 1 = some
+                               // node of its leaf-to-root chain changed.  A unit whose rows
+                               // and columns are all clean skips its work (an incremental
+                               // refresh: the launch's X / Y / flags / M still hold the
+                               // previous launch's values for the clean viewpoints)
 };
 
 // Words of a request's completion counters.

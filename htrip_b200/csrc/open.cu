@@ -789,16 +789,30 @@ __device__ void small_unit(const OpenLaunch& L, int l, int s, unsigned char* sme
             const int child = ((e.y / nx) * g + q / g) * T.lv[l - 1].nodes_x + ((e.y % nx) * g + q % g);
             if (__ldcg(T.lv[l - 1].dstamp + child) != T.stamp) continue;  // uniform
             const uint16_t* cm = node_mat(T.lv[l - 1], child, cNP);
-            for (int idx = tid; idx < nP * nP; idx += kThreads) {
-                const int p = idx / nP, pp = idx - p * nP;
-                const uint16_t w = __ldcg(cm + (size_t)G.child_ext[p] * cNP + G.child_ext[pp]);
-                const int a = q * nP + p, b = q * nP + pp;
-                if (w < Dm[a * NP + b]) {
-                    Dm[a * NP + b] = w;  // (b, a) is written by its own thread
-                    fl[a] = 1;
-                    fl[b] = 1;
-                    dec |= G.isext[a] && G.isext[b];
-                    chg = true;
+            constexpr int U = 4;  // a thread's loads of U entries first, then their updates
+            for (int b0 = tid; b0 < nP * nP; b0 += U * kThreads) {
+                uint16_t w[U];
+                int ab[U];
+#pragma unroll
+                for (int x = 0; x < U; ++x) {
+                    const int idx = b0 + x * kThreads;
+                    ab[x] = -1;
+                    if (idx < nP * nP) {
+                        const int p = idx / nP, pp = idx - p * nP;
+                        w[x] = __ldcg(cm + (size_t)G.child_ext[p] * cNP + G.child_ext[pp]);
+                        ab[x] = (q * nP + p) * NP + q * nP + pp;
+                    }
+                }
+#pragma unroll
+                for (int x = 0; x < U; ++x) {
+                    if (ab[x] >= 0 && w[x] < Dm[ab[x]]) {
+                        const int a = ab[x] / NP, b = ab[x] % NP;
+                        Dm[ab[x]] = w[x];  // (b, a) is written by its own thread
+                        fl[a] = 1;
+                        fl[b] = 1;
+                        dec |= G.isext[a] && G.isext[b];
+                        chg = true;
+                    }
                 }
             }
         }

@@ -268,6 +268,7 @@ plan_query_kernel(const int32_t* __restrict__ vps, const uint8_t* __restrict__ p
                 Pq->ctr = tmpl.ctr;
                 Pq->out = tmpl.out;
                 Pq->work = tmpl.work;
+                Pq->dirty = tmpl.dirty;
             }
         }
     }

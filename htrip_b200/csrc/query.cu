@@ -385,6 +385,11 @@ __device__ bool do_project(const QueryParams& P, const QueryLevel& L, const Quer
     const int gi = it[0], m0 = it[1], n0 = it[2];
     const int* G = L.groups + 5 * gi;
     const int node = G[0], q = G[1], slot0 = G[2];
+    if (P.dirty) {  // incremental refresh: rows of clean viewpoints keep their values
+        int any = 0;
+        for (int r = 0; r < min(RW, G[3] - m0); ++r) any |= P.dirty[G[4] + m0 + r];
+        if (!any) return L.split <= 1 || part == 0;  // a skipped item counts once
+    }
     const int nA = compact_flags(L.flags + (size_t)gi * L.nP, 0, L.nP, kl, wsum);
     const int kb = (int)((long)nA * part / L.split), ke = (int)((long)nA * (part + 1) / L.split);
     const uint16_t* D = L.D + (size_t)node * L.NP * L.NP + (size_t)q * L.nP * L.NP;
@@ -454,6 +459,14 @@ __device__ void do_meet(const QueryParams& P, const QueryLevel& L, int item, int
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int* it = L.meet + 7 * item;
     const int i0 = it[0], j0 = it[1], g2 = it[3], coloff = it[4], kb = it[5], ke = it[6];
+    if (P.dirty) {  // incremental refresh: a pair of clean viewpoints keeps its value
+        int any = 0;
+        for (int e = threadIdx.x; e < 64 * CP + RW; e += kThreads) {
+            const int v = e < 64 * CP ? im.col[e] : im.row[0][e - 64 * CP];
+            if (v >= 0) any |= P.dirty[v];
+        }
+        if (!__syncthreads_or(any)) return;
+    }
     const int nA = compact_flags(L.flags + (size_t)g2 * L.nP, kb, ke, kl, wsum);
     const uint16_t* Xp = P.X[l - 1] + j0;
     const uint16_t* Y = P.Y[l] + (size_t)coloff * P.ldv + i0;
@@ -536,7 +549,7 @@ __device__ bool run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum,
             for (int e = u * kQueryL0Chunk + tid; e < e1; e += kThreads) {
                 const int p = e / S1, s = e - p * S1;
                 const int j = P.l0[2 * s];
-                if (j < 0) continue;
+                if (j < 0 || (P.dirty && !P.dirty[j])) continue;
                 const int* v = P.vp0 + 4 * j;
                 const uint16_t d = P.leaves.base[((size_t)v[0] * P.leaves.NP + v[1]) * P.leaves.NP + P.ext0[p]];
                 P.X[0][(size_t)p * P.ldv + s] = d;
@@ -544,7 +557,8 @@ __device__ bool run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum,
             }
         } else {
             const int j = (u - n_fill) * kThreads + tid;
-            if (j < P.ns) {
+            // same-leaf viewpoints share their chain, hence their dirty flag
+            if (j < P.ns && (!P.dirty || P.dirty[j])) {
                 const int* v = P.vp0 + 4 * j;
                 const uint16_t* row = P.leaves.base + ((size_t)v[0] * P.leaves.NP + v[1]) * P.leaves.NP;
                 // atomicMin: the level-1 meets (intra-child shortcuts) may
