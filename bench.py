@@ -251,11 +251,30 @@ def bench_opening(device, steps=400):
     open_ms, query_ms, cells, entries = [], [], 0, 0
     ops = nbytes = 0
     warm = 10  # the stream's first calls grow the scratch arenas and load the kernels: untimed
+    # a fixed viewpoint set (the robots' starts and 48 cells observed at the
+    # start) refreshed after every call by queryAllPairsIncremental, beside a
+    # full query of the same set
+    from htrip_b200.minplus_oracle import IncrementalState
+    fixed = np.concatenate([starts, W.sample_free(obs, 48, 77)]).astype(np.int32)
+    inc_state = IncrementalState()
+    dev.queryAllPairsIncremental(fixed, obs, inc_state)
+    inc_ms, full_ms, inc_modes, inc_same = [], [], [], True
     for step, c in enumerate(batches):
         obs[c[:, 0], c[:, 1]] = W.FREE
         t = time.perf_counter()
         dev.onBatchCellsOpened(c, obs)
         ms = 1e3 * (time.perf_counter() - t)
+        t = time.perf_counter()
+        m_inc = dev.queryAllPairsIncremental(fixed, obs, inc_state)
+        ims = 1e3 * (time.perf_counter() - t)
+        t = time.perf_counter()
+        m_full = dev.queryAllPairs(fixed, obs)
+        fms = 1e3 * (time.perf_counter() - t)
+        inc_same &= bool(np.array_equal(m_inc, m_full))
+        if step >= warm:
+            inc_ms.append(ims)
+            full_ms.append(fms)
+            inc_modes.append(inc_state.last_mode)
         vps = np.concatenate([starts, W.frontier_cells(obs, 48, 1000 + step)]).astype(np.int32)
         t = time.perf_counter()
         dev.queryAllPairs(vps, obs)
@@ -283,7 +302,15 @@ def bench_opening(device, steps=400):
            "achieved_gb_per_s": nbytes / (1e-3 * sum(open_ms)) / 1e9,
            "open_ms_p50": _pct(open_ms, 50), "open_ms_p99": _pct(open_ms, 99),
            "query_entries_per_s": entries / (1e-3 * sum(query_ms)), "query_ms_p50": _pct(query_ms, 50),
-           "build_s": round(build_s, 4), "parity_vs_rebuild": parity}
+           "build_s": round(build_s, 4), "parity_vs_rebuild": parity,
+           "incremental_fixed_viewpoints": {
+               "workload": f"k={len(fixed)} fixed viewpoints (16 robot starts + 48 initially observed cells) "
+                           "refreshed after every call; host clock per call",
+               "incremental_ms_mean": float(np.mean(inc_ms)), "incremental_ms_p50": _pct(inc_ms, 50),
+               "full_query_ms_mean": float(np.mean(full_ms)), "full_query_ms_p50": _pct(full_ms, 50),
+               "calls_cached": inc_modes.count(0), "calls_relifted": inc_modes.count(2),
+               "calls_full": inc_modes.count(1),
+               "parity_vs_full_query": "bit-exact" if inc_same else "MISMATCH"}}
     del dev, fresh
     if ref_proc is not None:
         try:

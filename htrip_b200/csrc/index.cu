@@ -266,6 +266,10 @@ struct htrip_index {
     // stamp of the last device-driven opening call (per-node stamps in the
     // level arrays compare against it; never 0)
     uint32_t open_stamp = 0;
+    // the level arrays' stamps were (re)allocated this many times, and this
+    // many openings ran on the host-driven path (which does not stamp): an
+    // incremental query that saw other values re-lifts everything
+    uint64_t stamp_epoch = 0, host_opens = 0;
     uint64_t epoch = 0;           // build / root growth count (reference MinPlusOracle::epoch)
     uint64_t update_counter = 0;  // opening calls since creation
     int S = 0, H = 0, rows = 0, cols = 0, leaves_x = 0;
@@ -298,16 +302,6 @@ struct htrip_index {
     }
 };
 
-// Cached result of queryAllPairsIncremental (reference HTripIncrementalState,
-// minplus_oracle.hpp:262-273): the viewpoints, the index's build / root-growth
-// epoch and update count when the matrix was computed, and the matrix.
-struct htrip_incremental {
-    bool initialized = false;
-    const htrip_index* index = nullptr;
-    uint64_t epoch = 0, updates = 0;
-    std::vector<int32_t> vps;
-    std::vector<uint16_t> matrix;
-};
 
 // A launch context for batched calls over many indexes of one device
 // (htrip_query_batch / htrip_open_batch): its own stream and query arena.
@@ -516,6 +510,7 @@ void alloc_levels(htrip_index* h) {
         ck(cudaMemsetAsync(Lv.dstamp.p, 0, Lv.nnodes * sizeof(uint32_t), h->stream), "dstamp");
         ck(cudaMemsetAsync(Lv.mstamp.p, 0, Lv.nnodes * sizeof(uint32_t), h->stream), "mstamp");
     }
+    h->stamp_epoch++;
 }
 
 // Descriptor of matrix m of level Lv (an index's own level arrays).
@@ -1353,8 +1348,12 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
 }
 
 void run_open(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t st, int device) {
-    if (open_on_device()) run_open_device(tasks, A, st, device);
-    else run_open_tasks(tasks, A, st);
+    if (open_on_device()) {
+        run_open_device(tasks, A, st, device);
+    } else {
+        for (OpenTask* T : tasks) T->h->host_opens++;
+        run_open_tasks(tasks, A, st);
+    }
 }
 
 void do_open(htrip_index* h, const int32_t* rc, int n, const uint8_t* obs, int rows, int cols, bool record_stats) {
@@ -1708,7 +1707,7 @@ void query_units(const htrip_index* h, const QueryPlan& P, int n_phases, int* un
 }
 
 hb::QueryParams make_params(const htrip_index* h, const QueryPlan& P, unsigned char* base, const LaunchLayout& L,
-                            int i, uint16_t* out_dev) {
+                            int i, uint16_t* out_dev, const uint8_t* dirty = nullptr) {
     const int H = h->H;
     const int* plan = reinterpret_cast<const int*>(base + L.plan[i]);
     uint8_t* flags = base + L.flags[i];
@@ -1734,6 +1733,7 @@ hb::QueryParams make_params(const htrip_index* h, const QueryPlan& P, unsigned c
     // executed-work counters: single-request launches of an index that counts
     Q.work = h->count_work && L.n == 1 ? reinterpret_cast<unsigned long long*>(base + L.o_words + kWorkOffset)
                                         : nullptr;
+    Q.dirty = dirty;
     for (int l = 1; l <= H; ++l) {
         const Level& Lv = h->L[l];
         const QueryPlan::Lvl& PL = P.lv[l];
@@ -1764,9 +1764,13 @@ hb::QueryParams make_params(const htrip_index* h, const QueryPlan& P, unsigned c
 // memory), then issues on `st`: the head copy, the two presets and the
 // kernel, bracketed by ev[0] / ev[1] when given.  Returns the device
 // pointers of the results in `outs`.
+// With `dirty` (one request; an incremental refresh in an arena that holds
+// the previous launch of the same plan) the pair matrix and the finite-port
+// flags are kept instead of preset, and only the units of dirty viewpoints
+// work.
 void issue_query_launch(cudaStream_t st, int device, int& grid, int cfg, const std::vector<QueryReq>& R,
                         const LaunchLayout& L, unsigned char* base, unsigned char* stage, const cudaEvent_t* ev,
-                        std::vector<uint16_t*>& outs) {
+                        std::vector<uint16_t*>& outs, const uint8_t* dirty = nullptr) {
     for (const auto& r : R) check_query_shape(r.h);
     std::memset(stage, 0, L.head);
     outs.resize(R.size());
@@ -1777,15 +1781,25 @@ void issue_query_launch(cudaStream_t st, int device, int& grid, int cfg, const s
     for (int i = 0; i < L.n; ++i) {
         const QueryReq& r = R[i];
         outs[i] = r.out_dev ? r.out_dev : reinterpret_cast<uint16_t*>(base + L.out[i]);
-        params[i] = make_params(r.h, *r.P, base, L, i, outs[i]);
+        params[i] = make_params(r.h, *r.P, base, L, i, outs[i], dirty);
         std::memcpy(stage + L.plan[i], r.P->buf.data(), r.P->buf.size() * sizeof(int));
         query_units(r.h, *r.P, L.n_phases, units.data());
         for (int t = 0; t < L.n_phases; ++t)
             pre[(size_t)t * (L.n + 1) + i + 1] = pre[(size_t)t * (L.n + 1) + i] + units[t];
     }
     ck(cudaMemcpyAsync(base, stage, L.head, cudaMemcpyHostToDevice, st), "query launch head");
-    ck(cudaMemsetAsync(base + L.o_M, 0xFF, L.M_bytes, st), "pair matrix preset");
-    ck(cudaMemsetAsync(base + L.o_flags, 0, L.flags_bytes, st), "flag preset");
+    if (!dirty) {
+        ck(cudaMemsetAsync(base + L.o_M, 0xFF, L.M_bytes, st), "pair matrix preset");
+        ck(cudaMemsetAsync(base + L.o_flags, 0, L.flags_bytes, st), "flag preset");
+    } else {  // only the completion counters and the split items' tickets start at zero
+        for (size_t i = 0; i < R.size(); ++i) {
+            ck(cudaMemsetAsync(base + L.ctr[i], 0,
+                               hb::query_counter_words(R[i].h->H, R[i].P->k) * sizeof(unsigned), st), "counters");
+            const QueryPlan::Lvl& root = R[i].P->lv[R[i].h->H];
+            if (root.split > 1) ck(cudaMemsetAsync(base + L.ticket[i], 0, (size_t)root.n_items * sizeof(unsigned), st),
+                                   "tickets");
+        }
+    }
     if (grid == 0) grid = hb::query_grid_blocks(device);
     hb::QueryLaunch QL;
     QL.n_req = L.n;
@@ -1811,7 +1825,7 @@ void issue_query_launch(cudaStream_t st, int device, int& grid, int cfg, const s
 // whose out_dev is null are copied into host_out[i] (k*k each).  Returns
 // the kernel's status word (0 ok, 1 a bounded wait timed out); synchronous.
 int run_queries(QueryArena& A, int device, cudaStream_t st, const std::vector<QueryReq>& R,
-                const std::vector<uint16_t*>& host_out, bool sync) {
+                const std::vector<uint16_t*>& host_out, bool sync, const uint8_t* dirty = nullptr) {
     int cfg = 0;
     for (const auto& r : R) cfg = std::max(cfg, r.P->cfg);
     const LaunchLayout L = layout_launch(R);
@@ -1826,7 +1840,7 @@ int run_queries(QueryArena& A, int device, cudaStream_t st, const std::vector<Qu
         ck(cudaEventCreate(&A.ev[1]), "event");
     }
     std::vector<uint16_t*> outs;
-    issue_query_launch(st, device, A.grid, cfg, R, L, A.dev.p, A.stage.p, A.ev, outs);
+    issue_query_launch(st, device, A.grid, cfg, R, L, A.dev.p, A.stage.p, A.ev, outs, dirty);
     A.ev_valid = true;
     A.last_words = L.o_words;
     A.last_phases = L.n_phases;
@@ -2262,6 +2276,35 @@ unsigned char* noalloc_scratch(int dev) {
 
 }  // namespace
 
+// State of queryAllPairsIncremental (reference HTripIncrementalState,
+// minplus_oracle.hpp:262-293): the viewpoints and their passability, the
+// index's build / root-growth epoch, its opening count and opening stamp
+// when the matrix was computed, the matrix, and a query arena of its own
+// that keeps the last launch's port vectors, projections, finite-port flags
+// and pair matrix (the plan is kept too), so that a later refresh re-runs
+// only the work of viewpoints whose leaf-to-root chain changed.
+struct htrip_incremental {
+    bool initialized = false;
+    const htrip_index* index = nullptr;
+    uint64_t epoch = 0, updates = 0, stamp_epoch = 0, host_opens = 0;
+    uint32_t seen_stamp = 0;
+    std::vector<int32_t> vps;
+    std::vector<uint8_t> pf;
+    std::vector<uint16_t> matrix;
+    QueryPlan plan;
+    QueryArena q;
+    DevBuf<uint8_t> dirty;
+    int* n_dirty = nullptr;      // host-mapped count of dirty viewpoints
+    int* n_dirty_dev = nullptr;
+    int device = -1;
+    ~htrip_incremental() {
+        if (device >= 0) cudaSetDevice(device);
+        q.release();
+        dirty.release();
+        if (n_dirty) cudaFreeHost(n_dirty);
+    }
+};
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
@@ -2548,19 +2591,67 @@ htrip_status htrip_query_all_pairs_incremental(htrip_index* h, htrip_incremental
         return HTRIP_OK;
     }
     HTRIP_GUARD_BEGIN
-    s->matrix.resize((size_t)k * k);
-    const htrip_status st = htrip_query_all_pairs(h, vps, k, observed, rows, cols, s->matrix.data());
-    if (st != HTRIP_OK) {
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    if (s->device >= 0 && s->device != h->device) {  // the arena lives on another device: start over
+        s->q.release();
+        s->dirty.release();
         s->initialized = false;
-        return st;
     }
+    s->device = h->device;
+    std::vector<uint8_t> pf = viewpoint_flags(h, vps, k, observed, rows, cols);
+    // Every update since the last call was an opening on the device path
+    // (no build, root growth, rebuild or weight change: equal epoch; no
+    // host-path opening; no reallocation of the stamps): re-lift only the
+    // viewpoints under matrices those openings listed.  Distances only
+    // decrease under openings, so the pairs of the other viewpoints keep
+    // their values and the new ones are the minimum with the old.
+    const bool selective = s->initialized && s->index == h && s->epoch == h->epoch && same_vps && s->pf == pf &&
+                           s->stamp_epoch == h->stamp_epoch && s->host_opens == h->host_opens;
+    s->matrix.resize((size_t)k * k);
+    const std::vector<QueryReq> R{{h, &s->plan, nullptr}};
+    int status = 0;
+    if (!selective) {
+        s->initialized = false;
+        make_plan(h, vps, pf.data(), k, s->plan);
+        status = run_queries(s->q, h->device, h->stream, R, {s->matrix.data()}, true);
+        if (recomputed) *recomputed = 1;
+    } else {
+        const LaunchLayout L = layout_launch(R);  // the same plan: the same layout as the last launch
+        const int ns = s->plan.n_sorted;
+        if (!s->n_dirty) {
+            ck(cudaHostAlloc(reinterpret_cast<void**>(&s->n_dirty), sizeof(int), cudaHostAllocMapped), "cudaHostAlloc");
+            ck(cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->n_dirty_dev), s->n_dirty, 0), "mapped count");
+        }
+        *s->n_dirty = 0;
+        s->dirty.reserve(std::max(1, ns));
+        hb::IncrementalChain C{};
+        C.H = h->H;
+        C.g = h->g;
+        C.leaves_x = h->leaves_x;
+        for (int l = 0; l <= h->H; ++l) {
+            C.mstamp[l] = h->L[l].mstamp.p;
+            C.nodes_x[l] = h->L[l].nodes_x;
+        }
+        const int* vp0 = reinterpret_cast<const int*>(s->q.dev.p + L.plan[0]) + s->plan.o_vp0;
+        hb::launch_incremental_dirty(vp0, ns, C, s->seen_stamp, s->dirty.p, s->n_dirty_dev, h->stream);
+        ck(cudaGetLastError(), "dirty viewpoints");
+        ck(cudaStreamSynchronize(h->stream), "dirty viewpoints");
+        if (*s->n_dirty > 0) {
+            status = run_queries(s->q, h->device, h->stream, R, {s->matrix.data()}, true, s->dirty.p);
+            if (recomputed) *recomputed = 2;
+        }
+    }
+    if (status != 0) return fail(HTRIP_ERR_CUDA, "query kernel: a bounded wait timed out");
     s->vps.assign(vps, vps + 2 * (size_t)k);
+    s->pf = std::move(pf);
     s->index = h;
     s->epoch = h->epoch;
     s->updates = h->update_counter;
+    s->stamp_epoch = h->stamp_epoch;
+    s->host_opens = h->host_opens;
+    s->seen_stamp = h->open_stamp;
     s->initialized = true;
     std::memcpy(out, s->matrix.data(), (size_t)k * k * sizeof(uint16_t));
-    if (recomputed) *recomputed = 1;
     return HTRIP_OK;
     HTRIP_GUARD_END
 }

@@ -178,6 +178,18 @@ struct OpenLaunch {
 };
 constexpr int kOpenTrace = 1024;
 
+// An index's per-level "listed by opening call" stamps, for the dirty
+// flags of an incremental query (launch_incremental_dirty): viewpoint j
+// (sorted order, leaf vp0[4 j]) gets dirty[j] = 1 when a matrix of its
+// leaf-to-root chain carries a stamp newer than `seen`; *n_dirty counts them.
+struct IncrementalChain {
+    int H, g, leaves_x;
+    const uint32_t* mstamp[kOpenMaxLevels];
+    int nodes_x[kOpenMaxLevels];
+};
+void launch_incremental_dirty(const int* vp0, int ns, const IncrementalChain& C, unsigned seen, uint8_t* dirty,
+                              int* n_dirty, cudaStream_t st);
+
 // Shared memory and grid of the launch on `device`; the launch itself.
 size_t open_smem_bytes();
 int open_grid_blocks(int device);

@@ -166,6 +166,14 @@ __device__ void mark_dec(const OpenLaunch& L, int l, int task, int node) {
 // ---------------------------------------------------------------------------
 __device__ void stamp_phase(const OpenLaunch& L) {
     const int gt = blockIdx.x * kThreads + threadIdx.x, gs = gridDim.x * kThreads;
+    // the touched leaves too: an incremental query re-lifts the viewpoints
+    // under any listed matrix (htrip_query_all_pairs_incremental)
+    const int n0 = min(*(volatile int*)L.count, L.cap[0]);
+    for (int s = gt; s < n0; s += gs) {
+        const int4 e = L.slots[0][s];
+        const OpenTask& T = L.tasks[e.x];
+        T.lv[0].mstamp[e.y] = T.stamp;
+    }
     for (int l = 1; l <= L.maxH; ++l)
         for (int s = gt; s < L.n_seam[l]; s += gs) {
             const int4 e = ld_slot(L.slots[l] + s);
@@ -355,7 +363,7 @@ __device__ void compact_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
 }
 
 // ---------------------------------------------------------------------------
-// Panel phase of round r: unit = (slot, column tile of 64*CP columns).
+// Panel unit of round r: (slot, column tile of 64*CP columns; 64 in use).
 //   T* = closure of T = D[Kc, Kc] (Floyd-Warshall over the round's pivots, in
 //        shared memory; the reference's sequential relaxation restricted to
 //        the pivots),
@@ -417,6 +425,26 @@ __device__ __forceinline__ void panel_gemm(uint16_t (*Ts)[kTLD], const uint16_t*
     for (int rr = 0; rr < 8; ++rr)
 #pragma unroll
         for (int cc = 0; cc < CP; ++cc) acc[rr][cc] = INF2;
+    if constexpr (CP == 1) {
+        // one column pair per lane: little work per pivot, so the loop is
+        // latency-bound; it runs branch-free (the clamped form is exact for
+        // every value, INF included) and unrolled, so the shared-memory loads
+        // of later pivots overlap the arithmetic of earlier ones
+        (void)cls;
+#pragma unroll 4
+        for (int k = 0; k < mk; ++k) {
+            const uint32_t bv = reinterpret_cast<const uint32_t*>(Bs + k * ldb + lane * 2)[0];
+            const uint4 av = *reinterpret_cast<const uint4*>(&Ts[k][warp * 8]);
+            const uint32_t aw[4] = {av.x, av.y, av.z, av.w};
+#pragma unroll
+            for (int r2 = 0; r2 < 4; ++r2) {
+                const uint32_t a0 = splat(aw[r2]), a1 = splat(aw[r2] >> 16);
+                acc[2 * r2][0] = acc_clamp(acc[2 * r2][0], bv, a0, INF2 - a0);
+                acc[2 * r2 + 1][0] = acc_clamp(acc[2 * r2 + 1][0], bv, a1, INF2 - a1);
+            }
+        }
+        return;
+    }
     for (int k = 0; k < mk; ++k) {
         const int c = cls[k * kWarps + warp];
         if (c == 0) continue;  // uniform over the warp
@@ -541,16 +569,17 @@ __device__ void update_unit(const OpenLaunch& L, int l, int s, int I, int J, int
     {   // bounded wait for the two panel tiles this tile reads (units of lower
         // tickets, handed out first: every wait ends)
         __shared__ int s_ok;
-        if (threadIdx.x == 0) {
-            const int NT = NP >= 256 ? 256 : NP;
-            const unsigned* wi = L.pdone + (size_t)s * (NP / 64) + (I * TT / NT) * NT / 64;
-            const unsigned* wj = L.pdone + (size_t)s * (NP / 64) + (J * TT / NT) * NT / 64;
+        if (threadIdx.x == 0) {  // the 64-column panel tiles of the tile's rows and columns
+            const volatile unsigned* w = L.pdone + (size_t)s * (NP / 64);
             int ok = 1;
             unsigned it = 0;
-            while (*(volatile const unsigned*)wi != rid || *(volatile const unsigned*)wj != rid) {
-                if (*(volatile int*)L.status != 0) { ok = 0; break; }
-                if (++it > kBarrierPolls) { atomicCAS(L.status, 0, 1); ok = 0; break; }
-                __nanosleep(32);
+            for (int t = 0; t < 2 * (TT / 64) && ok; ++t) {
+                const int blk = (t < TT / 64 ? I : J) * (TT / 64) + t % (TT / 64);
+                while (w[blk] != rid) {
+                    if (*(volatile int*)L.status != 0) { ok = 0; break; }
+                    if (++it > kBarrierPolls) { atomicCAS(L.status, 0, 1); ok = 0; break; }
+                    __nanosleep(32);
+                }
             }
             __threadfence();
             s_ok = ok;
@@ -682,28 +711,36 @@ __device__ void update_unit(const OpenLaunch& L, int l, int s, int I, int J, int
     if (__any_sync(FULL, dec) && lane == 0) s_dec = 1;
     __syncthreads();  // the staging buffers are free from here on
     if (I != J && s_any) {
-        // the transposed tile, through shared memory: Tt[j][i], rows padded by 8
-        constexpr int LD = TT + 8;
+        // The transposed tile through shared memory, Tt[j][i] in 16-byte
+        // chunks of 8 rows i: a thread holds RW consecutive rows of each of
+        // its columns, i.e. whole chunks of a transposed row.  Chunk q of row
+        // j sits at q ^ ((j / (2 CP)) & 7), so the 8 lanes of a 16-byte store
+        // phase (8 different rows) hit 8 different bank groups.
         uint16_t* Tt = reinterpret_cast<uint16_t*>(smem);
 #pragma unroll
-        for (int rr = 0; rr < RW; ++rr) {
-            const int i = warp * RW + rr;
+        for (int cc = 0; cc < CP; ++cc)
 #pragma unroll
-            for (int cc = 0; cc < CP; ++cc) {
-                const int j = lane * 2 * CP + 2 * cc;
-                Tt[j * LD + i] = (uint16_t)(acc[rr][cc] & 0xffffu);
-                Tt[(j + 1) * LD + i] = (uint16_t)(acc[rr][cc] >> 16);
+            for (int x = 0; x < 2; ++x) {
+                const int j = lane * 2 * CP + 2 * cc + x;
+                const int key = (j / (2 * CP)) & 7;
+#pragma unroll
+                for (int h = 0; h < RW / 8; ++h) {
+                    uint32_t w4[4];
+#pragma unroll
+                    for (int t = 0; t < 4; ++t) {
+                        const uint32_t a = x ? (acc[8 * h + 2 * t][cc] >> 16) : (acc[8 * h + 2 * t][cc] & 0xffffu);
+                        const uint32_t b = x ? (acc[8 * h + 2 * t + 1][cc] >> 16) : (acc[8 * h + 2 * t + 1][cc] & 0xffffu);
+                        w4[t] = a | (b << 16);
+                    }
+                    const int q = warp * (RW / 8) + h;
+                    *reinterpret_cast<uint4*>(Tt + j * TT + ((q ^ key) * 8)) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+                }
             }
-        }
         __syncthreads();
         for (int idx = tid; idx < TT * (TT / 8); idx += kThreads) {
             const int j = idx / (TT / 8), c8 = idx % (TT / 8);
-            const uint16_t* src = Tt + j * LD + c8 * 8;
-            uint4 v;
-            v.x = src[0] | ((uint32_t)src[1] << 16);
-            v.y = src[2] | ((uint32_t)src[3] << 16);
-            v.z = src[4] | ((uint32_t)src[5] << 16);
-            v.w = src[6] | ((uint32_t)src[7] << 16);
+            const int key = (j / (2 * CP)) & 7;
+            const uint4 v = *reinterpret_cast<const uint4*>(Tt + j * TT + ((c8 ^ key) * 8));
             reinterpret_cast<uint4*>(D + (size_t)(jb + j) * NP + i0)[c8] = v;
         }
     }
@@ -721,14 +758,14 @@ __device__ __forceinline__ void tri_pair(int t, int nt, int& I, int& J) {
     J = i + t;
 }
 
-// One closure round of level l as one phase: the panel units (slot x column
-// tile) take the lower tickets, the update units (slot x upper-triangle tile
+// One closure round of level l as one phase: the panel units (slot x
+// 64-column tile) take the lower tickets, the update units (slot x upper-triangle tile
 // pair) the higher ones; an update unit waits only for the two panel tiles
 // it reads, so no grid barrier separates the panel from the update.
 __device__ void round_phase(const OpenLaunch& L, int l, int N, int r, unsigned rid, int* s_unit,
                             unsigned char* smem) {
     const int NP = L.geo[l].NP;
-    const int NT = NP >= 256 ? 256 : NP;
+    const int NT = 64;  // panel tiles of 64 columns: many short units (the CTAs are otherwise idle)
     const int tiles = NP / NT;
     const int TT = NP >= 128 ? 128 : 64;
     const int nt = NP / TT;
@@ -738,9 +775,7 @@ __device__ void round_phase(const OpenLaunch& L, int l, int N, int r, unsigned r
     for (int u = next_unit(L, s_unit); u < units; u = next_unit(L, s_unit)) {
         if (u < n_panel) {
             const int s = u / tiles, j0 = (u % tiles) * NT;
-            if (NT == 256) panel_unit<4>(L, l, s, j0, r, rid, smem);
-            else if (NT == 128) panel_unit<2>(L, l, s, j0, r, rid, smem);
-            else panel_unit<1>(L, l, s, j0, r, rid, smem);
+            panel_unit<1>(L, l, s, j0, r, rid, smem);
             continue;
         }
         const int v = u - n_panel;
@@ -1029,6 +1064,33 @@ __global__ void __launch_bounds__(kThreads, 2) open_persistent_kernel(const Open
 }
 
 }  // namespace
+
+// Dirty flags of an incremental query: viewpoint j (sorted order, leaf
+// vp0[4 j]) is dirty when a matrix of its leaf-to-root chain was listed by an
+// opening call after the stamp `seen` (stamps compare modulo 2^32).
+__global__ void incremental_dirty_kernel(const int* __restrict__ vp0, int ns, IncrementalChain C, unsigned seen,
+                                         uint8_t* dirty, int* n_dirty) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ns) return;
+    const int leaf = vp0[4 * j];
+    int tx = leaf % C.leaves_x, ty = leaf / C.leaves_x;
+    bool d = false;
+    for (int l = 0; l <= C.H; ++l) {
+        if (l > 0) {
+            tx /= C.g;
+            ty /= C.g;
+        }
+        d |= (int)(C.mstamp[l][ty * C.nodes_x[l] + tx] - seen) > 0;
+    }
+    dirty[j] = d ? 1 : 0;
+    if (d) atomicAdd(n_dirty, 1);
+}
+
+void launch_incremental_dirty(const int* vp0, int ns, const IncrementalChain& C, unsigned seen, uint8_t* dirty,
+                              int* n_dirty, cudaStream_t st) {
+    if (ns <= 0) return;
+    incremental_dirty_kernel<<<(ns + 255) / 256, 256, 0, st>>>(vp0, ns, C, seen, dirty, n_dirty);
+}
 
 size_t open_smem_bytes() { return kOpenSmem; }
 

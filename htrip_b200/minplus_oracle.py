@@ -434,7 +434,10 @@ class MinPlusOracle:
     def queryAllPairsIncremental(self, viewpoints, grid, state: "IncrementalState",
                                  out: np.ndarray | None = None) -> np.ndarray:
         """Reference queryAllPairsIncremental: the cached matrix when nothing
-        changed since `state` was filled, else a fresh full query."""
+        changed since `state` was filled; after openings only, a re-lift of
+        the viewpoints whose leaf-to-root chain changed; else a full query.
+        state.last_mode: 0 cached, 1 full query, 2 re-lift of the changed
+        viewpoints (state.last_recomputed: mode != 0)."""
         rc = _rc(viewpoints)
         k = len(rc)
         if out is None or out.shape != (k, k) or out.dtype != np.uint16 or not out.flags.c_contiguous:
@@ -443,7 +446,8 @@ class MinPlusOracle:
         rec = C.c_int32()
         _check(self.lib.htrip_query_all_pairs_incremental(self.h, state.h, rc.ctypes.data_as(_I32P), k, ptr, rows,
                                                           cols, out.ctypes.data_as(_U16P), C.byref(rec)))
-        state.last_recomputed = bool(rec.value)
+        state.last_mode = int(rec.value)
+        state.last_recomputed = rec.value != 0
         return out
 
     def queryAllPairsNoAlloc(self, viewpoints, grid, out: np.ndarray | None = None) -> np.ndarray:
@@ -620,6 +624,7 @@ class IncrementalState:
         _check(self.lib.htrip_incremental_create(C.byref(h)))
         self.h = h
         self.last_recomputed = False
+        self.last_mode = 0
 
     def __del__(self):
         h = getattr(self, "h", None)

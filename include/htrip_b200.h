@@ -155,11 +155,17 @@ htrip_status htrip_query_distance(htrip_index* h, int32_t r1, int32_t c1, int32_
 /* void queryAllPairsIncremental(vps, grid, out, scratch, state) const
  *                                              minplus_oracle.hpp:290-294
  * `state` caches the last matrix with the index's build / root-growth epoch
- * and its count of opening calls.  Same viewpoints, same epoch and no
- * opening since: the cached matrix is returned without device work (the
- * reference's fast path).  Otherwise the whole matrix is recomputed by one
- * query launch (the reference re-lifts only viewpoints under changed nodes;
- * both give the full query's matrix).  *recomputed (optional) tells which. */
+ * and its count of opening calls, and keeps a query arena of its own with
+ * the last launch's port vectors, projections and pair matrix.
+ *  - Same viewpoints, same epoch and no opening since: the cached matrix,
+ *    without device work (the reference's fast path).
+ *  - Same viewpoints (and passability) and only openings since: the
+ *    viewpoints whose leaf-to-root chain holds a matrix those openings
+ *    listed are re-lifted and only their pairs recomputed (the reference's
+ *    version-stamped re-lift, minplus_oracle.cpp:1444-2002); none: cached.
+ *  - Otherwise one full query launch.
+ * Every case gives the full query's matrix.  *recomputed (optional): 0
+ * cached, 1 full query, 2 re-lift of the changed viewpoints.             */
 typedef struct htrip_incremental htrip_incremental; /* opaque */
 htrip_status htrip_incremental_create(htrip_incremental** out);
 htrip_status htrip_incremental_destroy(htrip_incremental* s);
