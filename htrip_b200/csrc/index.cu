@@ -1145,7 +1145,7 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
         int maxH = 0;
         int cap[hb::kOpenMaxLevels] = {}, n_seam[hb::kOpenMaxLevels] = {};
         size_t o_tasks = 0, o_out = 0, o_words = 0, o_trace = 0, o_slots[hb::kOpenMaxLevels] = {}, o_trip = 0;
-        size_t o_dchild[hb::kOpenMaxLevels] = {}, o_rec[hb::kOpenMaxLevels] = {}, o_pdone = 0;
+        size_t o_dchild[hb::kOpenMaxLevels] = {}, o_rec[hb::kOpenMaxLevels] = {};
         size_t begin = 0, end = 0;
         int n_trip = 0;
     };
@@ -1189,7 +1189,6 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
                 cur = std::move(next);
             }
         }
-        size_t pdone_words = 1;
         for (int l = 0; l <= g.maxH; ++l) {
             // every task of the group that reaches level l has the same (b, g)
             // geometry there: take it from any of them
@@ -1198,7 +1197,6 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
                 if (T->h->H >= l) np = T->h->L[l].NP;
             panel_elems = std::max(panel_elems, (size_t)g.cap[l] * hb::kOpenB * np);
             pflag_bytes = std::max(pflag_bytes, (size_t)g.cap[l] * (np / 64));
-            pdone_words = std::max(pdone_words, (size_t)g.cap[l] * (np / 64));
         }
         g.begin = off;
         g.o_tasks = take(g.ts.size() * sizeof(hb::OpenTask));
@@ -1208,7 +1206,6 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
         for (int l = 0; l <= g.maxH; ++l) g.o_slots[l] = take((size_t)std::max(1, g.cap[l]) * sizeof(int4));
         for (int l = 1; l <= g.maxH; ++l) g.o_dchild[l] = take((size_t)std::max(1, g.cap[l - 1]) * sizeof(int4));
         for (int l = 0; l <= g.maxH; ++l) g.o_rec[l] = take((size_t)std::max(1, g.cap[l]) * sizeof(hb::OpenSlotRec));
-        g.o_pdone = take(pdone_words * sizeof(unsigned));  // zero at launch (the staging is cleared)
         g.o_trip = take((size_t)g.n_trip * 3 * sizeof(int));
         g.end = off;
         gl.push_back(std::move(g));
@@ -1216,8 +1213,12 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
     A.dev.reserve(off);
     A.stage.reserve(off);
     A.rb.reserve(off);
-    A.panel.reserve(panel_elems);
-    A.pflags.reserve(pflag_bytes);
+    // two panel and flag buffers: a round's panel is made while the update
+    // of the round before reads the other one
+    panel_elems = (panel_elems + 127) / 128 * 128;
+    pflag_bytes = (pflag_bytes + 255) / 256 * 256;
+    A.panel.reserve(2 * panel_elems);
+    A.pflags.reserve(2 * pflag_bytes);
     if (!A.open_grid) A.open_grid = hb::open_grid_blocks(device);
     unsigned char* base = A.dev.p;
     for (GL& g : gl) {
@@ -1310,7 +1311,8 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
         OL.panel = A.panel.p;
         OL.pflags = A.pflags.p;
         OL.trace = reinterpret_cast<unsigned long long*>(base + g.o_trace);
-        OL.pdone = reinterpret_cast<unsigned*>(base + g.o_pdone);
+        OL.panel_stride = panel_elems;
+        OL.pflag_stride = pflag_bytes;
         ck(cudaMemcpyAsync(base + g.begin, hs + g.begin, g.end - g.begin, cudaMemcpyHostToDevice, st), "open upload");
         coop_launch(device, st, [&] { return hb::launch_open(OL, A.open_grid, st); }, "opening kernel");
         // statistics and the status word back (the trace stays on the device)

@@ -164,14 +164,16 @@ struct OpenLaunch {
                                    // summary decreased (capacity: the child level's cap)
     int* dcount;                   // [kOpenMaxLevels] entries of dchild
     OpenSlotRec* rec[kOpenMaxLevels];  // per level and slot (capacity: the level's cap)
-    unsigned* pdone;               // per slot and 64-column block: id of the last round whose panel
-                                   // tile starting there is written (zero at launch)
     int cap[kOpenMaxLevels];       // capacity of each level's list
     int n_seam[kOpenMaxLevels];    // seam nodes at the head of each level's list (stamped first)
     int* maxk;                     // [kOpenMaxLevels] largest pivot count per level
     const int* triples;            // (u, v, w)
-    uint16_t* panel;               // per slot kOpenB x NP (the round's closed pivot rows)
-    uint8_t* pflags;               // per slot NP / 64: 64-column blocks of the panel holding a finite value
+    uint16_t* panel;               // two buffers (rounds alternate) of, per slot, kOpenB x NP: the
+                                   // round's closed pivot rows
+    uint8_t* pflags;               // two buffers of, per slot, NP / 64 flags: 64-column blocks of
+                                   // the panel holding a finite value
+    size_t panel_stride;           // elements between the two panel buffers
+    size_t pflag_stride;           // bytes between the two flag buffers
     int* status;                   // 0 ok, 1 a bounded barrier wait timed out, 2 a list overflowed
     unsigned* bar;                 // {arrived, generation, unit ticket}
     unsigned long long* trace;     // or null: [0] start, then one stamp per phase (max kOpenTrace)

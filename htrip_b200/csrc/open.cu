@@ -24,6 +24,9 @@
 //              update: D = min(D, P^T (x) P) over upper-triangle tiles, each
 //                also written transposed (D is symmetric), and only where an
 //                entry changed.
+//              Pipelined one round deep: the panel of round r runs in the
+//              same phase as the update of round r - 1 and applies that
+//              update to its own pivot rows (R rounds: R + 1 phases).
 //   A matrix whose exterior block decreased (refreshBoundarySummary,
 //   leaf_tile.cpp:253-273, internal_node.cpp:415-433) is seen where the
 //   decrease happens: an insert or an update tile lowers an entry whose row
@@ -65,41 +68,49 @@ __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
-// Grid barrier over every CTA of the launch; the last CTA to arrive resets
-// the unit ticket for the next phase.  Bounded: a CTA that polls too long
-// records status 1; a CTA that sees a non-zero status stops waiting.  Returns
-// false when the launch must end.
-__device__ bool open_barrier(const OpenLaunch& L) {
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid barrier ending phase `phase` (0, 1, ... in launch order): every CTA
+// adds one to the arrival count L.bar[0] (zero at launch, never reset) and
+// waits until it reaches (phase + 1) x grid, so the barrier costs one atomic
+// and the polls.  Bounded: a CTA that polls too long records status 1; a CTA
+// that sees a non-zero status stops waiting.  Returns false when the launch
+// must end.
+// Work tickets: phase p hands out units from counter L.bar[1 + p % 2]; CTA i
+// takes unit i first without a ticket.  CTA 0 clears the counter of phase
+// p + 1 before it arrives at barrier p (its last use was phase p - 1, and
+// the barrier publishes the store before phase p + 1 starts).
+// s_unit (shared): [0] the unit, [1] -1 until the CTA's first unit of the
+// phase is taken, [2] the phase's counter.
+__device__ bool open_barrier(const OpenLaunch& L, int phase, int* s_unit) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned* vgen = L.bar + 1;
-        const unsigned gen = *vgen;
+        if (blockIdx.x == 0) *(volatile unsigned*)(L.bar + 1 + ((phase + 1) & 1)) = 0u;
         __threadfence();
-        const unsigned arrived = atomicAdd(L.bar, 1u);
+        atomicAdd(L.bar, 1u);
+        const unsigned target = (unsigned)(phase + 1) * gridDim.x;
         int ok = 1;
-        if (arrived == gridDim.x - 1) {
-            atomicExch(L.bar, 0u);
-            atomicExch(L.bar + 2, 0u);
-            __threadfence();
-            atomicAdd(L.bar + 1, 1u);
-        } else {
-            unsigned it = 0;
-            while (*vgen == gen) {
-                if (*(volatile int*)L.status != 0) {
-                    ok = 0;
-                    break;
-                }
-                if (++it > kBarrierPolls) {
-                    atomicCAS(L.status, 0, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(32);
+        unsigned it = 0;
+        while (ld_acquire(L.bar) < target) {
+            if (*(volatile int*)L.status != 0) {
+                ok = 0;
+                break;
             }
+            if (++it > kBarrierPolls) {
+                atomicCAS(L.status, 0, 1);
+                ok = 0;
+                break;
+            }
+            __nanosleep(32);
         }
-        __threadfence();
         s_ok = ok && *(volatile int*)L.status == 0;
+        s_unit[1] = -1;
+        s_unit[2] = (phase + 1) & 1;
     }
     __syncthreads();
     return s_ok != 0;
@@ -108,9 +119,16 @@ __device__ bool open_barrier(const OpenLaunch& L) {
 // Next work unit of the phase for this CTA (all threads get it).
 __device__ __forceinline__ int next_unit(const OpenLaunch& L, int* s_unit) {
     __syncthreads();
-    if (threadIdx.x == 0) *s_unit = (int)atomicAdd(L.bar + 2, 1u);
+    if (threadIdx.x == 0) {
+        if (s_unit[1] < 0) {
+            s_unit[0] = (int)blockIdx.x;
+            s_unit[1] = 0;
+        } else {
+            s_unit[0] = (int)gridDim.x + (int)atomicAdd(L.bar + 1 + s_unit[2], 1u);
+        }
+    }
     __syncthreads();
-    return *s_unit;
+    return s_unit[0];
 }
 
 // Data that other CTAs of this launch wrote (work lists, slot records,
@@ -475,72 +493,106 @@ __device__ __forceinline__ void panel_gemm(uint16_t (*Ts)[kTLD], const uint16_t*
     }
 }
 
-template <int CP>
-__device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, unsigned rid, unsigned char* smem) {
-    constexpr int NT = 64 * CP;
+__device__ __forceinline__ uint16_t* panel_of(const OpenLaunch& L, int r, int s, int NP) {
+    return L.panel + (size_t)(r & 1) * L.panel_stride + (size_t)s * B * NP;
+}
+__device__ __forceinline__ uint8_t* pflags_of(const OpenLaunch& L, int r, int s, int NP) {
+    return L.pflags + (size_t)(r & 1) * L.pflag_stride + (size_t)s * (NP / 64);
+}
+
+// Panel unit of round r >= 1 runs beside the update of round r - 1 (the
+// look-ahead): the pivot rows D[Kc, :] it reads may not hold that update
+// yet, so it applies it itself from round r - 1's panel Pp (all of its
+// B rows in use: only the last round of a slot has fewer pivots),
+//   D[Kc[a]][j] = min(D[Kc[a]][j], min_c Pp[c][Kc[a]] (+) Pp[c][j]),
+// to the tile's columns and to the pivot block.  A value it reads either
+// still misses the update or already holds it; the minimum is the updated
+// value both ways, so the panel equals the one made after the update.
+__device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, unsigned char* smem) {
+    constexpr int NT = 64;
     const int NP = L.geo[l].NP;
     const OpenSlotRec rec = ld_rec(L.rec[l] + s);
     const int mk = min(B, rec.kcnt - r * B);
     if (mk <= 0) return;  // uniform
+    const bool ahead = r > 0;
     uint16_t (*Ts)[kTLD] = reinterpret_cast<uint16_t (*)[kTLD]>(smem);
-    uint16_t* Bs = reinterpret_cast<uint16_t*>(smem + B * kTLD * sizeof(uint16_t));  // [B][NT]
-    int* kc = reinterpret_cast<int*>(smem + B * kTLD * sizeof(uint16_t) + B * NT * sizeof(uint16_t));
-    uint8_t* cls = reinterpret_cast<uint8_t*>(kc + B);                                 // [B][kWarps]
-    __shared__ int tile_any[4];
+    uint16_t (*Ag)[kTLD] = reinterpret_cast<uint16_t (*)[kTLD]>(smem + B * kTLD * sizeof(uint16_t));  // Pp[c][Kc[a]]
+    uint16_t* Bs = reinterpret_cast<uint16_t*>(smem + 2 * B * kTLD * sizeof(uint16_t));                // [B][NT]
+    uint16_t* Pj = Bs + B * NT;                                                                        // Pp[c][j0 + j]
+    int* kc = reinterpret_cast<int*>(Pj + B * NT);
+    uint8_t* cls = reinterpret_cast<uint8_t*>(kc + B);  // [B][kWarps]
+    __shared__ int tile_any;
     const uint16_t* D = rec.mat;
+    const uint16_t* Pp = ahead ? panel_of(L, r - 1, s, NP) : nullptr;
     const int tid = threadIdx.x;
     if (tid < mk) kc[tid] = __ldcg(rec.klist + r * B + tid);
-    if (tid < 4) tile_any[tid] = 0;
+    if (tid == 0) tile_any = 0;
     __syncthreads();
-    {   // the tile's pivot rows by asynchronous copies, meanwhile the pivot
-        // block (scattered entries) with all of a thread's loads issued first
+    {   // the tile's pivot rows (and round r - 1's panel tile) by asynchronous
+        // copies, meanwhile the scattered pivot block (and its round r - 1
+        // panel columns) with all of a thread's loads issued first
         for (int idx = tid; idx < mk * (NT / 8); idx += kThreads) {
             const int a = idx / (NT / 8), c8 = idx % (NT / 8);
             cp_async16(Bs + a * NT + c8 * 8, D + (size_t)kc[a] * NP + j0 + c8 * 8);
         }
+        if (ahead)
+            for (int idx = tid; idx < B * (NT / 8); idx += kThreads) {
+                const int c = idx / (NT / 8), c8 = idx % (NT / 8);
+                cp_async16(Pj + c * NT + c8 * 8, Pp + (size_t)c * NP + j0 + c8 * 8);
+            }
         constexpr int NTB = B * B / kThreads;
-        uint16_t tv[NTB];
+        uint16_t tv[NTB], pv[NTB];
 #pragma unroll
         for (int x = 0; x < NTB; ++x) {
             const int idx = tid + x * kThreads, a = idx / B, c = idx % B;
             tv[x] = (a < mk && c < mk) ? __ldcg(D + (size_t)kc[a] * NP + kc[c]) : (a == c ? 0 : INF);
+            // pv: Pp[a][Kc[c]] (row a of the old panel at pivot c)
+            pv[x] = (ahead && c < mk) ? __ldcg(Pp + (size_t)a * NP + kc[c]) : INF;
         }
 #pragma unroll
         for (int x = 0; x < NTB; ++x) {
             const int idx = tid + x * kThreads;
             Ts[idx / B][idx % B] = tv[x];
+            Ag[idx / B][idx % B] = pv[x];
         }
         cp_async_wait_all();
     }
     __syncthreads();
+    const int warp = tid >> 5, lane = tid & 31;
+    uint32_t acc[8][1];
+    if (ahead) {  // round r - 1's update of the pivot rows: tile columns, then the pivot block
+        panel_gemm<1>(Ag, Pj, NT, B, nullptr, acc);
+        uint32_t* b32 = reinterpret_cast<uint32_t*>(Bs);
+#pragma unroll
+        for (int rr = 0; rr < 8; ++rr) {
+            const int a = warp * 8 + rr;
+            if (a < mk) b32[a * (NT / 2) + lane] = min2(b32[a * (NT / 2) + lane], acc[rr][0]);
+        }
+        panel_gemm<1>(Ag, &Ag[0][0], kTLD, B, nullptr, acc);
+#pragma unroll
+        for (int rr = 0; rr < 8; ++rr) {  // rows / columns >= mk: INF from Ag, the identity stays
+            uint32_t* t32 = reinterpret_cast<uint32_t*>(&Ts[warp * 8 + rr][0]);
+            t32[lane] = min2(t32[lane], acc[rr][0]);
+        }
+        __syncthreads();
+    }
     close_pivot_block(Ts, mk);
     panel_classes(Ts, mk, cls);
     __syncthreads();
-    const int warp = tid >> 5, lane = tid & 31;
-    uint32_t acc[8][CP];
-    panel_gemm<CP>(Ts, Bs, NT, mk, cls, acc);
-    uint16_t* P = L.panel + (size_t)s * B * NP;
+    panel_gemm<1>(Ts, Bs, NT, mk, cls, acc);
+    uint16_t* P = panel_of(L, r, s, NP);
     bool any = false;
-    const int col = j0 + lane * 2 * CP;
+    const int col = j0 + lane * 2;
 #pragma unroll
     for (int rr = 0; rr < 8; ++rr) {
         const int a = warp * 8 + rr;
         if (a >= mk) continue;
-        uint32_t* dst = reinterpret_cast<uint32_t*>(P + (size_t)a * NP + col);
-#pragma unroll
-        for (int cc = 0; cc < CP; ++cc) {
-            dst[cc] = acc[rr][cc];
-            any |= acc[rr][cc] != INF2;
-        }
+        reinterpret_cast<uint32_t*>(P + (size_t)a * NP + col)[0] = acc[rr][0];
+        any |= acc[rr][0] != INF2;
     }
-    if (any) tile_any[(lane * 2 * CP) / 64] = 1;
+    if (__any_sync(FULL, any) && lane == 0) tile_any = 1;
     __syncthreads();
-    if (tid < NT / 64) L.pflags[(size_t)s * (NP / 64) + j0 / 64 + tid] = tile_any[tid] ? 1 : 0;
-    __syncthreads();
-    if (tid == 0) {  // the tile (and its flags) is written: release it to the update units
-        __threadfence();
-        atomicExch(L.pdone + (size_t)s * (NP / 64) + j0 / 64, rid);
-    }
+    if (tid == 0) pflags_of(L, r, s, NP)[j0 / 64] = tile_any ? 1 : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -556,37 +608,15 @@ __device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, uns
 // wrap), 2 otherwise (3-op clamped form).
 // ---------------------------------------------------------------------------
 template <int RW, int CP>
-__device__ void update_unit(const OpenLaunch& L, int l, int s, int I, int J, int r, unsigned rid,
-                            unsigned char* smem) {
+__device__ void update_unit(const OpenLaunch& L, int l, int s, int I, int J, int r, unsigned char* smem) {
     constexpr int TT = 8 * RW;  // == 64 * CP
     static_assert(TT == 64 * CP, "square tiles");
     const OpenLevelGeom& G = L.geo[l];
     const int NP = G.NP;
-    const uint8_t* pf = L.pflags + (size_t)s * (NP / 64);
+    const uint8_t* pf = pflags_of(L, r, s, NP);
     const OpenSlotRec rec = ld_rec(L.rec[l] + s);
     const int mk = min(B, rec.kcnt - r * B);
     if (mk <= 0) return;  // uniform; no panel was made for this slot either
-    {   // bounded wait for the two panel tiles this tile reads (units of lower
-        // tickets, handed out first: every wait ends)
-        __shared__ int s_ok;
-        if (threadIdx.x == 0) {  // the 64-column panel tiles of the tile's rows and columns
-            const volatile unsigned* w = L.pdone + (size_t)s * (NP / 64);
-            int ok = 1;
-            unsigned it = 0;
-            for (int t = 0; t < 2 * (TT / 64) && ok; ++t) {
-                const int blk = (t < TT / 64 ? I : J) * (TT / 64) + t % (TT / 64);
-                while (w[blk] != rid) {
-                    if (*(volatile int*)L.status != 0) { ok = 0; break; }
-                    if (++it > kBarrierPolls) { atomicCAS(L.status, 0, 1); ok = 0; break; }
-                    __nanosleep(32);
-                }
-            }
-            __threadfence();
-            s_ok = ok;
-        }
-        __syncthreads();
-        if (!s_ok) return;
-    }
     bool live_i = false, live_j = false;
 #pragma unroll
     for (int t = 0; t < TT / 64; ++t) {
@@ -599,7 +629,7 @@ __device__ void update_unit(const OpenLaunch& L, int l, int s, int I, int J, int
     uint8_t* cls = smem + (size_t)B * TT * (sizeof(uint32_t) + sizeof(uint16_t));          // [B][kWarps]
     uint16_t* Os = reinterpret_cast<uint16_t*>(cls + B * kWarps);                          // [TT][TT] old tile
     __shared__ int s_any, s_dec;
-    const uint16_t* P = L.panel + (size_t)s * B * NP;
+    const uint16_t* P = panel_of(L, r, s, NP);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int i0 = I * TT, jb = J * TT;
     if (tid == 0) { s_any = 0; s_dec = 0; }
@@ -758,32 +788,34 @@ __device__ __forceinline__ void tri_pair(int t, int nt, int& I, int& J) {
     J = i + t;
 }
 
-// One closure round of level l as one phase: the panel units (slot x
-// 64-column tile) take the lower tickets, the update units (slot x upper-triangle tile
-// pair) the higher ones; an update unit waits only for the two panel tiles
-// it reads, so no grid barrier separates the panel from the update.
-__device__ void round_phase(const OpenLaunch& L, int l, int N, int r, unsigned rid, int* s_unit,
+// Stage t of level l's closure (t = 0 .. rounds) as one phase: the panel
+// units of round t (slot x 64-column tile; none in the last stage) take the
+// lower tickets, the update units of round t - 1 (slot x upper-triangle tile
+// pair; none in stage 0) the higher ones.  The panel of round t applies
+// round t - 1's update to its own pivot rows, so the two run side by side;
+// the grid barrier after the stage orders round t - 1's update before round
+// t's (both write the same tiles) and publishes round t's panel.
+__device__ void stage_phase(const OpenLaunch& L, int l, int N, int t, int rounds, int* s_unit,
                             unsigned char* smem) {
     const int NP = L.geo[l].NP;
-    const int NT = 64;  // panel tiles of 64 columns: many short units (the CTAs are otherwise idle)
+    const int NT = 64;  // panel tiles of 64 columns: many short units
     const int tiles = NP / NT;
     const int TT = NP >= 128 ? 128 : 64;
     const int nt = NP / TT;
     const int per = nt * (nt + 1) / 2;
-    const int n_panel = N * tiles;
-    const int units = n_panel + N * per;
+    const int n_panel = t < rounds ? N * tiles : 0;
+    const int units = n_panel + (t > 0 ? N * per : 0);
     for (int u = next_unit(L, s_unit); u < units; u = next_unit(L, s_unit)) {
         if (u < n_panel) {
-            const int s = u / tiles, j0 = (u % tiles) * NT;
-            panel_unit<1>(L, l, s, j0, r, rid, smem);
+            panel_unit(L, l, u / tiles, (u % tiles) * NT, t, smem);
             continue;
         }
         const int v = u - n_panel;
         const int s = v / per;
         int I, J;
         tri_pair(v % per, nt, I, J);
-        if (TT == 128) update_unit<16, 2>(L, l, s, I, J, r, rid, smem);
-        else update_unit<8, 1>(L, l, s, I, J, r, rid, smem);
+        if (TT == 128) update_unit<16, 2>(L, l, s, I, J, t - 1, smem);
+        else update_unit<8, 1>(L, l, s, I, J, t - 1, smem);
     }
 }
 
@@ -1021,7 +1053,7 @@ __device__ void small_phase(const OpenLaunch& L, int l, int N, int* s_unit, unsi
     }
 }
 
-constexpr size_t kPanelSmem = (size_t)B * kTLD * sizeof(uint16_t) + (size_t)B * 256 * sizeof(uint16_t) +
+constexpr size_t kPanelSmem = (size_t)2 * B * kTLD * sizeof(uint16_t) + (size_t)2 * B * 64 * sizeof(uint16_t) +
                               B * sizeof(int) + (size_t)B * kWarps;
 constexpr size_t kUpdateSmem = (size_t)B * 128 * (sizeof(uint32_t) + sizeof(uint16_t)) + (size_t)B * kWarps +
                                (size_t)128 * 128 * sizeof(uint16_t);
@@ -1030,13 +1062,16 @@ constexpr size_t kOpenSmem = std::max(kPanelSmem, std::max(kUpdateSmem, kTranspo
 
 __global__ void __launch_bounds__(kThreads, 2) open_persistent_kernel(const OpenLaunch L) {
     extern __shared__ __align__(16) unsigned char osm[];
-    __shared__ int s_unit;
+    __shared__ int s_unit[3];
+    if (threadIdx.x == 0) {
+        s_unit[1] = -1;
+        s_unit[2] = 0;
+    }
     int phase = 0;
-    unsigned rid = 0;  // closure rounds of the launch so far (panel tile release ids)
     const bool stamp = L.trace && blockIdx.x == 0 && threadIdx.x == 0;
     if (stamp) L.trace[0] = global_timer();
     auto end_phase = [&]() -> bool {
-        const bool ok = open_barrier(L);
+        const bool ok = open_barrier(L, phase, s_unit);
         if (stamp && phase < kOpenTrace - 1) L.trace[1 + phase] = global_timer();
         ++phase;
         return ok;
@@ -1047,17 +1082,17 @@ __global__ void __launch_bounds__(kThreads, 2) open_persistent_kernel(const Open
         const int N = min(*(volatile int*)(L.count + l), L.cap[l]);
         if (N == 0) continue;
         if (L.geo[l].NP <= 128) {  // the whole level in one phase, one matrix per unit
-            small_phase(L, l, N, &s_unit, osm);
+            small_phase(L, l, N, s_unit, osm);
             if (!end_phase()) return;
             continue;
         }
-        insert_phase(L, l, N, &s_unit);
+        insert_phase(L, l, N, s_unit);
         if (!end_phase()) return;
-        compact_phase(L, l, N, &s_unit);
+        compact_phase(L, l, N, s_unit);
         if (!end_phase()) return;
         const int rounds = (*(volatile int*)(L.maxk + l) + B - 1) / B;
-        for (int r = 0; r < rounds; ++r) {
-            round_phase(L, l, N, r, ++rid, &s_unit, osm);
+        for (int t = 0; rounds > 0 && t <= rounds; ++t) {
+            stage_phase(L, l, N, t, rounds, s_unit, osm);
             if (!end_phase()) return;
         }
     }
