@@ -500,12 +500,83 @@ __device__ __forceinline__ uint8_t* pflags_of(const OpenLaunch& L, int r, int s,
     return L.pflags + (size_t)(r & 1) * L.pflag_stride + (size_t)s * (NP / 64);
 }
 
+// 64 x 64 block product of the panel unit (kn <= B pivot steps):
+//   acc[i][q] = min_k A[k][row i] (+) Bm[k][column pair q]
+// Warp w owns rows 8w .. 8w + 7 and skips (class 0) or takes the 2-op form
+// (class 1) for pivot k by cls[k * kWarps + w]; lane 8 rp + cg holds rows
+// 8w + 2rp, 8w + 2rp + 1 and columns 8cg .. 8cg + 7 (four packed pairs), so
+// a pivot step is one 4-byte and one 16-byte shared load for 8 updates.
+__device__ __forceinline__ void gemm64(const uint16_t (*A)[kTLD], const uint16_t* Bm, int ldb, int kn,
+                                       const uint8_t* cls, uint32_t (&acc)[2][4]) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint16_t* ap = &A[0][warp * 8 + 2 * (lane >> 3)];
+    const uint16_t* bp = Bm + (lane & 7) * 8;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[i][q] = INF2;
+#pragma unroll 2
+    for (int k = 0; k < kn; ++k) {
+        const int c = cls[k * kWarps + warp];
+        if (c == 0) continue;  // uniform over the warp
+        const uint32_t a2 = *reinterpret_cast<const uint32_t*>(ap + k * kTLD);
+        const uint4 b4 = *reinterpret_cast<const uint4*>(bp + k * ldb);
+        const uint32_t b[4] = {b4.x, b4.y, b4.z, b4.w};
+        const uint32_t aa[2] = {splat(a2), splat(a2 >> 16)};
+        if (c == 1) {
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[i][q] = acc_fast(acc[i][q], b[q], aa[i]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const uint32_t tt = INF2 - aa[i];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[i][q] = acc_clamp(acc[i][q], b[q], aa[i], tt);
+            }
+        }
+    }
+}
+
+// dst[row i][8 cg .. 8 cg + 7] = min(dst, acc[i]) for the rows of gemm64's
+// thread layout below `rows`.
+__device__ __forceinline__ void min_into(uint16_t* dst, int ld, int rows, const uint32_t (&acc)[2][4]) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const int a = warp * 8 + 2 * (lane >> 3) + i;
+        if (a >= rows) continue;
+        uint4* p = reinterpret_cast<uint4*>(dst + a * ld + (lane & 7) * 8);
+        const uint4 o = *p;
+        *p = make_uint4(min2(o.x, acc[i][0]), min2(o.y, acc[i][1]), min2(o.z, acc[i][2]), min2(o.w, acc[i][3]));
+    }
+}
+
+// Class of step k for warp w's rows of a 64 x 64 operand A (entries
+// A[k][8w .. 8w+7]): 0 all INF (skip), 1 all <= INF_HEADROOM (2-op form),
+// 2 otherwise.
+__device__ __forceinline__ void block_classes(const uint16_t (*A)[kTLD], int kn, uint8_t* cls) {
+    for (int idx = threadIdx.x; idx < kn * kWarps; idx += kThreads) {
+        const int k = idx / kWarps, w = idx % kWarps;
+        const uint4 v = *reinterpret_cast<const uint4*>(&A[k][w * 8]);
+        const uint32_t x[4] = {v.x, v.y, v.z, v.w};
+        uint32_t mn = 0xffffu, mx = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            mn = min(mn, min(x[q] & 0xffffu, x[q] >> 16));
+            mx = max(mx, max(x[q] & 0xffffu, x[q] >> 16));
+        }
+        cls[idx] = mn >= INF ? 0 : (mx <= INF_HEADROOM ? 1 : 2);
+    }
+}
+
 // Panel unit of round r >= 1 runs beside the update of round r - 1 (the
 // look-ahead): the pivot rows D[Kc, :] it reads may not hold that update
 // yet, so it applies it itself from round r - 1's panel Pp (all of its
 // B rows in use: only the last round of a slot has fewer pivots),
 //   D[Kc[a]][j] = min(D[Kc[a]][j], min_c Pp[c][Kc[a]] (+) Pp[c][j]),
-// to the tile's columns and to the pivot block.  A value it reads either
+// to the pivot block and to the tile's columns.  A value it reads either
 // still misses the update or already holds it; the minimum is the updated
 // value both ways, so the panel equals the one made after the update.
 __device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, unsigned char* smem) {
@@ -520,7 +591,8 @@ __device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, uns
     uint16_t* Bs = reinterpret_cast<uint16_t*>(smem + 2 * B * kTLD * sizeof(uint16_t));                // [B][NT]
     uint16_t* Pj = Bs + B * NT;                                                                        // Pp[c][j0 + j]
     int* kc = reinterpret_cast<int*>(Pj + B * NT);
-    uint8_t* cls = reinterpret_cast<uint8_t*>(kc + B);  // [B][kWarps]
+    uint8_t* cls = reinterpret_cast<uint8_t*>(kc + B);  // [B][kWarps] of T*
+    uint8_t* clsA = cls + B * kWarps;                   // [B][kWarps] of Ag
     __shared__ int tile_any;
     const uint16_t* D = rec.mat;
     const uint16_t* Pp = ahead ? panel_of(L, r - 1, s, NP) : nullptr;
@@ -529,8 +601,9 @@ __device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, uns
     if (tid == 0) tile_any = 0;
     __syncthreads();
     {   // the tile's pivot rows (and round r - 1's panel tile) by asynchronous
-        // copies, meanwhile the scattered pivot block (and its round r - 1
-        // panel columns) with all of a thread's loads issued first
+        // copies, waited for only where they are used; meanwhile the
+        // scattered pivot block (and its round r - 1 panel columns) with
+        // all of a thread's loads issued first
         for (int idx = tid; idx < mk * (NT / 8); idx += kThreads) {
             const int a = idx / (NT / 8), c8 = idx % (NT / 8);
             cp_async16(Bs + a * NT + c8 * 8, D + (size_t)kc[a] * NP + j0 + c8 * 8);
@@ -540,6 +613,7 @@ __device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, uns
                 const int c = idx / (NT / 8), c8 = idx % (NT / 8);
                 cp_async16(Pj + c * NT + c8 * 8, Pp + (size_t)c * NP + j0 + c8 * 8);
             }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
         constexpr int NTB = B * B / kThreads;
         uint16_t tv[NTB], pv[NTB];
 #pragma unroll
@@ -555,40 +629,34 @@ __device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, uns
             Ts[idx / B][idx % B] = tv[x];
             Ag[idx / B][idx % B] = pv[x];
         }
-        cp_async_wait_all();
     }
     __syncthreads();
-    const int warp = tid >> 5, lane = tid & 31;
-    uint32_t acc[8][1];
-    if (ahead) {  // round r - 1's update of the pivot rows: tile columns, then the pivot block
-        panel_gemm<1>(Ag, Pj, NT, B, nullptr, acc);
-        uint32_t* b32 = reinterpret_cast<uint32_t*>(Bs);
-#pragma unroll
-        for (int rr = 0; rr < 8; ++rr) {
-            const int a = warp * 8 + rr;
-            if (a < mk) b32[a * (NT / 2) + lane] = min2(b32[a * (NT / 2) + lane], acc[rr][0]);
-        }
-        panel_gemm<1>(Ag, &Ag[0][0], kTLD, B, nullptr, acc);
-#pragma unroll
-        for (int rr = 0; rr < 8; ++rr) {  // rows / columns >= mk: INF from Ag, the identity stays
-            uint32_t* t32 = reinterpret_cast<uint32_t*>(&Ts[warp * 8 + rr][0]);
-            t32[lane] = min2(t32[lane], acc[rr][0]);
-        }
+    uint32_t acc[2][4];
+    if (ahead) {  // round r - 1's update of the pivot rows: the pivot block, then the tile's columns
+        block_classes(Ag, B, clsA);
         __syncthreads();
+        gemm64(Ag, &Ag[0][0], kTLD, B, clsA, acc);
+        min_into(&Ts[0][0], kTLD, B, acc);  // rows / columns >= mk: INF from Ag, the identity stays
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        __syncthreads();
+        gemm64(Ag, Pj, NT, B, clsA, acc);
+        min_into(Bs, NT, mk, acc);
     }
-    close_pivot_block(Ts, mk);
-    panel_classes(Ts, mk, cls);
+    close_pivot_block(Ts, mk);  // begins with a barrier-free read of Ts, ends with a barrier
+    block_classes(Ts, mk, cls);
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
-    panel_gemm<1>(Ts, Bs, NT, mk, cls, acc);
+    gemm64(Ts, Bs, NT, mk, cls, acc);
     uint16_t* P = panel_of(L, r, s, NP);
+    const int warp = tid >> 5, lane = tid & 31;
     bool any = false;
-    const int col = j0 + lane * 2;
 #pragma unroll
-    for (int rr = 0; rr < 8; ++rr) {
-        const int a = warp * 8 + rr;
+    for (int i = 0; i < 2; ++i) {
+        const int a = warp * 8 + 2 * (lane >> 3) + i;
         if (a >= mk) continue;
-        reinterpret_cast<uint32_t*>(P + (size_t)a * NP + col)[0] = acc[rr][0];
-        any |= acc[rr][0] != INF2;
+        *reinterpret_cast<uint4*>(P + (size_t)a * NP + j0 + (lane & 7) * 8) =
+            make_uint4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
+        any |= (acc[i][0] & acc[i][1] & acc[i][2] & acc[i][3]) != INF2;
     }
     if (__any_sync(FULL, any) && lane == 0) tile_any = 1;
     __syncthreads();
@@ -733,8 +801,12 @@ __device__ void update_unit(const OpenLaunch& L, int l, int s, int I, int J, int
         }
         if (ch) {
             any = true;
+            if constexpr (CP == 2) {
+                *reinterpret_cast<uint2*>(dp) = make_uint2(acc[rr][0], acc[rr][1]);  // one 8-byte store
+            } else {
 #pragma unroll
-            for (int cc = 0; cc < CP; ++cc) dp[cc] = acc[rr][cc];
+                for (int cc = 0; cc < CP; ++cc) dp[cc] = acc[rr][cc];
+            }
         }
     }
     if (__any_sync(FULL, any) && lane == 0) s_any = 1;
@@ -1054,7 +1126,7 @@ __device__ void small_phase(const OpenLaunch& L, int l, int N, int* s_unit, unsi
 }
 
 constexpr size_t kPanelSmem = (size_t)2 * B * kTLD * sizeof(uint16_t) + (size_t)2 * B * 64 * sizeof(uint16_t) +
-                              B * sizeof(int) + (size_t)B * kWarps;
+                              B * sizeof(int) + (size_t)2 * B * kWarps;
 constexpr size_t kUpdateSmem = (size_t)B * 128 * (sizeof(uint32_t) + sizeof(uint16_t)) + (size_t)B * kWarps +
                                (size_t)128 * 128 * sizeof(uint16_t);
 constexpr size_t kTransposeSmem = (size_t)128 * (128 + 8) * sizeof(uint16_t);
