@@ -52,7 +52,7 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int B = kOpenB;
 constexpr unsigned kBarrierPolls = 1u << 24;
-constexpr int kInsertChunk = 2048;  // child-summary entries per insert unit
+constexpr int kInsertSmem = 64 * 1024;  // staged child rows + node row segments per insert unit
 
 __device__ __forceinline__ unsigned long long global_timer() {
     unsigned long long t;
@@ -240,21 +240,38 @@ __device__ void insert_list(const OpenLaunch& L, int l, int4 e, int* new_pivots,
     *dec = __any_sync(FULL, d);
 }
 
+// Rows of a decreased child's summary an insert unit takes: the child rows
+// and the node's row segments of the block staged in shared memory fit
+// kInsertSmem bytes; 0 when one row does not fit (a unit then takes one row
+// and reads it from global memory).
+__device__ __forceinline__ int insert_rows(const OpenLevelGeom& G) {
+    const int seg = ((G.nP + 7) / 8 + 1) * 8;  // the node's row segment, 16-byte aligned, rounded out
+    const int per_row = (G.childNP + seg) * (int)sizeof(uint16_t);
+    return min(G.nP, (int)(kInsertSmem / per_row));
+}
+
 // Insert phase of level l.  Units: the slots' edge / seam lists (one warp
 // per slot), then, for levels >= 1, every child whose summary decreased in
-// this call (listed by mark_dec) in chunks of kInsertChunk entries of its
+// this call (listed by mark_dec) in blocks of at most insert_rows(G) rows of its
 // nP x nP summary: every summary entry smaller than the node's entry is
 // inserted (internal_node.cpp:343-353) - the same as inserting the
 // reference's decrease list, since an entry that did not decrease is never
-// smaller than the node's, which is <= the old summary.
-__device__ void insert_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
+// smaller than the node's, which is <= the old summary.  A unit stages the
+// whole child rows and the node's row segments in shared memory with
+// asynchronous 16-byte copies (one round trip), then compares there.
+__device__ void insert_phase(const OpenLaunch& L, int l, int N, int* s_unit, unsigned char* smem) {
     const OpenLevelGeom& G = L.geo[l];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     __shared__ int s_dec;
     const int list_units = (N + kWarps - 1) / kWarps;
     const int nd = l >= 1 ? min(*(volatile int*)(L.dcount + l), L.cap[l - 1]) : 0;
-    const int chunks = l >= 1 ? (G.nP * G.nP + kInsertChunk - 1) / kInsertChunk : 0;
-    const int units = list_units + nd * chunks;
+    const int R0 = l >= 1 ? insert_rows(G) : 1;
+    const bool staged = R0 > 0;
+    // about two row blocks per CTA over the level's decreased children,
+    // within what shared memory holds
+    const int R = staged ? max(1, min(R0, (G.nP * nd + 2 * (int)gridDim.x - 1) / (2 * (int)gridDim.x))) : 1;
+    const int blocks = l >= 1 ? (G.nP + R - 1) / R : 0;
+    const int units = list_units + nd * blocks;
     for (int u = next_unit(L, s_unit); u < units; u = next_unit(L, s_unit)) {
         if (u < list_units) {
             const int s = u * kWarps + warp;
@@ -274,41 +291,61 @@ __device__ void insert_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
             continue;
         }
         const int cu = u - list_units;
-        const int4 dc = ld_slot(L.dchild[l] + cu / chunks);  // {task, child, node, quad}
-        const int c = cu % chunks;
+        const int4 dc = ld_slot(L.dchild[l] + cu / blocks);  // {task, child, node, quad}
         const OpenTask& T = L.tasks[dc.x];
-        if (threadIdx.x == 0) s_dec = 0;
-        __syncthreads();
         const int NP = G.NP, nP = G.nP, cNP = G.childNP, q = dc.w;
+        const int p0 = (cu % blocks) * R, rows = min(R, nP - p0);
+        const int col0 = q * nP, c_lo = col0 & ~7;
+        const int seg = ((nP + 7) / 8 + 1) * 8;  // covers [c_lo, col0 + nP)
         const uint16_t* cm = node_mat(T.lv[l - 1], dc.y, cNP);
         uint16_t* D = node_mat(T.lv[l], dc.z, NP);
         uint8_t* f = T.lv[l].kflag + (size_t)dc.z * NP;
-        const int i0 = c * kInsertChunk, i1 = min(nP * nP, i0 + kInsertChunk);
+        uint16_t* Cs = reinterpret_cast<uint16_t*>(smem);  // [rows][cNP] child rows
+        uint16_t* Ps = Cs + (size_t)rows * cNP;            // [rows][seg] node row segments
+        if (threadIdx.x == 0) s_dec = 0;
         bool dec = false;
-        // batches of 4 entries per thread: all loads first, then the updates
-        constexpr int U = 4;
-        for (int b0 = i0 + threadIdx.x; b0 < i1; b0 += U * kThreads) {
-            uint16_t w[U], d[U];
-            int a[U], bb[U];
-#pragma unroll
-            for (int x = 0; x < U; ++x) {
-                const int idx = b0 + x * kThreads;
-                a[x] = -1;
-                if (idx < i1) {
-                    const int p = idx / nP, pp = idx - p * nP;
-                    a[x] = q * nP + p;
-                    bb[x] = q * nP + pp;
-                    w[x] = __ldcg(cm + (size_t)G.child_ext[p] * cNP + G.child_ext[pp]);
-                    d[x] = __ldcg(D + (size_t)a[x] * NP + bb[x]);
+        if (!staged) {  // one row straight from global memory
+            __syncthreads();
+            const int ra = col0 + p0;
+            const uint16_t* crow = cm + (size_t)G.child_ext[p0] * cNP;
+            for (int pp = threadIdx.x; pp < nP; pp += kThreads) {
+                const int cb = col0 + pp;
+                const uint16_t w = __ldcg(crow + G.child_ext[pp]);
+                if (w < __ldcg(D + (size_t)ra * NP + cb)) {
+                    D[(size_t)ra * NP + cb] = w;  // (cb, ra) is written by the unit of row cb
+                    f[ra] = 1;
+                    f[cb] = 1;
+                    dec |= G.isext[ra] && G.isext[cb];
                 }
             }
-#pragma unroll
-            for (int x = 0; x < U; ++x) {
-                if (a[x] >= 0 && w[x] < d[x]) {
-                    D[(size_t)a[x] * NP + bb[x]] = w[x];  // (b, a) is written by its own thread
-                    f[a[x]] = 1;
-                    f[bb[x]] = 1;
-                    dec |= G.isext[a[x]] && G.isext[bb[x]];
+        } else {
+            for (int idx = threadIdx.x; idx < rows * (cNP / 8); idx += kThreads) {
+                const int r = idx / (cNP / 8), c8 = idx - r * (cNP / 8);
+                cp_async16(Cs + (size_t)r * cNP + c8 * 8, cm + (size_t)G.child_ext[p0 + r] * cNP + c8 * 8);
+            }
+            for (int idx = threadIdx.x; idx < rows * (seg / 8); idx += kThreads) {
+                const int r = idx / (seg / 8), c8 = idx - r * (seg / 8);
+                // the segment's last chunk may reach past the row (into the
+                // next row, or past the matrix): only [col0, col0 + nP) is used
+                const size_t off = (size_t)(col0 + p0 + r) * NP + c_lo + c8 * 8;
+                if (off + 8 <= (size_t)NP * NP) cp_async16(Ps + r * seg + c8 * 8, D + off);
+            }
+            cp_async_wait_all();
+            __syncthreads();
+            int r = threadIdx.x / nP, pp = threadIdx.x - r * nP;  // entry (r, pp) = r nP + pp, walked
+            for (int idx = threadIdx.x; idx < rows * nP; idx += kThreads) {
+                const uint16_t w = Cs[(size_t)r * cNP + G.child_ext[pp]];
+                if (w < Ps[r * seg + (col0 - c_lo) + pp]) {
+                    const int ra = col0 + p0 + r, cb = col0 + pp;
+                    D[(size_t)ra * NP + cb] = w;  // (cb, ra) is written by the unit of row cb
+                    f[ra] = 1;
+                    f[cb] = 1;
+                    dec |= G.isext[ra] && G.isext[cb];
+                }
+                pp += kThreads;
+                while (pp >= nP) {
+                    pp -= nP;
+                    ++r;
                 }
             }
         }
@@ -1130,7 +1167,7 @@ constexpr size_t kPanelSmem = (size_t)2 * B * kTLD * sizeof(uint16_t) + (size_t)
 constexpr size_t kUpdateSmem = (size_t)B * 128 * (sizeof(uint32_t) + sizeof(uint16_t)) + (size_t)B * kWarps +
                                (size_t)128 * 128 * sizeof(uint16_t);
 constexpr size_t kTransposeSmem = (size_t)128 * (128 + 8) * sizeof(uint16_t);
-constexpr size_t kOpenSmem = std::max(kPanelSmem, std::max(kUpdateSmem, kTransposeSmem));
+constexpr size_t kOpenSmem = std::max(std::max(kPanelSmem, (size_t)kInsertSmem), std::max(kUpdateSmem, kTransposeSmem));
 
 __global__ void __launch_bounds__(kThreads, 2) open_persistent_kernel(const OpenLaunch L) {
     extern __shared__ __align__(16) unsigned char osm[];
@@ -1158,7 +1195,7 @@ __global__ void __launch_bounds__(kThreads, 2) open_persistent_kernel(const Open
             if (!end_phase()) return;
             continue;
         }
-        insert_phase(L, l, N, s_unit);
+        insert_phase(L, l, N, s_unit, osm);
         if (!end_phase()) return;
         compact_phase(L, l, N, s_unit);
         if (!end_phase()) return;
