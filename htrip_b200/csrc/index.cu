@@ -1145,7 +1145,7 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
         int maxH = 0;
         int cap[hb::kOpenMaxLevels] = {}, n_seam[hb::kOpenMaxLevels] = {};
         size_t o_tasks = 0, o_out = 0, o_words = 0, o_trace = 0, o_slots[hb::kOpenMaxLevels] = {}, o_trip = 0;
-        size_t o_dchild[hb::kOpenMaxLevels] = {}, o_rec[hb::kOpenMaxLevels] = {};
+        size_t o_dchild[hb::kOpenMaxLevels] = {}, o_rec[hb::kOpenMaxLevels] = {}, o_sm = 0;
         size_t begin = 0, end = 0;
         int n_trip = 0;
     };
@@ -1203,6 +1203,7 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
         g.o_out = take(g.ts.size() * sizeof(hb::OpenTaskOut));
         g.o_words = take((3 * hb::kOpenMaxLevels + 4) * sizeof(int));
         g.o_trace = take(hb::kOpenTrace * sizeof(unsigned long long));
+        g.o_sm = take((3 + hb::kOpenSmSlots) * sizeof(unsigned));  // zero at launch (the staging is cleared)
         for (int l = 0; l <= g.maxH; ++l) g.o_slots[l] = take((size_t)std::max(1, g.cap[l]) * sizeof(int4));
         for (int l = 1; l <= g.maxH; ++l) g.o_dchild[l] = take((size_t)std::max(1, g.cap[l - 1]) * sizeof(int4));
         for (int l = 0; l <= g.maxH; ++l) g.o_rec[l] = take((size_t)std::max(1, g.cap[l]) * sizeof(hb::OpenSlotRec));
@@ -1307,6 +1308,7 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
         OL.dcount = OL.count + 2 * hb::kOpenMaxLevels;
         OL.status = OL.count + 3 * hb::kOpenMaxLevels;
         OL.bar = reinterpret_cast<unsigned*>(OL.status + 1);
+        OL.sm = reinterpret_cast<unsigned*>(base + g.o_sm);
         OL.triples = reinterpret_cast<const int*>(base + g.o_trip);
         OL.panel = A.panel.p;
         OL.pflags = A.pflags.p;

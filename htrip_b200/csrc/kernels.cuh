@@ -175,10 +175,13 @@ struct OpenLaunch {
     size_t panel_stride;           // elements between the two panel buffers
     size_t pflag_stride;           // bytes between the two flag buffers
     int* status;                   // 0 ok, 1 a bounded barrier wait timed out, 2 a list overflowed
-    unsigned* bar;                 // {arrived, generation, unit ticket}
+    unsigned* bar;                 // {arrival count, unit tickets of even / odd phases}
+    unsigned* sm;                  // {first CTAs, other CTAs, SM id overflow, per-SM arrivals
+                                   //  [kOpenSmSlots]}: the CTAs' SM-aware order (zero at launch)
     unsigned long long* trace;     // or null: [0] start, then one stamp per phase (max kOpenTrace)
 };
 constexpr int kOpenTrace = 1024;
+constexpr int kOpenSmSlots = 256;
 
 // An index's per-level "listed by opening call" stamps, for the dirty
 // flags of an incremental query (launch_incremental_dirty): viewpoint j

@@ -85,7 +85,8 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
 // p + 1 before it arrives at barrier p (its last use was phase p - 1, and
 // the barrier publishes the store before phase p + 1 starts).
 // s_unit (shared): [0] the unit, [1] -1 until the CTA's first unit of the
-// phase is taken, [2] the phase's counter.
+// phase is taken, [2] the phase's counter, [3] the CTA's first unit (its
+// place in the SM-aware order, sm_order).
 __device__ bool open_barrier(const OpenLaunch& L, int phase, int* s_unit) {
     __shared__ int s_ok;
     __syncthreads();
@@ -121,7 +122,7 @@ __device__ __forceinline__ int next_unit(const OpenLaunch& L, int* s_unit) {
     __syncthreads();
     if (threadIdx.x == 0) {
         if (s_unit[1] < 0) {
-            s_unit[0] = (int)blockIdx.x;
+            s_unit[0] = s_unit[3];
             s_unit[1] = 0;
         } else {
             s_unit[0] = (int)gridDim.x + (int)atomicAdd(L.bar + 1 + s_unit[2], 1u);
@@ -1169,9 +1170,31 @@ constexpr size_t kUpdateSmem = (size_t)B * 128 * (sizeof(uint32_t) + sizeof(uint
 constexpr size_t kTransposeSmem = (size_t)128 * (128 + 8) * sizeof(uint16_t);
 constexpr size_t kOpenSmem = std::max(std::max(kPanelSmem, (size_t)kInsertSmem), std::max(kUpdateSmem, kTransposeSmem));
 
+// SM-aware order of the CTAs, for the units a CTA takes without a ticket:
+// the first CTA to start on each SM gets places 0 .. S - 1 (S SMs), the
+// others the places after them, so a phase of at most S units runs one unit
+// per SM (the block scheduler puts blocks b and b + 6 on one SM, for
+// instance).  sm_arrive runs at launch, sm_order after the first barrier.
+__device__ __forceinline__ void sm_arrive(const OpenLaunch& L, int* s_unit) {
+    if (threadIdx.x != 0) return;
+    unsigned smid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    int first = 0;
+    if (smid < (unsigned)kOpenSmSlots) first = atomicAdd(L.sm + 3 + smid, 1u) == 0;
+    else atomicOr(L.sm + 2, 1u);
+    s_unit[3] = (int)blockIdx.x;
+    s_unit[4] = first;
+    s_unit[5] = (int)atomicAdd(L.sm + (first ? 0 : 1), 1u);
+}
+__device__ __forceinline__ void sm_order(const OpenLaunch& L, int* s_unit) {
+    if (threadIdx.x != 0) return;
+    if (__ldcg(L.sm + 2) != 0u) return;  // an SM id beyond the table: launch order
+    s_unit[3] = s_unit[4] ? s_unit[5] : (int)__ldcg(L.sm) + s_unit[5];
+}
+
 __global__ void __launch_bounds__(kThreads, 2) open_persistent_kernel(const OpenLaunch L) {
     extern __shared__ __align__(16) unsigned char osm[];
-    __shared__ int s_unit[3];
+    __shared__ int s_unit[6];
     if (threadIdx.x == 0) {
         s_unit[1] = -1;
         s_unit[2] = 0;
@@ -1185,8 +1208,10 @@ __global__ void __launch_bounds__(kThreads, 2) open_persistent_kernel(const Open
         ++phase;
         return ok;
     };
+    sm_arrive(L, s_unit);
     stamp_phase(L);
     if (!end_phase()) return;
+    sm_order(L, s_unit);  // visible to the CTA at next_unit's barrier
     for (int l = 0; l <= L.maxH; ++l) {
         const int N = min(*(volatile int*)(L.count + l), L.cap[l]);
         if (N == 0) continue;
