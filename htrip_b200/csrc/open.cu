@@ -419,11 +419,12 @@ __device__ void compact_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
 }
 
 // ---------------------------------------------------------------------------
-// Panel unit of round r: (slot, column tile of 64*CP columns; 64 in use).
+// Panel unit of round r: (slot, column tile of 64 columns).
 //   T* = closure of T = D[Kc, Kc] (Floyd-Warshall over the round's pivots, in
 //        shared memory; the reference's sequential relaxation restricted to
 //        the pivots),
 //   P[a][j] = min_c T*[a][c] (+) D[Kc[c]][j]   for the tile's columns j,
+// both from one Floyd-Warshall pass over the pivot rows [T | D[Kc, tile]],
 // stored in the slot's panel, with the 64-column blocks holding a finite
 // value flagged for the update.
 // ---------------------------------------------------------------------------
@@ -451,6 +452,48 @@ __device__ __forceinline__ void close_pivot_block(uint16_t (*Ts)[kTLD], int mk) 
         for (int i = 0; i < 8; ++i) v[i] = acc_clamp(v[i], rw[i], aa, tt);
         *reinterpret_cast<uint4*>(&Ts[a][c0]) = make_uint4(v[0], v[1], v[2], v[3]);
         *reinterpret_cast<uint4*>(&Ts[a][c0 + 8]) = make_uint4(v[4], v[5], v[6], v[7]);
+        __syncthreads();
+    }
+}
+
+// Floyd-Warshall over the round's pivots on the augmented rows [T | Bt]:
+// T the pivot block as above, Bt the pivot rows of a 64-column tile.  After
+// the last pivot, Bt = T* (x) Bt: a shortest path from pivot a to column j
+// through pivots ends with one entry D[c][j] of a pivot row.  Thread t owns
+// row t / 4 and 16 columns of each part; its Bt values end in vb.  Row kk of
+// both parts is rewritten unchanged at step kk (T[kk][kk] = 0), so one
+// barrier per step; rows >= mk of Bt are never read (T[a][kk] = INF there).
+__device__ __forceinline__ void close_pivot_panel(uint16_t (*Ts)[kTLD], uint16_t (*Bt)[kTLD], int mk,
+                                                  uint32_t (&vb)[8]) {
+    const int tid = threadIdx.x;
+    const int a = tid >> 2, c0 = (tid & 3) * 16;
+    uint32_t v[8];
+    {
+        const uint4 x0 = *reinterpret_cast<const uint4*>(&Ts[a][c0]);
+        const uint4 y0 = *reinterpret_cast<const uint4*>(&Ts[a][c0 + 8]);
+        const uint4 x1 = *reinterpret_cast<const uint4*>(&Bt[a][c0]);
+        const uint4 y1 = *reinterpret_cast<const uint4*>(&Bt[a][c0 + 8]);
+        v[0] = x0.x; v[1] = x0.y; v[2] = x0.z; v[3] = x0.w; v[4] = y0.x; v[5] = y0.y; v[6] = y0.z; v[7] = y0.w;
+        vb[0] = x1.x; vb[1] = x1.y; vb[2] = x1.z; vb[3] = x1.w; vb[4] = y1.x; vb[5] = y1.y; vb[6] = y1.z; vb[7] = y1.w;
+    }
+    for (int kk = 0; kk < mk; ++kk) {
+        const uint32_t t = Ts[a][kk];
+        const uint4 x = *reinterpret_cast<const uint4*>(&Ts[kk][c0]);
+        const uint4 y = *reinterpret_cast<const uint4*>(&Ts[kk][c0 + 8]);
+        const uint4 xb = *reinterpret_cast<const uint4*>(&Bt[kk][c0]);
+        const uint4 yb = *reinterpret_cast<const uint4*>(&Bt[kk][c0 + 8]);
+        const uint32_t rw[8] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
+        const uint32_t rb[8] = {xb.x, xb.y, xb.z, xb.w, yb.x, yb.y, yb.z, yb.w};
+        const uint32_t aa = splat(t), tt = INF2 - aa;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            v[i] = acc_clamp(v[i], rw[i], aa, tt);
+            vb[i] = acc_clamp(vb[i], rb[i], aa, tt);
+        }
+        *reinterpret_cast<uint4*>(&Ts[a][c0]) = make_uint4(v[0], v[1], v[2], v[3]);
+        *reinterpret_cast<uint4*>(&Ts[a][c0 + 8]) = make_uint4(v[4], v[5], v[6], v[7]);
+        *reinterpret_cast<uint4*>(&Bt[a][c0]) = make_uint4(vb[0], vb[1], vb[2], vb[3]);
+        *reinterpret_cast<uint4*>(&Bt[a][c0 + 8]) = make_uint4(vb[4], vb[5], vb[6], vb[7]);
         __syncthreads();
     }
 }
@@ -626,11 +669,11 @@ __device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, uns
     const bool ahead = r > 0;
     uint16_t (*Ts)[kTLD] = reinterpret_cast<uint16_t (*)[kTLD]>(smem);
     uint16_t (*Ag)[kTLD] = reinterpret_cast<uint16_t (*)[kTLD]>(smem + B * kTLD * sizeof(uint16_t));  // Pp[c][Kc[a]]
-    uint16_t* Bs = reinterpret_cast<uint16_t*>(smem + 2 * B * kTLD * sizeof(uint16_t));                // [B][NT]
-    uint16_t* Pj = Bs + B * NT;                                                                        // Pp[c][j0 + j]
+    uint16_t (*Bt)[kTLD] = reinterpret_cast<uint16_t (*)[kTLD]>(smem + 2 * B * kTLD * sizeof(uint16_t));  // tile rows
+    uint16_t* Bs = &Bt[0][0];
+    uint16_t* Pj = Bs + B * kTLD;  // [B][NT]: Pp[c][j0 + j]
     int* kc = reinterpret_cast<int*>(Pj + B * NT);
-    uint8_t* cls = reinterpret_cast<uint8_t*>(kc + B);  // [B][kWarps] of T*
-    uint8_t* clsA = cls + B * kWarps;                   // [B][kWarps] of Ag
+    uint8_t* clsA = reinterpret_cast<uint8_t*>(kc + B);  // [B][kWarps] of Ag
     __shared__ int tile_any;
     const uint16_t* D = rec.mat;
     const uint16_t* Pp = ahead ? panel_of(L, r - 1, s, NP) : nullptr;
@@ -644,7 +687,7 @@ __device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, uns
         // all of a thread's loads issued first
         for (int idx = tid; idx < mk * (NT / 8); idx += kThreads) {
             const int a = idx / (NT / 8), c8 = idx % (NT / 8);
-            cp_async16(Bs + a * NT + c8 * 8, D + (size_t)kc[a] * NP + j0 + c8 * 8);
+            cp_async16(Bs + a * kTLD + c8 * 8, D + (size_t)kc[a] * NP + j0 + c8 * 8);
         }
         if (ahead)
             for (int idx = tid; idx < B * (NT / 8); idx += kThreads) {
@@ -678,23 +721,21 @@ __device__ void panel_unit(const OpenLaunch& L, int l, int s, int j0, int r, uns
         asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         __syncthreads();
         gemm64(Ag, Pj, NT, B, clsA, acc);
-        min_into(Bs, NT, mk, acc);
+        min_into(Bs, kTLD, mk, acc);
     }
-    close_pivot_block(Ts, mk);  // begins with a barrier-free read of Ts, ends with a barrier
-    block_classes(Ts, mk, cls);
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
-    gemm64(Ts, Bs, NT, mk, cls, acc);
+    uint32_t vb[8];
+    close_pivot_panel(Ts, Bt, mk, vb);
     uint16_t* P = panel_of(L, r, s, NP);
-    const int warp = tid >> 5, lane = tid & 31;
+    const int lane = tid & 31, a = tid >> 2, c0 = (tid & 3) * 16;
     bool any = false;
+    if (a < mk) {
+        uint4* dst = reinterpret_cast<uint4*>(P + (size_t)a * NP + j0 + c0);
+        dst[0] = make_uint4(vb[0], vb[1], vb[2], vb[3]);
+        dst[1] = make_uint4(vb[4], vb[5], vb[6], vb[7]);
 #pragma unroll
-    for (int i = 0; i < 2; ++i) {
-        const int a = warp * 8 + 2 * (lane >> 3) + i;
-        if (a >= mk) continue;
-        *reinterpret_cast<uint4*>(P + (size_t)a * NP + j0 + (lane & 7) * 8) =
-            make_uint4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
-        any |= (acc[i][0] & acc[i][1] & acc[i][2] & acc[i][3]) != INF2;
+        for (int i = 0; i < 8; ++i) any |= vb[i] != INF2;
     }
     if (__any_sync(FULL, any) && lane == 0) tile_any = 1;
     __syncthreads();
@@ -1163,8 +1204,8 @@ __device__ void small_phase(const OpenLaunch& L, int l, int N, int* s_unit, unsi
     }
 }
 
-constexpr size_t kPanelSmem = (size_t)2 * B * kTLD * sizeof(uint16_t) + (size_t)2 * B * 64 * sizeof(uint16_t) +
-                              B * sizeof(int) + (size_t)2 * B * kWarps;
+constexpr size_t kPanelSmem = (size_t)3 * B * kTLD * sizeof(uint16_t) + (size_t)B * 64 * sizeof(uint16_t) +
+                              B * sizeof(int) + (size_t)B * kWarps;
 constexpr size_t kUpdateSmem = (size_t)B * 128 * (sizeof(uint32_t) + sizeof(uint16_t)) + (size_t)B * kWarps +
                                (size_t)128 * 128 * sizeof(uint16_t);
 constexpr size_t kTransposeSmem = (size_t)128 * (128 + 8) * sizeof(uint16_t);
