@@ -270,6 +270,10 @@ struct htrip_index {
     // many openings ran on the host-driven path (which does not stamp): an
     // incremental query that saw other values re-lifts everything
     uint64_t stamp_epoch = 0, host_opens = 0;
+    // opening bucketing scratch (all -1 between calls; a call resets the
+    // entries it set): slot of a touched leaf / of a seam node per level
+    std::vector<int> open_leaf_slot;
+    std::vector<std::vector<int>> open_seam_slot;
     uint64_t epoch = 0;           // build / root growth count (reference MinPlusOracle::epoch)
     uint64_t update_counter = 0;  // opening calls since creation
     int S = 0, H = 0, rows = 0, cols = 0, leaves_x = 0;
@@ -848,7 +852,8 @@ struct OpenTask {
     std::vector<int> leaves;                             // touched leaves, first-touch order
     std::vector<std::vector<int>> edges;                 // per touched leaf: (u, v, w) triples
     std::vector<std::vector<std::vector<int>>> seams;    // [lvl][slot]: (u, v, w) V_U triples
-    std::vector<std::vector<int>> seam_nodes, seam_slot;
+    std::vector<std::vector<int>> seam_nodes;
+    std::vector<std::vector<int>> seam_slot;  // host path: [lvl][node] -> slot of seam_nodes, or -1
     // progress
     std::vector<int> act, cand;    // active matrices of this level / of the level below
     std::vector<uint8_t> cand_dec; // decrease flags of `cand` (read back after its close)
@@ -870,11 +875,15 @@ void open_prepare(OpenTask& T, htrip_index* h, const int32_t* rc, int n, const u
     static const int dr[4] = {-1, 1, 0, 0};
     static const int dc[4] = {0, 0, -1, 1};
     Level& L0 = h->L[0];
-    std::vector<int> leaf_slot(L0.nnodes, -1);
+    // node -> slot tables kept by the index (no per-call allocation of
+    // level-sized tables; the entries set here are reset at the end)
+    std::vector<int>& leaf_slot = h->open_leaf_slot;
+    if (leaf_slot.size() != (size_t)L0.nnodes) leaf_slot.assign(L0.nnodes, -1);
+    h->open_seam_slot.resize(H + 1);
+    for (int l = 1; l <= H; ++l)
+        if (h->open_seam_slot[l].size() != (size_t)h->L[l].nnodes) h->open_seam_slot[l].assign(h->L[l].nnodes, -1);
     T.seams.resize(H + 1);
     T.seam_nodes.resize(H + 1);
-    T.seam_slot.resize(H + 1);
-    for (int l = 1; l <= H; ++l) T.seam_slot[l].assign(h->L[l].nnodes, -1);
     for (int i = 0; i < n; ++i) {
         const int r = rc[2 * i], c = rc[2 * i + 1];
         if (r < 0 || c < 0 || r >= S || c >= S) continue;
@@ -883,6 +892,7 @@ void open_prepare(OpenTask& T, htrip_index* h, const int32_t* rc, int n, const u
             leaf_slot[leaf] = (int)T.leaves.size();
             T.leaves.push_back(leaf);
             T.edges.emplace_back();
+            T.edges.back().reserve(96);  // 8 cells' 4 edges
         }
         if (!weight_ok(r, c)) continue;
         for (int d = 0; d < 4; ++d) {
@@ -902,11 +912,12 @@ void open_prepare(OpenTask& T, htrip_index* h, const int32_t* rc, int n, const u
                 if (lca < 1 || lca > H) continue;
                 const Level& Lv = h->L[lca];
                 const int node = (r / Lv.side) * Lv.nodes_x + (c / Lv.side);
-                int& slot = T.seam_slot[lca][node];
+                int& slot = h->open_seam_slot[lca][node];
                 if (slot < 0) {
                     slot = (int)T.seam_nodes[lca].size();
                     T.seam_nodes[lca].push_back(node);
                     T.seams[lca].emplace_back();
+                    T.seams[lca].back().reserve(48);
                 }
                 const int u = vertex_index(Lv, g, r, c), v = vertex_index(Lv, g, nr, nc);
                 if (u >= 0 && v >= 0) {
@@ -917,6 +928,9 @@ void open_prepare(OpenTask& T, htrip_index* h, const int32_t* rc, int n, const u
             }
         }
     }
+    for (int leaf : T.leaves) leaf_slot[leaf] = -1;
+    for (int l = 1; l <= H; ++l)
+        for (int node : T.seam_nodes[l]) h->open_seam_slot[l][node] = -1;
     if (record_stats) h->stats = {0, 0, 0};
     h->open_ops = h->open_bytes = 0;
     h->open_levels.assign(H + 1, {0, 0, 0, 0});
@@ -952,6 +966,12 @@ void run_open_tasks(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t 
     for (size_t t = 0; t < tasks.size(); ++t) {
         tasks[t]->task = (int)t;
         maxH = std::max(maxH, tasks[t]->h->H);
+        OpenTask& T = *tasks[t];  // node -> seam slot tables of this path
+        T.seam_slot.assign(T.h->H + 1, {});
+        for (int l = 1; l <= T.h->H; ++l) {
+            T.seam_slot[l].assign(T.h->L[l].nnodes, -1);
+            for (size_t i = 0; i < T.seam_nodes[l].size(); ++i) T.seam_slot[l][T.seam_nodes[l][i]] = (int)i;
+        }
     }
     const int n_tasks = (int)tasks.size();
     for (int l = 0; l <= maxH; ++l) {
