@@ -707,7 +707,9 @@ def bench_served(device, server_rates=(1000.0, 2000.0, 5000.0, 10000.0, 20000.0,
                 "launches": int(st["launches_query"] + st["launches_open"]),
                 "query_launches": int(st["launches_query"]), "open_launches": int(st["launches_open"]),
                 "query_worker_busy_s": st["busy_query_us"] / 1e6,
-                "open_worker_busy_s": st["busy_open_us"] / 1e6}, outs
+                "open_worker_busy_s": st["busy_open_us"] / 1e6,
+                "evictions": int(st["evictions"]), "restores": int(st["restores"]),
+                "resident_gib": st["resident_bytes"] / 2**30, "budget_gib": st["budget_bytes"] / 2**30}, outs
 
     served, plain = [], []
     first_outs = None

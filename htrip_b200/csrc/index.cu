@@ -98,6 +98,54 @@ struct DevBuf {
     }
 };
 
+// Memory pool of a device for the scratch arenas (PoolBuf): it keeps what
+// is given back (release threshold: never), so a growing arena reuses it.
+cudaMemPool_t scratch_pool(int device) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    std::lock_guard<std::mutex> lk(mu);
+    cudaMemPool_t& pool = pools[std::clamp(device, 0, 63)];
+    if (!pool) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        ck(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
+        uint64_t keep = UINT64_MAX;
+        ck(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
+    }
+    return pool;
+}
+
+// Device scratch of the per-call paths (the query and update arenas): grows
+// like DevBuf, but stream-ordered on the stream that uses the arena, from
+// the device's scratch pool.  Growing a DevBuf frees the old block with
+// cudaFree, which synchronizes the device and, with most of the GPU's memory
+// held by resident indexes, measured up to 0.3 s for one call; a block freed
+// to the pool is reused instead, and nothing waits.
+template <class T>
+struct PoolBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void reserve(size_t m, cudaStream_t st) {
+        if (m <= n) return;
+        if (n) m = std::max(m, n + n / 2);
+        int device = 0;
+        ck(cudaGetDevice(&device), "cudaGetDevice");
+        if (p) ck(cudaFreeAsync(p, st), "cudaFreeAsync");
+        p = nullptr;
+        n = 0;
+        ck(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), m * sizeof(T), scratch_pool(device), st),
+           "cudaMallocFromPoolAsync");
+        n = m;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
 struct Level {
     int lvl = 0;
     int side = 0;      // tile side (b for leaves, s for nodes)
@@ -180,7 +228,7 @@ struct HostBuf {
 // (LaunchLayout), pinned staging of its head and of the results, the grid
 // size of the cooperative kernel and the events around the last launch.
 struct QueryArena {
-    DevBuf<unsigned char> dev;
+    PoolBuf<unsigned char> dev;
     HostBuf stage, outstage;
     int grid = 0;
     cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -221,10 +269,10 @@ struct QueryArena {
 // per-slot / per-task read-back words, exterior snapshots, closure panels
 // and tile flags; pinned staging for the upload and the read-backs.
 struct UpdateArena {
-    DevBuf<unsigned char> dev;
+    PoolBuf<unsigned char> dev;
     DevBuf<uint16_t> snap;
-    DevBuf<uint16_t> panel;
-    DevBuf<uint8_t> pflags;
+    PoolBuf<uint16_t> panel;
+    PoolBuf<uint8_t> pflags;
     HostBuf stage, rb;
     cudaEvent_t ev_cnt = nullptr;  // an opening level's pivot counts reached the host
     int open_grid = 0;             // CTAs of the persistent opening kernel
@@ -560,8 +608,8 @@ void close_slots(UpdateArena& A, const hb::Slot* d_slots, const int* cnt, int n,
             rounds = (maxk + hb::kPivotChunk - 1) / hb::kPivotChunk;
         }
         if (rounds <= r0) continue;
-        A.panel.reserve(hb::closure_scratch_elems(NP, nc));
-        A.pflags.reserve((size_t)nc * (NP / hb::kFlagTile));
+        A.panel.reserve(hb::closure_scratch_elems(NP, nc), st);
+        A.pflags.reserve((size_t)nc * (NP / hb::kFlagTile), st);
         for (int r = r0; r < rounds; ++r) {
             hb::launch_closure_round(d_slots + c0, nc, NP, r, A.panel.p, A.pflags.p, st);
             ck(cudaGetLastError(), "closure round");
@@ -579,7 +627,7 @@ void close_matrices(htrip_index* h, Level& Lv, const std::vector<int>& act) {
     const size_t slots_b = align256(n * sizeof(hb::Slot));
     A.stage.reserve(slots_b);
     A.rb.reserve(n * sizeof(int));
-    A.dev.reserve(slots_b + n * sizeof(int));
+    A.dev.reserve(slots_b + n * sizeof(int), st);
     auto* hs = reinterpret_cast<hb::Slot*>(A.stage.p);
     for (int i = 0; i < n; ++i) hs[i] = level_slot(Lv, nullptr, act[i], 0, 0);
     ck(cudaMemcpyAsync(A.dev.p, A.stage.p, n * sizeof(hb::Slot), cudaMemcpyHostToDevice, st), "slots");
@@ -1026,7 +1074,7 @@ void run_open_tasks(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t 
         const size_t o_piv = o_dec + align256(n_slots);
         const size_t total = o_piv + align256(n_tasks * sizeof(int));
         A.stage.reserve(total);
-        A.dev.reserve(total);
+        A.dev.reserve(total, st);
         A.rb.reserve(total - o_cnt);
         std::memset(A.stage.p + o_cnt, 0, total - o_cnt);
         auto* hs = reinterpret_cast<hb::Slot*>(A.stage.p);
@@ -1093,8 +1141,8 @@ void run_open_tasks(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t 
                 elems = std::max(elems, hb::closure_scratch_elems(NP, (int)nc));
                 fl = std::max(fl, nc * (NP / hb::kFlagTile));
             }
-            A.panel.reserve(elems);
-            A.pflags.reserve(fl);
+            A.panel.reserve(elems, st);
+            A.pflags.reserve(fl, st);
         }
         for (const Group& G : groups)
             close_slots(A, ds + G.s0, nullptr, G.s1 - G.s0, live[G.t0]->h->L[l].NP, st, 0);
@@ -1231,15 +1279,15 @@ void run_open_device(std::vector<OpenTask*>& tasks, UpdateArena& A, cudaStream_t
         g.end = off;
         gl.push_back(std::move(g));
     }
-    A.dev.reserve(off);
+    A.dev.reserve(off, st);
     A.stage.reserve(off);
     A.rb.reserve(off);
     // two panel and flag buffers: a round's panel is made while the update
     // of the round before reads the other one
     panel_elems = (panel_elems + 127) / 128 * 128;
     pflag_bytes = (pflag_bytes + 255) / 256 * 256;
-    A.panel.reserve(2 * panel_elems);
-    A.pflags.reserve(2 * pflag_bytes);
+    A.panel.reserve(2 * panel_elems, st);
+    A.pflags.reserve(2 * pflag_bytes, st);
     if (!A.open_grid) A.open_grid = hb::open_grid_blocks(device);
     unsigned char* base = A.dev.p;
     for (GL& g : gl) {
@@ -1856,7 +1904,7 @@ int run_queries(QueryArena& A, int device, cudaStream_t st, const std::vector<Qu
     // A stream-ordered launch (sync == false) may still be reading the
     // arena or the pinned staging: wait for it before reusing or growing them.
     if (A.ev_valid) ck(cudaEventSynchronize(A.ev[1]), "previous launch");
-    A.dev.reserve(L.total);
+    A.dev.reserve(L.total, st);
     A.stage.reserve(L.head);
     A.outstage.reserve(L.out_bytes + 256);
     if (!A.ev[0]) {
@@ -2161,7 +2209,7 @@ int run_devplan(htrip_index* h, int k, int cfg, const int32_t* vps_host, const u
     DevPlanLayout D = devplan_layout(h, k, cfg, to_host);
     if (D.total > A.dev.n) {
         if (A.ev_valid) ck(cudaEventSynchronize(A.ev[1]), "previous launch");
-        A.dev.reserve(D.total);
+        A.dev.reserve(D.total, st);
     }
     if (!A.ev[0]) {
         ck(cudaEventCreate(&A.ev[0]), "event");

@@ -589,6 +589,11 @@ htrip_status htrip_server_run_trace(htrip_server* S, const htrip_server_request*
     const auto start = Clock::now();
     for (int i = 0; i < n; ++i) {
         const auto due = start + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(arrival_s[i]));
+        // sleep until shortly before the arrival, then spin: a submitter
+        // spinning through every gap would hold a core the workers need (and
+        // under a CPU quota, get every thread of the process throttled)
+        if (due - Clock::now() > std::chrono::microseconds(300))
+            std::this_thread::sleep_until(due - std::chrono::microseconds(200));
         while (Clock::now() < due) {
         }
         const htrip_server_request& q = reqs[i];
