@@ -638,8 +638,8 @@ def bench_batched(device, n_maps=64):
             "parity_vs_plain": "bit-exact" if ok else "MISMATCH"}
 
 
-def bench_served(device, server_rates=(1000.0, 2000.0, 5000.0, 10000.0, 20000.0, 50000.0),
-                 plain_rates=(250.0, 500.0, 1000.0, 2000.0, 5000.0), seconds=1.0, min_requests=1000,
+def bench_served(device, server_rates=(1000.0, 2000.0, 3000.0, 4000.0, 5000.0, 10000.0, 20000.0, 50000.0),
+                 plain_rates=(250.0, 500.0, 1000.0, 2000.0, 3000.0, 4000.0, 5000.0), seconds=1.0, min_requests=1000,
                  max_requests=10000, budget_gb=120.0, n_sessions=256):
     """256 resident map sessions (128^2-1024^2, about 120 GB of indexes) under
     open-loop Poisson arrivals: 70% queryAllPairs with k log-uniform in
