@@ -149,7 +149,8 @@ struct OpenTask {
 struct OpenSlotRec {
     uint16_t* mat;
     const int* klist;
-    int kcnt, task, node, pad;
+    int kcnt, task, node;
+    int ready;  // 1 once the compaction wrote the record (zero at launch)
 };
 
 // Work list entry: {task, node, list_begin, list_end}; the list is the slot's

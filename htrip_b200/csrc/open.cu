@@ -26,7 +26,9 @@
 //                entry changed.
 //              Pipelined one round deep: the panel of round r runs in the
 //              same phase as the update of round r - 1 and applies that
-//              update to its own pivot rows (R rounds: R + 1 phases).
+//              update to its own pivot rows; round 0's panels run in the
+//              compaction's phase, each after its slot's record (R rounds:
+//              the compaction phase + R phases).
 //   A matrix whose exterior block decreased (refreshBoundarySummary,
 //   leaf_tile.cpp:253-273, internal_node.cpp:415-433) is seen where the
 //   decrease happens: an insert or an update tile lowers an entry whose row
@@ -357,16 +359,17 @@ __device__ void insert_phase(const OpenLaunch& L, int l, int N, int* s_unit, uns
 }
 
 // ---------------------------------------------------------------------------
-// Compact phase: one CTA per slot turns the pivot flags into the ascending
-// pivot list (and clears the flags); per-level statistics and the largest
-// pivot count of the level (which sets the number of rounds).
+// Compaction (one unit per slot): the pivot flags become the ascending pivot
+// list (and are cleared); per-level statistics and the largest pivot count
+// of the level (which sets the number of rounds); the slot's record, then
+// its ready flag.
 // ---------------------------------------------------------------------------
-__device__ void compact_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
+__device__ void compact_unit(const OpenLaunch& L, int l, int s) {
     const OpenLevelGeom& G = L.geo[l];
     __shared__ int warp_tot[kWarps];
     __shared__ int base;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int s = next_unit(L, s_unit); s < N; s = next_unit(L, s_unit)) {
+    {
         const int4 e = ld_slot(L.slots[l] + s);
         const OpenTask& T = L.tasks[e.x];
         uint8_t* f = T.lv[l].kflag + (size_t)e.y * G.NP;
@@ -405,6 +408,8 @@ __device__ void compact_phase(const OpenLaunch& L, int l, int N, int* s_unit) {
             const int k = base;
             T.lv[l].kcnt[e.y] = k;
             L.rec[l][s] = OpenSlotRec{node_mat(T.lv[l], e.y, G.NP), out, k, e.x, e.y, 0};
+            __threadfence();  // the pivot list and the record, then the release
+            atomicExch(&L.rec[l][s].ready, 1);
             atomicAdd(&T.out->level[l][0], 1);
             atomicAdd(&T.out->level[l][1], k);
             atomicMax(&T.out->level[l][2], k);
@@ -939,7 +944,44 @@ __device__ __forceinline__ void tri_pair(int t, int nt, int& I, int& J) {
     J = i + t;
 }
 
-// Stage t of level l's closure (t = 0 .. rounds) as one phase: the panel
+// Bounded wait (thread 0 polls, the CTA follows) for slot s's compaction
+// record; false after a timeout (status 1) or when another CTA recorded one.
+__device__ bool wait_rec_ready(const OpenLaunch& L, int l, int s) {
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        const unsigned* f = reinterpret_cast<const unsigned*>(&L.rec[l][s].ready);
+        int ok = 1;
+        unsigned it = 0;
+        while (ld_acquire(f) == 0u) {
+            if (*(volatile int*)L.status != 0) { ok = 0; break; }
+            if (++it > kBarrierPolls) { atomicCAS(L.status, 0, 1); ok = 0; break; }
+            __nanosleep(32);
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Compaction and round 0's panels of level l as one phase: the compaction
+// units (one per slot) take the first places, the panel units of round 0
+// (slot x 64-column tile) the later ones and wait only for their slot's
+// record - a unit of a lower place, already running, so every wait ends.
+__device__ void compact_panel_phase(const OpenLaunch& L, int l, int N, int* s_unit, unsigned char* smem) {
+    const int tiles = L.geo[l].NP / 64;
+    const int units = N + N * tiles;
+    for (int u = next_unit(L, s_unit); u < units; u = next_unit(L, s_unit)) {
+        if (u < N) {
+            compact_unit(L, l, u);
+            continue;
+        }
+        const int v = u - N, s = v / tiles;
+        if (!wait_rec_ready(L, l, s)) return;  // the next barrier ends the launch
+        panel_unit(L, l, s, (v % tiles) * 64, 0, smem);
+    }
+}
+
+// Stage t of level l's closure (t = 1 .. rounds; stage 0 is compact_panel_phase) as one phase: the panel
 // units of round t (slot x 64-column tile; none in the last stage) take the
 // lower tickets, the update units of round t - 1 (slot x upper-triangle tile
 // pair; none in stage 0) the higher ones.  The panel of round t applies
@@ -1263,10 +1305,10 @@ __global__ void __launch_bounds__(kThreads, 2) open_persistent_kernel(const Open
         }
         insert_phase(L, l, N, s_unit, osm);
         if (!end_phase()) return;
-        compact_phase(L, l, N, s_unit);
+        compact_panel_phase(L, l, N, s_unit, osm);  // stage 0 of the closure with the compaction
         if (!end_phase()) return;
         const int rounds = (*(volatile int*)(L.maxk + l) + B - 1) / B;
-        for (int t = 0; rounds > 0 && t <= rounds; ++t) {
+        for (int t = 1; rounds > 0 && t <= rounds; ++t) {
             stage_phase(L, l, N, t, rounds, s_unit, osm);
             if (!end_phase()) return;
         }
