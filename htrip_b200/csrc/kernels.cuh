@@ -186,8 +186,9 @@ constexpr int kOpenSmSlots = 256;
 
 // An index's per-level "listed by opening call" stamps, for the dirty
 // flags of an incremental query (launch_incremental_dirty): viewpoint j
-// (sorted order, leaf vp0[4 j]) gets dirty[j] = 1 when a matrix of its
-// leaf-to-root chain carries a stamp newer than `seen`; *n_dirty counts them.
+// (sorted order, leaf vp0[4 j]) gets dirty[j] = 1 + the lowest level whose
+// matrix on its leaf-to-root chain carries a stamp newer than `seen` (0: none);
+// *n_dirty counts the viewpoints with one.
 struct IncrementalChain {
     int H, g, leaves_x;
     const uint32_t* mstamp[kOpenMaxLevels];
@@ -253,11 +254,12 @@ struct QueryParams {
     unsigned long long* work;  // or null: [0] tile entries updated (operand rows streamed x
                                // tile rows x tile columns), [1] operand rows streamed,
                                // [2] operand rows skipped (no finite value in the tile)
-    const uint8_t* dirty;      // or null (every viewpoint): per sorted viewpoint, 1 = some
-                               // node of its leaf-to-root chain changed.  A unit whose rows
-                               // and columns are all clean skips its work (an incremental
-                               // refresh: the launch's X / Y / flags / M still hold the
-                               // previous launch's values for the clean viewpoints)
+    const uint8_t* dirty;      // or null (every viewpoint): per sorted viewpoint, 0 = no node
+                               // of its leaf-to-root chain changed, else 1 + the lowest level
+                               // whose node changed.  A unit of level l whose rows and columns
+                               // are all clean at l (no change at levels <= l) skips its work
+                               // (an incremental refresh: the launch's X / Y / flags / M still
+                               // hold the previous launch's values for them)
 };
 
 // Words of a request's completion counters.

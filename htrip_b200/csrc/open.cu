@@ -1317,25 +1317,26 @@ __global__ void __launch_bounds__(kThreads, 2) open_persistent_kernel(const Open
 
 }  // namespace
 
-// Dirty flags of an incremental query: viewpoint j (sorted order, leaf
-// vp0[4 j]) is dirty when a matrix of its leaf-to-root chain was listed by an
-// opening call after the stamp `seen` (stamps compare modulo 2^32).
+// Dirty levels of an incremental query: viewpoint j (sorted order, leaf
+// vp0[4 j]) gets 1 + the lowest level whose matrix on its leaf-to-root chain
+// was listed by an opening call after the stamp `seen` (stamps compare modulo
+// 2^32), 0 when none was: its projections below that level are unchanged.
 __global__ void incremental_dirty_kernel(const int* __restrict__ vp0, int ns, IncrementalChain C, unsigned seen,
                                          uint8_t* dirty, int* n_dirty) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ns) return;
     const int leaf = vp0[4 * j];
     int tx = leaf % C.leaves_x, ty = leaf / C.leaves_x;
-    bool d = false;
-    for (int l = 0; l <= C.H; ++l) {
+    int lo = -1;
+    for (int l = 0; l <= C.H && lo < 0; ++l) {
         if (l > 0) {
             tx /= C.g;
             ty /= C.g;
         }
-        d |= (int)(C.mstamp[l][ty * C.nodes_x[l] + tx] - seen) > 0;
+        if ((int)(C.mstamp[l][ty * C.nodes_x[l] + tx] - seen) > 0) lo = l;
     }
-    dirty[j] = d ? 1 : 0;
-    if (d) atomicAdd(n_dirty, 1);
+    dirty[j] = (uint8_t)(lo + 1);
+    if (lo >= 0) atomicAdd(n_dirty, 1);
 }
 
 void launch_incremental_dirty(const int* vp0, int ns, const IncrementalChain& C, unsigned seen, uint8_t* dirty,

@@ -377,6 +377,13 @@ __device__ bool combine_parts(const QueryLevel& L, int item, int part, uint32_t 
 // CTA's warps split the group's finite ports (part `part` of L.split of
 // them).  After the reduction the epilogue (Y stores and lift scatters) is
 // spread over the warps.  Returns whether the item is complete.
+// Incremental refresh: viewpoint j's level-l results changed (dirty[j] = 1 +
+// the lowest level whose node changed, 0 for none).
+__device__ __forceinline__ bool dirty_at(const uint8_t* dirty, int j, int l) {
+    const int d = dirty[j];
+    return d != 0 && d - 1 <= l;
+}
+
 template <int RW, int CP>
 __device__ bool do_project(const QueryParams& P, const QueryLevel& L, const QueryLevel* Ln, int item, int part,
                            int l, int* kl, int* wsum, uint32_t* red, ItemMeta& im) {
@@ -387,7 +394,7 @@ __device__ bool do_project(const QueryParams& P, const QueryLevel& L, const Quer
     const int node = G[0], q = G[1], slot0 = G[2];
     if (P.dirty) {  // incremental refresh: rows of clean viewpoints keep their values
         int any = 0;
-        for (int r = 0; r < min(RW, G[3] - m0); ++r) any |= P.dirty[G[4] + m0 + r];
+        for (int r = 0; r < min(RW, G[3] - m0); ++r) any |= dirty_at(P.dirty, G[4] + m0 + r, l);
         if (!any) return L.split <= 1 || part == 0;  // a skipped item counts once
     }
     const int nA = compact_flags(L.flags + (size_t)gi * L.nP, 0, L.nP, kl, wsum);
@@ -459,11 +466,11 @@ __device__ void do_meet(const QueryParams& P, const QueryLevel& L, int item, int
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int* it = L.meet + 7 * item;
     const int i0 = it[0], j0 = it[1], g2 = it[3], coloff = it[4], kb = it[5], ke = it[6];
-    if (P.dirty) {  // incremental refresh: a pair of clean viewpoints keeps its value
+    if (P.dirty) {  // incremental refresh: a pair of viewpoints clean at this level keeps its value
         int any = 0;
         for (int e = threadIdx.x; e < 64 * CP + RW; e += kThreads) {
             const int v = e < 64 * CP ? im.col[e] : im.row[0][e - 64 * CP];
-            if (v >= 0) any |= P.dirty[v];
+            if (v >= 0) any |= dirty_at(P.dirty, v, l);
         }
         if (!__syncthreads_or(any)) return;
     }
@@ -549,7 +556,7 @@ __device__ bool run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum,
             for (int e = u * kQueryL0Chunk + tid; e < e1; e += kThreads) {
                 const int p = e / S1, s = e - p * S1;
                 const int j = P.l0[2 * s];
-                if (j < 0 || (P.dirty && !P.dirty[j])) continue;
+                if (j < 0 || (P.dirty && !dirty_at(P.dirty, j, 0))) continue;
                 const int* v = P.vp0 + 4 * j;
                 const uint16_t d = P.leaves.base[((size_t)v[0] * P.leaves.NP + v[1]) * P.leaves.NP + P.ext0[p]];
                 P.X[0][(size_t)p * P.ldv + s] = d;
@@ -558,7 +565,7 @@ __device__ bool run_unit(const QueryParams& P, int t, int u, int* kl, int* wsum,
         } else {
             const int j = (u - n_fill) * kThreads + tid;
             // same-leaf viewpoints share their chain, hence their dirty flag
-            if (j < P.ns && (!P.dirty || P.dirty[j])) {
+            if (j < P.ns && (!P.dirty || dirty_at(P.dirty, j, 0))) {
                 const int* v = P.vp0 + 4 * j;
                 const uint16_t* row = P.leaves.base + ((size_t)v[0] * P.leaves.NP + v[1]) * P.leaves.NP;
                 // atomicMin: the level-1 meets (intra-child shortcuts) may
