@@ -689,8 +689,10 @@ def bench_served(device, server_rates=(1000.0, 2000.0, 3000.0, 4000.0, 5000.0, 1
             free = np.argwhere(obs == W.FREE).astype(np.int32)
             if len(free):
                 wq.append((i, 1, free[rng.choice(len(free), size=min(512, len(free)), replace=False)]))
-            tfree = np.argwhere(truth == W.FREE).astype(np.int32)  # a query of the largest k of the trace
-            wq.append((i, 0, tfree[rng.choice(len(tfree), size=min(512, len(tfree)), replace=False)]))
+            # a query of the largest k of the trace on observed free cells, so
+            # that every viewpoint counts and the arenas reach their size
+            ofree = free if len(free) else np.argwhere(truth == W.FREE).astype(np.int32)
+            wq.append((i, 0, ofree[rng.choice(len(ofree), size=min(512, len(ofree)), replace=False)]))
         srv.run_trace([(sids[s], k, rc) for s, k, rc in wq], np.zeros(len(wq)))
         outs, lat, wall = srv.run_trace([(sids[s], k, rc) for s, k, rc in reqs], arrival)
         st = srv.stats()

@@ -204,13 +204,15 @@ void coop_launch(int device, cudaStream_t st, F&& launch, const char* what) {
     c.st = st;
 }
 
-// Pinned host buffer (grows, never shrinks).
+// Pinned host buffer (grows, never shrinks).  Pinning pages costs about a
+// millisecond per allocation, so a first reservation takes at least 64 KB
+// and growth at least half again.
 struct HostBuf {
     unsigned char* p = nullptr;
     size_t n = 0;
     void reserve(size_t m) {
         if (m <= n) return;
-        if (n) m = std::max(m, n + n / 2);
+        m = std::max(m, n ? n + n / 2 : (size_t)64 * 1024);
         if (p) cudaFreeHost(p);
         p = nullptr;
         n = 0;
