@@ -547,33 +547,33 @@ __device__ __forceinline__ void panel_gemm(uint16_t (*Ts)[kTLD], const uint16_t*
                 acc[2 * r2 + 1][0] = acc_clamp(acc[2 * r2 + 1][0], bv, a1, INF2 - a1);
             }
         }
-        return;
-    }
-    for (int k = 0; k < mk; ++k) {
-        const int c = cls[k * kWarps + warp];
-        if (c == 0) continue;  // uniform over the warp
-        uint32_t bv[CP];
+    } else {
+        for (int k = 0; k < mk; ++k) {
+            const int c = cls[k * kWarps + warp];
+            if (c == 0) continue;  // uniform over the warp
+            uint32_t bv[CP];
 #pragma unroll
-        for (int cc = 0; cc < CP; ++cc) bv[cc] = reinterpret_cast<const uint32_t*>(Bs + k * ldb + lane * 2 * CP)[cc];
-        const uint4 av = *reinterpret_cast<const uint4*>(&Ts[k][warp * 8]);
-        const uint32_t aw[4] = {av.x, av.y, av.z, av.w};
-        uint32_t aa[8];
+            for (int cc = 0; cc < CP; ++cc) bv[cc] = reinterpret_cast<const uint32_t*>(Bs + k * ldb + lane * 2 * CP)[cc];
+            const uint4 av = *reinterpret_cast<const uint4*>(&Ts[k][warp * 8]);
+            const uint32_t aw[4] = {av.x, av.y, av.z, av.w};
+            uint32_t aa[8];
 #pragma unroll
-        for (int r2 = 0; r2 < 4; ++r2) {
-            aa[2 * r2] = splat(aw[r2]);
-            aa[2 * r2 + 1] = splat(aw[r2] >> 16);
-        }
-        if (c == 1) {
+            for (int r2 = 0; r2 < 4; ++r2) {
+                aa[2 * r2] = splat(aw[r2]);
+                aa[2 * r2 + 1] = splat(aw[r2] >> 16);
+            }
+            if (c == 1) {
 #pragma unroll
-            for (int rr = 0; rr < 8; ++rr)
+                for (int rr = 0; rr < 8; ++rr)
 #pragma unroll
-                for (int cc = 0; cc < CP; ++cc) acc[rr][cc] = acc_fast(acc[rr][cc], bv[cc], aa[rr]);
-        } else {
+                    for (int cc = 0; cc < CP; ++cc) acc[rr][cc] = acc_fast(acc[rr][cc], bv[cc], aa[rr]);
+            } else {
 #pragma unroll
-            for (int rr = 0; rr < 8; ++rr) {
-                const uint32_t tt = INF2 - aa[rr];
+                for (int rr = 0; rr < 8; ++rr) {
+                    const uint32_t tt = INF2 - aa[rr];
 #pragma unroll
-                for (int cc = 0; cc < CP; ++cc) acc[rr][cc] = acc_clamp(acc[rr][cc], bv[cc], aa[rr], tt);
+                    for (int cc = 0; cc < CP; ++cc) acc[rr][cc] = acc_clamp(acc[rr][cc], bv[cc], aa[rr], tt);
+                }
             }
         }
     }
